@@ -1,0 +1,946 @@
+// C ABI of the B200-native FDTD time step: simulation handle, device state,
+// launch sequencing (direct and CUDA-graph replay), spectra, snapshots.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/fdtd_b200.h"
+#include "kernels.cuh"
+#include "setup.h"
+
+using namespace fdtd;
+
+static thread_local std::string g_err;
+
+static fdtd_status fail(fdtd_status st, const std::string& msg) {
+  g_err = msg;
+  return st;
+}
+
+#define CUDA_TRY(expr)                                                                          \
+  do {                                                                                          \
+    cudaError_t e_ = (expr);                                                                    \
+    if (e_ != cudaSuccess)                                                                      \
+      return fail(FDTD_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_));          \
+  } while (0)
+
+namespace {
+
+// A device allocation that frees itself.
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+  cudaError_t alloc(size_t n) {
+    bytes = n;
+    cudaError_t e = cudaMalloc(&p, n ? n : 16);
+    if (e == cudaSuccess) e = cudaMemset(p, 0, n ? n : 16);
+    return e;
+  }
+  template <typename U>
+  U* as() const { return static_cast<U*>(p); }
+};
+
+}  // namespace
+
+struct fdtd_sim {
+  Setup su;
+  int device = 0;
+  bool fp64 = true;
+  int NX, NY, NZ, PX;
+  size_t plane, ncell;
+  int kchunk = 32;
+  // device state
+  std::vector<std::unique_ptr<DevBuf>> bufs;
+  void* E[3];
+  void* H[3];
+  uint8_t* mat = nullptr;
+  int mat_lo[3], mat_hi[3];
+  DevClock* clk = nullptr;
+  double* e_inc = nullptr;
+  double* h_inc = nullptr;
+  double* pulse = nullptr;
+  double* probe = nullptr;
+  int probe_cap = 0;
+  size_t probe_id = 0;
+  void* tables = nullptr;  // CPML tables of both precisions live here
+  // dispersive cells
+  int nmetal[3] = {0, 0, 0};
+  int4* mcell[3] = {nullptr, nullptr, nullptr};
+  void* mstate = nullptr;  // SoA state
+  int* slot_map[3] = {nullptr, nullptr, nullptr};
+  int box_lo[3] = {0, 0, 0}, box_dim[3] = {0, 0, 0};
+  // DFT
+  DftView dft;
+  void* ring = nullptr;
+  double* flux = nullptr;  // [12][nf]
+  bool dft_on = true;
+  int host_nsamp = 0;
+  // views (one of them is used, by precision)
+  SimView<float> vf;
+  SimView<double> vd;
+  MetalView<float> mf;
+  MetalView<double> md;
+  LineArgs line;
+  // host step counter
+  int t = 0;
+  // graph replay of a whole DFT period block
+  cudaGraphExec_t graph = nullptr;
+  int graph_len = 0;
+  cudaStream_t graph_stream = nullptr;
+  bool use_graphs = true;
+
+  ~fdtd_sim() {
+    if (graph) cudaGraphExecDestroy(graph);
+    if (graph_stream) cudaStreamDestroy(graph_stream);
+  }
+
+  // buffers that fdtd_reset zeroes (fields, psi, dispersive state, DFT,
+  // clock, incident line, probe); tables are not listed
+  std::vector<std::pair<void*, size_t>> state;
+
+  template <typename U>
+  cudaError_t alloc(U** out, size_t count, bool is_state = false) {
+    auto b = std::make_unique<DevBuf>();
+    cudaError_t e = b->alloc(count * sizeof(U));
+    if (e != cudaSuccess) return e;
+    *out = b->as<U>();
+    if (is_state) state.emplace_back(b->p, b->bytes);
+    bufs.push_back(std::move(b));
+    return cudaSuccess;
+  }
+};
+
+// ---------------------------------------------------------------------
+// parameters
+
+extern "C" void fdtd_params_default(fdtd_params* p) { params_default(p); }
+
+extern "C" size_t fdtd_params_size(void) { return sizeof(fdtd_params); }
+
+extern "C" fdtd_status fdtd_load_input_txt(const char* path, fdtd_params* p) {
+  if (!path || !p) return fail(FDTD_ERR_INVALID, "null argument");
+  int rc = read_input_txt(path, p);
+  if (rc == -1) return fail(FDTD_ERR_IO, std::string("cannot open ") + path);
+  if (rc != 0) return fail(FDTD_ERR_IO, std::string("malformed Input.txt: ") + path);
+  return FDTD_OK;
+}
+
+extern "C" fdtd_status fdtd_write_input_txt(const char* path, const fdtd_params* p) {
+  if (!path || !p) return fail(FDTD_ERR_INVALID, "null argument");
+  if (write_input_txt(path, p) != 0) return fail(FDTD_ERR_IO, std::string("cannot write ") + path);
+  return FDTD_OK;
+}
+
+extern "C" const char* fdtd_last_error(void) { return g_err.c_str(); }
+
+static void fill_dims(const Setup& su, fdtd_dims* d) {
+  std::memset(d, 0, sizeof(*d));
+  d->nx = su.NX; d->ny = su.NY; d->nz = su.NZ;
+  d->ntfsf_x = su.Nt[0]; d->ntfsf_y = su.Nt[1]; d->ntfsf_z = su.Nt[2];
+  d->inc_length = su.L; d->m0 = su.m0;
+  for (int a = 0; a < 3; a++) {
+    d->abs_start[a] = su.absS[a]; d->abs_end[a] = su.absE[a];
+    d->sca_start[a] = su.scaS[a]; d->sca_end[a] = su.scaE[a];
+  }
+  d->num_freq = su.p.NUM_freq;
+  const size_t n = (size_t)su.NX * su.NY * su.NZ;
+  for (int c = 0; c < 3; c++) {
+    int cnt = 0;
+    for (size_t q = 0; q < n; q++) cnt += is_dispersive(su.matc[c][q]);
+    d->n_metal_cells[c] = cnt;
+  }
+  d->hydro = su.hydro;
+  d->precision = su.p.precision;
+  d->dt = su.dt; d->delay = su.delay; d->width = su.width;
+}
+
+extern "C" fdtd_status fdtd_plan(const fdtd_params* p, fdtd_dims* out) {
+  if (!p || !out) return fail(FDTD_ERR_INVALID, "null argument");
+  Setup su;
+  if (const char* msg = setup_build(*p, su)) return fail(FDTD_ERR_INVALID, msg);
+  fill_dims(su, out);
+  return FDTD_OK;
+}
+
+extern "C" fdtd_status fdtd_rasterise(const fdtd_params* p, uint8_t* bits, size_t count) {
+  if (!p || !bits) return fail(FDTD_ERR_INVALID, "null argument");
+  Setup su;
+  if (const char* msg = setup_build(*p, su)) return fail(FDTD_ERR_INVALID, msg);
+  const size_t n = (size_t)su.NX * su.NY * su.NZ;
+  if (count != n) return fail(FDTD_ERR_INVALID, "count must be nx*ny*nz");
+  for (size_t q = 0; q < n; q++) {
+    uint8_t b = 0;
+    for (int c = 0; c < 3; c++) b |= (uint8_t)(is_dispersive(su.matc[c][q]) << c);
+    bits[q] = b;
+  }
+  return FDTD_OK;
+}
+
+extern "C" fdtd_status fdtd_coefficients(const fdtd_params* p, int which, double* out, size_t count,
+                                         size_t* len) {
+  if (!p || !out || !len) return fail(FDTD_ERR_INVALID, "null argument");
+  Setup su;
+  if (const char* msg = setup_build(*p, su)) return fail(FDTD_ERR_INVALID, msg);
+  std::vector<double> v;
+  if (which >= 0 && which < 6) {
+    v = which < 3 ? su.cp[which].ked : su.cp[which - 3].khd;
+  } else if (which >= 6 && which < 30) {
+    const CpmlTables& t = su.cp[(which - 6) / 8];
+    const std::vector<double>* tabs[8] = {&t.be_N, &t.ce_N, &t.be_F, &t.ce_F, &t.bh_N, &t.ch_N, &t.bh_F, &t.ch_F};
+    v = *tabs[(which - 6) % 8];
+  } else if (which == 100) {
+    v = {su.C_E, su.C_E_1, su.C_E_2, su.d1, su.d2, su.d3, su.d4, su.d5, su.dNL,
+         su.C1[0], su.C2[0], su.C3[0], su.C4[0], su.C5[0],
+         su.C1[1], su.C2[1], su.C3[1], su.C4[1], su.C5[1], su.dt, su.N_EQ, 0.0};
+  } else if (which == 101) {
+    v = su.freq;
+  } else if (which == 102) {
+    v = su.pulse;
+  } else {
+    return fail(FDTD_ERR_INVALID, "unknown table");
+  }
+  *len = v.size();
+  if (count < v.size()) return fail(FDTD_ERR_INVALID, "output buffer too small");
+  std::memcpy(out, v.data(), v.size() * sizeof(double));
+  return FDTD_OK;
+}
+
+// ---------------------------------------------------------------------
+// create
+
+template <typename T>
+static fdtd_status upload(T* dst, const std::vector<double>& src) {
+  std::vector<T> tmp(src.begin(), src.end());
+  if (!tmp.empty()) CUDA_TRY(cudaMemcpy(dst, tmp.data(), tmp.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return FDTD_OK;
+}
+
+template <typename T>
+static fdtd_status build_views(fdtd_sim* s) {
+  const Setup& su = s->su;
+  SimView<T>& v = *reinterpret_cast<SimView<T>*>(std::is_same<T, float>::value ? (void*)&s->vf : (void*)&s->vd);
+  MetalView<T>& m = *reinterpret_cast<MetalView<T>*>(std::is_same<T, float>::value ? (void*)&s->mf : (void*)&s->md);
+  std::memset(&v, 0, sizeof(v));
+  std::memset(&m, 0, sizeof(m));
+  v.NX = s->NX; v.NY = s->NY; v.NZ = s->NZ; v.PX = s->PX; v.plane = s->plane;
+  for (int c = 0; c < 3; c++) { v.E[c] = (T*)s->E[c]; v.H[c] = (T*)s->H[c]; }
+  v.mat = s->mat;
+  for (int a = 0; a < 3; a++) { v.mat_lo[a] = s->mat_lo[a]; v.mat_hi[a] = s->mat_hi[a]; }
+  for (int q = 0; q < kMaxClasses; q++) { v.cee[q] = (T)su.Cee; v.ceh[q] = (T)su.Ceh; }
+  v.chh = (T)su.Chh; v.che = (T)su.Che;
+  const double dxyz[3] = {su.p.dx, su.p.dy, su.p.dz};
+  const int N3[3] = {s->NX, s->NY, s->NZ};
+  for (int a = 0; a < 3; a++) {
+    const CpmlTables& t = su.cp[a];
+    const int Nc = su.Nc[a];
+    T* base;
+    const size_t need = 8 * (size_t)(Nc + 1) + (size_t)(Nc + 1) + 2 * (size_t)N3[a];
+    cudaError_t e = s->alloc(&base, need);
+    if (e != cudaSuccess) return fail(FDTD_ERR_ALLOC, cudaGetErrorString(e));
+    T* q = base;
+    auto put = [&](const std::vector<double>& src, size_t len) -> T* {
+      T* at = q;
+      std::vector<double> pad(src);
+      pad.resize(len, 0.0);
+      upload<T>(at, pad);
+      q += len;
+      return at;
+    };
+    CpmlAxis<T>& ca = v.cp[a];
+    ca.be_N = put(t.be_N, Nc + 1); ca.ce_N = put(t.ce_N, Nc + 1);
+    ca.be_F = put(t.be_F, Nc + 1); ca.ce_F = put(t.ce_F, Nc + 1);
+    ca.bh_N = put(t.bh_N, Nc + 1); ca.ch_N = put(t.ch_N, Nc + 1);
+    ca.bh_F = put(t.bh_F, Nc + 1); ca.ch_F = put(t.ch_F, Nc + 1);
+    std::vector<double> ik(N3[a]), ih(N3[a]);
+    for (int i = 0; i < N3[a]; i++) { ik[i] = 1.0 / t.ked[i]; ih[i] = 1.0 / t.khd[i]; }
+    ca.inv_ked = put(ik, N3[a]);
+    ca.inv_khd = put(ih, N3[a]);
+    ca.inv_d = (T)(1.0 / dxyz[a]);
+    ca.Nc = Nc;
+    ca.F = su.F[a];
+    v.dxyz[a] = (T)dxyz[a];
+    // Ey's near-x slab reads ce_y_N in the reference (main.cu:2891)
+    if (a == 0) {
+      const std::vector<double>& src = (su.p.fixes & FDTD_FIX_CE_EY_XN) ? su.cp[0].ce_N : su.cp[1].ce_N;
+      std::vector<double> pad(src);
+      pad.resize(Nc + 1, 0.0);
+      T* at = q;
+      upload<T>(at, pad);
+      q += Nc + 1;
+      ca.ce_N_ey = at;
+    }
+  }
+  v.cp[1].ce_N_ey = v.cp[1].ce_N;
+  v.cp[2].ce_N_ey = v.cp[2].ce_N;
+  // psi slabs
+  for (int c = 0; c < 3; c++)
+    for (int slot = 0; slot < 2; slot++) {
+      const int ax = (c + 1 + slot) % 3;
+      const int Nc = su.Nc[ax];
+      size_t cells_e, cells_h;
+      if (ax == 2) { cells_e = (size_t)(Nc + 1) * s->plane; cells_h = (size_t)Nc * s->plane; }
+      else if (ax == 1) { cells_e = (size_t)s->NZ * (Nc + 1) * s->PX; cells_h = (size_t)s->NZ * Nc * s->PX; }
+      else { cells_e = (size_t)s->NZ * s->NY * (Nc + 1); cells_h = (size_t)s->NZ * s->NY * Nc; }
+      T *a1, *a2, *a3, *a4;
+      cudaError_t e;
+      if ((e = s->alloc(&a1, cells_e, true)) != cudaSuccess || (e = s->alloc(&a2, cells_e, true)) != cudaSuccess ||
+          (e = s->alloc(&a3, cells_h, true)) != cudaSuccess || (e = s->alloc(&a4, cells_h, true)) != cudaSuccess)
+        return fail(FDTD_ERR_ALLOC, cudaGetErrorString(e));
+      v.psiE_N[c][slot] = a1; v.psiE_F[c][slot] = a2; v.psiH_N[c][slot] = a3; v.psiH_F[c][slot] = a4;
+    }
+  // TFSF
+  TfsfView& tf = v.tf;
+  tf.on = 1;
+  tf.Tx = su.Nt[0]; tf.Ty = su.Nt[1]; tf.Tz = su.Nt[2];
+  tf.i0 = su.i0; tf.j0 = su.j0; tf.k0 = su.k0; tf.m0 = su.m0;
+  tf.sth = su.sth; tf.cth = su.cth; tf.sph = su.sph; tf.cph = su.cph;
+  for (int c = 0; c < 3; c++) { tf.fe[c] = su.fe[c]; tf.fh[c] = su.fh[c]; }
+  tf.dscale = su.p.dx / su.d1D;
+  v.e_inc = s->e_inc;
+  v.h_inc = s->h_inc;
+  v.nonfinite = &s->clk->nonfinite;
+  // dispersive cells
+  for (int c = 0; c < 3; c++) { m.n[c] = s->nmetal[c]; m.cell[c] = s->mcell[c]; }
+  size_t maxn = std::max(s->nmetal[0], std::max(s->nmetal[1], s->nmetal[2]));
+  if (maxn > 0) {
+    // per component: en, en1, cpn[2], cpn1[2], pd[3], nd[2] = 11 arrays
+    T* st;
+    cudaError_t e = s->alloc(&st, (size_t)3 * 11 * maxn, true);
+    if (e != cudaSuccess) return fail(FDTD_ERR_ALLOC, cudaGetErrorString(e));
+    for (int c = 0; c < 3; c++) {
+      T* b = st + (size_t)c * 11 * maxn;
+      m.en[c] = b; m.en1[c] = b + maxn;
+      m.cpn[c][0] = b + 2 * maxn; m.cpn[c][1] = b + 3 * maxn;
+      m.cpn1[c][0] = b + 4 * maxn; m.cpn1[c][1] = b + 5 * maxn;
+      m.pd[c][0] = b + 6 * maxn; m.pd[c][1] = b + 7 * maxn; m.pd[c][2] = b + 8 * maxn;
+      m.nd[c][0] = b + 9 * maxn; m.nd[c][1] = b + 10 * maxn;
+      m.slot_map[c] = s->slot_map[c];
+    }
+    s->mstate = st;
+  }
+  for (int a = 0; a < 3; a++) { m.box_lo[a] = s->box_lo[a]; m.box_dim[a] = s->box_dim[a]; }
+  m.C_E = (T)su.C_E; m.C_E_1 = (T)su.C_E_1; m.C_E_2 = (T)su.C_E_2;
+  m.d1 = (T)su.d1; m.d2 = (T)su.d2; m.d3 = (T)su.d3; m.d4 = (T)su.d4; m.d5 = (T)su.d5; m.dNL = (T)su.dNL;
+  for (int q = 0; q < 2; q++) {
+    m.C1[q] = (T)su.C1[q]; m.C2[q] = (T)su.C2[q]; m.C3[q] = (T)su.C3[q]; m.C4[q] = (T)su.C4[q]; m.C5[q] = (T)su.C5[q];
+  }
+  m.dt = (T)su.dt; m.z0 = (T)su.z0; m.e0 = (T)su.e0; m.N_EQ = (T)su.N_EQ;
+  m.inv_dx = (T)(1.0 / su.p.dx); m.inv_dy = (T)(1.0 / su.p.dy); m.inv_dz = (T)(1.0 / su.p.dz);
+  m.hydro = su.hydro;
+  m.fix_cbrt = (su.p.fixes & FDTD_FIX_HYDRO_CBRT) ? 1 : 0;
+  // DFT sample ring
+  if (s->dft.rows > 0) {
+    T* r;
+    cudaError_t e = s->alloc(&r, (size_t)kSampleBlock * s->dft.rows, true);
+    if (e != cudaSuccess) return fail(FDTD_ERR_ALLOC, cudaGetErrorString(e));
+    s->ring = r;
+  }
+  return FDTD_OK;
+}
+
+static fdtd_status create_impl(const fdtd_params* p, int device, fdtd_sim** out) {
+  auto s = std::make_unique<fdtd_sim>();
+  if (const char* msg = setup_build(*p, s->su)) return fail(FDTD_ERR_INVALID, msg);
+  const Setup& su = s->su;
+  s->device = device;
+  s->fp64 = su.p.precision == FDTD_FP64;
+  CUDA_TRY(cudaSetDevice(device));
+  s->NX = su.NX; s->NY = su.NY; s->NZ = su.NZ;
+  s->PX = (su.NX + 7) / 8 * 8;
+  s->plane = (size_t)s->NY * s->PX;
+  s->ncell = s->plane * s->NZ;
+  s->kchunk = s->NZ >= 192 ? 32 : 16;
+  const size_t es = s->fp64 ? 8 : 4;
+  // fields
+  for (int c = 0; c < 3; c++) {
+    char* a;
+    char* b;
+    cudaError_t e;
+    if ((e = s->alloc(&a, s->ncell * es, true)) != cudaSuccess || (e = s->alloc(&b, s->ncell * es, true)) != cudaSuccess)
+      return fail(FDTD_ERR_ALLOC, std::string("field allocation: ") + cudaGetErrorString(e));
+    s->E[c] = a;
+    s->H[c] = b;
+  }
+  CUDA_TRY(s->alloc(&s->clk, 1, true));
+  CUDA_TRY(s->alloc(&s->e_inc, su.L, true));
+  CUDA_TRY(s->alloc(&s->h_inc, su.L, true));
+  CUDA_TRY(s->alloc(&s->pulse, su.pulse.size()));
+  CUDA_TRY(cudaMemcpy(s->pulse, su.pulse.data(), su.pulse.size() * sizeof(double), cudaMemcpyHostToDevice));
+  s->probe_cap = su.p.Tend + 2;
+  CUDA_TRY(s->alloc(&s->probe, (size_t)3 * s->probe_cap, true));
+  s->probe_id = (size_t)su.probe[2] * s->plane + (size_t)su.probe[1] * s->PX + su.probe[0];
+  // material bits in device layout + dispersive cell lists
+  {
+    std::vector<uint8_t> bits(s->ncell, 0);
+    int lo[3] = {s->NX, s->NY, s->NZ}, hi[3] = {0, 0, 0};
+    std::vector<int4> cells[3];
+    for (int k = 0; k < s->NZ; k++)
+      for (int j = 0; j < s->NY; j++)
+        for (int i = 0; i < s->NX; i++) {
+          const size_t r = ((size_t)i * s->NY + j) * s->NZ + k;
+          uint8_t b = 0;
+          for (int c = 0; c < 3; c++)
+            if (is_dispersive(su.matc[c][r])) {
+              b |= (uint8_t)(1u << c);
+              // only cells the reference's UPDATE_e* touches: index along c
+              // below N-1, the other two strictly inside (main.cu:1172,
+              // 1476, 1767); the curl there reads the -1 neighbours
+              const int q[3] = {i, j, k};
+              const int N3[3] = {s->NX, s->NY, s->NZ};
+              bool active = true;
+              for (int a = 0; a < 3; a++) {
+                if (q[a] >= N3[a] - 1) active = false;
+                if (a != c && q[a] < 1) active = false;
+              }
+              if (active) cells[c].push_back(make_int4(i, j, k, (int)cells[c].size()));
+            }
+          if (b) {
+            bits[(size_t)k * s->plane + (size_t)j * s->PX + i] = b;
+            lo[0] = std::min(lo[0], i); lo[1] = std::min(lo[1], j); lo[2] = std::min(lo[2], k);
+            hi[0] = std::max(hi[0], i + 1); hi[1] = std::max(hi[1], j + 1); hi[2] = std::max(hi[2], k + 1);
+          }
+        }
+    for (int a = 0; a < 3; a++) {
+      if (hi[a] <= lo[a]) { lo[a] = 0; hi[a] = 0; }
+      s->mat_lo[a] = lo[a];
+      s->mat_hi[a] = hi[a];
+    }
+    CUDA_TRY(s->alloc(&s->mat, s->ncell));
+    CUDA_TRY(cudaMemcpy(s->mat, bits.data(), s->ncell, cudaMemcpyHostToDevice));
+    // slot maps over the bounding box grown by one cell (hydro neighbours)
+    for (int a = 0; a < 3; a++) {
+      s->box_lo[a] = std::max(0, lo[a] - 1);
+      int h = std::min(a == 0 ? s->NX : a == 1 ? s->NY : s->NZ, hi[a] + 1);
+      s->box_dim[a] = std::max(0, h - s->box_lo[a]);
+    }
+    const size_t nbox = (size_t)s->box_dim[0] * s->box_dim[1] * s->box_dim[2];
+    for (int c = 0; c < 3; c++) {
+      s->nmetal[c] = (int)cells[c].size();
+      if (!cells[c].empty()) {
+        CUDA_TRY(s->alloc(&s->mcell[c], cells[c].size()));
+        CUDA_TRY(cudaMemcpy(s->mcell[c], cells[c].data(), cells[c].size() * sizeof(int4), cudaMemcpyHostToDevice));
+      }
+      if (nbox > 0) {
+        std::vector<int> map(nbox, -1);
+        for (const int4& e : cells[c]) {
+          size_t o = ((size_t)(e.z - s->box_lo[2]) * s->box_dim[1] + (e.y - s->box_lo[1])) * s->box_dim[0] +
+                     (e.x - s->box_lo[0]);
+          map[o] = e.w;
+        }
+        CUDA_TRY(s->alloc(&s->slot_map[c], nbox));
+        CUDA_TRY(cudaMemcpy(s->slot_map[c], map.data(), nbox * sizeof(int), cudaMemcpyHostToDevice));
+      }
+    }
+  }
+  // DFT faces: box b (0 Abs, 1 Sca), face f (-X +X -Y +Y -Z +Z)
+  {
+    static const int fcomp[3][4] = {{1, 2, 4, 5}, {0, 2, 3, 5}, {0, 1, 3, 4}};
+    DftView& d = s->dft;
+    std::memset(&d, 0, sizeof(d));
+    d.nfaces = 12;
+    long long row = 0;
+    for (int b = 0; b < 2; b++) {
+      const int* S = b == 0 ? su.absS : su.scaS;
+      const int* En = b == 0 ? su.absE : su.scaE;
+      for (int f = 0; f < 6; f++) {
+        DftFace& F = d.face[b * 6 + f];
+        F.ax = f / 2;
+        const int a1 = F.ax == 0 ? 1 : 0, a2 = F.ax == 2 ? 1 : 2;
+        F.pos = (f & 1) ? En[F.ax] - 1 : S[F.ax];
+        F.s1 = S[a1]; F.s2 = S[a2];
+        F.na = En[a1] - S[a1]; F.nb = En[a2] - S[a2];
+        for (int c = 0; c < 4; c++) F.comp[c] = fcomp[F.ax][c];
+        F.row0 = row;
+        row += 4LL * F.na * F.nb;
+      }
+    }
+    d.rows = row;
+    d.nf = su.p.NUM_freq;
+    d.dt = su.dt;
+    double* fq;
+    CUDA_TRY(s->alloc(&fq, d.nf));
+    CUDA_TRY(cudaMemcpy(fq, su.freq.data(), d.nf * sizeof(double), cudaMemcpyHostToDevice));
+    d.freq = fq;
+    cudaError_t e;
+    if ((e = s->alloc(&d.acc_re, (size_t)d.nf * d.rows, true)) != cudaSuccess ||
+        (e = s->alloc(&d.acc_im, (size_t)d.nf * d.rows, true)) != cudaSuccess)
+      return fail(FDTD_ERR_ALLOC, std::string("DFT accumulators: ") + cudaGetErrorString(e));
+    CUDA_TRY(s->alloc(&s->flux, (size_t)12 * d.nf));
+  }
+  s->dft_on = su.p.StaticField == 0;
+  fdtd_status st = s->fp64 ? build_views<double>(s.get()) : build_views<float>(s.get());
+  if (st != FDTD_OK) return st;
+  // line
+  LineArgs& L = s->line;
+  L.e_inc = s->e_inc; L.h_inc = s->h_inc; L.L = su.L; L.m0 = su.m0; L.src = su.m0 - su.p.source_offset;
+  L.ch = su.z0 * su.dt / (su.mu0 * su.d1D);
+  L.ce = su.dt / (su.z0 * su.ep0 * su.d1D);
+  const double factor = su.c0 * su.dt;
+  L.mur = (factor - su.d1D) / (factor + su.d1D);
+  L.pulse = s->pulse; L.tmax = (int)su.pulse.size();
+  L.clk = s->clk; L.probe = s->probe; L.probe_cap = s->probe_cap;
+  L.dft_every = s->dft_on ? su.p.dft_every : 0;
+  CUDA_TRY(cudaDeviceSynchronize());
+  *out = s.release();
+  return FDTD_OK;
+}
+
+extern "C" fdtd_status fdtd_create(const fdtd_params* p, int device, fdtd_sim** out) {
+  if (!p || !out) return fail(FDTD_ERR_INVALID, "null argument");
+  *out = nullptr;
+  try {
+    return create_impl(p, device, out);
+  } catch (const std::bad_alloc&) {
+    return fail(FDTD_ERR_ALLOC, "host allocation failed");
+  }
+}
+
+extern "C" fdtd_status fdtd_destroy(fdtd_sim* s) {
+  if (!s) return FDTD_OK;
+  cudaSetDevice(s->device);
+  cudaDeviceSynchronize();
+  delete s;
+  return FDTD_OK;
+}
+
+extern "C" fdtd_status fdtd_get_dims(const fdtd_sim* s, fdtd_dims* d) {
+  if (!s || !d) return fail(FDTD_ERR_INVALID, "null argument");
+  fill_dims(s->su, d);
+  return FDTD_OK;
+}
+
+extern "C" fdtd_status fdtd_reset(fdtd_sim* s) {
+  if (!s) return fail(FDTD_ERR_INVALID, "null argument");
+  CUDA_TRY(cudaSetDevice(s->device));
+  CUDA_TRY(cudaDeviceSynchronize());
+  for (const auto& b : s->state) CUDA_TRY(cudaMemset(b.first, 0, b.second));
+  s->t = 0;
+  s->host_nsamp = 0;
+  return FDTD_OK;
+}
+
+// ---------------------------------------------------------------------
+// launches
+
+template <typename T>
+static SimView<T>& view(fdtd_sim* s);
+template <>
+SimView<float>& view<float>(fdtd_sim* s) { return s->vf; }
+template <>
+SimView<double>& view<double>(fdtd_sim* s) { return s->vd; }
+template <typename T>
+static MetalView<T>& mview(fdtd_sim* s);
+template <>
+MetalView<float>& mview<float>(fdtd_sim* s) { return s->mf; }
+template <>
+MetalView<double>& mview<double>(fdtd_sim* s) { return s->md; }
+
+static dim3 pass_grid(const fdtd_sim* s) {
+  return dim3((s->NX + 31) / 32, (s->NY + 7) / 8, (s->NZ + s->kchunk - 1) / s->kchunk);
+}
+
+template <typename T>
+static void launch_h(fdtd_sim* s, cudaStream_t st) {
+  h_pass<T><<<pass_grid(s), dim3(32, 8), 0, st>>>(view<T>(s), s->kchunk);
+}
+template <typename T>
+static void launch_line(fdtd_sim* s, cudaStream_t st) {
+  line_step<T><<<1, 1024, 0, st>>>(s->line, view<T>(s), s->probe_id);
+}
+template <typename T>
+static void launch_e(fdtd_sim* s, cudaStream_t st) {
+  e_pass<T><<<pass_grid(s), dim3(32, 8), 0, st>>>(view<T>(s), s->kchunk);
+  const int ntot = s->nmetal[0] + s->nmetal[1] + s->nmetal[2];
+  if (ntot == 0) return;
+  if (!s->su.hydro) {
+    metal_e<T><<<(ntot + 127) / 128, 128, 0, st>>>(view<T>(s), mview<T>(s), s->clk);
+  } else {
+    hydro_p<T><<<(ntot + 127) / 128, 128, 0, st>>>(view<T>(s), mview<T>(s), s->clk);
+    for (int c = 0; c < 3; c++)
+      if (s->nmetal[c] > 0)
+        metal_e_hydro<T><<<(s->nmetal[c] + 127) / 128, 128, 0, st>>>(view<T>(s), mview<T>(s), s->clk, c);
+  }
+}
+template <typename T>
+static void launch_sample(fdtd_sim* s, cudaStream_t st) {
+  int maxn = 0;
+  for (int f = 0; f < 12; f++) maxn = std::max(maxn, s->dft.face[f].na * s->dft.face[f].nb);
+  dim3 g((maxn + 255) / 256, 12);
+  dft_sample<T><<<g, 256, 0, st>>>(view<T>(s), s->dft, (T*)s->ring, s->clk);
+}
+template <typename T>
+static void launch_contract(fdtd_sim* s, cudaStream_t st) {
+  dim3 g((unsigned)((s->dft.rows + kDftRows - 1) / kDftRows), (s->dft.nf + kDftFreqs - 1) / kDftFreqs);
+  dft_contract<T><<<g, kDftRows, 0, st>>>(s->dft, (const T*)s->ring, s->clk, 0);
+  dft_reset_count<<<1, 1, 0, st>>>(s->clk);
+}
+
+// One full step in the reference's order.  Host mirrors of the clock
+// decide which optional kernels run; the kernels read t from the device.
+template <typename T>
+static void enqueue_step(fdtd_sim* s, cudaStream_t st) {
+  launch_h<T>(s, st);
+  launch_line<T>(s, st);
+  launch_e<T>(s, st);
+  if (s->line.dft_every > 0 && s->t % s->line.dft_every == 0) {
+    launch_sample<T>(s, st);
+    if (++s->host_nsamp == kSampleBlock) {
+      launch_contract<T>(s, st);
+      s->host_nsamp = 0;
+    }
+  }
+  s->t++;
+}
+
+template <typename T>
+static fdtd_status step_impl(fdtd_sim* s, int nsteps, cudaStream_t st) {
+  const int every = s->line.dft_every > 0 ? s->line.dft_every : 1;
+  const int G = every * kSampleBlock;  // launch pattern period
+  int done = 0;
+  while (done < nsteps) {
+    const bool aligned = s->t % G == 0 && s->host_nsamp == 0 && nsteps - done >= G;
+    if (s->use_graphs && aligned) {
+      if (!s->graph) {
+        // capture one period on a private stream, then replay it
+        if (!s->graph_stream) CUDA_TRY(cudaStreamCreateWithFlags(&s->graph_stream, cudaStreamNonBlocking));
+        cudaGraph_t g;
+        const int t_save = s->t, n_save = s->host_nsamp;
+        CUDA_TRY(cudaStreamBeginCapture(s->graph_stream, cudaStreamCaptureModeThreadLocal));
+        for (int q = 0; q < G; q++) enqueue_step<T>(s, s->graph_stream);
+        CUDA_TRY(cudaStreamEndCapture(s->graph_stream, &g));
+        s->t = t_save;
+        s->host_nsamp = n_save;
+        cudaError_t e = cudaGraphInstantiate(&s->graph, g, 0);
+        cudaGraphDestroy(g);
+        CUDA_TRY(e);
+        s->graph_len = G;
+      }
+      CUDA_TRY(cudaGraphLaunch(s->graph, st));
+      s->t += G;
+      done += G;
+    } else {
+      enqueue_step<T>(s, st);
+      done++;
+    }
+  }
+  CUDA_TRY(cudaGetLastError());
+  return FDTD_OK;
+}
+
+static cudaStream_t as_stream(void* p) { return reinterpret_cast<cudaStream_t>(p); }
+
+extern "C" fdtd_status fdtd_step(fdtd_sim* s, int nsteps, void* stream) {
+  if (!s || nsteps < 0) return fail(FDTD_ERR_INVALID, "bad argument");
+  CUDA_TRY(cudaSetDevice(s->device));
+  return s->fp64 ? step_impl<double>(s, nsteps, as_stream(stream)) : step_impl<float>(s, nsteps, as_stream(stream));
+}
+
+extern "C" fdtd_status fdtd_run(fdtd_sim* s, void* stream) {
+  if (!s) return fail(FDTD_ERR_INVALID, "null argument");
+  const int left = s->su.p.Tend + 1 - s->t;
+  if (left <= 0) return FDTD_OK;
+  return fdtd_step(s, left, stream);
+}
+
+extern "C" fdtd_status fdtd_update_h(fdtd_sim* s, void* stream) {
+  if (!s) return fail(FDTD_ERR_INVALID, "null argument");
+  CUDA_TRY(cudaSetDevice(s->device));
+  if (s->fp64) launch_h<double>(s, as_stream(stream)); else launch_h<float>(s, as_stream(stream));
+  CUDA_TRY(cudaGetLastError());
+  return FDTD_OK;
+}
+extern "C" fdtd_status fdtd_update_line(fdtd_sim* s, void* stream) {
+  if (!s) return fail(FDTD_ERR_INVALID, "null argument");
+  CUDA_TRY(cudaSetDevice(s->device));
+  if (s->fp64) launch_line<double>(s, as_stream(stream)); else launch_line<float>(s, as_stream(stream));
+  CUDA_TRY(cudaGetLastError());
+  return FDTD_OK;
+}
+extern "C" fdtd_status fdtd_update_e(fdtd_sim* s, void* stream) {
+  if (!s) return fail(FDTD_ERR_INVALID, "null argument");
+  CUDA_TRY(cudaSetDevice(s->device));
+  if (s->fp64) launch_e<double>(s, as_stream(stream)); else launch_e<float>(s, as_stream(stream));
+  CUDA_TRY(cudaGetLastError());
+  return FDTD_OK;
+}
+extern "C" fdtd_status fdtd_spectral_accumulate(fdtd_sim* s, void* stream) {
+  if (!s) return fail(FDTD_ERR_INVALID, "null argument");
+  CUDA_TRY(cudaSetDevice(s->device));
+  cudaStream_t st = as_stream(stream);
+  if (s->line.dft_every > 0 && s->t % s->line.dft_every == 0) {
+    if (s->fp64) launch_sample<double>(s, st); else launch_sample<float>(s, st);
+    if (++s->host_nsamp == kSampleBlock) {
+      if (s->fp64) launch_contract<double>(s, st); else launch_contract<float>(s, st);
+      s->host_nsamp = 0;
+    }
+  }
+  s->t++;
+  CUDA_TRY(cudaGetLastError());
+  return FDTD_OK;
+}
+
+extern "C" fdtd_status fdtd_get_time(const fdtd_sim* s, int* t) {
+  if (!s || !t) return fail(FDTD_ERR_INVALID, "null argument");
+  *t = s->t;
+  return FDTD_OK;
+}
+
+extern "C" fdtd_status fdtd_check(fdtd_sim* s) {
+  if (!s) return fail(FDTD_ERR_INVALID, "null argument");
+  CUDA_TRY(cudaSetDevice(s->device));
+  DevClock c;
+  CUDA_TRY(cudaMemcpy(&c, s->clk, sizeof(c), cudaMemcpyDeviceToHost));
+  if (c.nonfinite) return fail(FDTD_ERR_NONFINITE, "non-finite field value detected");
+  return FDTD_OK;
+}
+
+// ---------------------------------------------------------------------
+// spectra
+
+static fdtd_status flush_dft(fdtd_sim* s) {
+  if (s->host_nsamp > 0) {
+    if (s->fp64) launch_contract<double>(s, 0); else launch_contract<float>(s, 0);
+    s->host_nsamp = 0;
+  }
+  CUDA_TRY(cudaGetLastError());
+  return FDTD_OK;
+}
+
+extern "C" fdtd_status fdtd_spectral_finalize(fdtd_sim* s, double* out) {
+  if (!s || !out) return fail(FDTD_ERR_INVALID, "null argument");
+  CUDA_TRY(cudaSetDevice(s->device));
+  CUDA_TRY(cudaDeviceSynchronize());
+  fdtd_status st = flush_dft(s);
+  if (st != FDTD_OK) return st;
+  const int nf = s->dft.nf;
+  flux_reduce<<<dim3(12, nf), 256>>>(s->dft, s->flux);
+  CUDA_TRY(cudaGetLastError());
+  std::vector<double> Q((size_t)12 * nf);
+  CUDA_TRY(cudaMemcpy(Q.data(), s->flux, Q.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  const Setup& su = s->su;
+  const double dxy = su.p.dx * su.p.dy;
+  const bool sphere = su.p.geometry == FDTD_GEOM_REFERENCE && su.p.nano_sphere == 1;
+  for (int m = 0; m < nf; m++) {
+    const double amp = std::abs(su.Einc[m]);
+    double q[2][6];
+    for (int b = 0; b < 2; b++)
+      for (int f = 0; f < 6; f++) q[b][f] = Q[(size_t)(b * 6 + f) * nf + m] * dxy / (amp * amp);
+    double sca = -q[1][0] + q[1][1] - q[1][2] + q[1][3] - q[1][4] + q[1][5];
+    double ab = -q[0][0] + q[0][1] - q[0][2] + q[0][3] - q[0][4] + q[0][5];
+    if (sphere) {
+      const double r = su.p.nano_sphere_radius;
+      sca = sca / (su.pi * r * r);
+      ab = -ab / (su.pi * r * r);
+    }
+    double* row = out + 19 * (size_t)m;
+    row[0] = su.c0 / su.freq[m];
+    row[1] = sca; row[2] = ab; row[3] = ab + sca;
+    for (int f = 0; f < 6; f++) { row[4 + f] = q[1][f]; row[10 + f] = q[0][f]; }
+    row[16] = amp; row[17] = su.Einc[m].real(); row[18] = su.Einc[m].imag();
+  }
+  return FDTD_OK;
+}
+
+extern "C" fdtd_status fdtd_write_scatabs(fdtd_sim* s, const char* path) {
+  if (!s || !path) return fail(FDTD_ERR_INVALID, "null argument");
+  std::vector<double> rows((size_t)19 * s->dft.nf);
+  fdtd_status st = fdtd_spectral_finalize(s, rows.data());
+  if (st != FDTD_OK) return st;
+  FILE* f = std::fopen(path, "w");
+  if (!f) return fail(FDTD_ERR_IO, std::string("cannot write ") + path);
+  for (int m = 0; m < s->dft.nf; m++) {
+    for (int c = 0; c < 19; c++) std::fprintf(f, c == 18 ? "%e\n" : "%e\t", rows[(size_t)19 * m + c]);
+  }
+  std::fclose(f);
+  return FDTD_OK;
+}
+
+extern "C" fdtd_status fdtd_get_dft(fdtd_sim* s, int box, int face, int comp, double* re, double* im,
+                                    size_t count) {
+  if (!s || !re || !im || box < 0 || box > 1 || face < 0 || face > 5 || comp < 0 || comp > 3)
+    return fail(FDTD_ERR_INVALID, "bad argument");
+  CUDA_TRY(cudaSetDevice(s->device));
+  CUDA_TRY(cudaDeviceSynchronize());
+  fdtd_status st = flush_dft(s);
+  if (st != FDTD_OK) return st;
+  const DftFace& F = s->dft.face[box * 6 + face];
+  const int A = F.na + 1, B = F.nb + 1, nf = s->dft.nf;
+  if (count != (size_t)nf * A * B) return fail(FDTD_ERR_INVALID, "count must be NUM_freq*(na+1)*(nb+1)");
+  std::memset(re, 0, count * sizeof(double));
+  std::memset(im, 0, count * sizeof(double));
+  const size_t n = (size_t)F.na * F.nb;
+  std::vector<double> r(n), i(n);
+  for (int m = 0; m < nf; m++) {
+    const size_t off = (size_t)m * s->dft.rows + F.row0 + (size_t)comp * n;
+    CUDA_TRY(cudaMemcpy(r.data(), s->dft.acc_re + off, n * sizeof(double), cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(i.data(), s->dft.acc_im + off, n * sizeof(double), cudaMemcpyDeviceToHost));
+    for (int u = 0; u < F.na; u++)
+      for (int v = 0; v < F.nb; v++) {
+        re[((size_t)m * A + u) * B + v] = r[(size_t)u * F.nb + v];
+        im[((size_t)m * A + u) * B + v] = i[(size_t)u * F.nb + v];
+      }
+  }
+  return FDTD_OK;
+}
+
+extern "C" fdtd_status fdtd_get_freqs(const fdtd_sim* s, double* freq, size_t count) {
+  if (!s || !freq || count != s->su.freq.size()) return fail(FDTD_ERR_INVALID, "bad argument");
+  std::memcpy(freq, s->su.freq.data(), count * sizeof(double));
+  return FDTD_OK;
+}
+
+extern "C" fdtd_status fdtd_get_incident(const fdtd_sim* s, double* re, double* im, size_t count) {
+  if (!s || !re || !im || count != s->su.Einc.size()) return fail(FDTD_ERR_INVALID, "bad argument");
+  for (size_t m = 0; m < count; m++) { re[m] = s->su.Einc[m].real(); im[m] = s->su.Einc[m].imag(); }
+  return FDTD_OK;
+}
+
+// ---------------------------------------------------------------------
+// fields, snapshots, probes
+
+static void* comp_ptr(fdtd_sim* s, int comp) { return comp < 3 ? s->E[comp] : s->H[comp - 3]; }
+
+extern "C" fdtd_status fdtd_get_field(fdtd_sim* s, int comp, double* out, size_t count) {
+  if (!s || !out || comp < 0 || comp > 5) return fail(FDTD_ERR_INVALID, "bad argument");
+  const size_t n = (size_t)s->NX * s->NY * s->NZ;
+  if (count != n) return fail(FDTD_ERR_INVALID, "count must be nx*ny*nz");
+  CUDA_TRY(cudaSetDevice(s->device));
+  double* tmp;
+  CUDA_TRY(cudaMalloc(&tmp, n * sizeof(double)));
+  const unsigned g = (unsigned)((n + 255) / 256);
+  if (s->fp64) to_ref_layout<double><<<g, 256>>>((const double*)comp_ptr(s, comp), tmp, s->NX, s->NY, s->NZ, s->PX);
+  else to_ref_layout<float><<<g, 256>>>((const float*)comp_ptr(s, comp), tmp, s->NX, s->NY, s->NZ, s->PX);
+  cudaError_t e = cudaMemcpy(out, tmp, n * sizeof(double), cudaMemcpyDeviceToHost);
+  cudaFree(tmp);
+  CUDA_TRY(e);
+  return FDTD_OK;
+}
+
+extern "C" fdtd_status fdtd_set_field(fdtd_sim* s, int comp, const double* in, size_t count) {
+  if (!s || !in || comp < 0 || comp > 5) return fail(FDTD_ERR_INVALID, "bad argument");
+  const size_t n = (size_t)s->NX * s->NY * s->NZ;
+  if (count != n) return fail(FDTD_ERR_INVALID, "count must be nx*ny*nz");
+  CUDA_TRY(cudaSetDevice(s->device));
+  double* tmp;
+  CUDA_TRY(cudaMalloc(&tmp, n * sizeof(double)));
+  cudaError_t e = cudaMemcpy(tmp, in, n * sizeof(double), cudaMemcpyHostToDevice);
+  const unsigned g = (unsigned)((n + 255) / 256);
+  if (e == cudaSuccess) {
+    if (s->fp64) from_ref_layout<double><<<g, 256>>>(tmp, (double*)comp_ptr(s, comp), s->NX, s->NY, s->NZ, s->PX);
+    else from_ref_layout<float><<<g, 256>>>(tmp, (float*)comp_ptr(s, comp), s->NX, s->NY, s->NZ, s->PX);
+    e = cudaDeviceSynchronize();
+  }
+  cudaFree(tmp);
+  CUDA_TRY(e);
+  return FDTD_OK;
+}
+
+template <typename T>
+__global__ void plane_gather(const T* src, double* dst, int NX, int NY, int NZ, int PX, int axis, int index) {
+  const int na = axis == 0 ? NY : NX;
+  const int nb = axis == 2 ? NY : NZ;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= na * nb) return;
+  const int a = q / nb, b = q - a * nb;
+  int i, j, k;
+  if (axis == 0) { i = index; j = a; k = b; }
+  else if (axis == 1) { i = a; j = index; k = b; }
+  else { i = a; j = b; k = index; }
+  dst[q] = (double)src[((size_t)k * NY + j) * PX + i];
+}
+
+extern "C" fdtd_status fdtd_snapshot_plane(fdtd_sim* s, int comp, int axis, int index, double* dst, size_t count,
+                                           void* stream) {
+  if (!s || !dst || comp < 0 || comp > 5 || axis < 0 || axis > 2) return fail(FDTD_ERR_INVALID, "bad argument");
+  const int N3[3] = {s->NX, s->NY, s->NZ};
+  if (index < 0 || index >= N3[axis]) return fail(FDTD_ERR_INVALID, "plane index outside the grid");
+  const int na = axis == 0 ? s->NY : s->NX, nb = axis == 2 ? s->NY : s->NZ;
+  if (count != (size_t)na * nb) return fail(FDTD_ERR_INVALID, "count must match the plane size");
+  CUDA_TRY(cudaSetDevice(s->device));
+  cudaPointerAttributes at;
+  CUDA_TRY(cudaPointerGetAttributes(&at, dst));
+  const bool on_dev = at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+  cudaStream_t st = as_stream(stream);
+  double* tgt = dst;
+  if (!on_dev) CUDA_TRY(cudaMalloc(&tgt, count * sizeof(double)));
+  const unsigned g = (unsigned)((count + 255) / 256);
+  if (s->fp64)
+    plane_gather<double><<<g, 256, 0, st>>>((const double*)comp_ptr(s, comp), tgt, s->NX, s->NY, s->NZ, s->PX, axis,
+                                            index);
+  else
+    plane_gather<float><<<g, 256, 0, st>>>((const float*)comp_ptr(s, comp), tgt, s->NX, s->NY, s->NZ, s->PX, axis,
+                                           index);
+  if (!on_dev) {
+    cudaError_t e = cudaMemcpyAsync(dst, tgt, count * sizeof(double), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(tgt);
+    CUDA_TRY(e);
+  }
+  CUDA_TRY(cudaGetLastError());
+  return FDTD_OK;
+}
+
+extern "C" fdtd_status fdtd_get_probe(fdtd_sim* s, double* out, size_t count, int* n) {
+  if (!s || !out || !n) return fail(FDTD_ERR_INVALID, "null argument");
+  CUDA_TRY(cudaSetDevice(s->device));
+  // record the E of the last completed step (the line kernel records
+  // the previous step at the start of each new one)
+  if (s->fp64) probe_record<double><<<1, 32>>>(s->vd, s->clk, s->probe, s->probe_cap, s->probe_id);
+  else probe_record<float><<<1, 32>>>(s->vf, s->clk, s->probe, s->probe_cap, s->probe_id);
+  CUDA_TRY(cudaDeviceSynchronize());
+  size_t have = (size_t)3 * std::min(s->t, s->probe_cap);
+  size_t m = std::min(have, count);
+  CUDA_TRY(cudaMemcpy(out, s->probe, m * sizeof(double), cudaMemcpyDeviceToHost));
+  *n = (int)(m / 3);
+  return FDTD_OK;
+}
+
+extern "C" fdtd_status fdtd_get_material(fdtd_sim* s, uint8_t* out, size_t count) {
+  if (!s || !out) return fail(FDTD_ERR_INVALID, "null argument");
+  const size_t n = (size_t)s->NX * s->NY * s->NZ;
+  if (count != n) return fail(FDTD_ERR_INVALID, "count must be nx*ny*nz");
+  for (int i = 0; i < s->NX; i++)
+    for (int j = 0; j < s->NY; j++)
+      for (int k = 0; k < s->NZ; k++) {
+        const size_t r = ((size_t)i * s->NY + j) * s->NZ + k;
+        uint8_t b = 0;
+        for (int c = 0; c < 3; c++) b |= (uint8_t)(is_dispersive(s->su.matc[c][r]) << c);
+        out[r] = b;
+      }
+  return FDTD_OK;
+}
+
+// ---------------------------------------------------------------------
+// not yet available entry points
+
+extern "C" fdtd_status fdtd_set_design(fdtd_sim*, const int*, const float*, size_t) {
+  return fail(FDTD_ERR_UNSUPPORTED, "fdtd_set_design is not built yet");
+}
+extern "C" fdtd_status fdtd_forward(fdtd_sim*, const int*, int, int, double*) {
+  return fail(FDTD_ERR_UNSUPPORTED, "fdtd_forward is not built yet");
+}
+extern "C" fdtd_status fdtd_backward(fdtd_sim*, float*, size_t, double*) {
+  return fail(FDTD_ERR_UNSUPPORTED, "fdtd_backward is not built yet");
+}
+extern "C" fdtd_status fdtd_batch_create(const fdtd_params*, int, int, fdtd_batch**) {
+  return fail(FDTD_ERR_UNSUPPORTED, "batched simulations are not built yet");
+}
+extern "C" fdtd_status fdtd_batch_run(fdtd_batch*, void*) {
+  return fail(FDTD_ERR_UNSUPPORTED, "batched simulations are not built yet");
+}
+extern "C" fdtd_status fdtd_batch_spectra(fdtd_batch*, int, double*) {
+  return fail(FDTD_ERR_UNSUPPORTED, "batched simulations are not built yet");
+}
+extern "C" fdtd_status fdtd_batch_destroy(fdtd_batch*) { return FDTD_OK; }

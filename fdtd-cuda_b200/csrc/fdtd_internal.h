@@ -1,0 +1,100 @@
+// Internal types shared by the host runtime and the CUDA kernels.
+//
+// Device layout (all per-sim state lives in HBM, allocated once at create):
+//   fields ex..hz      [NZ][NY][PX] of T, x fastest, PX = NX rounded up to 8
+//   material bits      [NZ][NY][PX] uint8 (bit c: component c is dispersive,
+//                      bits 3..7: dielectric class), read only inside the
+//                      material bounding box
+//   CPML psi slabs     z slabs [w][NY][PX], y slabs [NZ][w][PX],
+//                      x slabs [NZ][NY][w]; w = Ncpml (H) or Ncpml+1 (E)
+//   dispersive cells   compact per-component lists + SoA state per slot
+//   DFT                sample ring [TB][rows] of T, accumulators
+//                      [F][rows] of double (re, im)
+#pragma once
+#include <cstddef>
+#include <cstdint>
+
+#include "../../include/fdtd_b200.h"
+
+namespace fdtd {
+
+constexpr int kMaxClasses = 32;   // dielectric classes (bits 3..7)
+constexpr int kSampleBlock = 32;  // DFT samples per FP64 contraction
+
+// Step clock kept in device memory so captured graphs can be replayed.
+struct DevClock {
+  int t;          // steps completed by the 1D-line kernel (current step + 1)
+  int nsamp;      // DFT samples waiting in the ring
+  int nonfinite;  // watchdog flag
+  int samp_slot;  // ring slot of the current step's DFT sample
+  double e1, e2;  // Mur history of the incident line ends (main.cu:2835-2838)
+  int samp_t[kSampleBlock];
+};
+
+// Per-axis CPML tables.  The E tables have Nc+1 entries, the H tables Nc.
+template <typename T>
+struct CpmlAxis {
+  const T* be_N; const T* ce_N; const T* be_F; const T* ce_F;
+  const T* bh_N; const T* ch_N; const T* bh_F; const T* ch_F;
+  const T* ce_N_ey;  // ce_N used by Ey's near-x slab (reference passes ce_y_N)
+  const T* inv_ked;  // 1/(kappa_e * d), length N
+  const T* inv_khd;  // 1/(kappa_h * d), length N
+  T inv_d;           // 1/d
+  int Nc, F;         // slab width, first index of the far slab
+};
+
+// Incident-field geometry for the TFSF corrections (CORRECT_* main.cu:369).
+struct TfsfView {
+  int on;
+  int Tx, Ty, Tz;      // box faces at Tx and N-Tx (etc.)
+  int i0, j0, k0, m0;  // projection origin, line centre
+  float sth, cth, sph, cph;  // sinf/cosf of the angles (host-computed)
+  float fe[3], fh[3];        // E and H direction factors
+  double dscale;             // dx / d_1D
+};
+
+template <typename T>
+struct SimView {
+  int NX, NY, NZ, PX;
+  size_t plane;  // NY * PX
+  T* E[3];
+  T* H[3];
+  const uint8_t* mat;
+  int mat_lo[3], mat_hi[3];  // material bounding box, [lo, hi)
+  T cee[kMaxClasses], ceh[kMaxClasses];  // per dielectric class
+  T chh, che;
+  CpmlAxis<T> cp[3];
+  T* psiE_N[3][2]; T* psiE_F[3][2];  // [component][slot]: slot 0 = axis c+1
+  T* psiH_N[3][2]; T* psiH_F[3][2];
+  T dxyz[3];
+  TfsfView tf;
+  const double* e_inc;  // incident line (double in both precisions)
+  const double* h_inc;
+  int* nonfinite;
+};
+
+// Dispersive (Drude + 2 critical points, optionally hydrodynamic) cells.
+template <typename T>
+struct MetalView {
+  int n[3];             // cells per component
+  const int4* cell[3];  // (i, j, k, slot) per entry
+  // state, SoA per component: slot-major arrays
+  T* en[3]; T* en1[3];
+  T* cpn[3][2]; T* cpn1[3][2];
+  T* pd[3][3];          // Drude current ring (n, n-1, new) indexed by step
+  T* nd[3][2];          // hydro density ring
+  const float* rho[3];  // design blend per slot (null = 1)
+  // slot lookup over the dispersive bounding box (hydro neighbours)
+  const int* slot_map[3];
+  int box_lo[3], box_dim[3];
+  // coefficients
+  T C_E, C_E_1, C_E_2;
+  T d1, d2, d3, d4, d5, dNL;
+  T C1[2], C2[2], C3[2], C4[2], C5[2];
+  T dt, z0, e0, N_EQ;
+  T inv_dx, inv_dy, inv_dz;
+  int hydro;
+  int fix_cbrt;
+};
+
+}  // namespace fdtd

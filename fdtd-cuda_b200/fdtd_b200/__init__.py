@@ -1,0 +1,274 @@
+"""Python binding of libfdtd_b200.so -- the B200-native FDTD time step.
+
+The binding is a thin ctypes layer over the C ABI declared in
+include/fdtd_b200.h.  Nothing here computes fields: every numeric call goes
+to the CUDA library, and loading fails loudly if the library is missing.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from ._abi import (FACE_COMPONENTS, FDTD_FP32, FDTD_FP64, FIX_BH_X_F, FIX_CE_EY_XN,
+                   FIX_HYDRO_CBRT, GEOM_DISK_ARRAY, GEOM_REFERENCE, GEOM_ROD_DIMER,
+                   GEOM_SPHERE, STATUS, Dims, Params)
+
+__all__ = ["Params", "Dims", "Sim", "FdtdError", "lib", "default_params", "load_input_txt",
+           "FDTD_FP32", "FDTD_FP64", "GEOM_REFERENCE", "GEOM_ROD_DIMER", "GEOM_DISK_ARRAY",
+           "GEOM_SPHERE", "FIX_BH_X_F", "FIX_CE_EY_XN", "FIX_HYDRO_CBRT", "FACE_COMPONENTS"]
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libfdtd_b200.so")
+_LIB = None
+
+EXPORTS = [
+    "fdtd_params_default", "fdtd_params_size", "fdtd_load_input_txt", "fdtd_write_input_txt",
+    "fdtd_create", "fdtd_destroy", "fdtd_get_dims", "fdtd_reset", "fdtd_last_error",
+    "fdtd_update_h", "fdtd_update_line", "fdtd_update_e", "fdtd_spectral_accumulate",
+    "fdtd_step", "fdtd_run", "fdtd_get_time", "fdtd_check", "fdtd_spectral_finalize",
+    "fdtd_write_scatabs", "fdtd_get_dft", "fdtd_get_freqs", "fdtd_get_incident",
+    "fdtd_get_field", "fdtd_set_field", "fdtd_snapshot_plane", "fdtd_get_probe",
+    "fdtd_get_material", "fdtd_set_design", "fdtd_forward", "fdtd_backward",
+    "fdtd_batch_create", "fdtd_batch_run", "fdtd_batch_spectra", "fdtd_batch_destroy",
+    "fdtd_plan", "fdtd_rasterise", "fdtd_coefficients",
+]
+
+
+class FdtdError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+def lib():
+    """Load libfdtd_b200.so (raises if it has not been built)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with "
+                          "`python fdtd-cuda_b200/fdtd_b200/build.py` (there is no CPU fallback)")
+    L = C.CDLL(LIB_PATH)
+    P = C.POINTER
+    vp, dp, sz = C.c_void_p, P(C.c_double), C.c_size_t
+    sig = {
+        "fdtd_params_default": (None, [P(Params)]),
+        "fdtd_params_size": (sz, []),
+        "fdtd_load_input_txt": (C.c_int, [C.c_char_p, P(Params)]),
+        "fdtd_write_input_txt": (C.c_int, [C.c_char_p, P(Params)]),
+        "fdtd_create": (C.c_int, [P(Params), C.c_int, P(vp)]),
+        "fdtd_destroy": (C.c_int, [vp]),
+        "fdtd_get_dims": (C.c_int, [vp, P(Dims)]),
+        "fdtd_reset": (C.c_int, [vp]),
+        "fdtd_last_error": (C.c_char_p, []),
+        "fdtd_update_h": (C.c_int, [vp, vp]),
+        "fdtd_update_line": (C.c_int, [vp, vp]),
+        "fdtd_update_e": (C.c_int, [vp, vp]),
+        "fdtd_spectral_accumulate": (C.c_int, [vp, vp]),
+        "fdtd_step": (C.c_int, [vp, C.c_int, vp]),
+        "fdtd_run": (C.c_int, [vp, vp]),
+        "fdtd_get_time": (C.c_int, [vp, P(C.c_int)]),
+        "fdtd_check": (C.c_int, [vp]),
+        "fdtd_spectral_finalize": (C.c_int, [vp, dp]),
+        "fdtd_write_scatabs": (C.c_int, [vp, C.c_char_p]),
+        "fdtd_get_dft": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, dp, dp, sz]),
+        "fdtd_get_freqs": (C.c_int, [vp, dp, sz]),
+        "fdtd_get_incident": (C.c_int, [vp, dp, dp, sz]),
+        "fdtd_get_field": (C.c_int, [vp, C.c_int, dp, sz]),
+        "fdtd_set_field": (C.c_int, [vp, C.c_int, dp, sz]),
+        "fdtd_snapshot_plane": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, vp, sz, vp]),
+        "fdtd_get_probe": (C.c_int, [vp, dp, sz, P(C.c_int)]),
+        "fdtd_get_material": (C.c_int, [vp, P(C.c_ubyte), sz]),
+        "fdtd_set_design": (C.c_int, [vp, P(C.c_int), P(C.c_float), sz]),
+        "fdtd_forward": (C.c_int, [vp, P(C.c_int), C.c_int, C.c_int, dp]),
+        "fdtd_backward": (C.c_int, [vp, P(C.c_float), sz, dp]),
+        "fdtd_batch_create": (C.c_int, [P(Params), C.c_int, C.c_int, P(vp)]),
+        "fdtd_batch_run": (C.c_int, [vp, vp]),
+        "fdtd_batch_spectra": (C.c_int, [vp, C.c_int, dp]),
+        "fdtd_batch_destroy": (C.c_int, [vp]),
+        "fdtd_plan": (C.c_int, [P(Params), P(Dims)]),
+        "fdtd_rasterise": (C.c_int, [P(Params), P(C.c_ubyte), sz]),
+        "fdtd_coefficients": (C.c_int, [P(Params), C.c_int, dp, sz, P(sz)]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    if L.fdtd_params_size() != C.sizeof(Params):
+        raise ImportError("fdtd_params layout mismatch between the library and _abi.py")
+    _LIB = L
+    return L
+
+
+def _check(status):
+    if status != 0:
+        raise FdtdError(status, lib().fdtd_last_error().decode(errors="replace"))
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def default_params(**kw):
+    p = Params()
+    lib().fdtd_params_default(C.byref(p))
+    p.update(**kw)
+    return p
+
+
+def load_input_txt(path, p=None):
+    p = p or default_params()
+    _check(lib().fdtd_load_input_txt(os.fsencode(path), C.byref(p)))
+    return p
+
+
+def plan(p):
+    """Sizes fdtd_create would derive for these parameters (host only)."""
+    d = Dims()
+    _check(lib().fdtd_plan(C.byref(p), C.byref(d)))
+    return d
+
+
+def rasterise(p):
+    """Dispersive-component bits per cell, reference layout (host only)."""
+    d = plan(p)
+    out = np.empty((d.nx, d.ny, d.nz), np.uint8)
+    _check(lib().fdtd_rasterise(C.byref(p), out.ctypes.data_as(C.POINTER(C.c_ubyte)), out.size))
+    return out
+
+
+def coefficients(p, which):
+    """One setup table (see fdtd_coefficients in include/fdtd_b200.h)."""
+    buf = np.empty(1 << 16)
+    n = C.c_size_t()
+    _check(lib().fdtd_coefficients(C.byref(p), which, _dp(buf), buf.size, C.byref(n)))
+    return buf[: n.value].copy()
+
+
+def write_input_txt(path, p):
+    _check(lib().fdtd_write_input_txt(os.fsencode(path), C.byref(p)))
+
+
+class Sim:
+    """One simulation on one GPU (the reference's whole program state)."""
+
+    def __init__(self, params, device=0):
+        h = C.c_void_p()
+        _check(lib().fdtd_create(C.byref(params), device, C.byref(h)))
+        self.h = h
+        self.params = params
+        d = Dims()
+        _check(lib().fdtd_get_dims(self.h, C.byref(d)))
+        self.dims = d
+        self.shape = (d.nx, d.ny, d.nz)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().fdtd_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- stepping ------------------------------------------------------
+    def step(self, n=1, stream=None):
+        _check(lib().fdtd_step(self.h, int(n), stream))
+
+    def run(self, stream=None):
+        _check(lib().fdtd_run(self.h, stream))
+
+    def update_h(self, stream=None):
+        _check(lib().fdtd_update_h(self.h, stream))
+
+    def update_line(self, stream=None):
+        _check(lib().fdtd_update_line(self.h, stream))
+
+    def update_e(self, stream=None):
+        _check(lib().fdtd_update_e(self.h, stream))
+
+    def spectral_accumulate(self, stream=None):
+        _check(lib().fdtd_spectral_accumulate(self.h, stream))
+
+    def reset(self):
+        _check(lib().fdtd_reset(self.h))
+
+    def check(self):
+        _check(lib().fdtd_check(self.h))
+
+    @property
+    def t(self):
+        v = C.c_int()
+        _check(lib().fdtd_get_time(self.h, C.byref(v)))
+        return v.value
+
+    # -- outputs -------------------------------------------------------
+    def field(self, comp):
+        out = np.empty(self.shape, np.float64)
+        _check(lib().fdtd_get_field(self.h, comp, _dp(out), out.size))
+        return out
+
+    def set_field(self, comp, arr):
+        a = np.ascontiguousarray(arr, np.float64)
+        _check(lib().fdtd_set_field(self.h, comp, _dp(a), a.size))
+
+    def plane(self, comp, axis, index):
+        na = self.shape[1] if axis == 0 else self.shape[0]
+        nb = self.shape[1] if axis == 2 else self.shape[2]
+        out = np.empty((na, nb), np.float64)
+        _check(lib().fdtd_snapshot_plane(self.h, comp, axis, index, out.ctypes.data, out.size, None))
+        return out
+
+    def probe(self):
+        n = C.c_int()
+        out = np.empty((self.params.Tend + 2, 3))
+        _check(lib().fdtd_get_probe(self.h, _dp(out), out.size, C.byref(n)))
+        return out[: n.value]
+
+    def material(self):
+        out = np.empty(self.shape, np.uint8)
+        _check(lib().fdtd_get_material(self.h, out.ctypes.data_as(C.POINTER(C.c_ubyte)), out.size))
+        return out
+
+    def dft_shape(self, box, face):
+        d = self.dims
+        S = d.abs_start if box == 0 else d.sca_start
+        E = d.abs_end if box == 0 else d.sca_end
+        ax = face // 2
+        a1 = 1 if ax == 0 else 0
+        a2 = 1 if ax == 2 else 2
+        return (d.num_freq, E[a1] - S[a1] + 1, E[a2] - S[a2] + 1)
+
+    def dft(self, box, face, comp):
+        shp = self.dft_shape(box, face)
+        re = np.empty(shp)
+        im = np.empty(shp)
+        _check(lib().fdtd_get_dft(self.h, box, face, comp, _dp(re), _dp(im), re.size))
+        return re + 1j * im
+
+    def spectra(self):
+        out = np.empty((self.dims.num_freq, 19))
+        _check(lib().fdtd_spectral_finalize(self.h, _dp(out)))
+        return out
+
+    def write_scatabs(self, path):
+        _check(lib().fdtd_write_scatabs(self.h, os.fsencode(path)))
+
+    def freqs(self):
+        f = np.empty(self.dims.num_freq)
+        _check(lib().fdtd_get_freqs(self.h, _dp(f), f.size))
+        return f
+
+    def incident(self):
+        re = np.empty(self.dims.num_freq)
+        im = np.empty(self.dims.num_freq)
+        _check(lib().fdtd_get_incident(self.h, _dp(re), _dp(im), re.size))
+        return re + 1j * im

@@ -1,0 +1,324 @@
+/*
+ * fdtd_b200.h -- C ABI of the B200-native FDTD time-step loop.
+ *
+ * The reference (jbaxt089/FDTD-CUDA) is a monolithic main() over ~700
+ * globals.  This ABI exposes its entry points as functions on an opaque
+ * simulation handle.  Every function returns an fdtd_status, never exits,
+ * and keeps its error text for fdtd_last_error().  Plain C types only: no
+ * torch or CUDA-runtime types appear in the signatures (streams are passed
+ * as void* cudaStream_t).
+ *
+ * Reference entry point                        replaced by
+ * -------------------------------------------  -----------------------------
+ * READ_DATA_FILE        setup.cu:10-133        fdtd_load_input_txt
+ * SETUP_CONST           setup.cu:347-510       fdtd_create (derived sizes)
+ * MATERIAL_MATRIX       setup.cu:135-342       fdtd_create (rasteriser)
+ * SETUP_Drude_CP        setup.cu:979-1558      fdtd_create (ADE tables)
+ * SETUP_CPML            setup.cu:513-978       fdtd_create (CPML tables)
+ * SETUP_TFSF            tfsf2.cu:6-56          fdtd_create (pulse, line)
+ * DEF_UPDATE_COEFF_*    setup.cu:2015-2062     fdtd_create (Yee tables)
+ * UPDATE_hx/hy/hz       main.cu:762-1044       fdtd_update_h
+ * CORRECT_X/Y/Z         main.cu:369-758        fused into update_h/update_e
+ * UPDATE_h_inc/e_inc    main.cu:2280-2337      fdtd_update_line
+ * host Mur + source     main.cu:2831-2859      fdtd_update_line (on device)
+ * UpdateHydroPx/Py/Pz   main.cu:1916-2276      fdtd_update_e (metal pass)
+ * UPDATE_ex/ey/ez       main.cu:1048-1912      fdtd_update_e
+ * ScattAbs              main.cu:35-366         fdtd_spectral_accumulate
+ * CalculateAbsScatt     Spectral.cu:411-1177   fdtd_spectral_finalize
+ * SNAPSHOT_*            snapshot.cu:10-180     fdtd_get_field / fdtd_probe_*
+ * time loop             main.cu:2724-3175      fdtd_step
+ */
+#ifndef FDTD_B200_H
+#define FDTD_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum fdtd_status {
+  FDTD_OK = 0,
+  FDTD_ERR_INVALID = 1,     /* bad argument or parameter combination */
+  FDTD_ERR_CUDA = 2,        /* a CUDA runtime call failed */
+  FDTD_ERR_ALLOC = 3,       /* device allocation failed or over the cap */
+  FDTD_ERR_IO = 4,          /* Input.txt / output file problem */
+  FDTD_ERR_STATE = 5,       /* call out of order (e.g. finalize before run) */
+  FDTD_ERR_NONFINITE = 6,   /* watchdog saw NaN/Inf in the fields */
+  FDTD_ERR_TIMEOUT = 7,     /* a bounded device wait gave up */
+  FDTD_ERR_UNSUPPORTED = 8  /* feature outside the supported set */
+} fdtd_status;
+
+/* Arithmetic type of the fields (the reference's compile-time
+ * DOUBLEPRECISION / FlOATPRECISION switch, define.h:7, global_var.h:15). */
+typedef enum fdtd_precision { FDTD_FP32 = 0, FDTD_FP64 = 1 } fdtd_precision;
+
+/* Geometry kinds.  FDTD_GEOM_REFERENCE rasterises exactly what
+ * MATERIAL_MATRIX does from the Input.txt fields inf_disp_slab /
+ * nano_sphere / nano_sphere_radius (setup.cu:135-342).  The others are
+ * shapes the reference cannot express. */
+typedef enum fdtd_geometry {
+  FDTD_GEOM_REFERENCE = 0,
+  FDTD_GEOM_ROD_DIMER = 1,   /* two capped rods along an axis with a gap */
+  FDTD_GEOM_DISK_ARRAY = 2,  /* nx*ny disks on a dielectric slab */
+  FDTD_GEOM_SPHERE = 3       /* sphere of real radius at a real centre */
+} fdtd_geometry;
+
+/* Field components, in the reference's naming. */
+typedef enum fdtd_component {
+  FDTD_EX = 0, FDTD_EY = 1, FDTD_EZ = 2, FDTD_HX = 3, FDTD_HY = 4, FDTD_HZ = 5
+} fdtd_component;
+
+/* Behaviours of the reference that are reproduced by default so results
+ * match it bit-for-bit in structure.  Setting a bit switches to the
+ * physically intended behaviour instead. */
+enum fdtd_fix_bits {
+  /* setup.cu:681 uploads bh_z_F (not yet computed, SETUP_CPML_X runs before
+   * SETUP_CPML_Z) as bh_x_F; the reference therefore runs with bh_x_F = 0. */
+  FDTD_FIX_BH_X_F = 1 << 0,
+  /* main.cu:2891 passes ce_y_N where UPDATE_ey expects ce_x_N. */
+  FDTD_FIX_CE_EY_XN = 1 << 1,
+  /* UpdateHydroP* take the cube root with powf (FP32) even in FP64 builds
+   * (main.cu:2035); the fix uses the working precision. */
+  FDTD_FIX_HYDRO_CBRT = 1 << 2
+};
+
+/*
+ * Parameters.  The first block mirrors the 41 positional Input.txt values in
+ * file order (setup.cu:17-58).  NCELLX/Y/Z and NcpmlX/Y/Z are the raw file
+ * values; the grid actually allocated is N + 2*Ncpml + 1 per axis
+ * (setup.cu:377-393).  The second block turns the reference's hard-coded
+ * constants into parameters; fdtd_params_default() sets them to the
+ * reference's values.
+ */
+typedef struct fdtd_params {
+  /* ---- Input.txt (setup.cu:17-58) ---- */
+  int Tend;
+  double dx, dy, dz;
+  int num_trials, min_trials, max_trials;
+  int TE_TM;
+  int NCELLX, NCELLY, NCELLZ;
+  int NcpmlX, NcpmlY, NcpmlZ;
+  int inf_disp_slab;
+  int nano_sphere;
+  double nano_sphere_radius;
+  int material;           /* 2 = silver, 3 = gold (setup.cu:1164-1211) */
+  int first_medium;
+  int inc_plane;
+  int dispersive_slab;
+  int NUM_freq;
+  int WL_or_freq;         /* 1 = wavelength grid, else frequency grid */
+  int NUM_freq_inc;
+  int Tend_inc;
+  int Snap_in;
+  int Freq_start;
+  int Test_offset;
+  int Spect_loc;
+  double BandWidth;
+  int NONLOCAL;           /* 3 = hydrodynamic nonlocal model */
+  int Diverge_Gradient;
+  int t_skip, x_skip, y_skip, z_skip;
+  double Nonlocalend;
+  double MAX_AMP;
+  double TimeFactor;
+  double lam_0;
+  int StaticField;
+
+  /* ---- constants hard-coded in the reference ---- */
+  int tfsf_inset;          /* 10       setup.cu:428 */
+  int box_offset;          /* 5        setup.cu:435-452 (DFT boxes) */
+  int cpml_order;          /* 3        setup.cu:481 */
+  double cpml_kappa_max;   /* 5        setup.cu:482 */
+  double cpml_alpha_max;   /* 0.05     setup.cu:485 */
+  double cpml_sigma_factor;/* 0.8      setup.cu:483 (sigma_max=f(m+1)/(Z0 dx)) */
+  double lam_min, lam_max; /* 200e-9 / 700e-9   main.cu:2446-2447 */
+  double inc_theta_deg;    /* 0        tfsf2.cu:11-13 */
+  double inc_phi_deg;      /* 0  (E along -y); 90 gives E along +x */
+  double polar_psi_deg;    /* 0        main.cu:2424-2426 */
+  int source_offset;       /* 50       main.cu:2851 (source at m0-50) */
+  int dft_every;           /* 4        main.cu:2920 */
+  double hydro_D;          /* 2        setup.cu:981 (beta^2 = 3/(D+2) vF^2) */
+  double fermi_velocity;   /* 1.39e6   setup.cu:980 */
+  int precision;           /* fdtd_precision */
+  int fixes;               /* fdtd_fix_bits */
+
+  /* ---- material overrides (0 = use the table for `material`) ---- */
+  int metal_custom;
+  double eps_inf, omega_D, gamma_D;
+  double cp_A[2], cp_phi[2], cp_Omega[2], cp_Gamma[2];
+  double N_EQ;             /* hydro equilibrium density */
+
+  /* ---- extended geometry (FDTD_GEOM_*) ---- */
+  int geometry;
+  int axis;                /* rod axis / dimer axis: 0=x 1=y 2=z */
+  double rod_length, rod_diameter, gap;
+  double disk_diameter, disk_height, pitch;
+  int disk_nx, disk_ny;
+  double slab_eps, slab_thickness;
+  double sphere_radius, sphere_cx, sphere_cy, sphere_cz; /* metres, cells */
+
+  /* ---- probes ---- */
+  int probe_i, probe_j, probe_k; /* -1 = grid centre (OUT.txt, main.cu:2732) */
+} fdtd_params;
+
+typedef struct fdtd_sim fdtd_sim;   /* opaque */
+
+/* Sizes derived by setup, for callers that allocate host buffers. */
+typedef struct fdtd_dims {
+  int nx, ny, nz;          /* allocated grid (N + 2*Ncpml + 1) */
+  int ntfsf_x, ntfsf_y, ntfsf_z;
+  int inc_length, m0;
+  int abs_start[3], abs_end[3], sca_start[3], sca_end[3];
+  int num_freq;
+  int n_metal_cells[3];    /* ex/ey/ez cells with a dispersive update */
+  int hydro;               /* 1 when the hydrodynamic model is active */
+  int precision;
+  double dt;
+  double delay, width;     /* pulse, in steps (tfsf2.cu:37-40) */
+} fdtd_dims;
+
+/* ---------------------------------------------------------------------- */
+/* parameters                                                              */
+
+/* Reference defaults for every field (Input.txt fields zeroed). */
+void fdtd_params_default(fdtd_params* p);
+/* sizeof(fdtd_params) as compiled into the library (ABI check). */
+size_t fdtd_params_size(void);
+
+/* READ_DATA_FILE (setup.cu:10-133): reads the 41 positional values of an
+ * Input.txt into *p, leaving the other fields untouched. */
+fdtd_status fdtd_load_input_txt(const char* path, fdtd_params* p);
+
+/* Writes *p as an Input.txt the reference can read. */
+fdtd_status fdtd_write_input_txt(const char* path, const fdtd_params* p);
+
+/* Host-only queries (no GPU needed): the sizes fdtd_create would derive,
+ * the material class bits it would rasterise (reference layout [i][j][k],
+ * bit c set when component c is dispersive) and its coefficient tables.
+ * which: 0..2 kappa_e*d (x,y,z), 3..5 kappa_h*d, 6+8*axis+slot for the CPML
+ * tables be_N ce_N be_F ce_F bh_N ch_N bh_F ch_F (SETUP_CPML,
+ * setup.cu:584-668), 100 = ADE scalars C_E C_E_1 C_E_2 d1..d5 d_NL
+ * C1..C5 (pole 0) C1..C5 (pole 1) dt N_EQ (setup.cu:1282-1373), 101 =
+ * frequencies, 102 = source pulse per step. *len gets the table length. */
+fdtd_status fdtd_plan(const fdtd_params* p, fdtd_dims* out);
+fdtd_status fdtd_rasterise(const fdtd_params* p, uint8_t* bits, size_t count);
+fdtd_status fdtd_coefficients(const fdtd_params* p, int which, double* out,
+                              size_t count, size_t* len);
+
+/* ---------------------------------------------------------------------- */
+/* life cycle                                                              */
+
+/* SETUP_CONST + MATERIAL_MATRIX + SETUP_Drude_CP + ALLOCATE_MEM +
+ * SETUP_TFSF + DEF_* + SETUP_CPML (setup.cu:135-1558, tfsf2.cu:6-56,
+ * main.cu:2435-2643).  Builds every table on the host in FP64, uploads
+ * them and zeroes the state on `device`. */
+fdtd_status fdtd_create(const fdtd_params* p, int device, fdtd_sim** out);
+fdtd_status fdtd_destroy(fdtd_sim* s);
+fdtd_status fdtd_get_dims(const fdtd_sim* s, fdtd_dims* out);
+/* Zero every field, auxiliary state and DFT accumulator; t = 0. */
+fdtd_status fdtd_reset(fdtd_sim* s);
+const char* fdtd_last_error(void);
+
+/* ---------------------------------------------------------------------- */
+/* the time step, split the way the reference launches it                  */
+
+/* UPDATE_hx/hy/hz + the H half of CORRECT_X/Y/Z (main.cu:2735-2813). */
+fdtd_status fdtd_update_h(fdtd_sim* s, void* stream);
+/* UPDATE_h_inc + UPDATE_e_inc + Mur ends + source injection
+ * (main.cu:2791, 2822-2859). */
+fdtd_status fdtd_update_line(fdtd_sim* s, void* stream);
+/* E half of CORRECT_X/Y/Z, UpdateHydroP*, UPDATE_ex/ey/ez
+ * (main.cu:2798-2901). */
+fdtd_status fdtd_update_e(fdtd_sim* s, void* stream);
+/* ScattAbs (main.cu:2920-2934) for the current step when
+ * t % dft_every == 0; advances t. */
+fdtd_status fdtd_spectral_accumulate(fdtd_sim* s, void* stream);
+
+/* The fused fast path: nsteps full time steps (H, line, E, DFT), captured
+ * into CUDA graphs where the step pattern repeats. */
+fdtd_status fdtd_step(fdtd_sim* s, int nsteps, void* stream);
+/* Runs until t == Tend + 1 (the reference loop is t = 0..Tend inclusive). */
+fdtd_status fdtd_run(fdtd_sim* s, void* stream);
+fdtd_status fdtd_get_time(const fdtd_sim* s, int* t);
+
+/* Polls the device NaN/Inf watchdog; FDTD_ERR_NONFINITE if it fired. */
+fdtd_status fdtd_check(fdtd_sim* s);
+
+/* ---------------------------------------------------------------------- */
+/* spectra (CalculateAbsScatt, Spectral.cu:411-1177)                       */
+
+/* Flushes pending DFT samples and reduces the 12 face fluxes per
+ * frequency on the device in FP64.  out19 (NUM_freq x 19, row major) gets
+ * the reference's ScatAbs columns: lambda, Sca, Abs, Ext, the 12 face
+ * fluxes (Sca: -X +X -Y +Y -Z +Z, then Abs), |E_inc|, Re E_inc, Im E_inc. */
+fdtd_status fdtd_spectral_finalize(fdtd_sim* s, double* out19);
+/* Same, written as ScatAbs.<t>.txt in the reference's format. */
+fdtd_status fdtd_write_scatabs(fdtd_sim* s, const char* path);
+/* Raw DFT phasors of one face/component in the reference's layout
+ * [F][a][b] (main.cu:86 ThreeDMapD(f,II,JJ,...)), FP64 re/im.
+ * box: 0 = Abs, 1 = Sca.  face: 0..5 = -X +X -Y +Y -Z +Z.
+ * comp: 0..3 = the face's (E_a, E_b, H_a, H_b) in the reference's order
+ * (Z faces: Ex Ey Hx Hy; Y faces: Ex Ez Hx Hz; X faces: Ey Ez Hy Hz). */
+fdtd_status fdtd_get_dft(fdtd_sim* s, int box, int face, int comp,
+                         double* re, double* im, size_t count);
+fdtd_status fdtd_get_freqs(const fdtd_sim* s, double* freq, size_t count);
+/* Analytic incident spectrum E_incident[m] (main.cu:2632-2643). */
+fdtd_status fdtd_get_incident(const fdtd_sim* s, double* re, double* im,
+                              size_t count);
+
+/* ---------------------------------------------------------------------- */
+/* snapshots and probes (snapshot.cu:10-180, OUT.txt main.cu:2732)         */
+
+/* Whole component in the reference's layout [i][j][k] (z fastest), as
+ * double.  count must be nx*ny*nz. */
+fdtd_status fdtd_get_field(fdtd_sim* s, int comp, double* out, size_t count);
+/* Overwrites a whole component from the reference layout (test hook). */
+fdtd_status fdtd_set_field(fdtd_sim* s, int comp, const double* in,
+                           size_t count);
+/* One plane (axis 0/1/2 at `index`) of a component into a device or host
+ * buffer of doubles, layout [a][b] with the remaining axes in x,y,z order.
+ * Asynchronous on `stream` when dst is device memory. */
+fdtd_status fdtd_snapshot_plane(fdtd_sim* s, int comp, int axis, int index,
+                                double* dst, size_t count, void* stream);
+/* Probe record: ex, ey, ez at the probe cell after every completed step,
+ * [t][3]. n = number of steps recorded so far. */
+fdtd_status fdtd_get_probe(fdtd_sim* s, double* out, size_t count, int* n);
+/* Material class map used by the E pass (bit0..2: ex/ey/ez dispersive),
+ * reference layout, for rasteriser parity checks. */
+fdtd_status fdtd_get_material(fdtd_sim* s, uint8_t* out, size_t count);
+
+/* ---------------------------------------------------------------------- */
+/* adjoint (no counterpart in the reference)                               */
+
+/* Design region: per-cell blend rho in [0,1] between vacuum and the metal
+ * for a box [i0,i1)x[j0,j1)x[k0,k1), x fastest.  Cells with rho > 0 get a
+ * per-cell ADE update with linearly blended coefficients. */
+fdtd_status fdtd_set_design(fdtd_sim* s, const int box[6], const float* rho,
+                            size_t count);
+/* Objective: sum over the listed frequency indices of the absorbed power
+ * (AbsTot column).  Forward with checkpoints every K steps. */
+fdtd_status fdtd_forward(fdtd_sim* s, const int* freq_idx, int nfreq,
+                         int checkpoint_every, double* objective);
+/* Reverse-time adjoint with segment recompute.  dL_drho has the design
+ * box's cell count; dL_dparams gets d/d(omega_D), d/d(gamma_D). */
+fdtd_status fdtd_backward(fdtd_sim* s, float* dL_drho, size_t count,
+                          double* dL_dparams);
+
+/* ---------------------------------------------------------------------- */
+/* batched independent simulations (no counterpart in the reference; its
+ * trials loop, main.cu:2435, is sequential)                               */
+
+typedef struct fdtd_batch fdtd_batch;
+fdtd_status fdtd_batch_create(const fdtd_params* ps, int n, int device,
+                              fdtd_batch** out);
+/* Runs every sim to its Tend in one persistent kernel per step group,
+ * launched from CUDA graphs. */
+fdtd_status fdtd_batch_run(fdtd_batch* b, void* stream);
+fdtd_status fdtd_batch_spectra(fdtd_batch* b, int idx, double* out19);
+fdtd_status fdtd_batch_destroy(fdtd_batch* b);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FDTD_B200_H */

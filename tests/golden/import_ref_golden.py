@@ -1,0 +1,54 @@
+"""Turns the reference program's text outputs (from make_ref_golden.sh) into
+small .npz fixtures:
+
+  ey_centre[t]   ey at (NX/2, NY/2, NZ/2) after step t-1, printed by the
+                 reference's per-step printf (main.cu:2726), 7 digits
+  scatabs_<t>    the 19-column ScatAbs.<t>.txt (Spectral.cu:1157-1174)
+
+    python tests/golden/import_ref_golden.py gpurun_out/ref_golden
+"""
+import glob
+import os
+import re
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def load_case(d):
+    out = {}
+    t, ey = [], []
+    for line in open(os.path.join(d, "stdout.txt")):
+        parts = line.split()
+        if len(parts) == 4 and re.fullmatch(r"\d+", parts[0]) and parts[1] == "1":
+            t.append(int(parts[0]))
+            ey.append(float(parts[2]))
+    out["ey_t"] = np.array(t, np.int32)
+    out["ey_centre"] = np.array(ey)
+    files = sorted(glob.glob(os.path.join(d, "ScatAbs.*.txt")),
+                   key=lambda p: int(p.split(".")[-2]))
+    steps = [int(p.split(".")[-2]) for p in files]
+    # keep the last two dumps (the spectra the run converges to)
+    for p, s in list(zip(files, steps))[-2:]:
+        out[f"scatabs_{s}"] = np.loadtxt(p)
+    return out
+
+
+def main(src):
+    for d in sorted(glob.glob(os.path.join(src, "*"))):
+        if not os.path.isdir(d):
+            continue
+        rc = open(os.path.join(d, "rc.txt")).read()
+        if "rc=0" not in rc:
+            print("skip", d, rc)
+            continue
+        name = os.path.basename(d)
+        data = load_case(d)
+        np.savez_compressed(os.path.join(HERE, f"ref_{name}.npz"), **data)
+        print(name, {k: v.shape for k, v in data.items()})
+
+
+if __name__ == "__main__":
+    main(sys.argv[1])

@@ -1,0 +1,179 @@
+"""GPU parity: the CUDA path (through the C ABI) against the FP64 oracle.
+
+Tolerances: FP64 fields and spectra within 1e-11 relative (norm-wise for
+fields: max |a - b| / max |b|); FP32 within the bounds stated per test.
+"""
+import functools
+
+import numpy as np
+import pytest
+
+import fdtd_b200 as F
+import oracle as O
+from cases import CASES, make
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-11
+FP32_FIELD_TOL = 5e-5
+STEPS = 300
+
+
+@functools.lru_cache(maxsize=None)
+def oracle_run(name, steps, **over):
+    o = O.OracleSim(make(O, name, **dict(over)))
+    o.step(steps)
+    return o
+
+
+def oracle_fields(name, steps):
+    o = oracle_run(name, steps)
+    return [o.field(c) for c in range(6)], o.probe()
+
+
+def rel(a, b, scale=None):
+    if scale is None:
+        scale = np.max(np.abs(b))
+    return float(np.max(np.abs(a - b)) / max(scale, 1e-300))
+
+
+def field_errors(sim_fields, ref):
+    """Max error of each component on the scale of its whole E or H field
+    (cross-polarised components are rounding noise on their own)."""
+    se = max(np.max(np.abs(ref[c])) for c in range(3))
+    sh = max(np.max(np.abs(ref[c])) for c in range(3, 6))
+    return [rel(sim_fields[c], ref[c], se if c < 3 else sh) for c in range(6)]
+
+
+def run_sim(name, steps, prec, **over):
+    s = F.Sim(make(F, name, precision=prec, **over))
+    s.step(steps)
+    return s
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_fields_fp64(name):
+    ref, probe = oracle_fields(name, STEPS)
+    s = run_sim(name, STEPS, F.FDTD_FP64)
+    errs = field_errors([s.field(c) for c in range(6)], ref)
+    print(name, "fp64 field errors", ["%.2e" % e for e in errs])
+    assert max(errs) < FP64_TOL, errs
+    np.testing.assert_allclose(s.probe(), probe, rtol=0, atol=FP64_TOL * max(np.abs(probe).max(), 1e-30))
+    s.check()
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_fields_fp32(name):
+    ref, _ = oracle_fields(name, STEPS)
+    s = run_sim(name, STEPS, F.FDTD_FP32)
+    errs = field_errors([s.field(c) for c in range(6)], ref)
+    print(name, "fp32 field errors", ["%.2e" % e for e in errs])
+    assert max(errs) < FP32_FIELD_TOL, errs
+
+
+def spectra_pair(name, prec):
+    p = make(F, name, precision=prec)
+    o = oracle_run(name, p.Tend + 1)
+    s = F.Sim(p)
+    s.run()
+    return s, o
+
+
+@pytest.mark.parametrize("name", ["sphere_au", "cube_ag", "hydro", "sphere_ref", "dimer"])
+def test_spectra_fp64(name):
+    s, o = spectra_pair(name, F.FDTD_FP64)
+    a, b = s.spectra(), o.spectra()
+    # lambda and the incident spectrum are host FP64: identical
+    np.testing.assert_array_equal(a[:, 0], b[:, 0])
+    np.testing.assert_allclose(a[:, 16:], b[:, 16:], rtol=1e-15)
+    for col in (1, 2, 3):
+        err = rel(a[:, col], b[:, col])
+        assert err < FP64_TOL, (col, err)
+    for cols in (range(4, 10), range(10, 16)):  # faces on their box's flux scale
+        scale = max(np.max(np.abs(b[:, c])) for c in cols)
+        for col in cols:
+            err = rel(a[:, col], b[:, col], scale)
+            assert err < FP64_TOL, (col, err)
+    for box in (0, 1):
+        for face in range(6):
+            x = [s.dft(box, face, comp) for comp in range(4)]
+            y = [o.dft(box, face, comp) for comp in range(4)]
+            se = max(np.max(np.abs(v)) for v in y[:2])
+            sh = max(np.max(np.abs(v)) for v in y[2:])
+            for comp in range(4):
+                err = rel(x[comp], y[comp], se if comp < 2 else sh)
+                assert err < FP64_TOL, (box, face, comp, err)
+
+
+@pytest.mark.parametrize("name", ["sphere_au", "hydro", "dimer"])
+def test_spectra_fp32(name):
+    s, o = spectra_pair(name, F.FDTD_FP32)
+    a, b = s.spectra(), o.spectra()
+    errs = []
+    for col in (1, 2):
+        scale = np.max(np.abs(b[:, col]))
+        errs.append(float(np.max(np.abs(a[:, col] - b[:, col])) / scale))
+    print(name, "fp32 spectra errors (sca, abs)", errs)
+    assert max(errs) < 1e-4, errs  # measured 0.3e-5 .. 4e-5 on these cases
+
+
+def test_split_calls_equal_fused_step():
+    n = 40
+    a = run_sim("sphere_au", n, F.FDTD_FP64)
+    b = F.Sim(make(F, "sphere_au", precision=F.FDTD_FP64))
+    for _ in range(n):
+        b.update_h()
+        b.update_line()
+        b.update_e()
+        b.spectral_accumulate()
+    for c in range(6):
+        np.testing.assert_array_equal(a.field(c), b.field(c))
+    np.testing.assert_array_equal(a.dft(1, 4, 0), b.dft(1, 4, 0))
+
+
+def test_graph_replay_equals_direct_launches():
+    n = 300  # > one 128-step graph period
+    a = run_sim("hydro", n, F.FDTD_FP32)
+    b = F.Sim(make(F, "hydro", precision=F.FDTD_FP32))
+    for _ in range(n):
+        b.step(1)
+    for c in range(6):
+        np.testing.assert_array_equal(a.field(c), b.field(c))
+    np.testing.assert_array_equal(a.spectra(), b.spectra())
+
+
+def test_reset_restarts_identically():
+    s = run_sim("sphere_au", 150, F.FDTD_FP64)
+    first = s.field(1)
+    s.reset()
+    assert s.t == 0 and np.all(s.field(1) == 0)
+    s.step(150)
+    np.testing.assert_array_equal(s.field(1), first)
+
+
+def test_snapshot_plane_matches_field():
+    s = run_sim("sphere_au", 120, F.FDTD_FP32)
+    ey = s.field(1)
+    np.testing.assert_array_equal(s.plane(1, 0, 17), ey[17])
+    np.testing.assert_array_equal(s.plane(1, 1, 5), ey[:, 5, :])
+    np.testing.assert_array_equal(s.plane(1, 2, 20), ey[:, :, 20])
+
+
+def test_watchdog_reports_nonfinite():
+    s = run_sim("vacuum", 10, F.FDTD_FP32)
+    hx = s.field(3)
+    hx[17, 17, 17] = np.nan
+    s.set_field(3, hx)
+    s.step(2)
+    with pytest.raises(F.FdtdError) as e:
+        s.check()
+    assert e.value.status == 6
+
+
+def test_scatabs_file_format(tmp_path):
+    s = run_sim("sphere_au", 200, F.FDTD_FP64)
+    path = tmp_path / "ScatAbs.200.txt"
+    s.write_scatabs(str(path))
+    rows = np.loadtxt(path)
+    assert rows.shape == (s.dims.num_freq, 19)
+    np.testing.assert_allclose(rows, s.spectra(), rtol=1e-6)
