@@ -1,0 +1,458 @@
+#!/usr/bin/env python
+"""Benchmark of the FDTD time-step loop on B200.
+
+Workload (one GPU): the 256^3 gold nanorod dimer -- 40 nm rods, 10 nm
+diameter, hemispherical caps, 2 nm gap along x -- with Drude + 2CP and the
+hydrodynamic nonlocal current (beta = sqrt(3/5) v_F), 12-cell CPML, an
+x-polarised TFSF plane wave along +z and the 6-face DFT flux boxes at 201
+wavelengths (500-1200 nm), dx = 1 nm, S = 0.5.  Inputs are synthetic (the
+geometry is rasterised on the host; fields start at zero).
+
+A bench "step" is one block of 128 FDTD time steps: the launch period of the
+stepper (32 DFT samples taken every 4 time steps and one FP64 phasor
+contraction).  value = grid cells * time steps / seconds / 1e9, summed over
+ranks (independent replicas, one per GPU: the reference is single-GPU and the
+path is run as replicas only).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "fdtd-cuda_b200"))
+
+METRIC = "Gcell-steps/s at 256^3 vs plain; adjoint/forward time ratio; batched sims/s"
+BLOCK = 128  # time steps per bench step
+WORKLOAD = ("256^3 Au rod dimer (40 nm rods, 10 nm diameter, 2 nm gap), Drude+2CP + "
+            "hydrodynamic current, 12-cell CPML, TFSF x-polarised plane wave, "
+            "201-wavelength DFT flux boxes, dx = 1 nm, S = 0.5")
+
+
+def workload_params(mod, precision, grid=256, **over):
+    """The 256^3 nonlocal rod-dimer configuration as fdtd_params (grid
+    shrinks it for profiling captures)."""
+    n_in = grid - 2 * 12 - 1
+    kw = dict(
+        Tend=20000, dx=1e-9, dy=1e-9, dz=1e-9, NCELLX=n_in, NCELLY=n_in, NCELLZ=n_in,
+        NcpmlX=12, NcpmlY=12, NcpmlZ=12, material=3, first_medium=1, NUM_freq=201,
+        WL_or_freq=1, lam_min=500e-9, lam_max=1200e-9, BandWidth=7e14, lam_0=705e-9,
+        NONLOCAL=3, hydro_D=3.0, fermi_velocity=1.39e6, inc_phi_deg=90.0,
+        geometry=1, axis=0, rod_length=40e-9, rod_diameter=10e-9, gap=2e-9,
+        precision=precision,
+    )
+    kw.update(over)
+    return mod.default_params(**kw)
+
+
+# ----------------------------------------------------------------------
+# helpers
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while running."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.gpu)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, ValueError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.lines:
+            return None
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profile_traffic(key):
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f).get(key)
+    except (OSError, ValueError):
+        return None
+
+
+def pass_bytes(dims, params, esize, which):
+    """Algorithmic DRAM bytes of one E or H pass launch: each cell reads the
+    three components it updates and the three of the other field and
+    writes the three it updates (9 values per cell), and each psi value of
+    the six CPML slabs is read and written once (E extent: Nc+1 cells per
+    slab, H extent: Nc).  The material byte is read inside the dispersive
+    bounding box only and is not counted."""
+    nx, ny, nz = dims.nx, dims.ny, dims.nz
+    n3 = (nx, ny, nz)
+    total = nx * ny * nz * 9 * esize
+    nc = (params.NcpmlX, params.NcpmlY, params.NcpmlZ)
+    for ax in range(3):
+        w = nc[ax] + 1 if which == "e" else nc[ax]
+        # two slabs, two psi components each (the components other than ax)
+        total += 2 * 2 * w * (nx * ny * nz // n3[ax]) * 2 * esize
+    return total
+
+
+# ----------------------------------------------------------------------
+# the reference arm and the CPU baseline: the oracle port on host cores
+
+def cpu_sample(steps=8):
+    """Times the FP64 CPU restatement (oracle) on the same 256^3 workload for
+    a bounded number of time steps (DFT samples included at t = 0 and 4)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    cores = os.cpu_count() or 1
+    O.lib().orc_set_threads(cores)
+    p = workload_params(O, 1)
+    s = O.OracleSim(p, threads=cores)
+    s.step(1)  # first step allocates the DFT accumulators
+    t0 = time.perf_counter()
+    s.step(steps)
+    dt = time.perf_counter() - t0
+    cells = s.shape[0] * s.shape[1] * s.shape[2]
+    return {"value": cells * steps / dt / 1e9, "unit": "Gcell-steps/s", "cores": cores,
+            "kind": "port",
+            "sample": f"{steps} time steps of the 256^3 workload (FP64, incl. 2 DFT samples), "
+                      f"{dt:.1f} s"}
+
+
+def ref_deck_case(tend):
+    """The reference-geometry deck used to time the reference's own CUDA
+    build beside this one: the 256^3 grid of the workload (12-cell CPML,
+    dx = 1 nm) with the reference's gold sphere (r = 10 nm) and its
+    hydrodynamic model, 201 wavelengths."""
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    from ref_cases import BASE
+    n_in = 256 - 2 * 12 - 1
+    return dict(BASE, Tend=tend, dx=1e-9, dy=1e-9, dz=1e-9, NCELLX=n_in, NCELLY=n_in,
+                NCELLZ=n_in, NcpmlX=12, NcpmlY=12, NcpmlZ=12, nano_sphere=1,
+                nano_sphere_radius=10e-9, NUM_freq=201, NONLOCAL=3, BandWidth=7e14,
+                lam_0=705e-9)
+
+
+def ref_gpu_build(t1=40, t2=240):
+    """Times the unmodified reference program (oracle/_ref/fdtd_ref, its own
+    CUDA build for sm_100a) on the reference-geometry deck: wall time of two
+    runs of t1 and t2 time steps, so that set-up and output cancel."""
+    import shutil
+    import tempfile
+    binp = os.path.join(ROOT, "oracle", "_ref", "fdtd_ref")
+    if not os.access(binp, os.X_OK):
+        return {"unavailable": "oracle/_ref/fdtd_ref was not built"}
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    from ref_cases import deck
+    walls = []
+    for tend in (t1, t2):
+        d = tempfile.mkdtemp(prefix="fdtd_ref_")
+        try:
+            os.makedirs(os.path.join(d, "videofiles"), exist_ok=True)
+            with open(os.path.join(d, "Input.txt"), "w") as f:
+                f.write(deck(ref_deck_case(tend)))
+            t0 = time.perf_counter()
+            r = subprocess.run([binp], cwd=d, stdout=subprocess.DEVNULL, stderr=subprocess.PIPE,
+                               timeout=600)
+            walls.append(time.perf_counter() - t0)
+            if r.returncode != 0:
+                return {"unavailable": f"reference exited {r.returncode}: "
+                                       f"{r.stderr.decode(errors='replace')[-200:]}"}
+        finally:
+            shutil.rmtree(d, ignore_errors=True)
+    cells = 256 ** 3
+    rate = cells * (t2 - t1) / max(walls[1] - walls[0], 1e-9) / 1e9
+    return {"value": round(rate, 4), "unit": "Gcell-steps/s", "dtype": "f64",
+            "deck": "256^3, Au sphere r = 10 nm, hydrodynamic model, 12-cell CPML, "
+                    "201 wavelengths, dx = 1 nm",
+            "method": f"wall time of {t2} minus {t1} time steps of the whole program",
+            "wall_s": [round(w, 3) for w in walls]}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    cb = cpu_sample()
+    line = {
+        "impl": "reference", "metric": METRIC, "value": cb["value"], "unit": cb["unit"],
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "note": "the reference has no CPU implementation; "
+                   "this arm times the FP64 C restatement of its update equations (oracle/) "
+                   "on all host cores"},
+        "cpu_baseline": cb,
+        "e2e": {"value": cb["value"], "unit": cb["unit"], "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    if not args.no_ref_gpu:
+        try:
+            line["reference_cuda_build"] = ref_gpu_build()
+        except Exception as e:  # reported, not fatal: the CPU arm stands
+            line["reference_cuda_build"] = {"unavailable": f"{type(e).__name__}: {e}"[:200]}
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------
+# our arm
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--grid", type=int, default=256, help="smaller grids for ncu captures")
+    ap.add_argument("--num-freq", type=int, default=201)
+    ap.add_argument("--no-ref-gpu", action="store_true",
+                    help="reference arm: skip timing the reference's own CUDA build")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    import torch
+    import torch.distributed as dist
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", device_id=torch.device("cuda", local),
+                                timeout=__import__("datetime").timedelta(seconds=600))
+
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    import ctypes as C
+
+    import numpy as np
+
+    import fdtd_b200 as F
+    dev = local if world > 1 else 0
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream()
+    sp = C.c_void_p(stream.cuda_stream)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed_blocks(sim, k):
+        st0 = sim.stats()
+        barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(k):
+            sim.step(BLOCK, sp)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ms = max_over_ranks(e0.elapsed_time(e1))
+        st1 = sim.stats()
+        return ms, st1.kernels - st0.kernels
+
+    # --- FP32 headline ----------------------------------------------------
+    p32 = workload_params(F, F.FDTD_FP32, grid=args.grid, NUM_freq=args.num_freq)
+    sim = F.Sim(p32, device=dev)
+    d = sim.dims
+    tune = sim.stats()
+    cells = d.nx * d.ny * d.nz
+    for _ in range(args.warmup):
+        sim.step(BLOCK, sp)
+    torch.cuda.synchronize()
+    with ClockSampler(dev) as clk:
+        ms, launches = timed_blocks(sim, args.steps)
+    sim.check()
+    value = world * cells * BLOCK * args.steps / (ms / 1e3) / 1e9
+
+    # --- roofline of the dominant kernels ------------------------------------
+    # each kernel alone, 20 launches back to back on this stream, timed with
+    # CUDA events inside fdtd_time_kernel (the fields change; reset after)
+    kms = {name: sim.time_kernel(which, 20, sp) for name, which in (
+        ("e_pass", F.FDTD_KERNEL_E_PASS), ("h_pass", F.FDTD_KERNEL_H_PASS))}
+    torch.cuda.synchronize()
+    alg = pass_bytes(d, p32, 4, "e")
+    alg_h = pass_bytes(d, p32, 4, "h")
+    peak, peak_kind = measured_peak()
+    achieved = alg / (kms["e_pass"] / 1e3) / 1e9
+    roofline = {"bound": "hbm", "kernel": "e_pass_s<float> (Yee + CPML E pass, whole grid)",
+                "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4),
+                "traffic": profile_traffic("e_pass_fp32_256"),
+                "alg_bytes_per_launch": alg, "launch_ms": round(kms["e_pass"], 4),
+                "peak_source": peak_kind,
+                "h_pass": {"launch_ms": round(kms["h_pass"], 4),
+                           "achieved": round(alg_h / (kms["h_pass"] / 1e3) / 1e9, 1)}}
+
+    # --- end to end through the public API with host buffers --------------
+    # every bench step: pinned H2D of the block's source samples, the block,
+    # pinned D2H of the block's probe rows (ex, ey, ez at the gap centre)
+    sim.reset()
+    src = torch.empty(BLOCK, dtype=torch.float64, pin_memory=True)
+    src_np = src.numpy()
+    pulse = F.coefficients(p32, 102)
+    probe_host = torch.empty(BLOCK * 3, dtype=torch.float64, pin_memory=True)
+    for _ in range(0 if args.no_e2e else args.warmup):
+        t0 = sim.t
+        src_np[:] = pulse[t0:t0 + BLOCK]
+        sim.set_source(t0, BLOCK, src.data_ptr(), sp)
+        sim.step(BLOCK, sp)
+        sim.probe_range(t0, BLOCK, probe_host.data_ptr(), sp)
+        stream.synchronize()
+    barrier()
+    w0 = time.perf_counter()
+    for _ in range(0 if args.no_e2e else args.steps):
+        t0 = sim.t
+        src_np[:] = pulse[t0:t0 + BLOCK]
+        sim.set_source(t0, BLOCK, src.data_ptr(), sp)
+        sim.step(BLOCK, sp)
+        sim.probe_range(t0, BLOCK, probe_host.data_ptr(), sp)
+        stream.synchronize()
+    w1 = time.perf_counter()
+    barrier()
+    e2e_s = max_over_ranks(w1 - w0)
+    e2e = None if args.no_e2e else {"value": round(world * cells * BLOCK * args.steps / e2e_s / 1e9, 3),
+           "unit": "Gcell-steps/s", "h2d_bytes_per_step": BLOCK * 8,
+           "d2h_bytes_per_step": BLOCK * 3 * 8,
+           "note": "public C-ABI calls per step: fdtd_set_source (pinned H2D), fdtd_step, "
+                   "fdtd_get_probe_range (pinned D2H), stream sync"}
+    sim.close()
+
+    # --- FP64 build of the same workload -----------------------------------
+    fp64 = None
+    if not args.no_fp64:
+        sim64 = F.Sim(workload_params(F, F.FDTD_FP64, grid=args.grid, NUM_freq=args.num_freq),
+                      device=dev)
+        for _ in range(max(1, args.warmup)):
+            sim64.step(BLOCK, sp)
+        torch.cuda.synchronize()
+        ms64, _ = timed_blocks(sim64, args.steps)
+        sim64.check()
+        fp64 = {"value": round(world * cells * BLOCK * args.steps / (ms64 / 1e3) / 1e9, 3),
+                "unit": "Gcell-steps/s", "ms_per_step": round(ms64 / args.steps, 3)}
+        sim64.close()
+
+    # --- the reference-geometry deck (Input.txt through fdtd_load_input_txt),
+    # the one the reference's own CUDA build is timed on in the reference arm
+    refdeck = None
+    if not args.no_fp64 and args.grid == 256:
+        import tempfile
+        sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+        from ref_cases import deck
+        with tempfile.TemporaryDirectory() as td:
+            path = os.path.join(td, "Input.txt")
+            with open(path, "w") as f:
+                f.write(deck(ref_deck_case(20000)))
+            pr = F.load_input_txt(path)
+        refdeck = {"deck": "256^3, Au sphere r = 10 nm, hydrodynamic model, 12-cell CPML, "
+                           "201 wavelengths, dx = 1 nm (read from Input.txt)",
+                   "unit": "Gcell-steps/s"}
+        for prec, name in ((F.FDTD_FP64, "f64"), (F.FDTD_FP32, "f32")):
+            pr.precision = prec
+            sm = F.Sim(pr, device=dev)
+            for _ in range(max(1, args.warmup)):
+                sm.step(BLOCK, sp)
+            torch.cuda.synchronize()
+            msr, _ = timed_blocks(sm, args.steps)
+            sm.check()
+            refdeck[name] = round(world * sm.dims.nx * sm.dims.ny * sm.dims.nz * BLOCK * args.steps
+                                  / (msr / 1e3) / 1e9, 3)
+            sm.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu and args.grid == 256:
+        cpu = cpu_sample()
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": "Gcell-steps/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD if args.grid == 256 else f"{args.grid}^3 variant",
+                       "grid": [d.nx, d.ny, d.nz],
+                       "time_steps_per_step": BLOCK, "num_freq": d.num_freq,
+                       "dispersive_cells": list(d.n_metal_cells),
+                       "l2": "no flush: working set (403 MB of fields + 7 GB DFT) > 126 MB L2",
+                       "tuning": {k: getattr(tune, k) for k in ("h_staged", "h_stages", "h_minb", "h_ty", "h_kchunk", "e_staged", "e_stages", "e_minb", "e_ty", "e_kchunk", "h_ms", "e_ms")},
+                       "parallelism": f"replicas x{world}"},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "clocks": clk.summary(), "gpu_launches": launches, "fp64": fp64,
+            "reference_deck": refdeck,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

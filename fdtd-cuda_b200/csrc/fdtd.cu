@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -12,6 +13,8 @@
 
 #include "../../include/fdtd_b200.h"
 #include "kernels.cuh"
+#include "staged.cuh"
+#include "boundary.cuh"
 #include "setup.h"
 
 using namespace fdtd;
@@ -61,6 +64,14 @@ struct fdtd_sim {
   int NX, NY, NZ, PX;
   size_t plane, ncell;
   int kchunk = 32;
+  // launch shape of the E and H passes, chosen by tune_passes()
+  // staged = shared-memory pipelined kernels (minb unused), else the plain
+  // register z-march
+  struct PassCfg { int minb = 1, ty = 4, kchunk = 16, staged = 1, stages = 4; float ms = 0; };
+  ShellCells shell_h, shell_e;
+  const void* dview = nullptr;  // device copy of the view
+  PassCfg hcfg, ecfg;
+  bool tuned = false;
   // device state
   std::vector<std::unique_ptr<DevBuf>> bufs;
   void* E[3];
@@ -79,12 +90,12 @@ struct fdtd_sim {
   int nmetal[3] = {0, 0, 0};
   int4* mcell[3] = {nullptr, nullptr, nullptr};
   void* mstate = nullptr;  // SoA state
-  int* slot_map[3] = {nullptr, nullptr, nullptr};
-  int box_lo[3] = {0, 0, 0}, box_dim[3] = {0, 0, 0};
+  int* nbr[3] = {nullptr, nullptr, nullptr};  // hydrodynamic neighbour slots
   // DFT
   DftView dft;
   void* ring = nullptr;
   double* flux = nullptr;  // [12][nf]
+  double2* twiddles = nullptr;  // [2][kSampleBlock][nf]
   bool dft_on = true;
   int host_nsamp = 0;
   // views (one of them is used, by precision)
@@ -95,6 +106,9 @@ struct fdtd_sim {
   LineArgs line;
   // host step counter
   int t = 0;
+  // kernels enqueued by this handle (graph replays counted per node)
+  long long kernels = 0, steps_done = 0, graph_launches = 0;
+  long long graph_kernels = 0;
   // graph replay of a whole DFT period block
   cudaGraphExec_t graph = nullptr;
   int graph_len = 0;
@@ -326,11 +340,10 @@ static fdtd_status build_views(fdtd_sim* s) {
       m.cpn1[c][0] = b + 4 * maxn; m.cpn1[c][1] = b + 5 * maxn;
       m.pd[c][0] = b + 6 * maxn; m.pd[c][1] = b + 7 * maxn; m.pd[c][2] = b + 8 * maxn;
       m.nd[c][0] = b + 9 * maxn; m.nd[c][1] = b + 10 * maxn;
-      m.slot_map[c] = s->slot_map[c];
+      m.nbr[c] = s->nbr[c];
     }
     s->mstate = st;
   }
-  for (int a = 0; a < 3; a++) { m.box_lo[a] = s->box_lo[a]; m.box_dim[a] = s->box_dim[a]; }
   m.C_E = (T)su.C_E; m.C_E_1 = (T)su.C_E_1; m.C_E_2 = (T)su.C_E_2;
   m.d1 = (T)su.d1; m.d2 = (T)su.d2; m.d3 = (T)su.d3; m.d4 = (T)su.d4; m.d5 = (T)su.d5; m.dNL = (T)su.dNL;
   for (int q = 0; q < 2; q++) {
@@ -340,6 +353,16 @@ static fdtd_status build_views(fdtd_sim* s) {
   m.inv_dx = (T)(1.0 / su.p.dx); m.inv_dy = (T)(1.0 / su.p.dy); m.inv_dz = (T)(1.0 / su.p.dz);
   m.hydro = su.hydro;
   m.fix_cbrt = (su.p.fixes & FDTD_FIX_HYDRO_CBRT) ? 1 : 0;
+  // device copy of the view, read by the cold TFSF helpers of the staged
+  // passes (keeps the kernel parameter from escaping to memory)
+  {
+    SimView<T>* dv;
+    cudaError_t e = s->alloc(&dv, 1);
+    if (e != cudaSuccess) return fail(FDTD_ERR_ALLOC, cudaGetErrorString(e));
+    v.self = dv;
+    s->dview = dv;
+    CUDA_TRY(cudaMemcpy(dv, &v, sizeof(v), cudaMemcpyHostToDevice));
+  }
   // DFT sample ring
   if (s->dft.rows > 0) {
     T* r;
@@ -349,6 +372,9 @@ static fdtd_status build_views(fdtd_sim* s) {
   }
   return FDTD_OK;
 }
+
+template <typename T>
+static fdtd_status tune_passes(fdtd_sim* s);
 
 static fdtd_status create_impl(const fdtd_params* p, int device, fdtd_sim** out) {
   auto s = std::make_unique<fdtd_sim>();
@@ -362,6 +388,7 @@ static fdtd_status create_impl(const fdtd_params* p, int device, fdtd_sim** out)
   s->plane = (size_t)s->NY * s->PX;
   s->ncell = s->plane * s->NZ;
   s->kchunk = s->NZ >= 192 ? 32 : 16;
+  s->hcfg.kchunk = s->ecfg.kchunk = s->kchunk;
   const size_t es = s->fp64 ? 8 : 4;
   // fields
   for (int c = 0; c < 3; c++) {
@@ -419,29 +446,52 @@ static fdtd_status create_impl(const fdtd_params* p, int device, fdtd_sim** out)
     }
     CUDA_TRY(s->alloc(&s->mat, s->ncell));
     CUDA_TRY(cudaMemcpy(s->mat, bits.data(), s->ncell, cudaMemcpyHostToDevice));
-    // slot maps over the bounding box grown by one cell (hydro neighbours)
+    // slot lookup over the bounding box grown by one cell, used here to
+    // resolve each dispersive cell's hydrodynamic neighbours once
+    int box_lo[3], box_dim[3];
     for (int a = 0; a < 3; a++) {
-      s->box_lo[a] = std::max(0, lo[a] - 1);
+      box_lo[a] = std::max(0, lo[a] - 1);
       int h = std::min(a == 0 ? s->NX : a == 1 ? s->NY : s->NZ, hi[a] + 1);
-      s->box_dim[a] = std::max(0, h - s->box_lo[a]);
+      box_dim[a] = std::max(0, h - box_lo[a]);
     }
-    const size_t nbox = (size_t)s->box_dim[0] * s->box_dim[1] * s->box_dim[2];
+    const size_t nbox = (size_t)box_dim[0] * box_dim[1] * box_dim[2];
+    std::vector<int> map[3];
+    auto slot = [&](int a, int i, int j, int k) -> int {
+      const int x = i - box_lo[0], y = j - box_lo[1], z = k - box_lo[2];
+      if (x < 0 || y < 0 || z < 0 || x >= box_dim[0] || y >= box_dim[1] || z >= box_dim[2]) return -1;
+      return map[a][((size_t)z * box_dim[1] + y) * box_dim[0] + x];
+    };
     for (int c = 0; c < 3; c++) {
       s->nmetal[c] = (int)cells[c].size();
-      if (!cells[c].empty()) {
-        CUDA_TRY(s->alloc(&s->mcell[c], cells[c].size()));
-        CUDA_TRY(cudaMemcpy(s->mcell[c], cells[c].data(), cells[c].size() * sizeof(int4), cudaMemcpyHostToDevice));
-      }
-      if (nbox > 0) {
-        std::vector<int> map(nbox, -1);
-        for (const int4& e : cells[c]) {
-          size_t o = ((size_t)(e.z - s->box_lo[2]) * s->box_dim[1] + (e.y - s->box_lo[1])) * s->box_dim[0] +
-                     (e.x - s->box_lo[0]);
-          map[o] = e.w;
+      map[c].assign(nbox, -1);
+      for (const int4& e : cells[c])
+        map[c][((size_t)(e.z - box_lo[2]) * box_dim[1] + (e.y - box_lo[1])) * box_dim[0] + (e.x - box_lo[0])] = e.w;
+    }
+    for (int c = 0; c < 3; c++) {
+      if (cells[c].empty()) continue;
+      CUDA_TRY(s->alloc(&s->mcell[c], cells[c].size()));
+      CUDA_TRY(cudaMemcpy(s->mcell[c], cells[c].data(), cells[c].size() * sizeof(int4), cudaMemcpyHostToDevice));
+      // per cell and component a: a == c -> +e_c, 0, -e_c, unused;
+      // a != c -> +e_c, 0, +e_c - e_a, -e_a
+      std::vector<int> nb(cells[c].size() * 12, -1);
+      const int oc[3] = {c == 0, c == 1, c == 2};
+      for (size_t q = 0; q < cells[c].size(); q++) {
+        const int4 e = cells[c][q];
+        int* o = nb.data() + q * 12;
+        for (int a = 0; a < 3; a++) {
+          const int ob[3] = {a == 0, a == 1, a == 2};
+          o[a * 4 + 0] = slot(a, e.x + oc[0], e.y + oc[1], e.z + oc[2]);
+          o[a * 4 + 1] = slot(a, e.x, e.y, e.z);
+          if (a == c) {
+            o[a * 4 + 2] = slot(a, e.x - oc[0], e.y - oc[1], e.z - oc[2]);
+          } else {
+            o[a * 4 + 2] = slot(a, e.x + oc[0] - ob[0], e.y + oc[1] - ob[1], e.z + oc[2] - ob[2]);
+            o[a * 4 + 3] = slot(a, e.x - ob[0], e.y - ob[1], e.z - ob[2]);
+          }
         }
-        CUDA_TRY(s->alloc(&s->slot_map[c], nbox));
-        CUDA_TRY(cudaMemcpy(s->slot_map[c], map.data(), nbox * sizeof(int), cudaMemcpyHostToDevice));
       }
+      CUDA_TRY(s->alloc(&s->nbr[c], nb.size()));
+      CUDA_TRY(cudaMemcpy(s->nbr[c], nb.data(), nb.size() * sizeof(int), cudaMemcpyHostToDevice));
     }
   }
   // DFT faces: box b (0 Abs, 1 Sca), face f (-X +X -Y +Y -Z +Z)
@@ -463,7 +513,8 @@ static fdtd_status create_impl(const fdtd_params* p, int device, fdtd_sim** out)
         F.na = En[a1] - S[a1]; F.nb = En[a2] - S[a2];
         for (int c = 0; c < 4; c++) F.comp[c] = fcomp[F.ax][c];
         F.row0 = row;
-        row += 4LL * F.na * F.nb;
+        F.npad = ((long long)F.na * F.nb + kDftRows - 1) / kDftRows * kDftRows;
+        row += 4LL * F.npad;
       }
     }
     d.rows = row;
@@ -478,8 +529,17 @@ static fdtd_status create_impl(const fdtd_params* p, int device, fdtd_sim** out)
         (e = s->alloc(&d.acc_im, (size_t)d.nf * d.rows, true)) != cudaSuccess)
       return fail(FDTD_ERR_ALLOC, std::string("DFT accumulators: ") + cudaGetErrorString(e));
     CUDA_TRY(s->alloc(&s->flux, (size_t)12 * d.nf));
+    CUDA_TRY(s->alloc(&s->twiddles, (size_t)2 * kSampleBlock * d.nf));
   }
   s->dft_on = su.p.StaticField == 0;
+  // CPML slab cells and TFSF shells
+  {
+    int lo[3], hi[3];
+    for (int a = 0; a < 3; a++) { lo[a] = su.Nt[a] - 1; hi[a] = (a == 0 ? s->NX : a == 1 ? s->NY : s->NZ) - su.Nt[a]; }
+    s->shell_h.init(lo, hi);
+    for (int a = 0; a < 3; a++) lo[a] = su.Nt[a];
+    s->shell_e.init(lo, hi);
+  }
   fdtd_status st = s->fp64 ? build_views<double>(s.get()) : build_views<float>(s.get());
   if (st != FDTD_OK) return st;
   // line
@@ -493,6 +553,8 @@ static fdtd_status create_impl(const fdtd_params* p, int device, fdtd_sim** out)
   L.clk = s->clk; L.probe = s->probe; L.probe_cap = s->probe_cap;
   L.dft_every = s->dft_on ? su.p.dft_every : 0;
   CUDA_TRY(cudaDeviceSynchronize());
+  st = s->fp64 ? tune_passes<double>(s.get()) : tune_passes<float>(s.get());
+  if (st != FDTD_OK) return st;
   *out = s.release();
   return FDTD_OK;
 }
@@ -547,30 +609,181 @@ MetalView<float>& mview<float>(fdtd_sim* s) { return s->mf; }
 template <>
 MetalView<double>& mview<double>(fdtd_sim* s) { return s->md; }
 
-static dim3 pass_grid(const fdtd_sim* s) {
-  return dim3((s->NX + 31) / 32, (s->NY + 7) / 8, (s->NZ + s->kchunk - 1) / s->kchunk);
+static dim3 pass_grid(const fdtd_sim* s, const fdtd_sim::PassCfg& c) {
+  return dim3((s->NX + 31) / 32, (s->NY + c.ty - 1) / c.ty, (s->NZ + c.kchunk - 1) / c.kchunk);
+}
+
+template <typename T, int TY, int S>
+static size_t staged_smem() {
+  return (size_t)S * StageLayout<T, TY>::STAGE * sizeof(T);
+}
+
+// Staged-pass variants: tile height TY and a register cap given as the
+// minimum number of resident CTAs per SM (MINB; 1 = no cap).
+// and the ring depth S (S-2 planes of lookahead beyond the ones in use).
+#define FDTD_STAGED_VARIANTS(X) \
+  X(4, 1, 4) X(4, 6, 4) X(4, 8, 4) X(8, 3, 4) X(8, 4, 4) X(4, 6, 6) X(4, 8, 6) X(8, 3, 6) X(8, 2, 6)
+
+// Opt the staged kernels into more than 48 KB of dynamic shared memory once.
+template <typename T>
+static void staged_attributes() {
+  static bool done = false;
+  if (done) return;
+#define FDTD_ATTR(TY, MB, S)                                                                         \
+  cudaFuncSetAttribute(h_pass_s<T, TY, S, MB>, cudaFuncAttributeMaxDynamicSharedMemorySize,          \
+                       (int)staged_smem<T, TY, S>());                                                \
+  cudaFuncSetAttribute(e_pass_s<T, TY, S, MB>, cudaFuncAttributeMaxDynamicSharedMemorySize,          \
+                       (int)staged_smem<T, TY, S>());
+  FDTD_STAGED_VARIANTS(FDTD_ATTR)
+#undef FDTD_ATTR
+  done = true;
+}
+
+template <typename T>
+static void launch_h_cfg(fdtd_sim* s, const fdtd_sim::PassCfg& c, cudaStream_t st) {
+  const dim3 g = pass_grid(s, c), b(32, c.ty);
+  if (c.staged) {
+#define FDTD_LAUNCH(TY, MB, S)                                                                   \
+  if (c.ty == TY && c.minb == MB && c.stages == S) {                                             \
+    h_pass_s<T, TY, S, MB><<<g, b, staged_smem<T, TY, S>(), st>>>(view<T>(s), c.kchunk);        \
+    return;                                                                                      \
+  }
+    FDTD_STAGED_VARIANTS(FDTD_LAUNCH)
+#undef FDTD_LAUNCH
+  }
+}
+template <typename T>
+static void launch_e_cfg(fdtd_sim* s, const fdtd_sim::PassCfg& c, cudaStream_t st) {
+  const dim3 g = pass_grid(s, c), b(32, c.ty);
+  if (c.staged) {
+#define FDTD_LAUNCH(TY, MB, S)                                                                   \
+  if (c.ty == TY && c.minb == MB && c.stages == S) {                                             \
+    e_pass_s<T, TY, S, MB><<<g, b, staged_smem<T, TY, S>(), st>>>(view<T>(s), c.kchunk);        \
+    return;                                                                                      \
+  }
+    FDTD_STAGED_VARIANTS(FDTD_LAUNCH)
+#undef FDTD_LAUNCH
+  }
+}
+
+// Autotuner: times every launch shape of the E and H passes on the zero
+// state (which they leave at zero: no source has run yet) and keeps the
+// fastest.  Shapes: minimum CTAs per SM (register cap) x tile height x
+// z-chunk.  FDTD_TUNE=0 keeps the defaults.
+template <typename T>
+static fdtd_status tune_passes(fdtd_sim* s) {
+  staged_attributes<T>();
+  // defaults; FDTD_PASS=staged:TY:MINB:KCHUNK[:STAGES] forces a variant,
+  // FDTD_TUNE=0 skips the timing, small grids are not worth timing
+  fdtd_sim::PassCfg def;
+  def.staged = 1; def.ty = 4; def.minb = 1; def.stages = 4; def.kchunk = 16;
+  const char* force = std::getenv("FDTD_PASS");
+  if (force) {
+    const char* c = std::strchr(force, ':');
+    int ty, mb, kc;
+    int sg = 4;
+    if (c && std::sscanf(c + 1, "%d:%d:%d:%d", &ty, &mb, &kc, &sg) >= 3) {
+      def.ty = ty; def.minb = mb; def.kchunk = kc; def.stages = sg;
+    }
+  }
+  s->hcfg = s->ecfg = def;
+  const char* env = std::getenv("FDTD_TUNE");
+  if ((env && env[0] == '0') || force || s->ncell < (size_t)(1 << 18)) {
+    s->tuned = true;
+    return FDTD_OK;
+  }
+  cudaEvent_t a, b;
+  CUDA_TRY(cudaEventCreate(&a));
+  CUDA_TRY(cudaEventCreate(&b));
+  const char* venv = std::getenv("FDTD_TUNE_VERBOSE");
+  const bool verbose = venv && venv[0] == '1';
+  std::vector<fdtd_sim::PassCfg> cands;
+  const int variants[][3] = {{4, 1, 4}, {4, 6, 4}, {4, 8, 4}, {8, 3, 4}, {8, 4, 4},
+                              {4, 6, 6}, {4, 8, 6}, {8, 3, 6}, {8, 2, 6}};
+  for (const auto& v : variants)
+    for (int kc : {8, 16, 32}) {
+      fdtd_sim::PassCfg c;
+      c.staged = 1; c.ty = v[0]; c.minb = v[1]; c.stages = v[2]; c.kchunk = kc;
+      // skip variants whose shared memory does not fit (FP64 at depth 6)
+      const size_t sm = sizeof(T) * (size_t)c.stages * (c.ty == 4 ? StageLayout<T, 4>::STAGE : StageLayout<T, 8>::STAGE);
+      if (kc <= 2 * s->NZ && sm * std::max(1, c.minb) <= 220 * 1024) cands.push_back(c);
+    }
+  for (int pass = 0; pass < 2; pass++) {
+    fdtd_sim::PassCfg best;
+    best.ms = 1e30f;
+    for (fdtd_sim::PassCfg c : cands) {
+        {
+          auto go = [&]() { pass == 0 ? launch_h_cfg<T>(s, c, 0) : launch_e_cfg<T>(s, c, 0); };
+          go();
+          CUDA_TRY(cudaEventRecord(a));
+          for (int r = 0; r < 3; r++) go();
+          CUDA_TRY(cudaEventRecord(b));
+          CUDA_TRY(cudaEventSynchronize(b));
+          float ms;
+          CUDA_TRY(cudaEventElapsedTime(&ms, a, b));
+          c.ms = ms / 3;
+          if (verbose)
+            std::fprintf(stderr, "[fdtd tune] %s staged=%d minb=%d ty=%d kchunk=%d stages=%d %.4f ms\n",
+                         pass == 0 ? "H" : "E", c.staged, c.minb, c.ty, c.kchunk, c.stages, c.ms);
+          if (c.ms < best.ms) best = c;
+        }
+    }
+    (pass == 0 ? s->hcfg : s->ecfg) = best;
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  CUDA_TRY(cudaGetLastError());
+  s->tuned = true;
+  return FDTD_OK;
 }
 
 template <typename T>
 static void launch_h(fdtd_sim* s, cudaStream_t st) {
-  h_pass<T><<<pass_grid(s), dim3(32, 8), 0, st>>>(view<T>(s), s->kchunk);
+  launch_h_cfg<T>(s, s->hcfg, st);
+  const SimView<T>* dv = static_cast<const SimView<T>*>(s->dview);
+  const long long nf = s->shell_h.total();
+  if (nf > 0) tfsf_h_faces<T><<<(unsigned)((nf + 255) / 256), 256, 0, st>>>(dv, s->shell_h);
+  s->kernels += 1 + (nf > 0);
 }
 template <typename T>
 static void launch_line(fdtd_sim* s, cudaStream_t st) {
   line_step<T><<<1, 1024, 0, st>>>(s->line, view<T>(s), s->probe_id);
+  s->kernels++;
 }
 template <typename T>
+static void launch_metal(fdtd_sim* s, cudaStream_t st);
+
+template <typename T>
 static void launch_e(fdtd_sim* s, cudaStream_t st) {
-  e_pass<T><<<pass_grid(s), dim3(32, 8), 0, st>>>(view<T>(s), s->kchunk);
+  const SimView<T>* dv = static_cast<const SimView<T>*>(s->dview);
+  const long long nf = s->shell_e.total();
+  // E half of CORRECT_* before the update (main.cu:2798-2813)
+  if (nf > 0) tfsf_e_faces<T><<<(unsigned)((nf + 255) / 256), 256, 0, st>>>(dv, s->shell_e);
+  if (s->su.hydro) launch_metal<T>(s, st);  // UpdateHydroP* read E^n here
+  launch_e_cfg<T>(s, s->ecfg, st);
+  if (!s->su.hydro) launch_metal<T>(s, st);
+  s->kernels += 1 + (nf > 0);
+}
+
+template <typename T>
+static void launch_metal(fdtd_sim* s, cudaStream_t st) {
   const int ntot = s->nmetal[0] + s->nmetal[1] + s->nmetal[2];
   if (ntot == 0) return;
   if (!s->su.hydro) {
     metal_e<T><<<(ntot + 127) / 128, 128, 0, st>>>(view<T>(s), mview<T>(s), s->clk);
+    s->kernels++;
   } else {
-    hydro_p<T><<<(ntot + 127) / 128, 128, 0, st>>>(view<T>(s), mview<T>(s), s->clk);
-    for (int c = 0; c < 3; c++)
-      if (s->nmetal[c] > 0)
-        metal_e_hydro<T><<<(s->nmetal[c] + 127) / 128, 128, 0, st>>>(view<T>(s), mview<T>(s), s->clk, c);
+    // UpdateHydroP* of every cell fused with the Ex update, then Ey, Ez
+    hydro_p_ex<T><<<(ntot + 127) / 128, 128, 0, st>>>(view<T>(s), mview<T>(s), s->clk);
+    s->kernels++;
+    if (s->nmetal[1] > 0) {
+      hydro_e<T, 1><<<(s->nmetal[1] + 127) / 128, 128, 0, st>>>(view<T>(s), mview<T>(s), s->clk);
+      s->kernels++;
+    }
+    if (s->nmetal[2] > 0) {
+      hydro_e<T, 2><<<(s->nmetal[2] + 127) / 128, 128, 0, st>>>(view<T>(s), mview<T>(s), s->clk);
+      s->kernels++;
+    }
   }
 }
 template <typename T>
@@ -579,12 +792,16 @@ static void launch_sample(fdtd_sim* s, cudaStream_t st) {
   for (int f = 0; f < 12; f++) maxn = std::max(maxn, s->dft.face[f].na * s->dft.face[f].nb);
   dim3 g((maxn + 255) / 256, 12);
   dft_sample<T><<<g, 256, 0, st>>>(view<T>(s), s->dft, (T*)s->ring, s->clk);
+  s->kernels++;
 }
 template <typename T>
 static void launch_contract(fdtd_sim* s, cudaStream_t st) {
-  dim3 g((unsigned)((s->dft.rows + kDftRows - 1) / kDftRows), (s->dft.nf + kDftFreqs - 1) / kDftFreqs);
-  dft_contract<T><<<g, kDftRows, 0, st>>>(s->dft, (const T*)s->ring, s->clk, 0);
+  const int ntw = 2 * kSampleBlock * s->dft.nf;
+  dft_twiddles<<<(ntw + 255) / 256, 256, 0, st>>>(s->dft, s->clk, s->twiddles);
+  dft_contract<T><<<(unsigned)(s->dft.rows / kDftRows), 128, 0, st>>>(s->dft, (const T*)s->ring, s->clk,
+                                                                        s->twiddles);
   dft_reset_count<<<1, 1, 0, st>>>(s->clk);
+  s->kernels += 3;
 }
 
 // One full step in the reference's order.  Host mirrors of the clock
@@ -617,9 +834,12 @@ static fdtd_status step_impl(fdtd_sim* s, int nsteps, cudaStream_t st) {
         if (!s->graph_stream) CUDA_TRY(cudaStreamCreateWithFlags(&s->graph_stream, cudaStreamNonBlocking));
         cudaGraph_t g;
         const int t_save = s->t, n_save = s->host_nsamp;
+        const long long k_save = s->kernels;
         CUDA_TRY(cudaStreamBeginCapture(s->graph_stream, cudaStreamCaptureModeThreadLocal));
         for (int q = 0; q < G; q++) enqueue_step<T>(s, s->graph_stream);
         CUDA_TRY(cudaStreamEndCapture(s->graph_stream, &g));
+        s->graph_kernels = s->kernels - k_save;
+        s->kernels = k_save;
         s->t = t_save;
         s->host_nsamp = n_save;
         cudaError_t e = cudaGraphInstantiate(&s->graph, g, 0);
@@ -628,6 +848,8 @@ static fdtd_status step_impl(fdtd_sim* s, int nsteps, cudaStream_t st) {
         s->graph_len = G;
       }
       CUDA_TRY(cudaGraphLaunch(s->graph, st));
+      s->kernels += s->graph_kernels;
+      s->graph_launches++;
       s->t += G;
       done += G;
     } else {
@@ -635,6 +857,7 @@ static fdtd_status step_impl(fdtd_sim* s, int nsteps, cudaStream_t st) {
       done++;
     }
   }
+  s->steps_done += nsteps;
   CUDA_TRY(cudaGetLastError());
   return FDTD_OK;
 }
@@ -688,6 +911,41 @@ extern "C" fdtd_status fdtd_spectral_accumulate(fdtd_sim* s, void* stream) {
   }
   s->t++;
   CUDA_TRY(cudaGetLastError());
+  return FDTD_OK;
+}
+
+template <typename T>
+static void launch_one(fdtd_sim* s, int which, cudaStream_t st) {
+  switch (which) {
+    case FDTD_KERNEL_H_PASS: launch_h_cfg<T>(s, s->hcfg, st); break;
+    case FDTD_KERNEL_E_PASS: launch_e_cfg<T>(s, s->ecfg, st); break;
+  }
+}
+
+extern "C" fdtd_status fdtd_time_kernel(fdtd_sim* s, int which, int reps, void* stream, double* ms) {
+  if (!s || !ms || reps <= 0) return fail(FDTD_ERR_INVALID, "bad argument");
+  if (which != FDTD_KERNEL_H_PASS && which != FDTD_KERNEL_E_PASS) return fail(FDTD_ERR_INVALID, "unknown kernel");
+  CUDA_TRY(cudaSetDevice(s->device));
+  cudaStream_t st = as_stream(stream);
+  cudaEvent_t a, b;
+  CUDA_TRY(cudaEventCreate(&a));
+  CUDA_TRY(cudaEventCreate(&b));
+  for (int r = 0; r < 2; r++) {  // warm-up
+    if (s->fp64) launch_one<double>(s, which, st); else launch_one<float>(s, which, st);
+  }
+  cudaEventRecord(a, st);
+  for (int r = 0; r < reps; r++) {
+    if (s->fp64) launch_one<double>(s, which, st); else launch_one<float>(s, which, st);
+  }
+  cudaEventRecord(b, st);
+  cudaError_t e = cudaEventSynchronize(b);
+  float t = 0.f;
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&t, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  if (e != cudaSuccess) return fail(FDTD_ERR_CUDA, cudaGetErrorString(e));
+  s->kernels += reps + 2;
+  *ms = (double)t / reps;
   return FDTD_OK;
 }
 
@@ -783,7 +1041,7 @@ extern "C" fdtd_status fdtd_get_dft(fdtd_sim* s, int box, int face, int comp, do
   const size_t n = (size_t)F.na * F.nb;
   std::vector<double> r(n), i(n);
   for (int m = 0; m < nf; m++) {
-    const size_t off = (size_t)m * s->dft.rows + F.row0 + (size_t)comp * n;
+    const size_t off = (size_t)m * s->dft.rows + F.row0 + (size_t)comp * F.npad;
     CUDA_TRY(cudaMemcpy(r.data(), s->dft.acc_re + off, n * sizeof(double), cudaMemcpyDeviceToHost));
     CUDA_TRY(cudaMemcpy(i.data(), s->dft.acc_im + off, n * sizeof(double), cudaMemcpyDeviceToHost));
     for (int u = 0; u < F.na; u++)
@@ -904,6 +1162,40 @@ extern "C" fdtd_status fdtd_get_probe(fdtd_sim* s, double* out, size_t count, in
   size_t m = std::min(have, count);
   CUDA_TRY(cudaMemcpy(out, s->probe, m * sizeof(double), cudaMemcpyDeviceToHost));
   *n = (int)(m / 3);
+  return FDTD_OK;
+}
+
+extern "C" fdtd_status fdtd_get_probe_range(fdtd_sim* s, int t0, int n, double* out, void* stream) {
+  if (!s || !out || t0 < 0 || n < 0 || t0 + n > s->probe_cap) return fail(FDTD_ERR_INVALID, "bad probe range");
+  CUDA_TRY(cudaSetDevice(s->device));
+  cudaStream_t st = as_stream(stream);
+  if (t0 + n >= s->t) {  // the last step's row is written by the next line kernel
+    if (s->fp64) probe_record<double><<<1, 32, 0, st>>>(s->vd, s->clk, s->probe, s->probe_cap, s->probe_id);
+    else probe_record<float><<<1, 32, 0, st>>>(s->vf, s->clk, s->probe, s->probe_cap, s->probe_id);
+    s->kernels++;
+  }
+  CUDA_TRY(cudaMemcpyAsync(out, s->probe + (size_t)3 * t0, (size_t)3 * n * sizeof(double), cudaMemcpyDeviceToHost, st));
+  return FDTD_OK;
+}
+
+extern "C" fdtd_status fdtd_set_source(fdtd_sim* s, int t0, int n, const double* pulse, void* stream) {
+  if (!s || !pulse || t0 < 0 || n < 0 || (size_t)t0 + n > s->su.pulse.size())
+    return fail(FDTD_ERR_INVALID, "source range outside [0, Tend]");
+  CUDA_TRY(cudaSetDevice(s->device));
+  CUDA_TRY(cudaMemcpyAsync(s->pulse + t0, pulse, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, as_stream(stream)));
+  return FDTD_OK;
+}
+
+extern "C" fdtd_status fdtd_get_stats(const fdtd_sim* s, fdtd_stats* out) {
+  if (!s || !out) return fail(FDTD_ERR_INVALID, "null argument");
+  out->kernels = s->kernels;
+  out->steps = s->steps_done;
+  out->graph_launches = s->graph_launches;
+  out->h_minb = s->hcfg.minb; out->h_ty = s->hcfg.ty; out->h_kchunk = s->hcfg.kchunk;
+  out->e_minb = s->ecfg.minb; out->e_ty = s->ecfg.ty; out->e_kchunk = s->ecfg.kchunk;
+  out->h_ms = s->hcfg.ms; out->e_ms = s->ecfg.ms;
+  out->h_staged = s->hcfg.staged; out->e_staged = s->ecfg.staged;
+  out->h_stages = s->hcfg.stages; out->e_stages = s->ecfg.stages;
   return FDTD_OK;
 }
 

@@ -71,6 +71,7 @@ struct SimView {
   const double* e_inc;  // incident line (double in both precisions)
   const double* h_inc;
   int* nonfinite;
+  const SimView* self;  // a copy of this view in device memory (cold paths)
 };
 
 // Dispersive (Drude + 2 critical points, optionally hydrodynamic) cells.
@@ -84,9 +85,8 @@ struct MetalView {
   T* pd[3][3];          // Drude current ring (n, n-1, new) indexed by step
   T* nd[3][2];          // hydro density ring
   const float* rho[3];  // design blend per slot (null = 1)
-  // slot lookup over the dispersive bounding box (hydro neighbours)
-  const int* slot_map[3];
-  int box_lo[3], box_dim[3];
+  // hydrodynamic neighbour slots, 12 per cell (see hydro_neighbours)
+  const int* nbr[3];
   // coefficients
   T C_E, C_E_1, C_E_2;
   T d1, d2, d3, d4, d5, dNL;

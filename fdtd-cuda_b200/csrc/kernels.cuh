@@ -35,7 +35,7 @@ __device__ __forceinline__ size_t fidx(int PX, size_t plane, int i, int j, int k
 // single precision, half-cell offsets double*float*float; summed left to
 // right with C promotion.  Explicit _rn intrinsics keep the compiler from
 // contracting these into FMAs, so host and device round identically.
-__device__ __noinline__ double tf_proj(const TfsfView& tf, int hx2, int hy2, int hz2) {
+__device__ __forceinline__ double tf_proj(const TfsfView& tf, int hx2, int hy2, int hz2) {
   int h2[3] = {hx2, hy2, hz2};
   float fa[3] = {tf.sth, tf.sth, tf.cth};
   float fb[3] = {tf.cph, tf.sph, 1.0f};
@@ -82,7 +82,7 @@ __device__ __forceinline__ double hinc_at(const double* h, int m0, double d) {
 // The H half of CORRECT_X/Y/Z applied to H component c at (i,j,k), in the
 // reference's kernel order X, Y, Z.  v is the freshly updated value.
 template <typename T>
-__device__ __noinline__ T tfsf_h(const SimView<T>& s, int c, int i, int j, int k, T v) {
+__device__ __forceinline__ T tfsf_h(const SimView<T>& s, int c, int i, int j, int k, T v) {
   const TfsfView& tf = s.tf;
   const int NX = s.NX, NY = s.NY, NZ = s.NZ;
   const int Tx = tf.Tx, Ty = tf.Ty, Tz = tf.Tz;
@@ -157,7 +157,7 @@ __device__ __noinline__ T tfsf_h(const SimView<T>& s, int c, int i, int j, int k
 // E-on-H coefficient (the reference uses Cexh for ex and ey, Cezh for ez;
 // they are equal per cell).
 template <typename T>
-__device__ __noinline__ T tfsf_e(const SimView<T>& s, int c, int i, int j, int k, T v, T ceh) {
+__device__ __forceinline__ T tfsf_e(const SimView<T>& s, int c, int i, int j, int k, T v, T ceh) {
   const TfsfView& tf = s.tf;
   const int NX = s.NX, NY = s.NY, NZ = s.NZ;
   const int Tx = tf.Tx, Ty = tf.Ty, Tz = tf.Tz;
@@ -306,163 +306,6 @@ __device__ __forceinline__ void flag_nonfinite(const SimView<T>& s, T v) {
 }
 
 // ---------------------------------------------------------------------
-// H pass: UPDATE_hx/hy/hz (main.cu:762-1044) fused, + H CPML + H TFSF.
-
-template <typename T>
-__global__ void __launch_bounds__(256) h_pass(SimView<T> s, int kchunk) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int NX = s.NX, NY = s.NY, NZ = s.NZ, PX = s.PX;
-  if (i >= NX || j >= NY) return;
-  const int k0 = blockIdx.z * kchunk;
-  const int k1 = min(NZ, k0 + kchunk);
-  const size_t plane = s.plane;
-  const T* __restrict__ ex = s.E[0];
-  const T* __restrict__ ey = s.E[1];
-  const T* __restrict__ ez = s.E[2];
-  T* __restrict__ hx = s.H[0];
-  T* __restrict__ hy = s.H[1];
-  T* __restrict__ hz = s.H[2];
-  const bool hasx = i + 1 < NX, hasy = j + 1 < NY;
-  const bool xs = in_slab(s.cp[0], i), ys = in_slab(s.cp[1], j);
-  const T ikx = ldg(s.cp[0].inv_khd + i), iky = ldg(s.cp[1].inv_khd + j);
-  size_t id = fidx(PX, plane, i, j, k0);
-  T exk = ldg(ex + id), eyk = ldg(ey + id);
-  const T che = s.che, chh = s.chh;
-  for (int k = k0; k < k1; k++, id += plane) {
-    const bool hask = k + 1 < NZ;
-    const T exk1 = hask ? ldg(ex + id + plane) : T(0);
-    const T eyk1 = hask ? ldg(ey + id + plane) : T(0);
-    const T ezk = ldg(ez + id);
-    const T ez_j = hasy ? ldg(ez + id + PX) : T(0);
-    const T ex_j = hasy ? ldg(ex + id + PX) : T(0);
-    const T ey_i = hasx ? ldg(ey + id + 1) : T(0);
-    const T ez_i = hasx ? ldg(ez + id + 1) : T(0);
-    const T ikz = ldg(s.cp[2].inv_khd + k);
-    const bool in3 = hasx && hasy && hask;
-    const bool zs = in_slab(s.cp[2], k);
-    const bool tf = near_tfsf_h(s.tf, NX, NY, NZ, i, j, k);
-    if (hasy && hask) {  // hx
-      const T dey = eyk1 - eyk, dez = ez_j - ezk;
-      T v = chh * hx[id] + che * (dey * ikz - dez * iky);
-      if (in3 && (zs || ys)) {
-        v = cpml_h(s, 0, 1, 2, i, j, k, dey, v, T(1));
-        v = cpml_h(s, 0, 0, 1, i, j, k, dez, v, T(-1));
-      }
-      if (tf) v = tfsf_h(s, 0, i, j, k, v);
-      hx[id] = v;
-    }
-    if (hasx && hask) {  // hy
-      const T dez = ez_i - ezk, dex = exk1 - exk;
-      T v = chh * hy[id] + che * (dez * ikx - dex * ikz);
-      if (in3 && (zs || xs)) {
-        v = cpml_h(s, 1, 0, 2, i, j, k, dex, v, T(-1));
-        v = cpml_h(s, 1, 1, 0, i, j, k, dez, v, T(1));
-      }
-      if (tf) v = tfsf_h(s, 1, i, j, k, v);
-      hy[id] = v;
-    }
-    if (hasx && hasy) {  // hz
-      const T dex = ex_j - exk, dey = ey_i - eyk;
-      T v = chh * hz[id] + che * (dex * iky - dey * ikx);
-      if (in3 && (xs || ys)) {
-        v = cpml_h(s, 2, 0, 0, i, j, k, dey, v, T(-1));
-        v = cpml_h(s, 2, 1, 1, i, j, k, dex, v, T(1));
-      }
-      if (tf) v = tfsf_h(s, 2, i, j, k, v);
-      hz[id] = v;
-    }
-    exk = exk1;
-    eyk = eyk1;
-  }
-}
-
-// ---------------------------------------------------------------------
-// E pass: UPDATE_ex/ey/ez (main.cu:1048-1912) for non-dispersive
-// components, with the E half of the TFSF added first and the E CPML after.
-// Dispersive components are left untouched for metal_e*.
-
-template <typename T>
-__global__ void __launch_bounds__(256) e_pass(SimView<T> s, int kchunk) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int NX = s.NX, NY = s.NY, NZ = s.NZ, PX = s.PX;
-  if (i >= NX || j >= NY) return;
-  const int k0 = blockIdx.z * kchunk;
-  const int k1 = min(NZ, k0 + kchunk);
-  const size_t plane = s.plane;
-  T* __restrict__ ex = s.E[0];
-  T* __restrict__ ey = s.E[1];
-  T* __restrict__ ez = s.E[2];
-  const T* __restrict__ hx = s.H[0];
-  const T* __restrict__ hy = s.H[1];
-  const T* __restrict__ hz = s.H[2];
-  const bool hasx = i > 0, hasy = j > 0;
-  const bool okx = i < NX - 1, oky = j < NY - 1;
-  const bool xs = in_slab(s.cp[0], i), ys = in_slab(s.cp[1], j);
-  const T ikx = ldg(s.cp[0].inv_ked + i), iky = ldg(s.cp[1].inv_ked + j);
-  const bool inbox_xy = i >= s.mat_lo[0] && i < s.mat_hi[0] && j >= s.mat_lo[1] && j < s.mat_hi[1];
-  size_t id = fidx(PX, plane, i, j, k0);
-  T hxm = k0 > 0 ? ldg(hx + id - plane) : T(0);
-  T hym = k0 > 0 ? ldg(hy + id - plane) : T(0);
-  int bad = 0;
-  for (int k = k0; k < k1; k++, id += plane) {
-    const T hxk = ldg(hx + id), hyk = ldg(hy + id), hzk = ldg(hz + id);
-    const T hz_j = hasy ? ldg(hz + id - PX) : T(0);
-    const T hx_j = hasy ? ldg(hx + id - PX) : T(0);
-    const T hz_i = hasx ? ldg(hz + id - 1) : T(0);
-    const T hy_i = hasx ? ldg(hy + id - 1) : T(0);
-    const T ikz = ldg(s.cp[2].inv_ked + k);
-    const bool okz = k < NZ - 1, hasz = k > 0;
-    unsigned m = 0;
-    if (inbox_xy && k >= s.mat_lo[2] && k < s.mat_hi[2]) m = s.mat[id];
-    const int cls = m >> 3;
-    const T cee = s.cee[cls], ceh = s.ceh[cls];
-    const bool zs = in_slab(s.cp[2], k);
-    const bool tf = near_tfsf_e(s.tf, NX, NY, NZ, i, j, k);
-    if (okx && hasy && oky && hasz && okz && !(m & 1)) {  // ex
-      const T dhz = hzk - hz_j, dhy = hyk - hym;
-      T v = ex[id];
-      if (tf) v = tfsf_e(s, 0, i, j, k, v, ceh);
-      v = cee * v + ceh * (dhz * iky - dhy * ikz);
-      if (zs || ys) {
-        v = cpml_e(s, 0, 1, 2, i, j, k, dhy, v, T(-1), ceh);
-        v = cpml_e(s, 0, 0, 1, i, j, k, dhz, v, T(1), ceh);
-      }
-      bad |= !isfinite((double)v);
-      ex[id] = v;
-    }
-    if (hasx && okx && oky && hasz && okz && !(m & 2)) {  // ey
-      const T dhx = hxk - hxm, dhz = hzk - hz_i;
-      T v = ey[id];
-      if (tf) v = tfsf_e(s, 1, i, j, k, v, ceh);
-      v = cee * v + ceh * (dhx * ikz - dhz * ikx);
-      if (zs || xs) {
-        v = cpml_e(s, 1, 0, 2, i, j, k, dhx, v, T(1), ceh);
-        v = cpml_e(s, 1, 1, 0, i, j, k, dhz, v, T(-1), ceh);
-      }
-      bad |= !isfinite((double)v);
-      ey[id] = v;
-    }
-    if (hasx && okx && hasy && oky && okz && !(m & 4)) {  // ez
-      const T dhy = hyk - hy_i, dhx = hxk - hx_j;
-      T v = ez[id];
-      if (tf) v = tfsf_e(s, 2, i, j, k, v, ceh);
-      v = cee * v + ceh * (dhy * ikx - dhx * iky);
-      if (ys || xs) {
-        v = cpml_e(s, 2, 1, 1, i, j, k, dhx, v, T(-1), ceh);
-        v = cpml_e(s, 2, 0, 0, i, j, k, dhy, v, T(1), ceh);
-      }
-      bad |= !isfinite((double)v);
-      ez[id] = v;
-    }
-    hxm = hxk;
-    hym = hyk;
-  }
-  if (bad) atomicOr(s.nonfinite, 1);
-}
-
-// ---------------------------------------------------------------------
 // 1-D incident line (UPDATE_h_inc / UPDATE_e_inc, main.cu:2280-2337) with
 // the Mur ends and the soft source that the reference applies on the host
 // (main.cu:2831-2859).  One CTA.  Advances the device clock and records the
@@ -482,7 +325,7 @@ struct LineArgs {
 };
 
 template <typename T>
-__global__ void __launch_bounds__(1024) line_step(LineArgs a, SimView<T> s, size_t probe_id) {
+__global__ void __launch_bounds__(1024) line_step(const __grid_constant__ LineArgs a, const __grid_constant__ SimView<T> s, size_t probe_id) {
   const int t = a.clk->t;
   // probe: E after step t-1 (OUT.txt records it at the top of step t)
   if (threadIdx.x < 3 && t >= 1 && t - 1 < a.probe_cap)
@@ -517,7 +360,7 @@ __global__ void __launch_bounds__(1024) line_step(LineArgs a, SimView<T> s, size
 }
 
 template <typename T>
-__global__ void probe_record(SimView<T> s, DevClock* clk, double* probe, int cap, size_t probe_id) {
+__global__ void probe_record(const __grid_constant__ SimView<T> s, DevClock* clk, double* probe, int cap, size_t probe_id) {
   int t = clk->t;
   if (threadIdx.x < 3 && t >= 1 && t - 1 < cap)
     probe[3 * (size_t)(t - 1) + threadIdx.x] = (double)s.E[threadIdx.x][probe_id];
@@ -567,7 +410,7 @@ __device__ __forceinline__ T cpml_e_all(const SimView<T>& s, int c, int i, int j
 // Non-hydrodynamic dispersive update of all three components (they do not
 // couple within a step).  pd ring: n = t%3, n-1 = (t+2)%3, new = (t+1)%3.
 template <typename T>
-__global__ void metal_e(SimView<T> s, MetalView<T> m, const DevClock* clk) {
+__global__ void metal_e(const __grid_constant__ SimView<T> s, const __grid_constant__ MetalView<T> m, const DevClock* clk) {
   const int t = clk->t - 1;
   const int rn = t % 3, rn1 = (t + 2) % 3, rnew = (t + 1) % 3;
   int q = blockIdx.x * blockDim.x + threadIdx.x;
@@ -579,8 +422,8 @@ __global__ void metal_e(SimView<T> s, MetalView<T> m, const DevClock* clk) {
   const size_t id = fidx(s.PX, s.plane, i, j, k);
   const unsigned mb = s.mat[id];
   const T ceh = s.ceh[mb >> 3];
-  T v = s.E[c][id];
-  if (near_tfsf_e(s.tf, s.NX, s.NY, s.NZ, i, j, k)) v = tfsf_e(s, c, i, j, k, v, ceh);
+  // the E half of CORRECT_* has already been added by tfsf_e_faces
+  const T v = s.E[c][id];
   T da, db;
   const T curl = curl_h_at(s, c, i, j, k, &da, &db);
   const T pdn = m.pd[c][rn][sl], pdn1 = m.pd[c][rn1][sl];
@@ -612,120 +455,80 @@ __global__ void metal_e(SimView<T> s, MetalView<T> m, const DevClock* clk) {
   s.E[c][id] = nv;
 }
 
-// Slot lookup over the dispersive bounding box; -1 outside the metal.
-template <typename T>
-__device__ __forceinline__ int slot_of(const MetalView<T>& m, int a, int i, int j, int k) {
-  int x = i - m.box_lo[0], y = j - m.box_lo[1], z = k - m.box_lo[2];
-  if (x < 0 || y < 0 || z < 0 || x >= m.box_dim[0] || y >= m.box_dim[1] || z >= m.box_dim[2]) return -1;
-  return m.slot_map[a][((size_t)z * m.box_dim[1] + y) * m.box_dim[0] + x];
-}
-
-// Ring position of component a's "current" Drude current and density as
-// seen during component c's phase of step t (components before c have
-// already rotated, as the reference's sequential launches imply).
-template <typename T>
-__device__ __forceinline__ T pd_cur(const MetalView<T>& m, int a, int c, int t, int i, int j, int k) {
-  int sl = slot_of(m, a, i, j, k);
-  if (sl < 0) return T(0);
-  int r = (a < c) ? (t + 1) % 3 : t % 3;
-  return m.pd[a][r][sl];
-}
-template <typename T>
-__device__ __forceinline__ T nd_cur(const MetalView<T>& m, int a, int c, int t, int i, int j, int k) {
-  int sl = slot_of(m, a, i, j, k);
-  if (sl < 0) return T(0);
-  int r = ((a < c) ? (t + 1) : t) & 1;
-  return m.nd[a][r][sl];
-}
-
-// UpdateHydroPx/Py/Pz (main.cu:1916-2276): new hydrodynamic Drude current of
-// every dispersive cell from E^n (after the TFSF pre-add), its history and
-// the pressure term.  Convection and Lorentz terms are off in the reference.
-template <typename T>
-__global__ void hydro_p(SimView<T> s, MetalView<T> m, const DevClock* clk) {
-  const int t = clk->t - 1;
-  int q = blockIdx.x * blockDim.x + threadIdx.x;
-  int c = 0;
-  while (c < 3 && q >= m.n[c]) { q -= m.n[c]; c++; }
-  if (c >= 3) return;
-  const int4 e = m.cell[c][q];
-  const int i = e.x, j = e.y, k = e.z, sl = e.w;
-  const size_t id = fidx(s.PX, s.plane, i, j, k);
-  const T IX = m.inv_dx, IY = m.inv_dy, IZ = m.inv_dz;
-#define PA(a, ii, jj, kk) pd_cur(m, a, 0, t, ii, jj, kk)
-#define NA(a, ii, jj, kk) nd_cur(m, a, 0, t, ii, jj, kk)
-#define PN(a, ii, jj, kk) (PA(a, ii, jj, kk) * NA(a, ii, jj, kk))
-  T gd, gd2;
-  if (c == 0) {
-    gd2 = IX * IX * (PN(0, i + 1, j, k) - T(2) * PN(0, i, j, k) + PN(0, i - 1, j, k)) +
-          IX * IY * (PN(1, i + 1, j, k) - PN(1, i, j, k) - PN(1, i + 1, j - 1, k) + PN(1, i, j - 1, k)) +
-          IX * IZ * (PN(2, i + 1, j, k) - PN(2, i, j, k) - PN(2, i + 1, j, k - 1) + PN(2, i, j, k - 1));
-    gd = IX * IX * (PA(0, i + 1, j, k) - T(2) * PA(0, i, j, k) + PA(0, i - 1, j, k)) +
-         IX * IY * (PA(1, i + 1, j, k) - PA(1, i, j, k) - PA(1, i + 1, j - 1, k) + PA(1, i, j - 1, k)) +
-         IX * IZ * (PA(2, i + 1, j, k) - PA(2, i, j, k) - PA(2, i + 1, j, k - 1) + PA(2, i, j, k - 1));
-  } else if (c == 1) {
-    gd2 = IY * IY * (PN(1, i, j + 1, k) - T(2) * PN(1, i, j, k) + PN(1, i, j - 1, k)) +
-          IX * IY * (PN(0, i, j + 1, k) - PN(0, i, j, k) - PN(0, i - 1, j + 1, k) + PN(0, i - 1, j, k)) +
-          IY * IZ * (PN(2, i, j + 1, k) - PN(2, i, j, k) - PN(2, i, j + 1, k - 1) + PN(2, i, j, k - 1));
-    gd = IY * IY * (PA(1, i, j + 1, k) - T(2) * PA(1, i, j, k) + PA(1, i, j - 1, k)) +
-         IX * IY * (PA(0, i, j + 1, k) - PA(0, i, j, k) - PA(0, i - 1, j + 1, k) + PA(0, i - 1, j, k)) +
-         IY * IZ * (PA(2, i, j + 1, k) - PA(2, i, j, k) - PA(2, i, j + 1, k - 1) + PA(2, i, j, k - 1));
-  } else {
-    gd2 = IZ * IZ * (PN(2, i, j, k + 1) - T(2) * PN(2, i, j, k) + PN(2, i, j, k - 1)) +
-          IZ * IY * (PN(1, i, j, k + 1) - PN(1, i, j, k) - PN(1, i, j - 1, k + 1) + PN(1, i, j - 1, k)) +
-          IX * IZ * (PN(0, i, j, k + 1) - PN(0, i, j, k) - PN(0, i - 1, j, k + 1) + PN(0, i - 1, j, k));
-    gd = IZ * IZ * (PA(2, i, j, k + 1) - T(2) * PA(2, i, j, k) + PA(2, i, j, k - 1)) +
-         IZ * IY * (PA(1, i, j, k + 1) - PA(1, i, j, k) - PA(1, i, j - 1, k + 1) + PA(1, i, j - 1, k)) +
-         IX * IZ * (PA(0, i, j, k + 1) - PA(0, i, j, k) - PA(0, i - 1, j, k + 1) + PA(0, i - 1, j, k));
+// Neighbour values of a dispersive cell for the hydrodynamic model.  nbr
+// holds, per cell of component c and per component a, four slots (-1 =
+// not dispersive: value 0, the reference's untouched dense arrays): for
+// a == c the cells at +1, 0, -1 along c; for a != c the cells at +e_c, 0,
+// +e_c - e_a and -e_a.  cphase: components below it have already rotated
+// in this step (the reference launches UPDATE_ex, _ey, _ez in turn).
+template <typename T, int c, int cphase>
+__device__ __forceinline__ void hydro_neighbours(const MetalView<T>& m, int q, int t, T P[3][4], T N[3][4]) {
+  const int* nb = m.nbr[c] + (size_t)q * 12;
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    const int rp = (a < cphase) ? (t + 1) % 3 : t % 3;
+    const int rn = ((a < cphase) ? t + 1 : t) & 1;
+#pragma unroll
+    for (int x = 0; x < 4; x++) {
+      const int sl = nb[a * 4 + x];
+      P[a][x] = sl >= 0 ? m.pd[a][rp][sl] : T(0);
+      N[a][x] = sl >= 0 ? m.nd[a][rn][sl] : T(0);
+    }
   }
-#undef PA
-#undef NA
-#undef PN
-  const T nd_prev = m.nd[c][t & 1][sl];
-  const T ND1 = m.N_EQ + nd_prev;
+}
+
+// UpdateHydroPx/Py/Pz (main.cu:1916-2276): the new hydrodynamic Drude
+// current of one cell from E^n (after the TFSF pre-add), its history and
+// the pressure term d_NL (grad div J + grad div (N J) / N_EQ) / (N_EQ +
+// N)^(1/3).  Convection and Lorentz terms are off in the reference.
+template <typename T, int c>
+__device__ __forceinline__ T hydro_current(const MetalView<T>& m, int t, int sl, const T P[3][4], const T N[3][4],
+                                           T ev, T en_prev) {
+  const T IX = m.inv_dx, IY = m.inv_dy, IZ = m.inv_dz;
+  const T I3[3] = {IX, IY, IZ};
+  // the two other components in the reference's summation order, with
+  // their mixed-derivative coefficients
+  constexpr int a1 = c == 0 ? 1 : (c == 1 ? 0 : 1), a2 = c == 0 ? 2 : (c == 1 ? 2 : 0);
+  const T k1 = c == 2 ? IZ * IY : I3[c < a1 ? c : a1] * I3[c < a1 ? a1 : c];
+  const T k2 = I3[c < a2 ? c : a2] * I3[c < a2 ? a2 : c];
+  const T Ic = I3[c];
+  T PN[3][4];
+#pragma unroll
+  for (int a = 0; a < 3; a++)
+#pragma unroll
+    for (int x = 0; x < 4; x++) PN[a][x] = P[a][x] * N[a][x];
+  const T gd2 = Ic * Ic * (PN[c][0] - T(2) * PN[c][1] + PN[c][2]) +
+                k1 * (PN[a1][0] - PN[a1][1] - PN[a1][2] + PN[a1][3]) +
+                k2 * (PN[a2][0] - PN[a2][1] - PN[a2][2] + PN[a2][3]);
+  const T gd = Ic * Ic * (P[c][0] - T(2) * P[c][1] + P[c][2]) + k1 * (P[a1][0] - P[a1][1] - P[a1][2] + P[a1][3]) +
+               k2 * (P[a2][0] - P[a2][1] - P[a2][2] + P[a2][3]);
+  const T ND1 = m.N_EQ + N[c][1];
   T cb;
   if (m.fix_cbrt) cb = (T)cbrt((double)ND1);
   else cb = (T)powf((float)ND1, (float)(1.0 / 3.0));
-  // E^n after the TFSF pre-add: dispersive cells never sit on the TFSF faces
-  // in the hydrodynamic model (checked at create), so E is read as stored.
-  const T ev = s.E[c][id];
   const T pn = m.pd[c][t % 3][sl], pn1 = m.pd[c][(t + 2) % 3][sl];
-  const T npd = m.d1 * pn + m.d2 * pn1 + m.d3 * ev + m.d4 * m.en[c][sl] + m.d5 * T(0) +
-                m.dNL * (gd + gd2 / m.N_EQ) / cb;
-  m.pd[c][(t + 1) % 3][sl] = npd;
+  return m.d1 * pn + m.d2 * pn1 + m.d3 * ev + m.d4 * en_prev + m.d5 * T(0) + m.dNL * (gd + gd2 / m.N_EQ) / cb;
 }
 
-// Hydrodynamic E update of component c (UPDATE_e* hydro branch,
-// main.cu:1220-1271 and mirrors): continuity for the density
+// Hydrodynamic E update of one cell of component c (UPDATE_e* hydro
+// branch, main.cu:1220-1271 and mirrors): continuity for the density
 // perturbation, then E with the current source e0 (N_EQ + N) J.
-template <typename T>
-__global__ void metal_e_hydro(SimView<T> s, MetalView<T> m, const DevClock* clk, int c) {
-  const int t = clk->t - 1;
-  int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= m.n[c]) return;
-  const int4 e = m.cell[c][q];
+template <typename T, int c>
+__device__ __forceinline__ void hydro_e_cell(const SimView<T>& s, const MetalView<T>& m, int t, int4 e,
+                                             const T P[3][4], const T N[3][4], T jd) {
   const int i = e.x, j = e.y, k = e.z, sl = e.w;
   const size_t id = fidx(s.PX, s.plane, i, j, k);
-  const unsigned mb = s.mat[id];
-  const T ceh = s.ceh[mb >> 3];
-  // continuity
+  const T ceh = s.ceh[s.mat[id] >> 3];
   T V1[3], V2[3], N1[3], N2[3];
-  const int o0 = c == 0, o1 = c == 1, o2 = c == 2;
 #pragma unroll
   for (int a = 0; a < 3; a++) {
     if (a == c) {
-      V1[a] = pd_cur(m, a, c, t, i + o0, j + o1, k + o2);
-      V2[a] = pd_cur(m, a, c, t, i - o0, j - o1, k - o2);
-      N1[a] = nd_cur(m, a, c, t, i + o0, j + o1, k + o2);
-      N2[a] = nd_cur(m, a, c, t, i - o0, j - o1, k - o2);
+      V1[a] = P[a][0]; V2[a] = P[a][2]; N1[a] = N[a][0]; N2[a] = N[a][2];
     } else {
-      const int b0 = a == 0, b1 = a == 1, b2 = a == 2;
-      V1[a] = T(0.5) * (pd_cur(m, a, c, t, i + o0, j + o1, k + o2) + pd_cur(m, a, c, t, i, j, k));
-      V2[a] = T(0.5) * (pd_cur(m, a, c, t, i + o0 - b0, j + o1 - b1, k + o2 - b2) +
-                        pd_cur(m, a, c, t, i - b0, j - b1, k - b2));
-      N1[a] = T(0.5) * (nd_cur(m, a, c, t, i + o0, j + o1, k + o2) + nd_cur(m, a, c, t, i, j, k));
-      N2[a] = T(0.5) * (nd_cur(m, a, c, t, i + o0 - b0, j + o1 - b1, k + o2 - b2) +
-                        nd_cur(m, a, c, t, i - b0, j - b1, k - b2));
+      V1[a] = T(0.5) * (P[a][0] + P[a][1]);
+      V2[a] = T(0.5) * (P[a][2] + P[a][3]);
+      N1[a] = T(0.5) * (N[a][0] + N[a][1]);
+      N2[a] = T(0.5) * (N[a][2] + N[a][3]);
     }
   }
   const T ndm1 = m.nd[c][(t + 1) & 1][sl];  // N^{n-1}
@@ -743,7 +546,6 @@ __global__ void metal_e_hydro(SimView<T> s, MetalView<T> m, const DevClock* clk,
     nd = ndm1 - k2 * ((N1[0] * V1[0] - N2[0] * V2[0]) + (N1[1] * V1[1] - N2[1] * V2[1]) +
                       T(0.5) * (V1[2] - V2[2]) +
                       ((V1[0] - V2[0]) + (V1[1] - V2[1]) + T(0.5) * (V1[2] - V2[2])) * m.N_EQ);
-  // E update
   const T v = s.E[c][id];
   T da, db;
   const T curl = curl_h_at(s, c, i, j, k, &da, &db);
@@ -756,10 +558,8 @@ __global__ void metal_e_hydro(SimView<T> s, MetalView<T> m, const DevClock* clk,
   CP4 += m.C2[1] * cpn1_1;
   const T en1 = m.en[c][sl];
   const T en = v;
-  const T jd = m.pd[c][(t + 1) % 3][sl];  // current from hydro_p
   const T inv_CE = T(1) / m.C_E;
-  T nv = inv_CE * (m.dt * curl / m.z0 + m.dt * jd * m.e0 * (m.N_EQ + nd) + m.C_E_1 * en - m.C_E_2 * en1 - CP2 -
-                   CP4);
+  T nv = inv_CE * (m.dt * curl / m.z0 + m.dt * jd * m.e0 * (m.N_EQ + nd) + m.C_E_1 * en - m.C_E_2 * en1 - CP2 - CP4);
   const T ncp0 = m.C1[0] * cpn0 + m.C2[0] * cpn1_0 + m.C3[0] * nv + m.C4[0] * en + m.C5[0] * en1;
   const T ncp1 = m.C1[1] * cpn1 + m.C2[1] * cpn1_1 + m.C3[1] * nv + m.C4[1] * en + m.C5[1] * en1;
   m.en1[c][sl] = en1;
@@ -774,16 +574,59 @@ __global__ void metal_e_hydro(SimView<T> s, MetalView<T> m, const DevClock* clk,
   s.E[c][id] = nv;
 }
 
+template <typename T, int c>
+__device__ __forceinline__ void hydro_p_cell(const SimView<T>& s, const MetalView<T>& m, int t, int q) {
+  const int4 e = m.cell[c][q];
+  T P[3][4], N[3][4];
+  hydro_neighbours<T, c, 0>(m, q, t, P, N);
+  const size_t id = fidx(s.PX, s.plane, e.x, e.y, e.z);
+  const T jd = hydro_current<T, c>(m, t, e.w, P, N, s.E[c][id], m.en[c][e.w]);
+  m.pd[c][(t + 1) % 3][e.w] = jd;
+  if (c == 0) hydro_e_cell<T, 0>(s, m, t, e, P, N, jd);
+}
+
+// Phase 1 of the hydrodynamic step: UpdateHydroP* for every dispersive
+// cell, and the Ex update for the x cells (which needs only its own new
+// current and the state from before this step).
+template <typename T>
+__global__ void hydro_p_ex(const __grid_constant__ SimView<T> s, const __grid_constant__ MetalView<T> m,
+                           const DevClock* clk) {
+  const int t = clk->t - 1;
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  int c = 0;
+  while (c < 3 && q >= m.n[c]) { q -= m.n[c]; c++; }
+  if (c >= 3) return;
+  if (c == 0) hydro_p_cell<T, 0>(s, m, t, q);
+  else if (c == 1) hydro_p_cell<T, 1>(s, m, t, q);
+  else hydro_p_cell<T, 2>(s, m, t, q);
+}
+
+// Phases 2 and 3: the Ey, then the Ez update.
+template <typename T, int c>
+__global__ void hydro_e(const __grid_constant__ SimView<T> s, const __grid_constant__ MetalView<T> m,
+                        const DevClock* clk) {
+  const int t = clk->t - 1;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= m.n[c]) return;
+  const int4 e = m.cell[c][q];
+  T P[3][4], N[3][4];
+  hydro_neighbours<T, c, c>(m, q, t, P, N);
+  hydro_e_cell<T, c>(s, m, t, e, P, N, m.pd[c][(t + 1) % 3][e.w]);
+}
+
 // ---------------------------------------------------------------------
 // DFT flux planes (ScattAbs, main.cu:35-366).
 
-// One flux face: rows [row0, row0 + 4*na*nb), component-major, then u, v.
+// One flux face: component c occupies rows [row0 + c*npad, row0 + c*npad
+// + na*nb), u major then v; npad rounds na*nb up to kDftRows so every
+// contraction tile holds E rows only or H rows only.
 struct DftFace {
   int ax, pos;          // normal axis and plane index
   int s1, s2;           // start of the two tangential axes
   int na, nb;           // extents (END - START)
   int comp[4];          // field components 0..5
   long long row0;
+  long long npad;
 };
 
 struct DftView {
@@ -798,7 +641,7 @@ struct DftView {
 };
 
 template <typename T>
-__global__ void dft_sample(SimView<T> s, DftView d, T* ring, const DevClock* clk) {
+__global__ void dft_sample(const __grid_constant__ SimView<T> s, const __grid_constant__ DftView d, T* ring, const DevClock* clk) {
   const int slot = clk->samp_slot;
   if (slot < 0 || slot >= kSampleBlock) return;
   const int f = blockIdx.y;
@@ -816,63 +659,94 @@ __global__ void dft_sample(SimView<T> s, DftView d, T* ring, const DevClock* clk
     for (int c = 0; c < 4; c++) {
       const int comp = F.comp[c];
       const T x = comp < 3 ? s.E[comp][id] : s.H[comp - 3][id];
-      ring[(size_t)slot * d.rows + F.row0 + (size_t)c * n + q] = x;
+      ring[(size_t)slot * d.rows + F.row0 + (size_t)c * F.npad + q] = x;
     }
   }
 }
 
-// acc[f][r] += sum_s x[s][r] * exp(i 2 pi (t_s + delta) dt freq[f]), delta =
-// 1 for E rows and 1/2 for H rows (main.cu:62-76), in FP64.  Block: 128
-// rows x one frequency tile; the tile's phasors live in shared memory.
+// Phasors of the samples waiting in the ring: tw[h][s][f] = exp(i 2 pi
+// (t_s + delta_h) dt freq[f]) with delta = 1 for E (sampled after the E
+// update) and 1/2 for H (main.cu:62-76).  [2][kSampleBlock][nf] of double2.
+__global__ void dft_twiddles(const __grid_constant__ DftView d, const DevClock* clk, double2* tw) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= 2 * kSampleBlock * d.nf) return;
+  const int h = q / (kSampleBlock * d.nf);
+  const int r = q - h * kSampleBlock * d.nf;
+  const int sidx = r / d.nf, f = r - sidx * d.nf;
+  double c = 0, sv = 0;
+  if (sidx < min(kSampleBlock, clk->nsamp)) {
+    const int ts = clk->samp_t[sidx];
+    const double ph = (double)(float)2.0 * 3.1415926535897932384626433832795 * (ts + (h ? 0.5 : 1.0)) * d.dt * d.freq[f];
+    sincos(ph, &sv, &c);
+  }
+  tw[q] = make_double2(c, sv);
+}
+
+// acc[f][r] += sum_s x[s][r] tw[h(r)][s][f] in FP64.  A CTA owns kDftRows
+// rows (all E or all H thanks to the padding) and walks every frequency in
+// tiles of kDftFreqs; each thread accumulates a 4-row x 4-frequency
+// micro-tile, so one shared load feeds several FMAs.
 constexpr int kDftRows = 128;
 constexpr int kDftFreqs = 16;
 
 template <typename T>
-__global__ void __launch_bounds__(kDftRows) dft_contract(DftView d, const T* ring, DevClock* clk, int nsamp_arg) {
-  __shared__ double cs[2][kSampleBlock][kDftFreqs];  // E/H cos
-  __shared__ double sn[2][kSampleBlock][kDftFreqs];
-  const int nsamp = min(kSampleBlock, nsamp_arg > 0 ? nsamp_arg : clk->nsamp);
-  const int f0 = blockIdx.y * kDftFreqs;
-  const int nfl = min(kDftFreqs, d.nf - f0);
-  for (int q = threadIdx.x; q < 2 * kSampleBlock * kDftFreqs; q += blockDim.x) {
-    const int h = q / (kSampleBlock * kDftFreqs);
-    const int r = q - h * kSampleBlock * kDftFreqs;
-    const int sidx = r / kDftFreqs, fl = r - sidx * kDftFreqs;
-    double c = 0, sv = 0;
-    if (sidx < nsamp && fl < nfl) {
-      const int ts = clk->samp_t[sidx];
-      const double ph = (double)(float)2.0 * 3.1415926535897932384626433832795 * (ts + (h ? 0.5 : 1.0)) * d.dt *
-                        d.freq[f0 + fl];
-      sincos(ph, &sv, &c);
-    }
-    cs[h][sidx][fl] = c;
-    sn[h][sidx][fl] = sv;
-  }
-  __syncthreads();
-  const long long r = (long long)blockIdx.x * kDftRows + threadIdx.x;
-  if (r >= d.rows) return;
-  // which face / component this row belongs to (E or H twiddles)
+__global__ void __launch_bounds__(128) dft_contract(const __grid_constant__ DftView d, const T* ring,
+                                                     const DevClock* clk, const double2* tw) {
+  __shared__ double xs[kSampleBlock][kDftRows];
+  __shared__ double2 ws[kSampleBlock][kDftFreqs];
+  const int nsamp = min(kSampleBlock, clk->nsamp);
+  const long long r0 = (long long)blockIdx.x * kDftRows;
+  // E or H rows: the tile lies inside one (face, component) block
   int h = 0;
   for (int f = 0; f < d.nfaces; f++) {
-    const long long n = (long long)d.face[f].na * d.face[f].nb;
-    if (r >= d.face[f].row0 && r < d.face[f].row0 + 4 * n) {
-      h = (r - d.face[f].row0) >= 2 * n;
-      break;
-    }
+    const DftFace& F = d.face[f];
+    if (r0 >= F.row0 && r0 < F.row0 + 4 * F.npad) { h = (r0 - F.row0) >= 2 * F.npad; break; }
   }
-  double x[kSampleBlock];
-#pragma unroll
-  for (int q = 0; q < kSampleBlock; q++) x[q] = q < nsamp ? (double)ring[(size_t)q * d.rows + r] : 0.0;
-  for (int fl = 0; fl < nfl; fl++) {
-    double re = 0, im = 0;
-#pragma unroll
-    for (int q = 0; q < kSampleBlock; q++) {
-      re = fma(x[q], cs[h][q][fl], re);
-      im = fma(x[q], sn[h][q][fl], im);
+  const int tid = threadIdx.x;
+  for (int q = tid; q < kSampleBlock * kDftRows; q += 128) {
+    const int sidx = q / kDftRows, rr = q - sidx * kDftRows;
+    xs[sidx][rr] = sidx < nsamp ? (double)ring[(size_t)sidx * d.rows + r0 + rr] : 0.0;
+  }
+  const int rg = tid & 31, fg = tid >> 5;  // rows rg*4..+3, freqs fg*4..+3
+  const double2* twh = tw + (size_t)h * kSampleBlock * d.nf;
+  for (int f0 = 0; f0 < d.nf; f0 += kDftFreqs) {
+    __syncthreads();  // xs loaded / previous tile's ws consumed
+    for (int q = tid; q < kSampleBlock * kDftFreqs; q += 128) {
+      const int sidx = q / kDftFreqs, fl = q - sidx * kDftFreqs;
+      ws[sidx][fl] = (f0 + fl < d.nf) ? twh[(size_t)sidx * d.nf + f0 + fl] : make_double2(0.0, 0.0);
     }
-    const size_t o = (size_t)(f0 + fl) * d.rows + r;
-    d.acc_re[o] += re;
-    d.acc_im[o] += im;
+    __syncthreads();
+    double re[4][4], im[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+      for (int b = 0; b < 4; b++) re[a][b] = im[a][b] = 0.0;
+    for (int sidx = 0; sidx < nsamp; sidx++) {
+      const double2 x01 = *reinterpret_cast<const double2*>(&xs[sidx][rg * 4]);
+      const double2 x23 = *reinterpret_cast<const double2*>(&xs[sidx][rg * 4 + 2]);
+      const double xv[4] = {x01.x, x01.y, x23.x, x23.y};
+#pragma unroll
+      for (int b = 0; b < 4; b++) {
+        const double2 w = ws[sidx][fg * 4 + b];
+#pragma unroll
+        for (int a = 0; a < 4; a++) {
+          re[a][b] = fma(xv[a], w.x, re[a][b]);
+          im[a][b] = fma(xv[a], w.y, im[a][b]);
+        }
+      }
+    }
+#pragma unroll
+    for (int b = 0; b < 4; b++) {
+      const int f = f0 + fg * 4 + b;
+      if (f >= d.nf) continue;
+      double* pr = d.acc_re + (size_t)f * d.rows + r0 + rg * 4;
+      double* pi = d.acc_im + (size_t)f * d.rows + r0 + rg * 4;
+#pragma unroll
+      for (int a = 0; a < 4; a++) {
+        pr[a] += re[a][b];
+        pi[a] += im[a][b];
+      }
+    }
   }
 }
 
@@ -881,19 +755,19 @@ __global__ void dft_reset_count(DevClock* clk) { clk->nsamp = 0; }
 // Per (box-face, frequency): sum over the face of Re(cEx conj(HY) -
 // cEy conj(HX)) with the reference's component pairing
 // (CalculateAbsScatt, Spectral.cu:725-1132).  Y faces swap the pair.
-__global__ void flux_reduce(DftView d, double* out /* [12][nf] */) {
+__global__ void flux_reduce(const __grid_constant__ DftView d, double* out /* [12][nf] */) {
   const int f = blockIdx.x, m = blockIdx.y;
   const DftFace F = d.face[f];
-  const long long n = (long long)F.na * F.nb;
+  const long long n = (long long)F.na * F.nb, np = F.npad;
   const int qx = F.ax == 1 ? 1 : 0, qy = F.ax == 1 ? 0 : 1;
   const double* re = d.acc_re + (size_t)m * d.rows + F.row0;
   const double* im = d.acc_im + (size_t)m * d.rows + F.row0;
   double acc = 0;
   for (long long q = threadIdx.x; q < n; q += blockDim.x) {
-    const double exr = re[qx * n + q], exi = im[qx * n + q];
-    const double eyr = re[qy * n + q], eyi = im[qy * n + q];
-    const double hxr = re[(2 + qx) * n + q], hxi = im[(2 + qx) * n + q];
-    const double hyr = re[(2 + qy) * n + q], hyi = im[(2 + qy) * n + q];
+    const double exr = re[qx * np + q], exi = im[qx * np + q];
+    const double eyr = re[qy * np + q], eyi = im[qy * np + q];
+    const double hxr = re[(2 + qx) * np + q], hxi = im[(2 + qx) * np + q];
+    const double hyr = re[(2 + qy) * np + q], hyi = im[(2 + qy) * np + q];
     acc += (exr * hyr + exi * hyi) - (eyr * hxr + eyi * hxi);
   }
   __shared__ double red[256];

@@ -1,0 +1,475 @@
+// Shared-memory-staged E and H passes: the Yee updates of all cells with the
+// CPML psi recursions of the six absorbing slabs fused in (UPDATE_hx/hy/hz
+// and UPDATE_ex/ey/ez with their CPML blocks; the TFSF corrections and the
+// dispersive cells are applied by the kernels of boundary.cuh and
+// kernels.cuh).
+//
+// Each CTA owns a 32 x TY tile of (x, y) columns and marches along z through
+// its z-chunk.  The planes it needs are streamed into a ring of S shared-
+// memory stages with 16-byte cp.async copies, so two planes of loads are in
+// flight while a third is computed, independent of occupancy.  Per plane a
+// stage holds
+//   the "halo" family  (3 components, TY+1 rows, 32+CH columns): the field
+//                      read at the +-1 neighbours (E in the H pass, H in the
+//                      E pass), CH = 16 bytes / sizeof(T) columns of x halo
+//   the "own" family   (3 components, TY rows, 32 columns): the field being
+//                      updated
+// Out-of-grid rows, columns and planes are zero-filled by the copy (the
+// reference's PEC outer boundary).
+//
+// CPML: a z-slab plane is uniform across the CTA and a y-slab row across a
+// warp; only the x slabs split a warp (lanes 0..Nc of the first x tile and
+// the last lanes of the last).  The psi values of a cell for plane k+1 are
+// loaded into registers while plane k is computed, so their DRAM latency
+// overlaps one plane of work; every psi element belongs to one cell and is
+// read and written only by that cell's thread.
+#pragma once
+#include "kernels.cuh"
+
+namespace fdtd {
+
+// Which CPML slab a cell index lies in (side: 0 none, 1 near, 2 far), the
+// index inside it and the recursion coefficients there.  E extent: index <=
+// Nc or >= F; H extent: index < Nc or >= F.
+template <typename T>
+struct SlabAt {
+  int side;
+  int q;
+  T b, c;
+};
+
+template <typename T>
+__device__ __forceinline__ SlabAt<T> slab_e(const CpmlAxis<T>& a, int n, const T* ceN) {
+  SlabAt<T> r;
+  r.side = 0; r.q = 0; r.b = T(0); r.c = T(0);
+  if (n < a.Nc + 1) { r.side = 1; r.q = n; r.b = ldg(a.be_N + n); r.c = ldg(ceN + n); }
+  else if (n >= a.F) { r.side = 2; r.q = n - a.F; r.b = ldg(a.be_F + r.q); r.c = ldg(a.ce_F + r.q); }
+  return r;
+}
+template <typename T>
+__device__ __forceinline__ SlabAt<T> slab_h(const CpmlAxis<T>& a, int n) {
+  SlabAt<T> r;
+  r.side = 0; r.q = 0; r.b = T(0); r.c = T(0);
+  if (n < a.Nc) { r.side = 1; r.q = n; r.b = ldg(a.bh_N + n); r.c = ldg(a.ch_N + n); }
+  else if (n >= a.F) { r.side = 2; r.q = n - a.F; r.b = ldg(a.bh_F + r.q); r.c = ldg(a.ch_F + r.q); }
+  return r;
+}
+
+// psi <- b psi + c diff / d (the reference's recursion, main.cu:829-861 and
+// 1294-1318); stores and returns the new psi
+template <typename T>
+__device__ __forceinline__ T psi_apply(T* p, T old, T b, T c, T diff, T inv_d) {
+  const T ps = b * old + c * diff * inv_d;
+  *p = ps;
+  return ps;
+}
+
+
+__device__ __forceinline__ void cp_async16(unsigned dst, const void* src, int src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(src_bytes));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+template <typename T, int TY>
+struct StageLayout {
+  static constexpr int CH = 16 / (int)sizeof(T);   // elements per 16-byte chunk
+  static constexpr int HW = 32 + CH;               // halo row width
+  static constexpr int NCH_HALO = HW / CH;         // chunks per halo row
+  static constexpr int NCH_OWN = 32 / CH;          // chunks per own row
+  static constexpr int HALO = 3 * (TY + 1) * HW;   // elements per stage
+  static constexpr int OWN = 3 * TY * 32;
+  static constexpr int STAGE = HALO + OWN;
+  static constexpr int TASKS_HALO = 3 * (TY + 1) * NCH_HALO;
+  static constexpr int TASKS_OWN = 3 * TY * NCH_OWN;
+  static constexpr int TASKS = TASKS_HALO + TASKS_OWN;
+  static constexpr int NTHR = 32 * TY;
+  static constexpr int MAXT = (TASKS + NTHR - 1) / NTHR;  // copy tasks per thread
+};
+
+// The 16-byte copies one thread issues for every plane, resolved once: the
+// shared-memory byte address inside stage 0, the source of the next plane
+// to issue (advanced by one plane per issue) and whether the row and column
+// lie inside the grid (zero fill otherwise).
+template <typename T, int TY>
+struct CopyTasks {
+  using L = StageLayout<T, TY>;
+  unsigned dst[L::MAXT];
+  const T* src[L::MAXT];
+  bool ok[L::MAXT];
+  bool has[L::MAXT];
+
+  __device__ __forceinline__ void init(unsigned sbase, const T* h0, const T* h1, const T* h2, const T* o0,
+                                       const T* o1, const T* o2, int NY, int PX, size_t plane, int p0, int i0,
+                                       int j0, int halo_row0, int halo_col0) {
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+#pragma unroll
+    for (int t = 0; t < L::MAXT; t++) {
+      const int q = tid + t * L::NTHR;
+      has[t] = q < L::TASKS;
+      dst[t] = sbase;
+      src[t] = h0;
+      ok[t] = false;
+      if (!has[t]) continue;
+      int a, r, ch, gj, gi, d;
+      const T* base;
+      if (q < L::TASKS_HALO) {
+        a = q / ((TY + 1) * L::NCH_HALO);
+        const int rem = q - a * (TY + 1) * L::NCH_HALO;
+        r = rem / L::NCH_HALO;
+        ch = rem - r * L::NCH_HALO;
+        gj = j0 + halo_row0 + r;
+        gi = i0 + halo_col0 + ch * L::CH;
+        d = (a * (TY + 1) + r) * L::HW + ch * L::CH;
+        base = a == 0 ? h0 : a == 1 ? h1 : h2;
+      } else {
+        const int q2 = q - L::TASKS_HALO;
+        a = q2 / (TY * L::NCH_OWN);
+        const int rem = q2 - a * TY * L::NCH_OWN;
+        r = rem / L::NCH_OWN;
+        ch = rem - r * L::NCH_OWN;
+        gj = j0 + r;
+        gi = i0 + ch * L::CH;
+        d = L::HALO + (a * TY + r) * 32 + ch * L::CH;
+        base = a == 0 ? o0 : a == 1 ? o1 : o2;
+      }
+      dst[t] = sbase + (unsigned)(d * (int)sizeof(T));
+      ok[t] = gj >= 0 && gj < NY && gi >= 0 && gi < PX;
+      // plane p0 may be -1 (the E pass starts one plane below its chunk);
+      // the pointer is only dereferenced for planes inside the grid
+      if (ok[t]) src[t] = base + ((long long)p0 * (long long)plane + (long long)gj * PX + gi);
+    }
+  }
+
+  // the next plane (number p; outside [0, NZ) zero-fills) into the stage
+  // at byte offset soff
+  __device__ __forceinline__ void issue(unsigned soff, int p, int NZ, const T* any, size_t plane) {
+    const bool pz = (unsigned)p < (unsigned)NZ;
+#pragma unroll
+    for (int t = 0; t < L::MAXT; t++) {
+      if (!has[t]) continue;
+      const bool g = pz && ok[t];
+      cp_async16(dst[t] + soff, g ? src[t] : any, g ? 16 : 0);
+      src[t] += plane;
+    }
+  }
+};
+
+// ---------------------------------------------------------------------
+// H pass (UPDATE_hx/hy/hz, main.cu:762-1044).
+// Needs E at k and k+1 (halo family) and H at k (own family).  hx is
+// updated where j < NY-1 and k < NZ-1, hy where i < NX-1 and k < NZ-1, hz
+// where i < NX-1 and j < NY-1; the CPML terms apply where all three indices
+// are below N-1 (main.cu:829), per axis in the order z, x, y (hx: z then y;
+// hy: z then x; hz: x then y).  The stage ring is counted from the chunk's
+// first plane and the plane loop is unrolled by S, so every stage offset is
+// a compile-time constant.
+template <typename T, int TY, int S, int MINB>
+__global__ void __launch_bounds__(32 * TY, MINB) h_pass_s(const __grid_constant__ SimView<T> s, int kchunk) {
+  using L = StageLayout<T, TY>;
+  constexpr unsigned SB = L::STAGE * sizeof(T);  // stage bytes
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const T* sm = reinterpret_cast<const T*>(smem_raw);
+  const unsigned sbase = (unsigned)__cvta_generic_to_shared(smem_raw);
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int i0 = blockIdx.x * 32, j0 = blockIdx.y * TY;
+  const int i = i0 + tx, j = j0 + ty;
+  const int NX = s.NX, NY = s.NY, NZ = s.NZ, PX = s.PX;
+  const size_t plane = s.plane;
+  const int k0 = blockIdx.z * kchunk;
+  const int k1 = min(NZ, k0 + kchunk);
+  const T* any = s.E[0];
+  CopyTasks<T, TY> tasks;
+  tasks.init(sbase, s.E[0], s.E[1], s.E[2], s.H[0], s.H[1], s.H[2], NY, PX, plane, k0, i0, j0, 0, 0);
+  int pnext = k0;
+#pragma unroll
+  for (int q = 0; q < S - 1; q++) {  // prologue: planes k0 .. k0+S-2 into stages 0 .. S-2
+    tasks.issue(q * SB, pnext++, NZ, any, plane);
+    cp_async_commit();
+  }
+  const bool live = i < NX && j < NY;
+  const bool hasx = i + 1 < NX, hasy = j + 1 < NY;
+  const T ikx = live ? ldg(s.cp[0].inv_khd + i) : T(0);
+  const T iky = live ? ldg(s.cp[1].inv_khd + j) : T(0);
+  const T* __restrict__ ikzp = s.cp[2].inv_khd + k0;
+  const T che = s.che, chh = s.chh;
+  const size_t id0 = fidx(PX, plane, i, j, k0);
+  T* __restrict__ phx = s.H[0] + id0;
+  T* __restrict__ phy = s.H[1] + id0;
+  T* __restrict__ phz = s.H[2] + id0;
+  const int o = ty * L::HW + tx, oo = ty * 32 + tx;
+  constexpr int FH = (TY + 1) * L::HW;  // one halo component
+  // CPML of this column: x and y slabs are fixed, z slabs follow the plane
+  const bool pml_xy = live && hasx && hasy;  // i < NX-1 and j < NY-1
+  SlabAt<T> sx, sy;
+  sx.side = sy.side = 0; sx.q = sy.q = 0; sx.b = sx.c = sy.b = sy.c = T(0);
+  if (pml_xy) { sx = slab_h(s.cp[0], i); sy = slab_h(s.cp[1], j); }
+  const T idx_ = s.cp[0].inv_d, idy_ = s.cp[1].inv_d, idz_ = s.cp[2].inv_d;
+  const int Ncz = s.cp[2].Nc, Fz = s.cp[2].F;
+  const size_t xstep = (size_t)NY * s.cp[0].Nc, ystep = (size_t)s.cp[1].Nc * PX;
+  T* bx0 = nullptr;  // psi_hy(x) at plane 0
+  T* bx1 = nullptr;  // psi_hz(x)
+  T* by0 = nullptr;  // psi_hx(y)
+  T* by1 = nullptr;  // psi_hz(y)
+  if (sx.side) {
+    const size_t q = (size_t)j * s.cp[0].Nc + sx.q;
+    bx0 = (sx.side == 1 ? s.psiH_N[1][1] : s.psiH_F[1][1]) + q;
+    bx1 = (sx.side == 1 ? s.psiH_N[2][0] : s.psiH_F[2][0]) + q;
+  }
+  if (sy.side) {
+    const size_t q = (size_t)sy.q * PX + i;
+    by0 = (sy.side == 1 ? s.psiH_N[0][0] : s.psiH_F[0][0]) + q;
+    by1 = (sy.side == 1 ? s.psiH_N[2][1] : s.psiH_F[2][1]) + q;
+  }
+  const size_t jrow = (size_t)j * PX + i;
+  // psi of the next plane, prefetched one plane ahead
+  T nz0 = 0, nz1 = 0, nx0 = 0, nx1 = 0, ny0 = 0, ny1 = 0;
+  auto zside = [&](int kk, int& q) -> int {
+    if (kk < Ncz) { q = kk; return 1; }
+    if (kk >= Fz) { q = kk - Fz; return 2; }
+    q = 0;
+    return 0;
+  };
+  auto fetch = [&](int kk) {
+    if (!pml_xy || kk >= NZ - 1) return;
+    int q;
+    const int zs = zside(kk, q);
+    if (zs) {
+      const size_t off = (size_t)q * plane + jrow;
+      nz0 = (zs == 1 ? s.psiH_N[0][1] : s.psiH_F[0][1])[off];
+      nz1 = (zs == 1 ? s.psiH_N[1][0] : s.psiH_F[1][0])[off];
+    }
+    if (sx.side) { nx0 = bx0[(size_t)kk * xstep]; nx1 = bx1[(size_t)kk * xstep]; }
+    if (sy.side) { ny0 = by0[(size_t)kk * ystep]; ny1 = by1[(size_t)kk * ystep]; }
+  };
+  fetch(k0);
+  for (int k = k0; k < k1;) {
+#pragma unroll
+    for (int u = 0; u < S; u++) {
+      if (k < k1) {
+        const T cz0 = nz0, cz1 = nz1, cx0 = nx0, cx1 = nx1, cy0 = ny0, cy1 = ny1;
+        if (k + 1 < k1) fetch(k + 1);
+        cp_async_wait<S - 3>();  // planes up to k+1 have landed
+        __syncthreads();
+        // stage (u+S-1)%S held plane k-1, last read in the previous iteration
+        tasks.issue(((u + S - 1) % S) * SB, pnext++, NZ, any, plane);
+        cp_async_commit();
+        if (live) {
+          const T* eh = sm + u * L::STAGE;
+          const T* en = sm + ((u + 1) % S) * L::STAGE;
+          const T* hown = eh + L::HALO;
+          const T exk = eh[o], eyk = eh[FH + o], ezk = eh[2 * FH + o];
+          const T ex_j = eh[o + L::HW], ez_j = eh[2 * FH + o + L::HW];
+          const T ey_i = eh[FH + o + 1], ez_i = eh[2 * FH + o + 1];
+          const T exk1 = en[o], eyk1 = en[FH + o];
+          const T ikz = ldg(ikzp);
+          const bool hask = k + 1 < NZ;
+          T vx = chh * hown[oo] + che * ((eyk1 - eyk) * ikz - (ez_j - ezk) * iky);
+          T vy = chh * hown[TY * 32 + oo] + che * ((ez_i - ezk) * ikx - (exk1 - exk) * ikz);
+          T vz = chh * hown[2 * TY * 32 + oo] + che * ((ex_j - exk) * iky - (ey_i - eyk) * ikx);
+          if (pml_xy && hask) {
+            int q;
+            const int zs = zside(k, q);
+            if (zs) {
+              const size_t off = (size_t)q * plane + jrow;
+              const T b = ldg((zs == 1 ? s.cp[2].bh_N : s.cp[2].bh_F) + q);
+              const T c = ldg((zs == 1 ? s.cp[2].ch_N : s.cp[2].ch_F) + q);
+              vx += che * psi_apply((zs == 1 ? s.psiH_N[0][1] : s.psiH_F[0][1]) + off, cz0, b, c, eyk1 - eyk, idz_);
+              vy -= che * psi_apply((zs == 1 ? s.psiH_N[1][0] : s.psiH_F[1][0]) + off, cz1, b, c, exk1 - exk, idz_);
+            }
+            if (sx.side) {
+              const size_t off = (size_t)k * xstep;
+              vy += che * psi_apply(bx0 + off, cx0, sx.b, sx.c, ez_i - ezk, idx_);
+              vz -= che * psi_apply(bx1 + off, cx1, sx.b, sx.c, ey_i - eyk, idx_);
+            }
+            if (sy.side) {
+              const size_t off = (size_t)k * ystep;
+              vx -= che * psi_apply(by0 + off, cy0, sy.b, sy.c, ez_j - ezk, idy_);
+              vz += che * psi_apply(by1 + off, cy1, sy.b, sy.c, ex_j - exk, idy_);
+            }
+          }
+          if (hasy && hask) *phx = vx;
+          if (hasx && hask) *phy = vy;
+          if (hasx && hasy) *phz = vz;
+        }
+        phx += plane; phy += plane; phz += plane; ikzp++;
+        k++;
+      }
+    }
+  }
+  cp_async_wait<0>();
+}
+
+// ---------------------------------------------------------------------
+// E pass (UPDATE_ex/ey/ez, main.cu:1048-1912).
+// Needs H at k and k-1 (halo family, one row/column of -1 halo) and E at k
+// (own family).  Dispersive components are skipped (the dispersive-cell
+// kernels update them, CPML included); dielectric classes select their
+// coefficients.  CPML per axis in the order z, y, x (ex: z then y; ey: z
+// then x; ez: y then x).  The stage ring is counted from plane k0-1.
+template <typename T, int TY, int S, int MINB>
+__global__ void __launch_bounds__(32 * TY, MINB) e_pass_s(const __grid_constant__ SimView<T> s, int kchunk) {
+  using L = StageLayout<T, TY>;
+  constexpr unsigned SB = L::STAGE * sizeof(T);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const T* sm = reinterpret_cast<const T*>(smem_raw);
+  const unsigned sbase = (unsigned)__cvta_generic_to_shared(smem_raw);
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int i0 = blockIdx.x * 32, j0 = blockIdx.y * TY;
+  const int i = i0 + tx, j = j0 + ty;
+  const int NX = s.NX, NY = s.NY, NZ = s.NZ, PX = s.PX;
+  const size_t plane = s.plane;
+  const int k0 = blockIdx.z * kchunk;
+  const int k1 = min(NZ, k0 + kchunk);
+  const T* any = s.H[0];
+  CopyTasks<T, TY> tasks;
+  tasks.init(sbase, s.H[0], s.H[1], s.H[2], s.E[0], s.E[1], s.E[2], NY, PX, plane, k0 - 1, i0, j0, -1, -L::CH);
+  int pnext = k0 - 1;
+#pragma unroll
+  for (int q = 0; q < S - 1; q++) {  // prologue: planes k0-1 .. k0+S-3 into stages 0 .. S-2
+    tasks.issue(q * SB, pnext++, NZ, any, plane);
+    cp_async_commit();
+  }
+  const bool live = i < NX && j < NY;
+  // active-range masks of ex, ey, ez in this column (main.cu:1172, 1476, 1767)
+  const bool okx = i < NX - 1, oky = j < NY - 1;
+  const bool colx = live && okx && j > 0 && oky;
+  const bool coly = live && i > 0 && okx && oky;
+  const bool colz = live && i > 0 && okx && j > 0 && oky;
+  const T ikx = live ? ldg(s.cp[0].inv_ked + i) : T(0);
+  const T iky = live ? ldg(s.cp[1].inv_ked + j) : T(0);
+  const T* __restrict__ ikzp = s.cp[2].inv_ked + k0;
+  const int mlo_z = s.mat_lo[2], mhi_z = s.mat_hi[2];
+  const bool inbox_xy = i >= s.mat_lo[0] && i < s.mat_hi[0] && j >= s.mat_lo[1] && j < s.mat_hi[1];
+  const T cee0 = s.cee[0], ceh0 = s.ceh[0];
+  const size_t id0 = fidx(PX, plane, i, j, k0);
+  T* __restrict__ pex = s.E[0] + id0;
+  T* __restrict__ pey = s.E[1] + id0;
+  T* __restrict__ pez = s.E[2] + id0;
+  const int o = (ty + 1) * L::HW + tx + L::CH, oo = ty * 32 + tx;
+  constexpr int FH = (TY + 1) * L::HW;
+  // CPML of this column: x and y slabs are fixed, z slabs follow the plane
+  const bool pml_xy = live && okx && oky;  // i < NX-1 and j < NY-1
+  SlabAt<T> sx, sy;
+  sx.side = sy.side = 0; sx.q = sy.q = 0; sx.b = sx.c = sy.b = sy.c = T(0);
+  T cx_ey = T(0);
+  if (pml_xy) {
+    sy = slab_e(s.cp[1], j, s.cp[1].ce_N);
+    sx = slab_e(s.cp[0], i, s.cp[0].ce_N);
+    // Ey's near-x slab takes ce_y_N in the reference (main.cu:2891)
+    cx_ey = sx.side == 1 ? ldg(s.cp[0].ce_N_ey + sx.q) : sx.c;
+  }
+  const T idx_ = s.cp[0].inv_d, idy_ = s.cp[1].inv_d, idz_ = s.cp[2].inv_d;
+  const int Ncz = s.cp[2].Nc, Fz = s.cp[2].F;
+  const size_t xstep = (size_t)NY * (s.cp[0].Nc + 1), ystep = (size_t)(s.cp[1].Nc + 1) * PX;
+  T* bx0 = nullptr;  // psi_ey(x) at plane 0
+  T* bx1 = nullptr;  // psi_ez(x)
+  T* by0 = nullptr;  // psi_ex(y)
+  T* by1 = nullptr;  // psi_ez(y)
+  if (sx.side) {
+    const size_t q = (size_t)j * (s.cp[0].Nc + 1) + sx.q;
+    bx0 = (sx.side == 1 ? s.psiE_N[1][1] : s.psiE_F[1][1]) + q;
+    bx1 = (sx.side == 1 ? s.psiE_N[2][0] : s.psiE_F[2][0]) + q;
+  }
+  if (sy.side) {
+    const size_t q = (size_t)sy.q * PX + i;
+    by0 = (sy.side == 1 ? s.psiE_N[0][0] : s.psiE_F[0][0]) + q;
+    by1 = (sy.side == 1 ? s.psiE_N[2][1] : s.psiE_F[2][1]) + q;
+  }
+  const size_t jrow = (size_t)j * PX + i;
+  T nz0 = 0, nz1 = 0, nx0 = 0, nx1 = 0, ny0 = 0, ny1 = 0;
+  auto zside = [&](int kk, int& q) -> int {
+    if (kk <= Ncz) { q = kk; return 1; }
+    if (kk >= Fz) { q = kk - Fz; return 2; }
+    q = 0;
+    return 0;
+  };
+  auto fetch = [&](int kk) {
+    if (!pml_xy || kk >= NZ - 1) return;
+    int q;
+    const int zs = zside(kk, q);
+    if (zs) {
+      const size_t off = (size_t)q * plane + jrow;
+      nz0 = (zs == 1 ? s.psiE_N[0][1] : s.psiE_F[0][1])[off];
+      nz1 = (zs == 1 ? s.psiE_N[1][0] : s.psiE_F[1][0])[off];
+    }
+    if (sx.side) { nx0 = bx0[(size_t)kk * xstep]; nx1 = bx1[(size_t)kk * xstep]; }
+    if (sy.side) { ny0 = by0[(size_t)kk * ystep]; ny1 = by1[(size_t)kk * ystep]; }
+  };
+  fetch(k0);
+  T check = T(0);
+  for (int k = k0; k < k1;) {
+#pragma unroll
+    for (int u = 0; u < S; u++) {
+      if (k < k1) {
+        const T cz0 = nz0, cz1 = nz1, cx0 = nx0, cx1 = nx1, cy0 = ny0, cy1 = ny1;
+        if (k + 1 < k1) fetch(k + 1);
+        cp_async_wait<S - 3>();  // planes up to k have landed
+        __syncthreads();
+        // stage (u+S-1)%S held plane k-2, last read in the previous iteration
+        tasks.issue(((u + S - 1) % S) * SB, pnext++, NZ, any, plane);
+        cp_async_commit();
+        if (live) {
+          const T* cur = sm + ((u + 1) % S) * L::STAGE;
+          const T* prv = sm + u * L::STAGE;
+          const T hxk = cur[o], hyk = cur[FH + o], hzk = cur[2 * FH + o];
+          const T hx_j = cur[o - L::HW], hz_j = cur[2 * FH + o - L::HW];
+          const T hy_i = cur[FH + o - 1], hz_i = cur[2 * FH + o - 1];
+          const T hxm = prv[o], hym = prv[FH + o];
+          const T* eown = cur + L::HALO;
+          const T ikz = ldg(ikzp);
+          const bool okz = k < NZ - 1, hasz = k > 0;
+          unsigned m = 0;
+          T cee = cee0, ceh = ceh0;
+          if (inbox_xy && k >= mlo_z && k < mhi_z) {
+            m = s.mat[id0 + (size_t)(k - k0) * plane];
+            if (m >> 3) {
+              cee = s.cee[m >> 3];
+              ceh = s.ceh[m >> 3];
+            }
+          }
+          T vx = cee * eown[oo] + ceh * ((hzk - hz_j) * iky - (hyk - hym) * ikz);
+          T vy = cee * eown[TY * 32 + oo] + ceh * ((hxk - hxm) * ikz - (hzk - hz_i) * ikx);
+          T vz = cee * eown[2 * TY * 32 + oo] + ceh * ((hyk - hy_i) * ikx - (hxk - hx_j) * iky);
+          const bool wx = colx && hasz && okz && !(m & 1);
+          const bool wy = coly && hasz && okz && !(m & 2);
+          const bool wz = colz && okz && !(m & 4);
+          if (pml_xy && okz) {
+            int q;
+            const int zs = zside(k, q);
+            if (zs) {
+              const size_t off = (size_t)q * plane + jrow;
+              const T b = ldg((zs == 1 ? s.cp[2].be_N : s.cp[2].be_F) + q);
+              const T c = ldg((zs == 1 ? s.cp[2].ce_N : s.cp[2].ce_F) + q);
+              if (wx) vx -= ceh * psi_apply((zs == 1 ? s.psiE_N[0][1] : s.psiE_F[0][1]) + off, cz0, b, c, hyk - hym, idz_);
+              if (wy) vy += ceh * psi_apply((zs == 1 ? s.psiE_N[1][0] : s.psiE_F[1][0]) + off, cz1, b, c, hxk - hxm, idz_);
+            }
+            if (sy.side) {
+              const size_t off = (size_t)k * ystep;
+              if (wx) vx += ceh * psi_apply(by0 + off, cy0, sy.b, sy.c, hzk - hz_j, idy_);
+              if (wz) vz -= ceh * psi_apply(by1 + off, cy1, sy.b, sy.c, hxk - hx_j, idy_);
+            }
+            if (sx.side) {
+              const size_t off = (size_t)k * xstep;
+              if (wy) vy -= ceh * psi_apply(bx0 + off, cx0, sx.b, cx_ey, hzk - hz_i, idx_);
+              if (wz) vz += ceh * psi_apply(bx1 + off, cx1, sx.b, sx.c, hyk - hy_i, idx_);
+            }
+          }
+          if (wx) { *pex = vx; check += vx; }
+          if (wy) { *pey = vy; check += vy; }
+          if (wz) { *pez = vz; check += vz; }
+        }
+        pex += plane; pey += plane; pez += plane; ikzp++;
+        k++;
+      }
+    }
+  }
+  cp_async_wait<0>();
+  // NaN/Inf watchdog: a non-finite value makes the running sum non-finite
+  if (!isfinite(check)) atomicOr(s.nonfinite, 1);
+}
+
+}  // namespace fdtd

@@ -9,13 +9,15 @@ import os
 
 import numpy as np
 
-from ._abi import (FACE_COMPONENTS, FDTD_FP32, FDTD_FP64, FIX_BH_X_F, FIX_CE_EY_XN,
-                   FIX_HYDRO_CBRT, GEOM_DISK_ARRAY, GEOM_REFERENCE, GEOM_ROD_DIMER,
-                   GEOM_SPHERE, STATUS, Dims, Params)
+from ._abi import (FACE_COMPONENTS, FDTD_FP32, FDTD_FP64, FDTD_KERNEL_E_PASS,
+                   FDTD_KERNEL_H_PASS, FIX_BH_X_F,
+                   FIX_CE_EY_XN, FIX_HYDRO_CBRT, GEOM_DISK_ARRAY, GEOM_REFERENCE, GEOM_ROD_DIMER,
+                   GEOM_SPHERE, STATUS, Dims, Params, Stats)
 
 __all__ = ["Params", "Dims", "Sim", "FdtdError", "lib", "default_params", "load_input_txt",
            "FDTD_FP32", "FDTD_FP64", "GEOM_REFERENCE", "GEOM_ROD_DIMER", "GEOM_DISK_ARRAY",
-           "GEOM_SPHERE", "FIX_BH_X_F", "FIX_CE_EY_XN", "FIX_HYDRO_CBRT", "FACE_COMPONENTS"]
+           "GEOM_SPHERE", "FIX_BH_X_F", "FIX_CE_EY_XN", "FIX_HYDRO_CBRT", "FACE_COMPONENTS",
+           "FDTD_KERNEL_H_PASS", "FDTD_KERNEL_E_PASS"]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libfdtd_b200.so")
@@ -30,7 +32,8 @@ EXPORTS = [
     "fdtd_get_field", "fdtd_set_field", "fdtd_snapshot_plane", "fdtd_get_probe",
     "fdtd_get_material", "fdtd_set_design", "fdtd_forward", "fdtd_backward",
     "fdtd_batch_create", "fdtd_batch_run", "fdtd_batch_spectra", "fdtd_batch_destroy",
-    "fdtd_plan", "fdtd_rasterise", "fdtd_coefficients",
+    "fdtd_plan", "fdtd_rasterise", "fdtd_coefficients", "fdtd_get_probe_range",
+    "fdtd_set_source", "fdtd_get_stats", "fdtd_time_kernel",
 ]
 
 
@@ -89,6 +92,10 @@ def lib():
         "fdtd_plan": (C.c_int, [P(Params), P(Dims)]),
         "fdtd_rasterise": (C.c_int, [P(Params), P(C.c_ubyte), sz]),
         "fdtd_coefficients": (C.c_int, [P(Params), C.c_int, dp, sz, P(sz)]),
+        "fdtd_get_probe_range": (C.c_int, [vp, C.c_int, C.c_int, vp, vp]),
+        "fdtd_set_source": (C.c_int, [vp, C.c_int, C.c_int, vp, vp]),
+        "fdtd_get_stats": (C.c_int, [vp, P(Stats)]),
+        "fdtd_time_kernel": (C.c_int, [vp, C.c_int, C.c_int, vp, dp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -232,6 +239,26 @@ class Sim:
         out = np.empty((self.params.Tend + 2, 3))
         _check(lib().fdtd_get_probe(self.h, _dp(out), out.size, C.byref(n)))
         return out[: n.value]
+
+    def probe_range(self, t0, n, out_ptr, stream=None):
+        """Async D2H of probe rows [t0, t0+n) into host memory at out_ptr."""
+        _check(lib().fdtd_get_probe_range(self.h, t0, n, out_ptr, stream))
+
+    def set_source(self, t0, n, src_ptr, stream=None):
+        """Async H2D of soft-source samples for steps [t0, t0+n)."""
+        _check(lib().fdtd_set_source(self.h, t0, n, src_ptr, stream))
+
+    def stats(self):
+        st = Stats()
+        _check(lib().fdtd_get_stats(self.h, C.byref(st)))
+        return st
+
+    def time_kernel(self, which, reps=20, stream=None):
+        """Mean device time (ms) of one launch of a single time-step kernel
+        (FDTD_KERNEL_*), from CUDA events; leaves the fields changed."""
+        ms = C.c_double()
+        _check(lib().fdtd_time_kernel(self.h, int(which), int(reps), stream, C.byref(ms)))
+        return ms.value
 
     def material(self):
         out = np.empty(self.shape, np.uint8)

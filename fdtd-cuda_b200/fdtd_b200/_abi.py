@@ -82,6 +82,7 @@ class Dims(C.Structure):
 
 
 FDTD_FP32, FDTD_FP64 = 0, 1
+FDTD_KERNEL_H_PASS, FDTD_KERNEL_E_PASS = 0, 1
 GEOM_REFERENCE, GEOM_ROD_DIMER, GEOM_DISK_ARRAY, GEOM_SPHERE = 0, 1, 2, 3
 FIX_BH_X_F, FIX_CE_EY_XN, FIX_HYDRO_CBRT = 1, 2, 4
 STATUS = {0: "OK", 1: "INVALID", 2: "CUDA", 3: "ALLOC", 4: "IO", 5: "STATE",
@@ -89,3 +90,13 @@ STATUS = {0: "OK", 1: "INVALID", 2: "CUDA", 3: "ALLOC", 4: "IO", 5: "STATE",
 
 # the face component order of the DFT arrays (see fdtd_get_dft)
 FACE_COMPONENTS = {0: (1, 2, 4, 5), 1: (0, 2, 3, 5), 2: (0, 1, 3, 4)}
+
+
+class Stats(C.Structure):
+    _fields_ = [("kernels", C.c_longlong), ("steps", C.c_longlong),
+                ("graph_launches", C.c_longlong),
+                ("h_minb", C.c_int), ("h_ty", C.c_int), ("h_kchunk", C.c_int),
+                ("e_minb", C.c_int), ("e_ty", C.c_int), ("e_kchunk", C.c_int),
+                ("h_ms", C.c_float), ("e_ms", C.c_float),
+                ("h_staged", C.c_int), ("e_staged", C.c_int),
+                ("h_stages", C.c_int), ("e_stages", C.c_int)]

@@ -284,6 +284,41 @@ fdtd_status fdtd_snapshot_plane(fdtd_sim* s, int comp, int axis, int index,
 /* Probe record: ex, ey, ez at the probe cell after every completed step,
  * [t][3]. n = number of steps recorded so far. */
 fdtd_status fdtd_get_probe(fdtd_sim* s, double* out, size_t count, int* n);
+/* Rows [t0, t0+n) of the probe record into host memory, asynchronously on
+ * `stream` (the rows must belong to steps already enqueued on it). */
+fdtd_status fdtd_get_probe_range(fdtd_sim* s, int t0, int n, double* out,
+                                 void* stream);
+/* Replaces the soft-source samples injected at steps [t0, t0+n) (the
+ * reference's pulse at e_inc[m0-50], main.cu:2845-2851) from host memory,
+ * asynchronously on `stream`. */
+fdtd_status fdtd_set_source(fdtd_sim* s, int t0, int n, const double* pulse,
+                            void* stream);
+
+/* Counters: kernels this handle has enqueued (graph replays included). */
+typedef struct fdtd_stats {
+  long long kernels;
+  long long steps;
+  long long graph_launches;
+  /* launch shapes picked by the autotuner (min CTAs/SM, tile height,
+   * z-chunk) and their measured time per launch, for the H and E passes */
+  int h_minb, h_ty, h_kchunk, e_minb, e_ty, e_kchunk;
+  float h_ms, e_ms;
+  int h_staged, e_staged;  /* 1 = shared-memory pipelined pass */
+  int h_stages, e_stages;  /* its ring depth */
+} fdtd_stats;
+fdtd_status fdtd_get_stats(const fdtd_sim* s, fdtd_stats* out);
+/* Measurement hook (no counterpart in the reference): launches one kernel
+ * of the time step reps times back to back (after two untimed launches) on
+ * `stream` and stores its mean device time per launch, from CUDA events on
+ * that stream, in *ms.  The launches change the fields: call fdtd_reset
+ * before using the simulation again. */
+enum {
+  FDTD_KERNEL_H_PASS = 0, /* the H pass (Yee + CPML) over the whole grid */
+  FDTD_KERNEL_E_PASS = 1  /* the E pass (Yee + CPML) over the whole grid,
+                             dispersive cells excluded */
+};
+fdtd_status fdtd_time_kernel(fdtd_sim* s, int which, int reps, void* stream,
+                             double* ms);
 /* Material class map used by the E pass (bit0..2: ex/ey/ez dispersive),
  * reference layout, for rasteriser parity checks. */
 fdtd_status fdtd_get_material(fdtd_sim* s, uint8_t* out, size_t count);
