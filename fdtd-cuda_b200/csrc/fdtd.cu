@@ -8,6 +8,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1147,6 +1148,73 @@ extern "C" fdtd_status fdtd_snapshot_plane(fdtd_sim* s, int comp, int axis, int 
     CUDA_TRY(e);
   }
   CUDA_TRY(cudaGetLastError());
+  return FDTD_OK;
+}
+
+// ---------------------------------------------------------------------
+// Plane snapshot that allocates nothing.  fdtd_snapshot_plane needs a
+// temporary device buffer for a host destination; its cudaMalloc/cudaFree
+// pair synchronises the whole device and can fail once the simulation has
+// filled the GPU.  A snapshot writer called every few hundred steps inside
+// a pipelined time loop, or a host that sized the grid to the device memory,
+// cannot afford either, so this variant gathers into one fixed scratch array
+// in the module's static device memory instead.
+//
+// Limits and rules: a plane of at most kPlaneScratchCells cells; nothing in
+// the scratch has to start at zero (the gather writes every element that is
+// copied back); the scratch is one per device, shared by every simulation
+// in the process, so calls that overlap in time on the same device (from
+// several host threads, or on streams that run concurrently) race on it and
+// must be serialised by the caller.  The first call on each device resolves
+// the scratch address with cudaGetSymbolAddress and should come before any
+// stream capture is begun.
+constexpr size_t kPlaneScratchCells = (size_t)1 << 20;  // 8 MiB of doubles
+static __device__ __align__(256) double g_plane_scratch[kPlaneScratchCells];
+
+static fdtd_status plane_scratch(int device, double** out) {
+  constexpr int kMaxDevices = 64;
+  static std::mutex mu;
+  static double* ptr[kMaxDevices] = {};
+  if (device < 0 || device >= kMaxDevices) return fail(FDTD_ERR_INVALID, "device index out of range");
+  std::lock_guard<std::mutex> lock(mu);
+  if (!ptr[device]) {
+    // the device is current (the caller set it)
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_plane_scratch);
+    if (e != cudaSuccess || !p) return fail(FDTD_ERR_CUDA, std::string("scratch address: ") + cudaGetErrorString(e));
+    ptr[device] = static_cast<double*>(p);
+  }
+  *out = ptr[device];
+  return FDTD_OK;
+}
+
+extern "C" fdtd_status fdtd_snapshot_plane_static(fdtd_sim* s, int comp, int axis, int index, double* dst,
+                                                  size_t count, void* stream) {
+  if (!s || !dst || comp < 0 || comp > 5 || axis < 0 || axis > 2) return fail(FDTD_ERR_INVALID, "bad argument");
+  const int N3[3] = {s->NX, s->NY, s->NZ};
+  if (index < 0 || index >= N3[axis]) return fail(FDTD_ERR_INVALID, "plane index outside the grid");
+  const int na = axis == 0 ? s->NY : s->NX, nb = axis == 2 ? s->NY : s->NZ;
+  if (count != (size_t)na * nb) return fail(FDTD_ERR_INVALID, "count must match the plane size");
+  if (count > kPlaneScratchCells)
+    return fail(FDTD_ERR_INVALID, "plane of " + std::to_string(count) + " cells exceeds the " +
+                                      std::to_string(kPlaneScratchCells) +
+                                      "-cell scratch of fdtd_snapshot_plane_static; use fdtd_snapshot_plane");
+  CUDA_TRY(cudaSetDevice(s->device));
+  double* scratch = nullptr;
+  const fdtd_status st0 = plane_scratch(s->device, &scratch);
+  if (st0 != FDTD_OK) return st0;
+  cudaStream_t st = as_stream(stream);
+  const unsigned g = (unsigned)((count + 255) / 256);
+  if (s->fp64)
+    plane_gather<double><<<g, 256, 0, st>>>((const double*)comp_ptr(s, comp), scratch, s->NX, s->NY, s->NZ, s->PX,
+                                            axis, index);
+  else
+    plane_gather<float><<<g, 256, 0, st>>>((const float*)comp_ptr(s, comp), scratch, s->NX, s->NY, s->NZ, s->PX,
+                                           axis, index);
+  CUDA_TRY(cudaGetLastError());
+  s->kernels++;
+  CUDA_TRY(cudaMemcpyAsync(dst, scratch, count * sizeof(double), cudaMemcpyDefault, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
   return FDTD_OK;
 }
 

@@ -281,6 +281,17 @@ fdtd_status fdtd_set_field(fdtd_sim* s, int comp, const double* in,
  * Asynchronous on `stream` when dst is device memory. */
 fdtd_status fdtd_snapshot_plane(fdtd_sim* s, int comp, int axis, int index,
                                 double* dst, size_t count, void* stream);
+/* The same plane as fdtd_snapshot_plane, with no memory allocation of any
+ * kind: the plane is gathered into a fixed scratch array in the library's
+ * static device memory and copied to dst (host or device) on `stream`; the
+ * call returns once the copy is done.  No counterpart in the reference.
+ * Limit: count <= 1048576 cells (FDTD_ERR_INVALID beyond).  The scratch is
+ * one per device and shared by all simulations: calls that overlap in time
+ * on one device race and must be serialised by the caller.  Make the first
+ * call on each device before beginning any stream capture. */
+fdtd_status fdtd_snapshot_plane_static(fdtd_sim* s, int comp, int axis,
+                                       int index, double* dst, size_t count,
+                                       void* stream);
 /* Probe record: ex, ey, ez at the probe cell after every completed step,
  * [t][3]. n = number of steps recorded so far. */
 fdtd_status fdtd_get_probe(fdtd_sim* s, double* out, size_t count, int* n);
