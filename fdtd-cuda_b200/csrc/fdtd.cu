@@ -69,6 +69,15 @@ struct fdtd_sim {
   // staged = shared-memory pipelined kernels (minb unused), else the plain
   // register z-march
   struct PassCfg { int minb = 1, ty = 4, kchunk = 16, staged = 1, stages = 4; float ms = 0; };
+  // pass tiles for one (tile height, z-chunk): the interior box of tiles
+  // that touch no CPML slab and the table of the others
+  struct TileSet {
+    int ty = 0, kchunk = 0;
+    dim3 inner;
+    TileMap inner_map{0, 0, 0, nullptr}, edge_map{0, 0, 0, nullptr};
+    unsigned nedge = 0;
+  };
+  std::vector<TileSet> tilesets;
   ShellCells shell_h, shell_e;
   const void* dview = nullptr;  // device copy of the view
   PassCfg hcfg, ecfg;
@@ -116,9 +125,17 @@ struct fdtd_sim {
   cudaStream_t graph_stream = nullptr;
   bool use_graphs = true;
 
+  // side stream on which a pass's edge-tile launch runs beside its
+  // interior launch (fork/join by events, also inside graph capture)
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+
   ~fdtd_sim() {
     if (graph) cudaGraphExecDestroy(graph);
     if (graph_stream) cudaStreamDestroy(graph_stream);
+    if (side) cudaStreamDestroy(side);
+    if (fork_ev) cudaEventDestroy(fork_ev);
+    if (join_ev) cudaEventDestroy(join_ev);
   }
 
   // buffers that fdtd_reset zeroes (fields, psi, dispersive state, DFT,
@@ -553,6 +570,9 @@ static fdtd_status create_impl(const fdtd_params* p, int device, fdtd_sim** out)
   L.pulse = s->pulse; L.tmax = (int)su.pulse.size();
   L.clk = s->clk; L.probe = s->probe; L.probe_cap = s->probe_cap;
   L.dft_every = s->dft_on ? su.p.dft_every : 0;
+  CUDA_TRY(cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking));
+  CUDA_TRY(cudaEventCreateWithFlags(&s->fork_ev, cudaEventDisableTiming));
+  CUDA_TRY(cudaEventCreateWithFlags(&s->join_ev, cudaEventDisableTiming));
   CUDA_TRY(cudaDeviceSynchronize());
   st = s->fp64 ? tune_passes<double>(s.get()) : tune_passes<float>(s.get());
   if (st != FDTD_OK) return st;
@@ -610,10 +630,6 @@ MetalView<float>& mview<float>(fdtd_sim* s) { return s->mf; }
 template <>
 MetalView<double>& mview<double>(fdtd_sim* s) { return s->md; }
 
-static dim3 pass_grid(const fdtd_sim* s, const fdtd_sim::PassCfg& c) {
-  return dim3((s->NX + 31) / 32, (s->NY + c.ty - 1) / c.ty, (s->NZ + c.kchunk - 1) / c.kchunk);
-}
-
 template <typename T, int TY, int S>
 static size_t staged_smem() {
   return (size_t)S * StageLayout<T, TY>::STAGE * sizeof(T);
@@ -622,8 +638,7 @@ static size_t staged_smem() {
 // Staged-pass variants: tile height TY and a register cap given as the
 // minimum number of resident CTAs per SM (MINB; 1 = no cap).
 // and the ring depth S (S-2 planes of lookahead beyond the ones in use).
-#define FDTD_STAGED_VARIANTS(X) \
-  X(4, 1, 4) X(4, 6, 4) X(4, 8, 4) X(8, 3, 4) X(8, 4, 4) X(4, 6, 6) X(4, 8, 6) X(8, 3, 6) X(8, 2, 6)
+#define FDTD_STAGED_VARIANTS(X) X(4, 1, 4) X(4, 6, 4) X(4, 8, 4) X(8, 3, 4) X(4, 6, 6)
 
 // Opt the staged kernels into more than 48 KB of dynamic shared memory once.
 template <typename T>
@@ -631,40 +646,123 @@ static void staged_attributes() {
   static bool done = false;
   if (done) return;
 #define FDTD_ATTR(TY, MB, S)                                                                         \
-  cudaFuncSetAttribute(h_pass_s<T, TY, S, MB>, cudaFuncAttributeMaxDynamicSharedMemorySize,          \
+  cudaFuncSetAttribute(h_pass_s<T, TY, S, MB, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,   \
                        (int)staged_smem<T, TY, S>());                                                \
-  cudaFuncSetAttribute(e_pass_s<T, TY, S, MB>, cudaFuncAttributeMaxDynamicSharedMemorySize,          \
+  cudaFuncSetAttribute(h_pass_s<T, TY, S, MB, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,    \
+                       (int)staged_smem<T, TY, S>());                                                \
+  cudaFuncSetAttribute(e_pass_s<T, TY, S, MB, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,   \
+                       (int)staged_smem<T, TY, S>());                                                \
+  cudaFuncSetAttribute(e_pass_s<T, TY, S, MB, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,    \
                        (int)staged_smem<T, TY, S>());
   FDTD_STAGED_VARIANTS(FDTD_ATTR)
 #undef FDTD_ATTR
   done = true;
 }
 
+// Interior box and edge table of the pass tiles for a tile height and
+// z-chunk.  A tile is interior when none of its cells lies in a CPML slab
+// of the E extent (index <= Nc or >= F, a superset of the H extent).
+static fdtd_status build_tiles(fdtd_sim* s, int ty, int kc) {
+  for (const auto& t : s->tilesets)
+    if (t.ty == ty && t.kchunk == kc) return FDTD_OK;
+  fdtd_sim::TileSet ts;
+  ts.ty = ty; ts.kchunk = kc;
+  const int nb[3] = {(s->NX + 31) / 32, (s->NY + ty - 1) / ty, (s->NZ + kc - 1) / kc};
+  const int w[3] = {32, ty, kc};
+  int lo[3], hi[3];  // interior tile range [lo, hi)
+  for (int a = 0; a < 3; a++) {
+    const int Nc = s->su.Nc[a], F = s->su.F[a];
+    lo[a] = (Nc + 1 + w[a] - 1) / w[a];
+    hi[a] = F >= w[a] ? (F - w[a]) / w[a] + 1 : 0;
+    hi[a] = std::min(hi[a], nb[a]);
+    if (hi[a] < lo[a]) hi[a] = lo[a];
+  }
+  const bool inner = hi[0] > lo[0] && hi[1] > lo[1] && hi[2] > lo[2];
+  ts.inner = inner ? dim3(hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]) : dim3(0, 0, 0);
+  ts.inner_map = TileMap{lo[0], lo[1], lo[2], nullptr};
+  std::vector<int4> edge;
+  for (int bz = 0; bz < nb[2]; bz++)
+    for (int by = 0; by < nb[1]; by++)
+      for (int bx = 0; bx < nb[0]; bx++) {
+        const bool in = inner && bx >= lo[0] && bx < hi[0] && by >= lo[1] && by < hi[1] && bz >= lo[2] && bz < hi[2];
+        if (!in) edge.push_back(make_int4(bx, by, bz, 0));
+      }
+  ts.nedge = (unsigned)edge.size();
+  if (!edge.empty()) {
+    int4* d;
+    CUDA_TRY(s->alloc(&d, edge.size()));
+    CUDA_TRY(cudaMemcpy(d, edge.data(), edge.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    ts.edge_map = TileMap{0, 0, 0, d};
+  }
+  s->tilesets.push_back(ts);
+  return FDTD_OK;
+}
+static const fdtd_sim::TileSet& tiles(const fdtd_sim* s, const fdtd_sim::PassCfg& c) {
+  for (const auto& t : s->tilesets)
+    if (t.ty == c.ty && t.kchunk == c.kchunk) return t;
+  return s->tilesets.front();  // unreachable: every configuration is built at create
+}
+
+// Launches one pass as its interior box (PML-free) and its edge table, the
+// edge launch on the side stream so that the two overlap; returns the
+// number of launches.
 template <typename T>
-static void launch_h_cfg(fdtd_sim* s, const fdtd_sim::PassCfg& c, cudaStream_t st) {
-  const dim3 g = pass_grid(s, c), b(32, c.ty);
-  if (c.staged) {
-#define FDTD_LAUNCH(TY, MB, S)                                                                   \
-  if (c.ty == TY && c.minb == MB && c.stages == S) {                                             \
-    h_pass_s<T, TY, S, MB><<<g, b, staged_smem<T, TY, S>(), st>>>(view<T>(s), c.kchunk);        \
-    return;                                                                                      \
+static int launch_h_cfg(fdtd_sim* s, const fdtd_sim::PassCfg& c, cudaStream_t st) {
+  const fdtd_sim::TileSet& ts = tiles(s, c);
+  const dim3 b(32, c.ty);
+#define FDTD_LAUNCH(TY, MB, S)                                                                          \
+  if (c.ty == TY && c.minb == MB && c.stages == S) {                                                    \
+    const bool fork = ts.inner.x && ts.nedge;                                                           \
+    cudaStream_t est = st;                                                                              \
+    if (fork) {                                                                                         \
+      cudaEventRecord(s->fork_ev, st);                                                                  \
+      cudaStreamWaitEvent(s->side, s->fork_ev, 0);                                                      \
+      est = s->side;                                                                                    \
+    }                                                                                                   \
+    if (ts.nedge)                                                                                       \
+      h_pass_s<T, TY, S, MB, true><<<ts.nedge, b, staged_smem<T, TY, S>(), est>>>(view<T>(s), c.kchunk, \
+                                                                                   ts.edge_map);       \
+    if (ts.inner.x)                                                                                     \
+      h_pass_s<T, TY, S, MB, false><<<ts.inner, b, staged_smem<T, TY, S>(), st>>>(view<T>(s), c.kchunk, \
+                                                                                   ts.inner_map);      \
+    if (fork) {                                                                                         \
+      cudaEventRecord(s->join_ev, s->side);                                                             \
+      cudaStreamWaitEvent(st, s->join_ev, 0);                                                           \
+    }                                                                                                   \
+    return (ts.inner.x ? 1 : 0) + (ts.nedge ? 1 : 0);                                                   \
   }
-    FDTD_STAGED_VARIANTS(FDTD_LAUNCH)
+  FDTD_STAGED_VARIANTS(FDTD_LAUNCH)
 #undef FDTD_LAUNCH
-  }
+  return 0;
 }
 template <typename T>
-static void launch_e_cfg(fdtd_sim* s, const fdtd_sim::PassCfg& c, cudaStream_t st) {
-  const dim3 g = pass_grid(s, c), b(32, c.ty);
-  if (c.staged) {
-#define FDTD_LAUNCH(TY, MB, S)                                                                   \
-  if (c.ty == TY && c.minb == MB && c.stages == S) {                                             \
-    e_pass_s<T, TY, S, MB><<<g, b, staged_smem<T, TY, S>(), st>>>(view<T>(s), c.kchunk);        \
-    return;                                                                                      \
+static int launch_e_cfg(fdtd_sim* s, const fdtd_sim::PassCfg& c, cudaStream_t st) {
+  const fdtd_sim::TileSet& ts = tiles(s, c);
+  const dim3 b(32, c.ty);
+#define FDTD_LAUNCH(TY, MB, S)                                                                          \
+  if (c.ty == TY && c.minb == MB && c.stages == S) {                                                    \
+    const bool fork = ts.inner.x && ts.nedge;                                                           \
+    cudaStream_t est = st;                                                                              \
+    if (fork) {                                                                                         \
+      cudaEventRecord(s->fork_ev, st);                                                                  \
+      cudaStreamWaitEvent(s->side, s->fork_ev, 0);                                                      \
+      est = s->side;                                                                                    \
+    }                                                                                                   \
+    if (ts.nedge)                                                                                       \
+      e_pass_s<T, TY, S, MB, true><<<ts.nedge, b, staged_smem<T, TY, S>(), est>>>(view<T>(s), c.kchunk, \
+                                                                                   ts.edge_map);       \
+    if (ts.inner.x)                                                                                     \
+      e_pass_s<T, TY, S, MB, false><<<ts.inner, b, staged_smem<T, TY, S>(), st>>>(view<T>(s), c.kchunk, \
+                                                                                   ts.inner_map);      \
+    if (fork) {                                                                                         \
+      cudaEventRecord(s->join_ev, s->side);                                                             \
+      cudaStreamWaitEvent(st, s->join_ev, 0);                                                           \
+    }                                                                                                   \
+    return (ts.inner.x ? 1 : 0) + (ts.nedge ? 1 : 0);                                                   \
   }
-    FDTD_STAGED_VARIANTS(FDTD_LAUNCH)
+  FDTD_STAGED_VARIANTS(FDTD_LAUNCH)
 #undef FDTD_LAUNCH
-  }
+  return 0;
 }
 
 // Autotuner: times every launch shape of the E and H passes on the zero
@@ -687,7 +785,18 @@ static fdtd_status tune_passes(fdtd_sim* s) {
       def.ty = ty; def.minb = mb; def.kchunk = kc; def.stages = sg;
     }
   }
+  {
+    bool known = false;
+#define FDTD_KNOWN(TY, MB, S) known = known || (def.ty == TY && def.minb == MB && def.stages == S);
+    FDTD_STAGED_VARIANTS(FDTD_KNOWN)
+#undef FDTD_KNOWN
+    if (!known || def.kchunk < 1) return fail(FDTD_ERR_INVALID, "FDTD_PASS names a pass variant that is not built");
+  }
   s->hcfg = s->ecfg = def;
+  {
+    const fdtd_status st = build_tiles(s, def.ty, def.kchunk);
+    if (st != FDTD_OK) return st;
+  }
   const char* env = std::getenv("FDTD_TUNE");
   if ((env && env[0] == '0') || force || s->ncell < (size_t)(1 << 18)) {
     s->tuned = true;
@@ -699,15 +808,18 @@ static fdtd_status tune_passes(fdtd_sim* s) {
   const char* venv = std::getenv("FDTD_TUNE_VERBOSE");
   const bool verbose = venv && venv[0] == '1';
   std::vector<fdtd_sim::PassCfg> cands;
-  const int variants[][3] = {{4, 1, 4}, {4, 6, 4}, {4, 8, 4}, {8, 3, 4}, {8, 4, 4},
-                              {4, 6, 6}, {4, 8, 6}, {8, 3, 6}, {8, 2, 6}};
+  const int variants[][3] = {{4, 1, 4}, {4, 6, 4}, {4, 8, 4}, {8, 3, 4}, {4, 6, 6}};
   for (const auto& v : variants)
     for (int kc : {8, 16, 32}) {
       fdtd_sim::PassCfg c;
       c.staged = 1; c.ty = v[0]; c.minb = v[1]; c.stages = v[2]; c.kchunk = kc;
       // skip variants whose shared memory does not fit (FP64 at depth 6)
       const size_t sm = sizeof(T) * (size_t)c.stages * (c.ty == 4 ? StageLayout<T, 4>::STAGE : StageLayout<T, 8>::STAGE);
-      if (kc <= 2 * s->NZ && sm * std::max(1, c.minb) <= 220 * 1024) cands.push_back(c);
+      if (kc <= 2 * s->NZ && sm * std::max(1, c.minb) <= 220 * 1024) {
+        const fdtd_status st = build_tiles(s, c.ty, c.kchunk);
+        if (st != FDTD_OK) return st;
+        cands.push_back(c);
+      }
     }
   for (int pass = 0; pass < 2; pass++) {
     fdtd_sim::PassCfg best;
@@ -740,7 +852,7 @@ static fdtd_status tune_passes(fdtd_sim* s) {
 
 template <typename T>
 static void launch_h(fdtd_sim* s, cudaStream_t st) {
-  launch_h_cfg<T>(s, s->hcfg, st);
+  s->kernels += launch_h_cfg<T>(s, s->hcfg, st) - 1;
   const SimView<T>* dv = static_cast<const SimView<T>*>(s->dview);
   const long long nf = s->shell_h.total();
   if (nf > 0) tfsf_h_faces<T><<<(unsigned)((nf + 255) / 256), 256, 0, st>>>(dv, s->shell_h);
@@ -761,7 +873,7 @@ static void launch_e(fdtd_sim* s, cudaStream_t st) {
   // E half of CORRECT_* before the update (main.cu:2798-2813)
   if (nf > 0) tfsf_e_faces<T><<<(unsigned)((nf + 255) / 256), 256, 0, st>>>(dv, s->shell_e);
   if (s->su.hydro) launch_metal<T>(s, st);  // UpdateHydroP* read E^n here
-  launch_e_cfg<T>(s, s->ecfg, st);
+  s->kernels += launch_e_cfg<T>(s, s->ecfg, st) - 1;
   if (!s->su.hydro) launch_metal<T>(s, st);
   s->kernels += 1 + (nf > 0);
 }
@@ -916,11 +1028,8 @@ extern "C" fdtd_status fdtd_spectral_accumulate(fdtd_sim* s, void* stream) {
 }
 
 template <typename T>
-static void launch_one(fdtd_sim* s, int which, cudaStream_t st) {
-  switch (which) {
-    case FDTD_KERNEL_H_PASS: launch_h_cfg<T>(s, s->hcfg, st); break;
-    case FDTD_KERNEL_E_PASS: launch_e_cfg<T>(s, s->ecfg, st); break;
-  }
+static int launch_one(fdtd_sim* s, int which, cudaStream_t st) {
+  return which == FDTD_KERNEL_H_PASS ? launch_h_cfg<T>(s, s->hcfg, st) : launch_e_cfg<T>(s, s->ecfg, st);
 }
 
 extern "C" fdtd_status fdtd_time_kernel(fdtd_sim* s, int which, int reps, void* stream, double* ms) {
@@ -932,11 +1041,11 @@ extern "C" fdtd_status fdtd_time_kernel(fdtd_sim* s, int which, int reps, void* 
   CUDA_TRY(cudaEventCreate(&a));
   CUDA_TRY(cudaEventCreate(&b));
   for (int r = 0; r < 2; r++) {  // warm-up
-    if (s->fp64) launch_one<double>(s, which, st); else launch_one<float>(s, which, st);
+    s->kernels += s->fp64 ? launch_one<double>(s, which, st) : launch_one<float>(s, which, st);
   }
   cudaEventRecord(a, st);
   for (int r = 0; r < reps; r++) {
-    if (s->fp64) launch_one<double>(s, which, st); else launch_one<float>(s, which, st);
+    s->kernels += s->fp64 ? launch_one<double>(s, which, st) : launch_one<float>(s, which, st);
   }
   cudaEventRecord(b, st);
   cudaError_t e = cudaEventSynchronize(b);
@@ -945,7 +1054,6 @@ extern "C" fdtd_status fdtd_time_kernel(fdtd_sim* s, int which, int reps, void* 
   cudaEventDestroy(a);
   cudaEventDestroy(b);
   if (e != cudaSuccess) return fail(FDTD_ERR_CUDA, cudaGetErrorString(e));
-  s->kernels += reps + 2;
   *ms = (double)t / reps;
   return FDTD_OK;
 }

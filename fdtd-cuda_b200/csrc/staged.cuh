@@ -74,6 +74,24 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
 
+// Which tile a CTA of a pass owns: a box launch (grid = box of tiles,
+// origin added) or a table launch (one (bx, by, bz) entry per CTA).  The
+// passes are launched twice per half step: the interior box, whose tiles
+// touch no CPML slab and use the PML-free instantiation, and the table of
+// the remaining tiles.
+struct TileMap {
+  int ox, oy, oz;
+  const int4* table;
+};
+__device__ __forceinline__ void tile_of(const TileMap& tm, int& bx, int& by, int& bz) {
+  if (tm.table) {
+    const int4 t = tm.table[blockIdx.x];
+    bx = t.x; by = t.y; bz = t.z;
+  } else {
+    bx = tm.ox + (int)blockIdx.x; by = tm.oy + (int)blockIdx.y; bz = tm.oz + (int)blockIdx.z;
+  }
+}
+
 template <typename T, int TY>
 struct StageLayout {
   static constexpr int CH = 16 / (int)sizeof(T);   // elements per 16-byte chunk
@@ -167,19 +185,22 @@ struct CopyTasks {
 // hy: z then x; hz: x then y).  The stage ring is counted from the chunk's
 // first plane and the plane loop is unrolled by S, so every stage offset is
 // a compile-time constant.
-template <typename T, int TY, int S, int MINB>
-__global__ void __launch_bounds__(32 * TY, MINB) h_pass_s(const __grid_constant__ SimView<T> s, int kchunk) {
+template <typename T, int TY, int S, int MINB, bool PML>
+__global__ void __launch_bounds__(32 * TY, MINB) h_pass_s(const __grid_constant__ SimView<T> s, int kchunk,
+                                                      const __grid_constant__ TileMap tm) {
   using L = StageLayout<T, TY>;
   constexpr unsigned SB = L::STAGE * sizeof(T);  // stage bytes
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const T* sm = reinterpret_cast<const T*>(smem_raw);
   const unsigned sbase = (unsigned)__cvta_generic_to_shared(smem_raw);
   const int tx = threadIdx.x, ty = threadIdx.y;
-  const int i0 = blockIdx.x * 32, j0 = blockIdx.y * TY;
+  int bx, by, bz;
+  tile_of(tm, bx, by, bz);
+  const int i0 = bx * 32, j0 = by * TY;
   const int i = i0 + tx, j = j0 + ty;
   const int NX = s.NX, NY = s.NY, NZ = s.NZ, PX = s.PX;
   const size_t plane = s.plane;
-  const int k0 = blockIdx.z * kchunk;
+  const int k0 = bz * kchunk;
   const int k1 = min(NZ, k0 + kchunk);
   const T* any = s.E[0];
   CopyTasks<T, TY> tasks;
@@ -203,7 +224,7 @@ __global__ void __launch_bounds__(32 * TY, MINB) h_pass_s(const __grid_constant_
   const int o = ty * L::HW + tx, oo = ty * 32 + tx;
   constexpr int FH = (TY + 1) * L::HW;  // one halo component
   // CPML of this column: x and y slabs are fixed, z slabs follow the plane
-  const bool pml_xy = live && hasx && hasy;  // i < NX-1 and j < NY-1
+  const bool pml_xy = PML && live && hasx && hasy;  // i < NX-1 and j < NY-1
   SlabAt<T> sx, sy;
   sx.side = sy.side = 0; sx.q = sy.q = 0; sx.b = sx.c = sy.b = sy.c = T(0);
   if (pml_xy) { sx = slab_h(s.cp[0], i); sy = slab_h(s.cp[1], j); }
@@ -310,19 +331,22 @@ __global__ void __launch_bounds__(32 * TY, MINB) h_pass_s(const __grid_constant_
 // kernels update them, CPML included); dielectric classes select their
 // coefficients.  CPML per axis in the order z, y, x (ex: z then y; ey: z
 // then x; ez: y then x).  The stage ring is counted from plane k0-1.
-template <typename T, int TY, int S, int MINB>
-__global__ void __launch_bounds__(32 * TY, MINB) e_pass_s(const __grid_constant__ SimView<T> s, int kchunk) {
+template <typename T, int TY, int S, int MINB, bool PML>
+__global__ void __launch_bounds__(32 * TY, MINB) e_pass_s(const __grid_constant__ SimView<T> s, int kchunk,
+                                                      const __grid_constant__ TileMap tm) {
   using L = StageLayout<T, TY>;
   constexpr unsigned SB = L::STAGE * sizeof(T);
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const T* sm = reinterpret_cast<const T*>(smem_raw);
   const unsigned sbase = (unsigned)__cvta_generic_to_shared(smem_raw);
   const int tx = threadIdx.x, ty = threadIdx.y;
-  const int i0 = blockIdx.x * 32, j0 = blockIdx.y * TY;
+  int bx, by, bz;
+  tile_of(tm, bx, by, bz);
+  const int i0 = bx * 32, j0 = by * TY;
   const int i = i0 + tx, j = j0 + ty;
   const int NX = s.NX, NY = s.NY, NZ = s.NZ, PX = s.PX;
   const size_t plane = s.plane;
-  const int k0 = blockIdx.z * kchunk;
+  const int k0 = bz * kchunk;
   const int k1 = min(NZ, k0 + kchunk);
   const T* any = s.H[0];
   CopyTasks<T, TY> tasks;
@@ -352,7 +376,7 @@ __global__ void __launch_bounds__(32 * TY, MINB) e_pass_s(const __grid_constant_
   const int o = (ty + 1) * L::HW + tx + L::CH, oo = ty * 32 + tx;
   constexpr int FH = (TY + 1) * L::HW;
   // CPML of this column: x and y slabs are fixed, z slabs follow the plane
-  const bool pml_xy = live && okx && oky;  // i < NX-1 and j < NY-1
+  const bool pml_xy = PML && live && okx && oky;  // i < NX-1 and j < NY-1
   SlabAt<T> sx, sy;
   sx.side = sy.side = 0; sx.q = sy.q = 0; sx.b = sx.c = sy.b = sy.c = T(0);
   T cx_ey = T(0);

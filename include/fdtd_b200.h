@@ -318,11 +318,11 @@ typedef struct fdtd_stats {
   int h_stages, e_stages;  /* its ring depth */
 } fdtd_stats;
 fdtd_status fdtd_get_stats(const fdtd_sim* s, fdtd_stats* out);
-/* Measurement hook (no counterpart in the reference): launches one kernel
- * of the time step reps times back to back (after two untimed launches) on
- * `stream` and stores its mean device time per launch, from CUDA events on
- * that stream, in *ms.  The launches change the fields: call fdtd_reset
- * before using the simulation again. */
+/* Measurement hook (no counterpart in the reference): runs one Yee pass
+ * (its interior-tile and CPML-edge-tile launches) reps times back to back,
+ * after two untimed runs, on `stream` and stores its mean device time per
+ * pass, from CUDA events on that stream, in *ms.  The runs change the
+ * fields: call fdtd_reset before using the simulation again. */
 enum {
   FDTD_KERNEL_H_PASS = 0, /* the H pass (Yee + CPML) over the whole grid */
   FDTD_KERNEL_E_PASS = 1  /* the E pass (Yee + CPML) over the whole grid,

@@ -186,7 +186,7 @@ def test_pass_variants_agree(prec, monkeypatch):
     register cap, ring depth) change data movement only: fields agree to
     rounding."""
     out = []
-    for spec in ("staged:4:1:16:4", "staged:8:3:8:6", "staged:4:8:32:4"):
+    for spec in ("staged:4:1:16:4", "staged:8:3:8:4", "staged:4:6:32:6"):
         monkeypatch.setenv("FDTD_PASS", spec)
         s = run_sim("cube_ag", 200, prec)
         st = s.stats()
@@ -195,3 +195,10 @@ def test_pass_variants_agree(prec, monkeypatch):
     for other in out[1:]:
         errs = field_errors(other, out[0])
         assert max(errs) < (1e-13 if prec == F.FDTD_FP64 else 1e-5), errs
+
+
+def test_unbuilt_pass_variant_is_rejected(monkeypatch):
+    monkeypatch.setenv("FDTD_PASS", "staged:8:5:16:4")
+    with pytest.raises(F.FdtdError) as e:
+        F.Sim(make(F, "vacuum", precision=F.FDTD_FP32))
+    assert e.value.status == 1 and "not built" in str(e.value)
