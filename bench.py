@@ -173,6 +173,74 @@ def cpu_sample(steps=8):
                       f"{dt:.1f} s"}
 
 
+BATCH_SEED = 20261203
+
+
+def batch_members(mod, n=64, steps=3000, seed=BATCH_SEED):
+    """The batched workload: n independent gold-sphere simulations, cubic
+    grids with total edges drawn uniformly from 48..128 cells, dx = 2 nm,
+    Drude+2CP gold, 10-cell CPML, TFSF pulse centred at 600 nm, 51
+    wavelengths 400-900 nm, FP32.  Sphere radii are drawn from 5-25 nm and
+    clamped so that the sphere stays inside the absorption box of the grid
+    (a TFSF inset of 4 and a box offset of 2 cells keep the smallest grids
+    usable)."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        edge = int(rng.integers(48, 129))
+        r_nm = float(rng.uniform(5.0, 25.0))
+        half_box = (edge - 2 * (10 + 4 + 2)) / 2.0  # cells from the centre to the abs box
+        r_nm = min(r_nm, 2.0 * (half_box - 1.5))
+        n_in = edge - 2 * 10 - 1
+        out.append(mod.default_params(
+            Tend=steps - 1, dx=2e-9, dy=2e-9, dz=2e-9, NCELLX=n_in, NCELLY=n_in, NCELLZ=n_in,
+            NcpmlX=10, NcpmlY=10, NcpmlZ=10, nano_sphere=1, nano_sphere_radius=r_nm * 1e-9,
+            material=3, first_medium=1, NUM_freq=51, WL_or_freq=1, lam_min=400e-9,
+            lam_max=900e-9, lam_0=600e-9, BandWidth=3e15, tfsf_inset=4, box_offset=2,
+            cpml_kappa_max=1.0, precision=mod.FDTD_FP32))
+    return out
+
+
+def batch_bench(mod, torch, stream, sp, dev, n, steps):
+    """sims/s of the batched path (fdtd_batch_run: all members in one
+    persistent pass kernel per half step) against the same members run one
+    after another with fdtd_run, both timed with CUDA events on one stream;
+    creation is outside both timed regions."""
+    params = batch_members(mod, n, steps)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    b = mod.Batch(params, device=dev)
+    torch.cuda.synchronize()
+    ev[0].record(stream)
+    b.run(sp)
+    ev[1].record(stream)
+    torch.cuda.synchronize()
+    t_batch = ev[0].elapsed_time(ev[1]) / 1e3
+    launches = b.stats()[0]
+    for i in range(n):
+        b.sim(i).check()
+    cells = sum(p.NCELLX + 21 for p in params)
+    b.close()
+    t_seq = 0.0
+    for p in params:
+        s = mod.Sim(p, device=dev)
+        torch.cuda.synchronize()
+        ev[0].record(stream)
+        s.run(sp)
+        ev[1].record(stream)
+        torch.cuda.synchronize()
+        t_seq += ev[0].elapsed_time(ev[1]) / 1e3
+        s.check()
+        s.close()
+    edges = [p.NCELLX + 21 for p in params]
+    total = sum(e ** 3 for e in edges) * steps
+    return {"sims_per_s": round(n / t_batch, 3), "sequential_sims_per_s": round(n / t_seq, 3),
+            "speedup": round(t_seq / t_batch, 2), "members": n, "time_steps": steps,
+            "batched_s": round(t_batch, 3), "sequential_s": round(t_seq, 3),
+            "batched_gcell_steps_per_s": round(total / t_batch / 1e9, 2),
+            "edges": [min(edges), max(edges)], "seed": BATCH_SEED, "gpu_launches": launches}
+
+
 def ref_deck_case(tend):
     """The reference-geometry deck used to time the reference's own CUDA
     build beside this one: the 256^3 grid of the workload (12-cell CPML,
@@ -261,6 +329,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--grid", type=int, default=256, help="smaller grids for ncu captures")
     ap.add_argument("--num-freq", type=int, default=201)
+    ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--batch-members", type=int, default=64)
+    ap.add_argument("--batch-steps", type=int, default=3000)
     ap.add_argument("--no-ref-gpu", action="store_true",
                     help="reference arm: skip timing the reference's own CUDA build")
     args = ap.parse_args()
@@ -427,6 +498,10 @@ def main():
                                   / (msr / 1e3) / 1e9, 3)
             sm.close()
 
+    batched = None
+    if not args.no_batch and args.grid == 256:
+        batched = batch_bench(F, torch, stream, sp, dev, args.batch_members, args.batch_steps)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu and args.grid == 256:
         cpu = cpu_sample()
@@ -446,7 +521,7 @@ def main():
                        "parallelism": f"replicas x{world}"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "clocks": clk.summary(), "gpu_launches": launches, "fp64": fp64,
-            "reference_deck": refdeck,
+            "reference_deck": refdeck, "batched": batched,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -50,10 +50,9 @@ struct ShellCells {
 };
 
 template <typename T>
-__global__ void tfsf_h_faces(const SimView<T>* __restrict__ gv, const ShellCells sh) {
+__device__ __forceinline__ void tfsf_h_faces_body(const SimView<T>& g, const ShellCells& sh) {
   const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= sh.total()) return;
-  const SimView<T>& g = *gv;
   int i, j, k;
   sh.cell(q, i, j, k);
   const size_t id = fidx(g.PX, g.plane, i, j, k);
@@ -62,12 +61,15 @@ __global__ void tfsf_h_faces(const SimView<T>* __restrict__ gv, const ShellCells
     g.H[c][id] = tfsf_h(g, c, i, j, k, g.H[c][id]);
   }
 }
+template <typename T>
+__global__ void tfsf_h_faces(const SimView<T>* __restrict__ gv, const ShellCells sh) {
+  tfsf_h_faces_body(*gv, sh);
+}
 
 template <typename T>
-__global__ void tfsf_e_faces(const SimView<T>* __restrict__ gv, const ShellCells sh) {
+__device__ __forceinline__ void tfsf_e_faces_body(const SimView<T>& g, const ShellCells& sh) {
   const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= sh.total()) return;
-  const SimView<T>& g = *gv;
   int i, j, k;
   sh.cell(q, i, j, k);
   const size_t id = fidx(g.PX, g.plane, i, j, k);
@@ -80,6 +82,10 @@ __global__ void tfsf_e_faces(const SimView<T>* __restrict__ gv, const ShellCells
   for (int c = 0; c < 3; c++) {
     g.E[c][id] = tfsf_e(g, c, i, j, k, g.E[c][id], ceh);
   }
+}
+template <typename T>
+__global__ void tfsf_e_faces(const SimView<T>* __restrict__ gv, const ShellCells sh) {
+  tfsf_e_faces_body(*gv, sh);
 }
 
 }  // namespace fdtd

@@ -392,9 +392,9 @@ static fdtd_status build_views(fdtd_sim* s) {
 }
 
 template <typename T>
-static fdtd_status tune_passes(fdtd_sim* s);
+static fdtd_status tune_passes(fdtd_sim* s, bool time_variants);
 
-static fdtd_status create_impl(const fdtd_params* p, int device, fdtd_sim** out) {
+static fdtd_status create_impl(const fdtd_params* p, int device, fdtd_sim** out, bool tune = true) {
   auto s = std::make_unique<fdtd_sim>();
   if (const char* msg = setup_build(*p, s->su)) return fail(FDTD_ERR_INVALID, msg);
   const Setup& su = s->su;
@@ -574,7 +574,7 @@ static fdtd_status create_impl(const fdtd_params* p, int device, fdtd_sim** out)
   CUDA_TRY(cudaEventCreateWithFlags(&s->fork_ev, cudaEventDisableTiming));
   CUDA_TRY(cudaEventCreateWithFlags(&s->join_ev, cudaEventDisableTiming));
   CUDA_TRY(cudaDeviceSynchronize());
-  st = s->fp64 ? tune_passes<double>(s.get()) : tune_passes<float>(s.get());
+  st = s->fp64 ? tune_passes<double>(s.get(), tune) : tune_passes<float>(s.get(), tune);
   if (st != FDTD_OK) return st;
   *out = s.release();
   return FDTD_OK;
@@ -770,7 +770,7 @@ static int launch_e_cfg(fdtd_sim* s, const fdtd_sim::PassCfg& c, cudaStream_t st
 // fastest.  Shapes: minimum CTAs per SM (register cap) x tile height x
 // z-chunk.  FDTD_TUNE=0 keeps the defaults.
 template <typename T>
-static fdtd_status tune_passes(fdtd_sim* s) {
+static fdtd_status tune_passes(fdtd_sim* s, bool time_variants) {
   staged_attributes<T>();
   // defaults; FDTD_PASS=staged:TY:MINB:KCHUNK[:STAGES] forces a variant,
   // FDTD_TUNE=0 skips the timing, small grids are not worth timing
@@ -798,7 +798,7 @@ static fdtd_status tune_passes(fdtd_sim* s) {
     if (st != FDTD_OK) return st;
   }
   const char* env = std::getenv("FDTD_TUNE");
-  if ((env && env[0] == '0') || force || s->ncell < (size_t)(1 << 18)) {
+  if (!time_variants || (env && env[0] == '0') || force || s->ncell < (size_t)(1 << 18)) {
     s->tuned = true;
     return FDTD_OK;
   }
@@ -1402,13 +1402,4 @@ extern "C" fdtd_status fdtd_forward(fdtd_sim*, const int*, int, int, double*) {
 extern "C" fdtd_status fdtd_backward(fdtd_sim*, float*, size_t, double*) {
   return fail(FDTD_ERR_UNSUPPORTED, "fdtd_backward is not built yet");
 }
-extern "C" fdtd_status fdtd_batch_create(const fdtd_params*, int, int, fdtd_batch**) {
-  return fail(FDTD_ERR_UNSUPPORTED, "batched simulations are not built yet");
-}
-extern "C" fdtd_status fdtd_batch_run(fdtd_batch*, void*) {
-  return fail(FDTD_ERR_UNSUPPORTED, "batched simulations are not built yet");
-}
-extern "C" fdtd_status fdtd_batch_spectra(fdtd_batch*, int, double*) {
-  return fail(FDTD_ERR_UNSUPPORTED, "batched simulations are not built yet");
-}
-extern "C" fdtd_status fdtd_batch_destroy(fdtd_batch*) { return FDTD_OK; }
+#include "batch.cuh"

@@ -325,7 +325,7 @@ struct LineArgs {
 };
 
 template <typename T>
-__global__ void __launch_bounds__(1024) line_step(const __grid_constant__ LineArgs a, const __grid_constant__ SimView<T> s, size_t probe_id) {
+__device__ __forceinline__ void line_step_body(const LineArgs& a, const SimView<T>& s, size_t probe_id) {
   const int t = a.clk->t;
   // probe: E after step t-1 (OUT.txt records it at the top of step t)
   if (threadIdx.x < 3 && t >= 1 && t - 1 < a.probe_cap)
@@ -357,6 +357,10 @@ __global__ void __launch_bounds__(1024) line_step(const __grid_constant__ LineAr
     }
     a.clk->t = t + 1;
   }
+}
+template <typename T>
+__global__ void __launch_bounds__(1024) line_step(const __grid_constant__ LineArgs a, const __grid_constant__ SimView<T> s, size_t probe_id) {
+  line_step_body(a, s, probe_id);
 }
 
 template <typename T>
@@ -410,7 +414,7 @@ __device__ __forceinline__ T cpml_e_all(const SimView<T>& s, int c, int i, int j
 // Non-hydrodynamic dispersive update of all three components (they do not
 // couple within a step).  pd ring: n = t%3, n-1 = (t+2)%3, new = (t+1)%3.
 template <typename T>
-__global__ void metal_e(const __grid_constant__ SimView<T> s, const __grid_constant__ MetalView<T> m, const DevClock* clk) {
+__device__ __forceinline__ void metal_e_body(const SimView<T>& s, const MetalView<T>& m, const DevClock* clk) {
   const int t = clk->t - 1;
   const int rn = t % 3, rn1 = (t + 2) % 3, rnew = (t + 1) % 3;
   int q = blockIdx.x * blockDim.x + threadIdx.x;
@@ -453,6 +457,10 @@ __global__ void metal_e(const __grid_constant__ SimView<T> s, const __grid_const
   nv = cpml_e_all(s, c, i, j, k, da, db, nv, ceh);
   if (!isfinite((double)nv)) atomicOr(s.nonfinite, 1);
   s.E[c][id] = nv;
+}
+template <typename T>
+__global__ void metal_e(const __grid_constant__ SimView<T> s, const __grid_constant__ MetalView<T> m, const DevClock* clk) {
+  metal_e_body(s, m, clk);
 }
 
 // Neighbour values of a dispersive cell for the hydrodynamic model.  nbr
@@ -641,7 +649,7 @@ struct DftView {
 };
 
 template <typename T>
-__global__ void dft_sample(const __grid_constant__ SimView<T> s, const __grid_constant__ DftView d, T* ring, const DevClock* clk) {
+__device__ __forceinline__ void dft_sample_body(const SimView<T>& s, const DftView& d, T* ring, const DevClock* clk) {
   const int slot = clk->samp_slot;
   if (slot < 0 || slot >= kSampleBlock) return;
   const int f = blockIdx.y;
@@ -663,11 +671,15 @@ __global__ void dft_sample(const __grid_constant__ SimView<T> s, const __grid_co
     }
   }
 }
+template <typename T>
+__global__ void dft_sample(const __grid_constant__ SimView<T> s, const __grid_constant__ DftView d, T* ring, const DevClock* clk) {
+  dft_sample_body(s, d, ring, clk);
+}
 
 // Phasors of the samples waiting in the ring: tw[h][s][f] = exp(i 2 pi
 // (t_s + delta_h) dt freq[f]) with delta = 1 for E (sampled after the E
 // update) and 1/2 for H (main.cu:62-76).  [2][kSampleBlock][nf] of double2.
-__global__ void dft_twiddles(const __grid_constant__ DftView d, const DevClock* clk, double2* tw) {
+__device__ __forceinline__ void dft_twiddles_body(const DftView& d, const DevClock* clk, double2* tw) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= 2 * kSampleBlock * d.nf) return;
   const int h = q / (kSampleBlock * d.nf);
@@ -681,6 +693,9 @@ __global__ void dft_twiddles(const __grid_constant__ DftView d, const DevClock* 
   }
   tw[q] = make_double2(c, sv);
 }
+__global__ void dft_twiddles(const __grid_constant__ DftView d, const DevClock* clk, double2* tw) {
+  dft_twiddles_body(d, clk, tw);
+}
 
 // acc[f][r] += sum_s x[s][r] tw[h(r)][s][f] in FP64.  A CTA owns kDftRows
 // rows (all E or all H thanks to the padding) and walks every frequency in
@@ -690,12 +705,13 @@ constexpr int kDftRows = 128;
 constexpr int kDftFreqs = 16;
 
 template <typename T>
-__global__ void __launch_bounds__(128) dft_contract(const __grid_constant__ DftView d, const T* ring,
-                                                     const DevClock* clk, const double2* tw) {
+__device__ __forceinline__ void dft_contract_body(const DftView& d, const T* ring, const DevClock* clk,
+                                                  const double2* tw) {
   __shared__ double xs[kSampleBlock][kDftRows];
   __shared__ double2 ws[kSampleBlock][kDftFreqs];
   const int nsamp = min(kSampleBlock, clk->nsamp);
   const long long r0 = (long long)blockIdx.x * kDftRows;
+  if (r0 >= d.rows) return;  // batched launches size the grid for the largest simulation
   // E or H rows: the tile lies inside one (face, component) block
   int h = 0;
   for (int f = 0; f < d.nfaces; f++) {
@@ -748,6 +764,11 @@ __global__ void __launch_bounds__(128) dft_contract(const __grid_constant__ DftV
       }
     }
   }
+}
+template <typename T>
+__global__ void __launch_bounds__(128) dft_contract(const __grid_constant__ DftView d, const T* ring,
+                                                     const DevClock* clk, const double2* tw) {
+  dft_contract_body(d, ring, clk, tw);
 }
 
 __global__ void dft_reset_count(DevClock* clk) { clk->nsamp = 0; }

@@ -185,17 +185,14 @@ struct CopyTasks {
 // hy: z then x; hz: x then y).  The stage ring is counted from the chunk's
 // first plane and the plane loop is unrolled by S, so every stage offset is
 // a compile-time constant.
-template <typename T, int TY, int S, int MINB, bool PML>
-__global__ void __launch_bounds__(32 * TY, MINB) h_pass_s(const __grid_constant__ SimView<T> s, int kchunk,
-                                                      const __grid_constant__ TileMap tm) {
+template <typename T, int TY, int S, bool PML>
+__device__ __forceinline__ void h_pass_tile(const SimView<T>& s, int kchunk, int bx, int by, int bz) {
   using L = StageLayout<T, TY>;
   constexpr unsigned SB = L::STAGE * sizeof(T);  // stage bytes
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const T* sm = reinterpret_cast<const T*>(smem_raw);
   const unsigned sbase = (unsigned)__cvta_generic_to_shared(smem_raw);
   const int tx = threadIdx.x, ty = threadIdx.y;
-  int bx, by, bz;
-  tile_of(tm, bx, by, bz);
   const int i0 = bx * 32, j0 = by * TY;
   const int i = i0 + tx, j = j0 + ty;
   const int NX = s.NX, NY = s.NY, NZ = s.NZ, PX = s.PX;
@@ -323,6 +320,32 @@ __global__ void __launch_bounds__(32 * TY, MINB) h_pass_s(const __grid_constant_
   }
   cp_async_wait<0>();
 }
+template <typename T, int TY, int S, int MINB, bool PML>
+__global__ void __launch_bounds__(32 * TY, MINB) h_pass_s(const __grid_constant__ SimView<T> s, int kchunk,
+                                                      const __grid_constant__ TileMap tm) {
+  int bx, by, bz;
+  tile_of(tm, bx, by, bz);
+  h_pass_tile<T, TY, S, PML>(s, kchunk, bx, by, bz);
+}
+
+// Batched form: a persistent grid that takes (simulation, tile) work items
+// from a queue shared by every simulation of a batch; the views live in
+// device memory, one per simulation.
+template <typename T, int TY, int S, int MINB>
+__global__ void __launch_bounds__(32 * TY, MINB) h_pass_batch(const SimView<T>* __restrict__ views,
+                                                           const int4* __restrict__ items, int nitems,
+                                                           int* __restrict__ queue, int kchunk) {
+  __shared__ int next;
+  for (;;) {
+    __syncthreads();  // the previous item is finished with the stage ring and with next
+    if (threadIdx.x == 0 && threadIdx.y == 0) next = atomicAdd(queue, 1);
+    __syncthreads();
+    const int it = next;
+    if (it >= nitems) return;
+    const int4 w = items[it];  // (simulation, bx, by, bz)
+    h_pass_tile<T, TY, S, true>(views[w.x], kchunk, w.y, w.z, w.w);
+  }
+}
 
 // ---------------------------------------------------------------------
 // E pass (UPDATE_ex/ey/ez, main.cu:1048-1912).
@@ -331,17 +354,14 @@ __global__ void __launch_bounds__(32 * TY, MINB) h_pass_s(const __grid_constant_
 // kernels update them, CPML included); dielectric classes select their
 // coefficients.  CPML per axis in the order z, y, x (ex: z then y; ey: z
 // then x; ez: y then x).  The stage ring is counted from plane k0-1.
-template <typename T, int TY, int S, int MINB, bool PML>
-__global__ void __launch_bounds__(32 * TY, MINB) e_pass_s(const __grid_constant__ SimView<T> s, int kchunk,
-                                                      const __grid_constant__ TileMap tm) {
+template <typename T, int TY, int S, bool PML>
+__device__ __forceinline__ void e_pass_tile(const SimView<T>& s, int kchunk, int bx, int by, int bz) {
   using L = StageLayout<T, TY>;
   constexpr unsigned SB = L::STAGE * sizeof(T);
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const T* sm = reinterpret_cast<const T*>(smem_raw);
   const unsigned sbase = (unsigned)__cvta_generic_to_shared(smem_raw);
   const int tx = threadIdx.x, ty = threadIdx.y;
-  int bx, by, bz;
-  tile_of(tm, bx, by, bz);
   const int i0 = bx * 32, j0 = by * TY;
   const int i = i0 + tx, j = j0 + ty;
   const int NX = s.NX, NY = s.NY, NZ = s.NZ, PX = s.PX;
@@ -494,6 +514,32 @@ __global__ void __launch_bounds__(32 * TY, MINB) e_pass_s(const __grid_constant_
   cp_async_wait<0>();
   // NaN/Inf watchdog: a non-finite value makes the running sum non-finite
   if (!isfinite(check)) atomicOr(s.nonfinite, 1);
+}
+template <typename T, int TY, int S, int MINB, bool PML>
+__global__ void __launch_bounds__(32 * TY, MINB) e_pass_s(const __grid_constant__ SimView<T> s, int kchunk,
+                                                      const __grid_constant__ TileMap tm) {
+  int bx, by, bz;
+  tile_of(tm, bx, by, bz);
+  e_pass_tile<T, TY, S, PML>(s, kchunk, bx, by, bz);
+}
+
+// Batched form: a persistent grid that takes (simulation, tile) work items
+// from a queue shared by every simulation of a batch; the views live in
+// device memory, one per simulation.
+template <typename T, int TY, int S, int MINB>
+__global__ void __launch_bounds__(32 * TY, MINB) e_pass_batch(const SimView<T>* __restrict__ views,
+                                                           const int4* __restrict__ items, int nitems,
+                                                           int* __restrict__ queue, int kchunk) {
+  __shared__ int next;
+  for (;;) {
+    __syncthreads();  // the previous item is finished with the stage ring and with next
+    if (threadIdx.x == 0 && threadIdx.y == 0) next = atomicAdd(queue, 1);
+    __syncthreads();
+    const int it = next;
+    if (it >= nitems) return;
+    const int4 w = items[it];  // (simulation, bx, by, bz)
+    e_pass_tile<T, TY, S, true>(views[w.x], kchunk, w.y, w.z, w.w);
+  }
 }
 
 }  // namespace fdtd

@@ -14,7 +14,7 @@ from ._abi import (FACE_COMPONENTS, FDTD_FP32, FDTD_FP64, FDTD_KERNEL_E_PASS,
                    FIX_CE_EY_XN, FIX_HYDRO_CBRT, GEOM_DISK_ARRAY, GEOM_REFERENCE, GEOM_ROD_DIMER,
                    GEOM_SPHERE, STATUS, Dims, Params, Stats)
 
-__all__ = ["Params", "Dims", "Sim", "FdtdError", "lib", "default_params", "load_input_txt",
+__all__ = ["Params", "Dims", "Sim", "Batch", "FdtdError", "lib", "default_params", "load_input_txt",
            "FDTD_FP32", "FDTD_FP64", "GEOM_REFERENCE", "GEOM_ROD_DIMER", "GEOM_DISK_ARRAY",
            "GEOM_SPHERE", "FIX_BH_X_F", "FIX_CE_EY_XN", "FIX_HYDRO_CBRT", "FACE_COMPONENTS",
            "FDTD_KERNEL_H_PASS", "FDTD_KERNEL_E_PASS"]
@@ -32,6 +32,7 @@ EXPORTS = [
     "fdtd_get_field", "fdtd_set_field", "fdtd_snapshot_plane", "fdtd_get_probe",
     "fdtd_get_material", "fdtd_set_design", "fdtd_forward", "fdtd_backward",
     "fdtd_batch_create", "fdtd_batch_run", "fdtd_batch_spectra", "fdtd_batch_destroy",
+    "fdtd_batch_step", "fdtd_batch_sim", "fdtd_batch_get_stats",
     "fdtd_plan", "fdtd_rasterise", "fdtd_coefficients", "fdtd_get_probe_range",
     "fdtd_set_source", "fdtd_get_stats", "fdtd_time_kernel",
 ]
@@ -89,6 +90,9 @@ def lib():
         "fdtd_batch_run": (C.c_int, [vp, vp]),
         "fdtd_batch_spectra": (C.c_int, [vp, C.c_int, dp]),
         "fdtd_batch_destroy": (C.c_int, [vp]),
+        "fdtd_batch_step": (C.c_int, [vp, C.c_int, vp]),
+        "fdtd_batch_sim": (C.c_int, [vp, C.c_int, P(vp)]),
+        "fdtd_batch_get_stats": (C.c_int, [vp, P(C.c_longlong), P(C.c_longlong)]),
         "fdtd_plan": (C.c_int, [P(Params), P(Dims)]),
         "fdtd_rasterise": (C.c_int, [P(Params), P(C.c_ubyte), sz]),
         "fdtd_coefficients": (C.c_int, [P(Params), C.c_int, dp, sz, P(sz)]),
@@ -159,10 +163,14 @@ def write_input_txt(path, p):
 class Sim:
     """One simulation on one GPU (the reference's whole program state)."""
 
-    def __init__(self, params, device=0):
-        h = C.c_void_p()
-        _check(lib().fdtd_create(C.byref(params), device, C.byref(h)))
+    def __init__(self, params, device=0, _handle=None, _owner=None):
+        if _handle is None:
+            h = C.c_void_p()
+            _check(lib().fdtd_create(C.byref(params), device, C.byref(h)))
+        else:
+            h = _handle  # a batch member: borrowed, the batch frees it
         self.h = h
+        self._owner = _owner
         self.params = params
         d = Dims()
         _check(lib().fdtd_get_dims(self.h, C.byref(d)))
@@ -171,7 +179,8 @@ class Sim:
 
     def close(self):
         if getattr(self, "h", None):
-            lib().fdtd_destroy(self.h)
+            if self._owner is None:
+                lib().fdtd_destroy(self.h)
             self.h = None
 
     def __del__(self):
@@ -299,3 +308,50 @@ class Sim:
         im = np.empty(self.dims.num_freq)
         _check(lib().fdtd_get_incident(self.h, _dp(re), _dp(im), re.size))
         return re + 1j * im
+
+
+class Batch:
+    """Independent simulations advanced together (fdtd_batch_*): the Yee
+    passes of all members share one persistent kernel per half step."""
+
+    def __init__(self, params_list, device=0):
+        self.params = list(params_list)
+        arr = (Params * len(self.params))(*self.params)
+        h = C.c_void_p()
+        _check(lib().fdtd_batch_create(arr, len(self.params), device, C.byref(h)))
+        self.h = h
+        self.n = len(self.params)
+
+    def step(self, n=1, stream=None):
+        _check(lib().fdtd_batch_step(self.h, int(n), stream))
+
+    def run(self, stream=None):
+        _check(lib().fdtd_batch_run(self.h, stream))
+
+    def sim(self, idx):
+        """Member idx as a Sim view (borrowed: valid while the batch lives)."""
+        h = C.c_void_p()
+        _check(lib().fdtd_batch_sim(self.h, int(idx), C.byref(h)))
+        return Sim(self.params[idx], _handle=h, _owner=self)
+
+    def spectra(self, idx):
+        d = self.sim(idx).dims
+        out = np.empty((d.num_freq, 19))
+        _check(lib().fdtd_batch_spectra(self.h, int(idx), _dp(out)))
+        return out
+
+    def stats(self):
+        k, g = C.c_longlong(), C.c_longlong()
+        _check(lib().fdtd_batch_get_stats(self.h, C.byref(k), C.byref(g)))
+        return k.value, g.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().fdtd_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

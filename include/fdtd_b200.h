@@ -356,12 +356,26 @@ fdtd_status fdtd_backward(fdtd_sim* s, float* dL_drho, size_t count,
  * trials loop, main.cu:2435, is sequential)                               */
 
 typedef struct fdtd_batch fdtd_batch;
+/* n independent simulations on one device, each from its own parameters
+ * (grid sizes may differ); all members share precision, the hydrodynamic
+ * switch, the DFT sampling period and Tend. */
 fdtd_status fdtd_batch_create(const fdtd_params* ps, int n, int device,
                               fdtd_batch** out);
-/* Runs every sim to its Tend in one persistent kernel per step group,
- * launched from CUDA graphs. */
+/* Advances every member by nsteps.  Per time step the two Yee passes of
+ * all members run as one persistent kernel each, fed from a shared
+ * (member, tile) work queue, and every other kernel of the step runs as one
+ * launch over all members; runs of 32*dft_every steps replay a CUDA graph. */
+fdtd_status fdtd_batch_step(fdtd_batch* b, int nsteps, void* stream);
+/* Runs every member to Tend (fdtd_batch_step with the remaining steps). */
 fdtd_status fdtd_batch_run(fdtd_batch* b, void* stream);
+/* Member idx as a borrowed simulation handle (fields, probes, spectra);
+ * owned by the batch, valid until fdtd_batch_destroy. */
+fdtd_status fdtd_batch_sim(fdtd_batch* b, int idx, fdtd_sim** out);
+/* The 19-column ScatAbs table of member idx (fdtd_spectral_finalize). */
 fdtd_status fdtd_batch_spectra(fdtd_batch* b, int idx, double* out19);
+/* Kernel launches and graph replays issued by the batch so far. */
+fdtd_status fdtd_batch_get_stats(const fdtd_batch* b, long long* kernels,
+                                 long long* graph_launches);
 fdtd_status fdtd_batch_destroy(fdtd_batch* b);
 
 #ifdef __cplusplus

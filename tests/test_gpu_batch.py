@@ -1,0 +1,85 @@
+"""Batched simulations (fdtd_batch_*) against the same members run one at a
+time through fdtd_step: the batch changes scheduling only, so fields,
+probes and spectra agree to rounding."""
+import numpy as np
+import pytest
+
+import fdtd_b200 as F
+from cases import make
+
+pytestmark = pytest.mark.gpu
+
+MEMBERS = [("sphere_au", {}), ("vacuum", dict(NCELLX=27, NCELLY=23, NCELLZ=19)),
+           ("sphere_au", dict(NCELLX=31, NCELLY=31, NCELLZ=37, nano_sphere_radius=10e-9)),
+           ("cube_ag", {})]
+
+
+def rel(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def family_errors(sa, sb):
+    """Max error of E and of H, each relative to its family's peak."""
+    out = []
+    for fam in ((0, 1, 2), (3, 4, 5)):
+        a = [sa.field(c) for c in fam]
+        b = [sb.field(c) for c in fam]
+        scale = max(np.abs(x).max() for x in b)
+        out.append(max(float(np.abs(x - y).max()) for x, y in zip(a, b)) / scale)
+    return out
+
+
+@pytest.mark.parametrize("prec", [F.FDTD_FP32, F.FDTD_FP64])
+def test_batch_matches_sequential(prec):
+    params = [make(F, name, precision=prec, **over) for name, over in MEMBERS]
+    steps = 300  # two graph periods of 128 plus an eager tail
+    b = F.Batch(params)
+    b.step(steps)
+    tol = 1e-12 if prec == F.FDTD_FP64 else 2e-6
+    for i, p in enumerate(params):
+        alone = F.Sim(p)
+        alone.step(steps)
+        m = b.sim(i)
+        assert m.t == alone.t == steps
+        errs = family_errors(m, alone)
+        print(i, "field errors", errs)
+        assert max(errs) < tol, (i, errs)
+        pa, pb = m.probe(), alone.probe()
+        assert pa.shape == pb.shape
+        assert rel(pa, pb) < tol * 10
+        sa, sb = b.spectra(i), alone.spectra()
+        assert rel(sa[:, 1:4], sb[:, 1:4]) < (1e-10 if prec == F.FDTD_FP64 else 1e-4)
+        alone.close()
+    kernels, graphs = b.stats()
+    assert graphs == 2 and kernels > 0
+    b.close()
+
+
+def test_batch_launches_do_not_grow_with_members():
+    one = F.Batch([make(F, "sphere_au", precision=F.FDTD_FP32)])
+    four = F.Batch([make(F, "sphere_au", precision=F.FDTD_FP32) for _ in range(4)])
+    one.step(5)
+    four.step(5)
+    assert one.stats()[0] == four.stats()[0]
+    one.close()
+    four.close()
+
+
+def test_batch_hydro_members():
+    params = [make(F, "hydro", precision=F.FDTD_FP64),
+              make(F, "hydro", precision=F.FDTD_FP64, NCELLX=25, nano_sphere_radius=8e-9)]
+    b = F.Batch(params)
+    b.step(150)
+    for i, p in enumerate(params):
+        alone = F.Sim(p)
+        alone.step(150)
+        assert max(family_errors(b.sim(i), alone)) < 1e-12
+        alone.close()
+    b.close()
+
+
+def test_batch_rejects_mixed_members():
+    with pytest.raises(F.FdtdError) as e:
+        F.Batch([make(F, "sphere_au", precision=F.FDTD_FP32),
+                 make(F, "sphere_au", precision=F.FDTD_FP32, Tend=500)])
+    assert e.value.status == 1 and "Tend" in str(e.value)
