@@ -241,6 +241,55 @@ def batch_bench(mod, torch, stream, sp, dev, n, steps):
             "edges": [min(edges), max(edges)], "seed": BATCH_SEED, "gpu_launches": launches}
 
 
+def adjoint_params(mod, steps=4000, precision=None):
+    """The adjoint workload: 96^3 grid (10-cell CPML), dx = 2 nm, FP32 fields,
+    a 32 x 32 x 16-cell design region at the centre whose cells blend
+    between vacuum and Drude+2CP gold, TFSF pulse centred at 600 nm and a
+    wavelength grid of 1 nm steps from 550 to 785 nm so that 550, 633 and
+    785 nm are DFT frequencies (indices 0, 83, 235)."""
+    n_in = 96 - 2 * 10 - 1
+    c = 48
+    box = [c - 16, c + 16, c - 16, c + 16, c - 8, c + 8]
+    return mod.default_params(
+        Tend=steps - 1, dx=2e-9, dy=2e-9, dz=2e-9, NCELLX=n_in, NCELLY=n_in, NCELLZ=n_in,
+        NcpmlX=10, NcpmlY=10, NcpmlZ=10, nano_sphere=0, material=3, first_medium=1,
+        NUM_freq=236, WL_or_freq=1, lam_min=550e-9, lam_max=785e-9, lam_0=600e-9,
+        BandWidth=3e15, design_box=box,
+        precision=mod.FDTD_FP32 if precision is None else precision)
+
+
+ADJOINT_FREQS = [0, 83, 235]
+
+
+def adjoint_bench(mod, torch, stream, dev, steps=4000, every=200):
+    """Forward (with checkpoints) and backward (segment recompute + reverse
+    sweep) wall time of the adjoint workload; ratio = backward / forward."""
+    import numpy as np
+    p = adjoint_params(mod, steps)
+    s = mod.Sim(p, device=dev)
+    b = list(p.design_box)
+    rng = np.random.default_rng(BATCH_SEED)
+    s.set_design(rng.uniform(0, 1, (b[5] - b[4], b[3] - b[2], b[1] - b[0])))
+    s.forward(ADJOINT_FREQS, every)  # warm-up: buffers, graphs
+    s.backward()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    L = s.forward(ADJOINT_FREQS, every)
+    t1 = time.perf_counter()
+    g, gp = s.backward()
+    t2 = time.perf_counter()
+    s.check()
+    cells = (96 ** 3) * steps
+    out = {"forward_s": round(t1 - t0, 4), "backward_s": round(t2 - t1, 4),
+           "ratio": round((t2 - t1) / (t1 - t0), 3), "objective": L,
+           "grad_rho_max": float(np.abs(g).max()), "grad_params": [float(x) for x in gp],
+           "forward_gcell_steps_per_s": round(cells / (t1 - t0) / 1e9, 2),
+           "time_steps": steps, "checkpoint_every": every, "grid": 96, "design": [32, 32, 16],
+           "timing": "host wall clock around each blocking C-ABI call"}
+    s.close()
+    return out
+
+
 def ref_deck_case(tend):
     """The reference-geometry deck used to time the reference's own CUDA
     build beside this one: the 256^3 grid of the workload (12-cell CPML,
@@ -330,6 +379,7 @@ def main():
     ap.add_argument("--grid", type=int, default=256, help="smaller grids for ncu captures")
     ap.add_argument("--num-freq", type=int, default=201)
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--batch-members", type=int, default=64)
     ap.add_argument("--batch-steps", type=int, default=3000)
     ap.add_argument("--no-ref-gpu", action="store_true",
@@ -498,6 +548,10 @@ def main():
                                   / (msr / 1e3) / 1e9, 3)
             sm.close()
 
+    adjoint = None
+    if not args.no_adjoint and args.grid == 256:
+        adjoint = adjoint_bench(F, torch, stream, dev)
+
     batched = None
     if not args.no_batch and args.grid == 256:
         batched = batch_bench(F, torch, stream, sp, dev, args.batch_members, args.batch_steps)
@@ -521,7 +575,7 @@ def main():
                        "parallelism": f"replicas x{world}"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "clocks": clk.summary(), "gpu_launches": launches, "fp64": fp64,
-            "reference_deck": refdeck, "batched": batched,
+            "reference_deck": refdeck, "batched": batched, "adjoint": adjoint,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -1,0 +1,382 @@
+// Reverse-time discrete adjoint of the time step (no counterpart in the
+// reference).  The step without the hydrodynamic model is linear in the
+// state (E, H, the CPML psi, the dispersive-cell ADE states) plus sources
+// that do not depend on it (TFSF corrections, the 1D line), so its adjoint
+// is the transposed step run backwards:
+//
+//   lambda^n = M^T lambda^{n+1} + dL/dx^n,   dL/drho = sum_n lambda^{n+1} (dM/drho) x^n
+//
+// The transposed Yee/CPML sub-steps are written in gather form: a first
+// kernel turns each updated component's adjoint into the coefficients of
+// the field differences it read ("a" arrays, one per component and
+// difference axis) and applies the psi recursions transposed; a second
+// kernel gathers those coefficients into the adjoint of the other field
+// (each difference D = F(p) - F(p - e) read by cell p contributes +a(p) to
+// F(p) and -a(p) to F(p - e)).  The dispersive (design) cells transpose
+// their ADE recursions locally and accumulate dL/drho and the Drude
+// parameter gradients from the forward values recorded during the segment
+// recompute.  Objective: the absorbed power (AbsTot column) summed over
+// chosen frequencies, a bilinear form of the DFT accumulators, whose
+// derivative enters at every DFT sample step.
+#pragma once
+#include "kernels.cuh"
+
+namespace fdtd {
+
+template <typename T>
+struct AdjView {
+  T* lE[3];
+  T* lH[3];
+  T* lpE_N[3][2];
+  T* lpE_F[3][2];
+  T* lpH_N[3][2];
+  T* lpH_F[3][2];
+  T* a[3][2];  // difference coefficients of component c, slot q (axis (c+1+q)%3)
+  // dispersive-cell adjoint states per component slot: Drude current J^{n+1}
+  // and J^n, the two CP polarisations P^{n+1} and P^n, the E history
+  T* lJa[3];
+  T* lJb[3];
+  T* lPa[3][2];
+  T* lPb[3][2];
+  T* lEh[3];
+  double* grho[3];  // dL/drho per slot
+  double* gpar;     // [2]: dL/d omega_D, dL/d gamma
+  // derivatives of the metal coefficients: [p] = d/d omega_D, d/d gamma
+  T dCE[2], dCE1[2], dCE2[2], dd1[2], dd2[2], dd3[2], dd4[2], dd5[2];
+  int* step;        // adjoint clock: the step being transposed
+};
+
+// psi element of component c, slot q at cell (i, j, k) for slab axis ax;
+// returns nullptr outside the slab.  w = slab width (Nc+1 for E, Nc for H).
+template <typename T>
+__device__ __forceinline__ T* adj_psi(const SimView<T>& s, T* const* nearp, T* const* farp, int ax, bool e_extent,
+                                      int i, int j, int k, int* qout) {
+  const CpmlAxis<T>& a = s.cp[ax];
+  const int n = ax == 0 ? i : ax == 1 ? j : k;
+  const int w = e_extent ? a.Nc + 1 : a.Nc;
+  if (e_extent ? n <= a.Nc : n < a.Nc) {
+    *qout = n;
+    return nearp[0] + slab_idx(s, ax, w, i, j, k);
+  }
+  if (n >= a.F) {
+    const int q2 = n - a.F;
+    *qout = -1 - q2;  // far side, index q2
+    return farp[0] + slab_idx(s, ax, w, ax == 0 ? q2 : i, ax == 1 ? q2 : j, ax == 2 ? q2 : k);
+  }
+  return nullptr;
+}
+
+// E sub-step transposed, per cell: coefficients of the H differences, the
+// old-E adjoint and the psi_E adjoints.  Dispersive components are left to
+// adj_e_design (their coefficients are zeroed here).
+template <typename T>
+__global__ void adj_e_coef(const __grid_constant__ SimView<T> s, const __grid_constant__ AdjView<T> a) {
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long n = (long long)s.NX * s.NY * s.NZ;
+  if (q >= n) return;
+  const int i = (int)(q % s.NX);
+  const long long r = q / s.NX;
+  const int j = (int)(r % s.NY), k = (int)(r / s.NY);
+  const size_t id = fidx(s.PX, s.plane, i, j, k);
+  unsigned m = 0;
+  if (i >= s.mat_lo[0] && i < s.mat_hi[0] && j >= s.mat_lo[1] && j < s.mat_hi[1] && k >= s.mat_lo[2] &&
+      k < s.mat_hi[2])
+    m = s.mat[id];
+  const T cee = s.cee[m >> 3], ceh = s.ceh[m >> 3];
+  const int NX = s.NX, NY = s.NY, NZ = s.NZ;
+  const int ijk[3] = {i, j, k};
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    // active range of component c (main.cu:1172, 1476, 1767)
+    bool act = true;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      const int N = d == 0 ? NX : d == 1 ? NY : NZ;
+      if (ijk[d] >= N - 1) act = false;
+      if (d != c && ijk[d] < 1) act = false;
+    }
+    if (!act || (m & (1u << c))) {
+      a.a[c][0][id] = T(0);
+      a.a[c][1][id] = T(0);
+      continue;  // not updated (or dispersive): adjoint passes through here
+    }
+    const T lam = a.lE[c][id];
+#pragma unroll
+    for (int sl = 0; sl < 2; sl++) {
+      const int ax = (c + 1 + sl) % 3;
+      const T sg = sl == 0 ? T(1) : T(-1);
+      const CpmlAxis<T>& cp = s.cp[ax];
+      const int nn = ijk[ax];
+      T coef = sg * ceh * ldg(cp.inv_ked + nn) * lam;
+      int qs;
+      T* lp = adj_psi(s, &a.lpE_N[c][sl], &a.lpE_F[c][sl], ax, true, i, j, k, &qs);
+      if (lp) {
+        T b, cc;
+        if (qs >= 0) {
+          b = ldg(cp.be_N + qs);
+          cc = ldg(((c == 1 && ax == 0) ? cp.ce_N_ey : cp.ce_N) + qs);
+        } else {
+          b = ldg(cp.be_F + (-1 - qs));
+          cc = ldg(cp.ce_F + (-1 - qs));
+        }
+        const T tot = *lp + sg * ceh * lam;
+        *lp = b * tot;
+        coef += cc * cp.inv_d * tot;
+      }
+      a.a[c][sl][id] = coef;
+    }
+    a.lE[c][id] = cee * lam;
+  }
+}
+
+// Dispersive (design) cells, transposed: one thread per (component, cell).
+// The forward map is
+//   nv  = (dt/z0 curl + CE1 v - CE2 e1 - (d1-1) J - d2 Jm - sum (C1q-1) Pq - C2q Pqm) / CE
+//   Pq' = C1q Pq + C2q Pqm + C3q nv + C4q v + C5q e1,   J' = d1 J + d2 Jm + d3 nv + d4 v + d5 e1
+// with v = E^n, e1 = E^{n-1}; the coupling coefficients are blended by rho.
+template <typename T>
+__global__ void adj_e_design(const __grid_constant__ SimView<T> s, const __grid_constant__ MetalView<T> m,
+                             const __grid_constant__ AdjView<T> a, const T* __restrict__ rec, int rec_rows) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  int c = 0;
+  while (c < 3 && q >= m.n[c]) { q -= m.n[c]; c++; }
+  double gp0 = 0, gp1 = 0;
+  if (c < 3) {
+    const int4 e = m.cell[c][q];
+    const int sl = e.w;
+    const size_t id = fidx(s.PX, s.plane, e.x, e.y, e.z);
+    const int n = *a.step;
+    const T* r = rec + (size_t)(n % rec_rows) * 5 * m.rec_slots + m.rec_off[c] + sl;
+    const T v = r[0], e1 = r[m.rec_slots], J = r[2 * m.rec_slots], Jm = r[3 * m.rec_slots],
+            nv = r[4 * m.rec_slots];
+    const T rho = m.rho[c] ? (T)m.rho[c][sl] : T(1);
+    const T CE = m.vac + rho * (m.C_E - m.vac), CE1 = m.vac + rho * (m.C_E_1 - m.vac), CE2 = rho * m.C_E_2;
+    const T D3 = rho * m.d3, D4 = rho * m.d4, D5 = rho * m.d5;
+    const T C3[2] = {rho * m.C3[0], rho * m.C3[1]}, C4[2] = {rho * m.C4[0], rho * m.C4[1]},
+            C5[2] = {rho * m.C5[0], rho * m.C5[1]};
+    const T lnv = a.lE[c][id];
+    const T al = a.lJa[c][sl], be = a.lJb[c][sl], ep = a.lEh[c][sl];
+    const T aq[2] = {a.lPa[c][0][sl], a.lPa[c][1][sl]}, bq[2] = {a.lPb[c][0][sl], a.lPb[c][1][sl]};
+    const T Lam = lnv + C3[0] * aq[0] + C3[1] * aq[1] + D3 * al;
+    const T mu = Lam / CE;
+    // adjoint of E^n (the field and the stored history both read it)
+    a.lE[c][id] = CE1 * mu + C4[0] * aq[0] + C4[1] * aq[1] + D4 * al + ep;
+    // curl(H) coefficients: nv has dt/z0 curl/CE, curl = s0 ik0 D0 + s1 ik1 D1
+    const int ijk[3] = {e.x, e.y, e.z};
+    const T f = m.dt / m.z0 * mu;
+#pragma unroll
+    for (int sq = 0; sq < 2; sq++) {
+      const int ax = (c + 1 + sq) % 3;
+      a.a[c][sq][id] = (sq == 0 ? f : -f) * ldg(s.cp[ax].inv_ked + ijk[ax]);
+    }
+    // states one step back
+    a.lJa[c][sl] = be + m.d1 * al - (m.d1 - T(1)) * mu;
+    a.lJb[c][sl] = m.d2 * al - m.d2 * mu;
+#pragma unroll
+    for (int p = 0; p < 2; p++) {
+      a.lPa[c][p][sl] = bq[p] + m.C1[p] * aq[p] - (m.C1[p] - T(1)) * mu;
+      a.lPb[c][p][sl] = m.C2[p] * aq[p] - m.C2[p] * mu;
+    }
+    a.lEh[c][sl] = -CE2 * mu + C5[0] * aq[0] + C5[1] * aq[1] + D5 * al;
+    // dL/drho: every coupling coefficient is vac + rho (metal - vac)
+    const double g = (double)mu * (-(double)nv * ((double)m.C_E - (double)m.vac) +
+                                   (double)v * ((double)m.C_E_1 - (double)m.vac) - (double)e1 * (double)m.C_E_2) +
+                     (double)aq[0] * ((double)nv * m.C3[0] + (double)v * m.C4[0] + (double)e1 * m.C5[0]) +
+                     (double)aq[1] * ((double)nv * m.C3[1] + (double)v * m.C4[1] + (double)e1 * m.C5[1]) +
+                     (double)al * ((double)nv * m.d3 + (double)v * m.d4 + (double)e1 * m.d5);
+    a.grho[c][sl] += g;
+    // Drude parameters: coupling terms scale with rho, the pole dynamics
+    // (d1, d2) do not
+    double gpp[2];
+#pragma unroll
+    for (int p = 0; p < 2; p++)
+      gpp[p] = (double)rho * ((double)mu * (-(double)nv * a.dCE[p] + (double)v * a.dCE1[p] - (double)e1 * a.dCE2[p]) +
+                              (double)al * ((double)nv * a.dd3[p] + (double)v * a.dd4[p] + (double)e1 * a.dd5[p])) +
+               ((double)al - (double)mu) * ((double)J * a.dd1[p] + (double)Jm * a.dd2[p]);
+    gp0 = gpp[0];
+    gp1 = gpp[1];
+  }
+  // block sum of the parameter gradients
+  __shared__ double red[2][32];
+  for (int o = 16; o > 0; o >>= 1) {
+    gp0 += __shfl_down_sync(0xffffffffu, gp0, o);
+    gp1 += __shfl_down_sync(0xffffffffu, gp1, o);
+  }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) { red[0][w] = gp0; red[1][w] = gp1; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s0 = 0, s1 = 0;
+    for (int x = 0; x < (int)(blockDim.x >> 5); x++) { s0 += red[0][x]; s1 += red[1][x]; }
+    if (s0 != 0.0) atomicAdd(a.gpar, s0);
+    if (s1 != 0.0) atomicAdd(a.gpar + 1, s1);
+  }
+}
+
+// lambda_H += gather of the E-sub-step coefficients: H component h is read
+// by the E components c != h through D = H_h(p) - H_h(p - e_ax), ax the
+// third axis.
+template <typename T>
+__global__ void adj_gather_h(const __grid_constant__ SimView<T> s, const __grid_constant__ AdjView<T> a) {
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long n = (long long)s.NX * s.NY * s.NZ;
+  if (q >= n) return;
+  const int i = (int)(q % s.NX);
+  const long long r = q / s.NX;
+  const int j = (int)(r % s.NY), k = (int)(r / s.NY);
+  const size_t id = fidx(s.PX, s.plane, i, j, k);
+  const bool nx = i + 1 < s.NX, ny = j + 1 < s.NY, nz = k + 1 < s.NZ;
+  const size_t sx = 1, sy = s.PX, sz = s.plane;
+  // Hx: Ey slot 0 (z), Ez slot 1 (y)
+  a.lH[0][id] += a.a[1][0][id] - (nz ? a.a[1][0][id + sz] : T(0)) + a.a[2][1][id] - (ny ? a.a[2][1][id + sy] : T(0));
+  // Hy: Ex slot 1 (z), Ez slot 0 (x)
+  a.lH[1][id] += a.a[0][1][id] - (nz ? a.a[0][1][id + sz] : T(0)) + a.a[2][0][id] - (nx ? a.a[2][0][id + sx] : T(0));
+  // Hz: Ex slot 0 (y), Ey slot 1 (x)
+  a.lH[2][id] += a.a[0][0][id] - (ny ? a.a[0][0][id + sy] : T(0)) + a.a[1][1][id] - (nx ? a.a[1][1][id + sx] : T(0));
+}
+
+// H sub-step transposed, per cell: coefficients of the E differences
+// D = E_e(p + e_ax) - E_e(p), the old-H adjoint and the psi_H adjoints.
+template <typename T>
+__global__ void adj_h_coef(const __grid_constant__ SimView<T> s, const __grid_constant__ AdjView<T> a) {
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long n = (long long)s.NX * s.NY * s.NZ;
+  if (q >= n) return;
+  const int i = (int)(q % s.NX);
+  const long long r = q / s.NX;
+  const int j = (int)(r % s.NY), k = (int)(r / s.NY);
+  const size_t id = fidx(s.PX, s.plane, i, j, k);
+  const int NX = s.NX, NY = s.NY, NZ = s.NZ;
+  const int ijk[3] = {i, j, k};
+  const bool cellok = i < NX - 1 && j < NY - 1 && k < NZ - 1;  // CPML range (main.cu:829)
+  const T che = s.che, chh = s.chh;
+#pragma unroll
+  for (int h = 0; h < 3; h++) {
+    // Yee range: the two other indices below N-1
+    bool act = true;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      const int N = d == 0 ? NX : d == 1 ? NY : NZ;
+      if (d != h && ijk[d] >= N - 1) act = false;
+    }
+    if (!act) {
+      a.a[h][0][id] = T(0);
+      a.a[h][1][id] = T(0);
+      continue;
+    }
+    const T lam = a.lH[h][id];
+#pragma unroll
+    for (int sl = 0; sl < 2; sl++) {
+      const int ax = (h + 1 + sl) % 3;
+      const T sg = sl == 0 ? T(-1) : T(1);
+      const CpmlAxis<T>& cp = s.cp[ax];
+      T coef = sg * che * ldg(cp.inv_khd + ijk[ax]) * lam;
+      if (cellok) {
+        int qs;
+        T* lp = adj_psi(s, &a.lpH_N[h][sl], &a.lpH_F[h][sl], ax, false, i, j, k, &qs);
+        if (lp) {
+          T b, cc;
+          if (qs >= 0) { b = ldg(cp.bh_N + qs); cc = ldg(cp.ch_N + qs); }
+          else { b = ldg(cp.bh_F + (-1 - qs)); cc = ldg(cp.ch_F + (-1 - qs)); }
+          const T tot = *lp + sg * che * lam;
+          *lp = b * tot;
+          coef += cc * cp.inv_d * tot;
+        }
+      }
+      a.a[h][sl][id] = coef;
+    }
+    a.lH[h][id] = chh * lam;
+  }
+}
+
+// lambda_E += gather of the H-sub-step coefficients: D = E_e(p + e_ax) -
+// E_e(p) read by H cell p contributes +a(p - e_ax) and -a(p) to E_e(p).
+template <typename T>
+__global__ void adj_gather_e(const __grid_constant__ SimView<T> s, const __grid_constant__ AdjView<T> a) {
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long n = (long long)s.NX * s.NY * s.NZ;
+  if (q >= n) return;
+  const int i = (int)(q % s.NX);
+  const long long r = q / s.NX;
+  const int j = (int)(r % s.NY), k = (int)(r / s.NY);
+  const size_t id = fidx(s.PX, s.plane, i, j, k);
+  const bool px = i > 0, py = j > 0, pz = k > 0;
+  const size_t sx = 1, sy = s.PX, sz = s.plane;
+  // Ex: Hy slot 0 (z), Hz slot 1 (y)
+  a.lE[0][id] += (pz ? a.a[1][0][id - sz] : T(0)) - a.a[1][0][id] + (py ? a.a[2][1][id - sy] : T(0)) - a.a[2][1][id];
+  // Ey: Hx slot 1 (z), Hz slot 0 (x)
+  a.lE[1][id] += (pz ? a.a[0][1][id - sz] : T(0)) - a.a[0][1][id] + (px ? a.a[2][0][id - sx] : T(0)) - a.a[2][0][id];
+  // Ez: Hx slot 0 (y), Hy slot 1 (x)
+  a.lE[2][id] += (py ? a.a[0][0][id - sy] : T(0)) - a.a[0][0][id] + (px ? a.a[1][1][id - sx] : T(0)) - a.a[1][1][id];
+}
+
+// Objective derivative at a DFT sample step n: for every absorption-box
+// face cell and tangential component, g = sum_m Re(P_m conj(w_m)) with
+// w_m = exp(i 2 pi (n + delta) dt f_m) (delta = 1 for E, 1/2 for H) and
+// P_m the weighted partner accumulator (adj_partner).
+template <typename T>
+__global__ void adj_source(const __grid_constant__ SimView<T> s, const __grid_constant__ DftView d,
+                           const __grid_constant__ AdjView<T> a, const double2* __restrict__ P,
+                           const double* __restrict__ fsel, int nsel, long long prows) {
+  const int f = blockIdx.y;  // absorption-box faces 0..5
+  const DftFace F = d.face[f];
+  const int nc = F.na * F.nb;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nc) return;
+  const int n = *a.step;
+  const int u = q / F.nb, v = q - u * F.nb;
+  int ijk[3];
+  const int a1 = F.ax == 0 ? 1 : 0, a2 = F.ax == 2 ? 1 : 2;
+  ijk[F.ax] = F.pos;
+  ijk[a1] = F.s1 + u;
+  ijk[a2] = F.s2 + v;
+  const size_t id = fidx(s.PX, s.plane, ijk[0], ijk[1], ijk[2]);
+#pragma unroll
+  for (int cs = 0; cs < 4; cs++) {
+    const long long row = F.row0 + (long long)cs * F.npad + q;
+    const double del = cs < 2 ? 1.0 : 0.5;
+    double g = 0.0;
+    for (int m = 0; m < nsel; m++) {
+      const double ph = (double)(float)2.0 * 3.1415926535897932384626433832795 * (n + del) * d.dt * fsel[m];
+      double sv, cv;
+      sincos(ph, &sv, &cv);
+      const double2 p = P[(size_t)m * prows + row];
+      g += p.x * cv + p.y * sv;
+    }
+    const int comp = F.comp[cs];
+    T* dst = comp < 3 ? a.lE[comp] : a.lH[comp - 3];
+    atomicAdd(dst + id, (T)g);
+  }
+}
+
+// Weighted partner accumulators of the absorption-box rows for the chosen
+// frequencies: AbsTot = sum_f sgn_f dxy/|Einc|^2 sum Re(Ex conj(Hy) - Ey
+// conj(Hx)) (per face pairing), so d/d(sample of Ex) pairs with Hy, etc.
+__global__ void adj_partner(const __grid_constant__ DftView d, const int* __restrict__ sel,
+                            const double* __restrict__ wsel, int nsel, double2* __restrict__ P, long long prows) {
+  const int f = blockIdx.y;
+  const int m = blockIdx.z;
+  const DftFace F = d.face[f];
+  const int nc = F.na * F.nb;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nc || m >= nsel) return;
+  const int qx = F.ax == 1 ? 1 : 0, qy = F.ax == 1 ? 0 : 1;
+  const double K = ((f & 1) ? 1.0 : -1.0) * wsel[m];
+  const int fm = sel[m];
+#pragma unroll
+  for (int cs = 0; cs < 4; cs++) {
+    int ps;
+    double sg;
+    if (cs == qx) { ps = 2 + qy; sg = 1.0; }
+    else if (cs == qy) { ps = 2 + qx; sg = -1.0; }
+    else if (cs == 2 + qx) { ps = qy; sg = -1.0; }
+    else { ps = qx; sg = 1.0; }
+    const long long pr = F.row0 + (long long)ps * F.npad + q;
+    const double re = d.acc_re[(size_t)fm * d.rows + pr], im = d.acc_im[(size_t)fm * d.rows + pr];
+    P[(size_t)m * prows + F.row0 + (long long)cs * F.npad + q] = make_double2(K * sg * re, K * sg * im);
+  }
+}
+
+__global__ void adj_step_back(int* step) { *step -= 1; }
+
+}  // namespace fdtd

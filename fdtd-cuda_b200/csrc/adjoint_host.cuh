@@ -1,0 +1,327 @@
+// Host side of the adjoint (no counterpart in the reference): design-region
+// blend, forward run with field checkpoints, and the reverse sweep with
+// segment recompute.  Included at the end of fdtd.cu (it uses the
+// simulation internals defined there).
+//
+// fdtd_forward runs the whole time loop from zero fields, copying the state
+// (fields, psi, dispersive-cell states, incident line, clock) aside at the
+// start of every checkpoint_every steps.  fdtd_backward walks the segments
+// from the last: it restores a segment's checkpoint, recomputes its steps
+// with DFT sampling off while the dispersive-cell kernel records, per step,
+// the local values the gradient needs, then runs the transposed steps of
+// that segment in reverse.  The transposed Yee and CPML operators need no
+// forward values (the step is linear with fixed coefficients), so only the
+// dispersive cells are recorded.
+
+struct fdtd_sim::Adjoint {
+  std::vector<std::unique_ptr<DevBuf>> bufs;
+  // checkpoints
+  std::vector<std::pair<void*, size_t>> ck_bufs;  // state buffers that are checkpointed
+  size_t ck_bytes = 0;
+  std::unique_ptr<DevBuf> ck;  // nseg * ck_bytes
+  int every = 0, nseg = 0, tend = 0;
+  // objective
+  std::vector<int> sel;
+  double objective = 0;
+  bool forward_done = false;
+  std::unique_ptr<DevBuf> P, fsel;  // weighted partner accumulators, chosen frequencies
+  // adjoint state (allocated on the first backward)
+  bool ready = false;
+  void* view = nullptr;  // AdjView<T> on the host, as bytes
+  std::vector<char> view_bytes;
+  std::vector<std::pair<void*, size_t>> zero;  // buffers zeroed before each sweep
+  void* rec = nullptr;
+  long long rec_slots = 0;
+  int rec_off[3] = {0, 0, 0};
+  double* grho[3] = {nullptr, nullptr, nullptr};
+  double* gpar = nullptr;
+  int* step = nullptr;
+
+  template <typename U>
+  cudaError_t alloc(U** out, size_t count, bool zeroed_each_sweep) {
+    auto b = std::make_unique<DevBuf>();
+    cudaError_t e = b->alloc(count * sizeof(U));
+    if (e != cudaSuccess) return e;
+    *out = b->as<U>();
+    if (zeroed_each_sweep) zero.emplace_back(b->p, b->bytes);
+    bufs.push_back(std::move(b));
+    return cudaSuccess;
+  }
+};
+
+fdtd_sim::~fdtd_sim() { destroy_streams(); }
+
+extern "C" fdtd_status fdtd_set_design(fdtd_sim* s, const int box[6], const float* rho, size_t count) {
+  if (!s || !box || !rho) return fail(FDTD_ERR_INVALID, "null argument");
+  if (!s->has_design) return fail(FDTD_ERR_STATE, "the simulation was created without params.design_box");
+  for (int a = 0; a < 6; a++)
+    if (box[a] != s->dbox[a]) return fail(FDTD_ERR_INVALID, "box differs from params.design_box");
+  const size_t nb = s->dslot[0].size();
+  if (count != nb) return fail(FDTD_ERR_INVALID, "count must be the design box's cell count");
+  for (size_t q = 0; q < nb; q++)
+    if (!(rho[q] >= 0.0f && rho[q] <= 1.0f)) return fail(FDTD_ERR_INVALID, "rho must lie in [0, 1]");
+  CUDA_TRY(cudaSetDevice(s->device));
+  CUDA_TRY(cudaDeviceSynchronize());
+  for (int c = 0; c < 3; c++) {
+    if (!s->rho_d[c]) continue;
+    std::vector<float> h(s->nmetal[c], 1.0f);
+    for (size_t q = 0; q < nb; q++)
+      if (s->dslot[c][q] >= 0) h[s->dslot[c][q]] = rho[q];
+    CUDA_TRY(cudaMemcpy(s->rho_d[c], h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice));
+  }
+  if (s->adj) s->adj->forward_done = false;
+  return FDTD_OK;
+}
+
+static fdtd_status adj_checks(fdtd_sim* s) {
+  if (!s->has_design) return fail(FDTD_ERR_STATE, "the simulation was created without params.design_box");
+  if (s->su.hydro) return fail(FDTD_ERR_UNSUPPORTED, "the adjoint needs the local (non-hydrodynamic) model");
+  if (s->pml_metal) return fail(FDTD_ERR_UNSUPPORTED, "the adjoint needs every dispersive cell outside the CPML");
+  if (!s->dft_on || s->line.dft_every <= 0) return fail(FDTD_ERR_STATE, "the objective needs the DFT (StaticField = 0)");
+  return FDTD_OK;
+}
+
+extern "C" fdtd_status fdtd_forward(fdtd_sim* s, const int* freq_idx, int nfreq, int checkpoint_every,
+                                    double* objective) {
+  if (!s || !freq_idx || nfreq <= 0 || checkpoint_every <= 0 || !objective)
+    return fail(FDTD_ERR_INVALID, "bad argument");
+  fdtd_status st = adj_checks(s);
+  if (st != FDTD_OK) return st;
+  const int nf = s->dft.nf;
+  for (int m = 0; m < nfreq; m++)
+    if (freq_idx[m] < 0 || freq_idx[m] >= nf) return fail(FDTD_ERR_INVALID, "frequency index out of range");
+  if (!s->adj) s->adj = std::make_unique<fdtd_sim::Adjoint>();
+  fdtd_sim::Adjoint& A = *s->adj;
+  A.sel.assign(freq_idx, freq_idx + nfreq);
+  A.forward_done = false;
+  st = fdtd_reset(s);
+  if (st != FDTD_OK) return st;
+  CUDA_TRY(cudaSetDevice(s->device));
+  // checkpointed buffers: the state without the DFT accumulators, the
+  // sample ring and the probe record
+  A.ck_bufs.clear();
+  A.ck_bytes = 0;
+  const void* skip[4] = {s->dft.acc_re, s->dft.acc_im, s->ring, s->probe};
+  for (const auto& b : s->state) {
+    bool keep = true;
+    for (const void* k : skip) keep = keep && b.first != k;
+    if (keep) { A.ck_bufs.push_back(b); A.ck_bytes += (b.second + 255) / 256 * 256; }
+  }
+  A.every = checkpoint_every;
+  A.tend = s->su.p.Tend;
+  const int total = A.tend + 1;
+  A.nseg = (total + A.every - 1) / A.every;
+  const size_t need = (size_t)A.nseg * A.ck_bytes;
+  if (!A.ck || A.ck->bytes < need) {
+    A.ck.reset();
+    auto b = std::make_unique<DevBuf>();
+    CUDA_TRY(b->alloc(need));
+    A.ck = std::move(b);
+  }
+  for (int seg = 0; seg < A.nseg; seg++) {
+    char* dst = static_cast<char*>(A.ck->p) + (size_t)seg * A.ck_bytes;
+    for (const auto& b : A.ck_bufs) {
+      CUDA_TRY(cudaMemcpyAsync(dst, b.first, b.second, cudaMemcpyDeviceToDevice, 0));
+      dst += (b.second + 255) / 256 * 256;
+    }
+    const int n = std::min(A.every, total - seg * A.every);
+    st = fdtd_step(s, n, nullptr);
+    if (st != FDTD_OK) return st;
+  }
+  CUDA_TRY(cudaDeviceSynchronize());
+  // objective: AbsTot (ScatAbs column 2) summed over the chosen frequencies
+  std::vector<double> rows((size_t)nf * 19);
+  st = fdtd_spectral_finalize(s, rows.data());
+  if (st != FDTD_OK) return st;
+  A.objective = 0;
+  for (int m : A.sel) A.objective += rows[(size_t)m * 19 + 2];
+  *objective = A.objective;
+  // d AbsTot / d(face flux sum) per chosen frequency (CalculateAbsScatt)
+  const Setup& su = s->su;
+  const bool sphere = su.p.geometry == FDTD_GEOM_REFERENCE && su.p.nano_sphere == 1;
+  std::vector<double> w(nfreq), fs(nfreq);
+  for (int m = 0; m < nfreq; m++) {
+    const double amp = std::abs(su.Einc[A.sel[m]]);
+    w[m] = su.p.dx * su.p.dy / (amp * amp);
+    if (sphere) w[m] *= -1.0 / (su.pi * su.p.nano_sphere_radius * su.p.nano_sphere_radius);
+    fs[m] = su.freq[A.sel[m]];
+  }
+  auto Pb = std::make_unique<DevBuf>();
+  CUDA_TRY(Pb->alloc((size_t)nfreq * s->dft.rows * sizeof(double2)));
+  auto Fb = std::make_unique<DevBuf>();
+  CUDA_TRY(Fb->alloc((size_t)nfreq * (2 * sizeof(double) + sizeof(int))));
+  double* dw = static_cast<double*>(Fb->p);
+  double* dfs = dw + nfreq;
+  int* dsel = reinterpret_cast<int*>(dfs + nfreq);
+  CUDA_TRY(cudaMemcpy(dw, w.data(), nfreq * sizeof(double), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(dfs, fs.data(), nfreq * sizeof(double), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(dsel, A.sel.data(), nfreq * sizeof(int), cudaMemcpyHostToDevice));
+  int maxn = 0;
+  for (int f = 0; f < 6; f++) maxn = std::max(maxn, s->dft.face[f].na * s->dft.face[f].nb);
+  adj_partner<<<dim3((maxn + 255) / 256, 6, nfreq), 256>>>(s->dft, dsel, dw, nfreq, static_cast<double2*>(Pb->p),
+                                                          s->dft.rows);
+  CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(cudaDeviceSynchronize());
+  A.P = std::move(Pb);
+  A.fsel = std::move(Fb);
+  A.forward_done = true;
+  return FDTD_OK;
+}
+
+template <typename T>
+static fdtd_status adj_prepare(fdtd_sim* s) {
+  fdtd_sim::Adjoint& A = *s->adj;
+  AdjView<T> a;
+  std::memset(&a, 0, sizeof(a));
+  const size_t nc = s->ncell;
+  for (int c = 0; c < 3; c++) {
+    CUDA_TRY(A.alloc(&a.lE[c], nc, true));
+    CUDA_TRY(A.alloc(&a.lH[c], nc, true));
+    for (int q = 0; q < 2; q++) CUDA_TRY(A.alloc(&a.a[c][q], nc, false));
+  }
+  // psi adjoints, the shapes of the psi slabs
+  const Setup& su = s->su;
+  for (int c = 0; c < 3; c++)
+    for (int slot = 0; slot < 2; slot++) {
+      const int ax = (c + 1 + slot) % 3;
+      const int Nc = su.Nc[ax];
+      size_t ce, ch;
+      if (ax == 2) { ce = (size_t)(Nc + 1) * s->plane; ch = (size_t)Nc * s->plane; }
+      else if (ax == 1) { ce = (size_t)s->NZ * (Nc + 1) * s->PX; ch = (size_t)s->NZ * Nc * s->PX; }
+      else { ce = (size_t)s->NZ * s->NY * (Nc + 1); ch = (size_t)s->NZ * s->NY * Nc; }
+      CUDA_TRY(A.alloc(&a.lpE_N[c][slot], ce, true));
+      CUDA_TRY(A.alloc(&a.lpE_F[c][slot], ce, true));
+      CUDA_TRY(A.alloc(&a.lpH_N[c][slot], ch, true));
+      CUDA_TRY(A.alloc(&a.lpH_F[c][slot], ch, true));
+    }
+  long long slots = 0;
+  for (int c = 0; c < 3; c++) {
+    const size_t n = std::max(1, s->nmetal[c]);
+    CUDA_TRY(A.alloc(&a.lJa[c], n, true));
+    CUDA_TRY(A.alloc(&a.lJb[c], n, true));
+    CUDA_TRY(A.alloc(&a.lEh[c], n, true));
+    for (int q = 0; q < 2; q++) {
+      CUDA_TRY(A.alloc(&a.lPa[c][q], n, true));
+      CUDA_TRY(A.alloc(&a.lPb[c][q], n, true));
+    }
+    CUDA_TRY(A.alloc(&a.grho[c], n, true));
+    A.grho[c] = a.grho[c];
+    A.rec_off[c] = (int)slots;
+    slots += s->nmetal[c];
+  }
+  CUDA_TRY(A.alloc(&a.gpar, 2, true));
+  A.gpar = a.gpar;
+  CUDA_TRY(A.alloc(&a.step, 1, false));
+  A.step = a.step;
+  A.rec_slots = std::max(1LL, slots);
+  T* rec;
+  CUDA_TRY(A.alloc(&rec, (size_t)A.every * 5 * A.rec_slots, false));
+  A.rec = rec;
+  // derivatives of the metal's coupling and dynamics coefficients with
+  // respect to omega_D and gamma (ade_coefficients, non-hydrodynamic form)
+  const double dt = su.dt, wD = su.wD, gam = su.gam;
+  const double dd = 1.0 / (dt * dt) + gam / (2.0 * dt), g1 = 1.0 / (2.0 * dt);
+  const double dd3[2] = {2.0 * su.d3 / wD, -su.d3 * g1 / dd};
+  const double dd4[2] = {2.0 * su.d4 / wD, -su.d4 * g1 / dd};
+  const double dd5[2] = {2.0 * su.d5 / wD, -su.d5 * g1 / dd};
+  const double dd1[2] = {0.0, -su.d1 * g1 / dd};
+  const double dd2[2] = {0.0, g1 * (1.0 - su.d2) / dd};
+  for (int p = 0; p < 2; p++) {
+    a.dd1[p] = (T)dd1[p]; a.dd2[p] = (T)dd2[p];
+    a.dd3[p] = (T)dd3[p]; a.dd4[p] = (T)dd4[p]; a.dd5[p] = (T)dd5[p];
+    a.dCE[p] = (T)dd3[p]; a.dCE1[p] = (T)(-dd4[p]); a.dCE2[p] = (T)dd5[p];
+  }
+  A.view_bytes.assign(reinterpret_cast<const char*>(&a), reinterpret_cast<const char*>(&a) + sizeof(a));
+  A.ready = true;
+  return FDTD_OK;
+}
+
+template <typename T>
+static fdtd_status adj_sweep(fdtd_sim* s) {
+  fdtd_sim::Adjoint& A = *s->adj;
+  const AdjView<T>& a = *reinterpret_cast<const AdjView<T>*>(A.view_bytes.data());
+  for (const auto& z : A.zero) CUDA_TRY(cudaMemset(z.first, 0, z.second));
+  MetalView<T>& m = mview<T>(s);
+  m.rec = static_cast<T*>(A.rec);
+  m.rec_rows = A.every;
+  m.rec_slots = A.rec_slots;
+  for (int c = 0; c < 3; c++) m.rec_off[c] = A.rec_off[c];
+  const int every_dft = s->line.dft_every;
+  const bool graphs = s->use_graphs;
+  s->line.dft_every = 0;  // the recompute needs no DFT samples
+  s->use_graphs = false;
+  const long long ncell = (long long)s->NX * s->NY * s->NZ;
+  const unsigned gc = (unsigned)((ncell + 255) / 256);
+  const int ntot = s->nmetal[0] + s->nmetal[1] + s->nmetal[2];
+  int maxn = 0;
+  for (int f = 0; f < 6; f++) maxn = std::max(maxn, s->dft.face[f].na * s->dft.face[f].nb);
+  const double* fsel = static_cast<const double*>(A.fsel->p) + A.sel.size();
+  const int total = A.tend + 1;
+  fdtd_status st = FDTD_OK;
+  for (int seg = A.nseg - 1; seg >= 0 && st == FDTD_OK; seg--) {
+    const int n0 = seg * A.every, n1 = std::min(total, n0 + A.every);
+    const char* src = static_cast<const char*>(A.ck->p) + (size_t)seg * A.ck_bytes;
+    for (const auto& b : A.ck_bufs) {
+      CUDA_TRY(cudaMemcpyAsync(b.first, src, b.second, cudaMemcpyDeviceToDevice, 0));
+      src += (b.second + 255) / 256 * 256;
+    }
+    s->t = n0;
+    s->host_nsamp = 0;
+    st = step_impl<T>(s, n1 - n0, 0);  // records the dispersive cells, row n % every
+    if (st != FDTD_OK) break;
+    const int last = n1 - 1;
+    CUDA_TRY(cudaMemcpyAsync(A.step, &last, sizeof(int), cudaMemcpyHostToDevice, 0));
+    CUDA_TRY(cudaStreamSynchronize(0));  // &last lives on this stack frame
+    for (int n = n1 - 1; n >= n0; n--) {
+      if (n % every_dft == 0)
+        adj_source<T><<<dim3((maxn + 255) / 256, 6), 256>>>(view<T>(s), s->dft, a,
+                                                             static_cast<const double2*>(A.P->p), fsel,
+                                                             (int)A.sel.size(), s->dft.rows);
+      adj_e_coef<T><<<gc, 256>>>(view<T>(s), a);
+      if (ntot > 0) adj_e_design<T><<<(ntot + 127) / 128, 128>>>(view<T>(s), m, a, static_cast<const T*>(A.rec), A.every);
+      adj_gather_h<T><<<gc, 256>>>(view<T>(s), a);
+      adj_h_coef<T><<<gc, 256>>>(view<T>(s), a);
+      adj_gather_e<T><<<gc, 256>>>(view<T>(s), a);
+      adj_step_back<<<1, 1>>>(A.step);
+      s->kernels += 6 + (ntot > 0) + (n % every_dft == 0);
+    }
+    CUDA_TRY(cudaGetLastError());
+  }
+  m.rec = nullptr;
+  s->line.dft_every = every_dft;
+  s->use_graphs = graphs;
+  CUDA_TRY(cudaDeviceSynchronize());
+  return st;
+}
+
+extern "C" fdtd_status fdtd_backward(fdtd_sim* s, float* dL_drho, size_t count, double* dL_dparams) {
+  if (!s) return fail(FDTD_ERR_INVALID, "null argument");
+  fdtd_status st = adj_checks(s);
+  if (st != FDTD_OK) return st;
+  if (!s->adj || !s->adj->forward_done) return fail(FDTD_ERR_STATE, "fdtd_backward needs a completed fdtd_forward");
+  if (dL_drho && count != s->dslot[0].size()) return fail(FDTD_ERR_INVALID, "count must be the design box's cell count");
+  CUDA_TRY(cudaSetDevice(s->device));
+  CUDA_TRY(cudaDeviceSynchronize());
+  fdtd_sim::Adjoint& A = *s->adj;
+  if (!A.ready) {
+    st = s->fp64 ? adj_prepare<double>(s) : adj_prepare<float>(s);
+    if (st != FDTD_OK) return st;
+  }
+  st = s->fp64 ? adj_sweep<double>(s) : adj_sweep<float>(s);
+  if (st != FDTD_OK) return st;
+  if (dL_drho) {
+    std::vector<double> g[3];
+    for (int c = 0; c < 3; c++) {
+      g[c].resize(std::max(1, s->nmetal[c]));
+      CUDA_TRY(cudaMemcpy(g[c].data(), A.grho[c], g[c].size() * sizeof(double), cudaMemcpyDeviceToHost));
+    }
+    for (size_t q = 0; q < count; q++) {
+      double v = 0;
+      for (int c = 0; c < 3; c++)
+        if (s->dslot[c][q] >= 0) v += g[c][s->dslot[c][q]];
+      dL_drho[q] = (float)v;
+    }
+  }
+  if (dL_dparams) CUDA_TRY(cudaMemcpy(dL_dparams, A.gpar, 2 * sizeof(double), cudaMemcpyDeviceToHost));
+  return FDTD_OK;
+}

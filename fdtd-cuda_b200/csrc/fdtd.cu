@@ -16,6 +16,7 @@
 #include "kernels.cuh"
 #include "staged.cuh"
 #include "boundary.cuh"
+#include "adjoint.cuh"
 #include "setup.h"
 
 using namespace fdtd;
@@ -125,12 +126,22 @@ struct fdtd_sim {
   cudaStream_t graph_stream = nullptr;
   bool use_graphs = true;
 
+  // adjoint design region (fdtd_set_design / fdtd_forward / fdtd_backward)
+  bool has_design = false;
+  int dbox[6] = {0, 0, 0, 0, 0, 0};
+  std::vector<int> dslot[3];     // design-box cell (x fastest) -> slot of component c, -1 none
+  float* rho_d[3] = {nullptr, nullptr, nullptr};  // blend per slot of component c
+  bool pml_metal = false;        // a dispersive cell lies in a CPML slab
+  struct Adjoint;
+  std::unique_ptr<Adjoint> adj;
+  ~fdtd_sim();
+
   // side stream on which a pass's edge-tile launch runs beside its
   // interior launch (fork/join by events, also inside graph capture)
   cudaStream_t side = nullptr;
   cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
 
-  ~fdtd_sim() {
+  void destroy_streams() {
     if (graph) cudaGraphExecDestroy(graph);
     if (graph_stream) cudaStreamDestroy(graph_stream);
     if (side) cudaStreamDestroy(side);
@@ -370,6 +381,11 @@ static fdtd_status build_views(fdtd_sim* s) {
   m.dt = (T)su.dt; m.z0 = (T)su.z0; m.e0 = (T)su.e0; m.N_EQ = (T)su.N_EQ;
   m.inv_dx = (T)(1.0 / su.p.dx); m.inv_dy = (T)(1.0 / su.p.dy); m.inv_dz = (T)(1.0 / su.p.dz);
   m.hydro = su.hydro;
+  m.vac = (T)su.ep0;
+  for (int c = 0; c < 3; c++) { m.rho[c] = nullptr; m.rec_off[c] = 0; }
+  m.rec = nullptr;
+  m.rec_rows = 1;
+  m.rec_slots = 0;
   m.fix_cbrt = (su.p.fixes & FDTD_FIX_HYDRO_CBRT) ? 1 : 0;
   // device copy of the view, read by the cold TFSF helpers of the staged
   // passes (keeps the kernel parameter from escaping to memory)
@@ -461,6 +477,32 @@ static fdtd_status create_impl(const fdtd_params* p, int device, fdtd_sim** out,
       if (hi[a] <= lo[a]) { lo[a] = 0; hi[a] = 0; }
       s->mat_lo[a] = lo[a];
       s->mat_hi[a] = hi[a];
+    }
+    // adjoint design box: slot of every box cell per component, blend
+    // arrays (rho = 1 until fdtd_set_design), and whether any dispersive
+    // cell sits in a CPML slab (the adjoint leaves those out)
+    {
+      const int* b = su.p.design_box;
+      s->has_design = b[1] > b[0] && b[3] > b[2] && b[5] > b[4];
+      for (int c = 0; c < 3 && s->has_design; c++) {
+        for (int a = 0; a < 6; a++) s->dbox[a] = b[a];
+        const int bx = b[1] - b[0], by = b[3] - b[2];
+        s->dslot[c].assign((size_t)bx * by * (b[5] - b[4]), -1);
+        for (const int4& e : cells[c])
+          if (e.x >= b[0] && e.x < b[1] && e.y >= b[2] && e.y < b[3] && e.z >= b[4] && e.z < b[5])
+            s->dslot[c][((size_t)(e.z - b[4]) * by + (e.y - b[2])) * bx + (e.x - b[0])] = e.w;
+        if (!cells[c].empty()) {
+          std::vector<float> ones(cells[c].size(), 1.0f);
+          CUDA_TRY(s->alloc(&s->rho_d[c], ones.size()));
+          CUDA_TRY(cudaMemcpy(s->rho_d[c], ones.data(), ones.size() * sizeof(float), cudaMemcpyHostToDevice));
+        }
+      }
+      for (int c = 0; c < 3; c++)
+        for (const int4& e : cells[c]) {
+          const int q[3] = {e.x, e.y, e.z};
+          for (int a = 0; a < 3; a++)
+            if (q[a] <= su.Nc[a] + 1 || q[a] >= su.F[a] - 1) s->pml_metal = true;
+        }
     }
     CUDA_TRY(s->alloc(&s->mat, s->ncell));
     CUDA_TRY(cudaMemcpy(s->mat, bits.data(), s->ncell, cudaMemcpyHostToDevice));
@@ -560,6 +602,10 @@ static fdtd_status create_impl(const fdtd_params* p, int device, fdtd_sim** out,
   }
   fdtd_status st = s->fp64 ? build_views<double>(s.get()) : build_views<float>(s.get());
   if (st != FDTD_OK) return st;
+  if (s->has_design)
+    for (int c = 0; c < 3; c++) {
+      if (s->fp64) s->md.rho[c] = s->rho_d[c]; else s->mf.rho[c] = s->rho_d[c];
+    }
   // line
   LineArgs& L = s->line;
   L.e_inc = s->e_inc; L.h_inc = s->h_inc; L.L = su.L; L.m0 = su.m0; L.src = su.m0 - su.p.source_offset;
@@ -1390,16 +1436,5 @@ extern "C" fdtd_status fdtd_get_material(fdtd_sim* s, uint8_t* out, size_t count
   return FDTD_OK;
 }
 
-// ---------------------------------------------------------------------
-// not yet available entry points
-
-extern "C" fdtd_status fdtd_set_design(fdtd_sim*, const int*, const float*, size_t) {
-  return fail(FDTD_ERR_UNSUPPORTED, "fdtd_set_design is not built yet");
-}
-extern "C" fdtd_status fdtd_forward(fdtd_sim*, const int*, int, int, double*) {
-  return fail(FDTD_ERR_UNSUPPORTED, "fdtd_forward is not built yet");
-}
-extern "C" fdtd_status fdtd_backward(fdtd_sim*, float*, size_t, double*) {
-  return fail(FDTD_ERR_UNSUPPORTED, "fdtd_backward is not built yet");
-}
 #include "batch.cuh"
+#include "adjoint_host.cuh"

@@ -84,7 +84,15 @@ struct MetalView {
   T* cpn[3][2]; T* cpn1[3][2];
   T* pd[3][3];          // Drude current ring (n, n-1, new) indexed by step
   T* nd[3][2];          // hydro density ring
-  const float* rho[3];  // design blend per slot (null = 1)
+  const float* rho[3];  // design blend per slot (null: plain metal coefficients)
+  T vac;                // vacuum C_E = C_E_1 = ep0, the rho = 0 end of the blend
+  // forward record for the adjoint (null = off): per step row (t % rec_rows)
+  // five values per slot, [row][value][rec_off[c] + slot], value = E^n,
+  // E^{n-1}, J^n, J^{n-1}, E^{n+1}
+  T* rec;
+  int rec_rows;
+  int rec_off[3];
+  long long rec_slots;
   // hydrodynamic neighbour slots, 12 per cell (see hydro_neighbours)
   const int* nbr[3];
   // coefficients

@@ -442,11 +442,28 @@ __device__ __forceinline__ void metal_e_body(const SimView<T>& s, const MetalVie
   CP4 += m.C2[1] * cpn1_1;
   const T en1 = m.en[c][sl];  // e_n becomes e_n_1
   const T en = v;             // current E becomes e_n
-  const T inv_CE = T(1) / m.C_E;
-  T nv = inv_CE * (m.dt * curl / m.z0 + m.C_E_1 * en - m.C_E_2 * en1 - CP1 - CP2 - CP3 - CP4 - T(0));
-  const T ncp0 = m.C1[0] * cpn0 + m.C2[0] * cpn1_0 + m.C3[0] * nv + m.C4[0] * en + m.C5[0] * en1;
-  const T ncp1 = m.C1[1] * cpn1 + m.C2[1] * cpn1_1 + m.C3[1] * nv + m.C4[1] * en + m.C5[1] * en1;
-  const T npd = m.d1 * pdn + m.d2 * pdn1 + m.d3 * nv + m.d4 * en + m.d5 * en1 + m.dNL * T(0);
+  // coefficients coupling E to the poles; an adjoint design region blends
+  // them linearly between vacuum (rho = 0) and the metal (rho = 1)
+  T CE = m.C_E, CE1 = m.C_E_1, CE2 = m.C_E_2, D3 = m.d3, D4 = m.d4, D5 = m.d5;
+  T C3[2] = {m.C3[0], m.C3[1]}, C4[2] = {m.C4[0], m.C4[1]}, C5[2] = {m.C5[0], m.C5[1]};
+  if (m.rho[c]) {
+    const T r = (T)m.rho[c][sl];
+    CE = m.vac + r * (m.C_E - m.vac);
+    CE1 = m.vac + r * (m.C_E_1 - m.vac);
+    CE2 = r * m.C_E_2;
+    D3 = r * m.d3; D4 = r * m.d4; D5 = r * m.d5;
+#pragma unroll
+    for (int q = 0; q < 2; q++) { C3[q] = r * m.C3[q]; C4[q] = r * m.C4[q]; C5[q] = r * m.C5[q]; }
+  }
+  const T inv_CE = T(1) / CE;
+  T nv = inv_CE * (m.dt * curl / m.z0 + CE1 * en - CE2 * en1 - CP1 - CP2 - CP3 - CP4 - T(0));
+  const T ncp0 = m.C1[0] * cpn0 + m.C2[0] * cpn1_0 + C3[0] * nv + C4[0] * en + C5[0] * en1;
+  const T ncp1 = m.C1[1] * cpn1 + m.C2[1] * cpn1_1 + C3[1] * nv + C4[1] * en + C5[1] * en1;
+  const T npd = m.d1 * pdn + m.d2 * pdn1 + D3 * nv + D4 * en + D5 * en1 + m.dNL * T(0);
+  if (m.rec) {
+    T* r = m.rec + (size_t)(t % m.rec_rows) * 5 * m.rec_slots + m.rec_off[c] + sl;
+    r[0] = en; r[m.rec_slots] = en1; r[2 * m.rec_slots] = pdn; r[3 * m.rec_slots] = pdn1; r[4 * m.rec_slots] = nv;
+  }
   m.en1[c][sl] = en1;
   m.en[c][sl] = en;
   m.cpn1[c][0][sl] = cpn0;

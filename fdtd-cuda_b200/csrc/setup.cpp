@@ -160,6 +160,8 @@ static void ade_coefficients(Setup& s) {
     s.C4[q] = a0 / (2.0 * Cc);
     s.C5[q] = (a0 / 4.0 - a1 / (2.0 * dt)) / Cc;
   }
+  s.wD = mt.wD;
+  s.gam = mt.gam;
   const double dd = 1.0 / (dt * dt) + mt.gam / (2.0 * dt);
   s.d1 = 2.0 / (dd * dt * dt);
   s.d2 = (mt.gam / (2.0 * dt) - 1.0 / (dt * dt)) / dd;
@@ -347,6 +349,22 @@ const char* setup_build(const fdtd_params& pin, Setup& s) {
   if (!(p.fixes & FDTD_FIX_BH_X_F))
     for (auto& v : s.cp[0].bh_F) v = 0.0;
   rasterise(s);
+  {
+    // adjoint design region: dispersive for all three components
+    const int* b = p.design_box;
+    if (b[1] > b[0] || b[3] > b[2] || b[5] > b[4]) {
+      if (!(b[1] > b[0] && b[3] > b[2] && b[5] > b[4])) return "design_box is empty along one axis";
+      if (s.hydro) return "the design region needs the local (non-hydrodynamic) model";
+      if (p.first_medium != 1) return "the design region blends towards vacuum: first_medium must be 1";
+      for (int a = 0; a < 3; a++)
+        if (b[2 * a] < s.absS[a] + 1 || b[2 * a + 1] > s.absE[a] - 1)
+          return "design_box must lie inside the absorption box";
+      for (int c = 0; c < 3; c++)
+        for (int i = b[0]; i < b[1]; i++)
+          for (int j = b[2]; j < b[3]; j++)
+            for (int k = b[4]; k < b[5]; k++) s.matc[c][((size_t)i * s.NY + j) * s.NZ + k] = p.material;
+    }
+  }
   if (s.hydro) {
     if (p.first_medium != 1) return "hydrodynamic model needs first_medium == 1";
     for (int c = 0; c < 3; c++)

@@ -31,6 +31,7 @@ struct Setup {
   CpmlTables cp[3];
   // ADE
   double C_E = 0, C_E_1 = 0, C_E_2 = 0, d1 = 0, d2 = 0, d3 = 0, d4 = 0, d5 = 0, dNL = 0, N_EQ = 0;
+  double wD = 0, gam = 0;  // Drude plasma frequency and damping in use
   double C1[2], C2[2], C3[2], C4[2], C5[2];
   // TFSF
   float sth, cth, sph, cph, fe[3], fh[3];

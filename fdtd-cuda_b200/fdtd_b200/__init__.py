@@ -262,6 +262,32 @@ class Sim:
         _check(lib().fdtd_get_stats(self.h, C.byref(st)))
         return st
 
+    # -- adjoint ---------------------------------------------------------
+    def set_design(self, rho):
+        """Blend per design-box cell (params.design_box), shape (nz, ny, nx)
+        of the box, values in [0, 1]."""
+        b = list(self.params.design_box)
+        rho = np.ascontiguousarray(rho, dtype=np.float32)
+        assert rho.shape == (b[5] - b[4], b[3] - b[2], b[1] - b[0]), rho.shape
+        box = (C.c_int * 6)(*b)
+        _check(lib().fdtd_set_design(self.h, box, rho.ctypes.data_as(C.POINTER(C.c_float)), rho.size))
+
+    def forward(self, freq_idx, checkpoint_every=200):
+        """Runs t = 0..Tend from zero fields with checkpoints; returns the
+        objective (AbsTot summed over freq_idx)."""
+        idx = (C.c_int * len(freq_idx))(*[int(x) for x in freq_idx])
+        out = C.c_double()
+        _check(lib().fdtd_forward(self.h, idx, len(freq_idx), int(checkpoint_every), C.byref(out)))
+        return out.value
+
+    def backward(self):
+        """dL/drho (box shape) and dL/d(omega_D, gamma) of the last forward."""
+        b = list(self.params.design_box)
+        g = np.empty((b[5] - b[4], b[3] - b[2], b[1] - b[0]), np.float32)
+        gp = np.empty(2)
+        _check(lib().fdtd_backward(self.h, g.ctypes.data_as(C.POINTER(C.c_float)), g.size, _dp(gp)))
+        return g, gp
+
     def time_kernel(self, which, reps=20, stream=None):
         """Mean device time (ms) of one launch of a single time-step kernel
         (FDTD_KERNEL_*), from CUDA events; leaves the fields changed."""

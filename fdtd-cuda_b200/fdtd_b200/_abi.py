@@ -42,6 +42,8 @@ _PARAM_FIELDS = [
     ("sphere_cz", C.c_double),
     # probe
     ("probe_i", C.c_int), ("probe_j", C.c_int), ("probe_k", C.c_int),
+    # adjoint design region
+    ("design_box", C.c_int * 6),
 ]
 
 

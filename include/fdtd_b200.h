@@ -160,6 +160,13 @@ typedef struct fdtd_params {
 
   /* ---- probes ---- */
   int probe_i, probe_j, probe_k; /* -1 = grid centre (OUT.txt, main.cu:2732) */
+
+  /* ---- adjoint design region (no counterpart in the reference) ---- */
+  /* [i0, i1) x [j0, j1) x [k0, k1) in grid cells; empty (i1 <= i0) = none.
+   * Its cells are dispersive (class `material`) for all three components;
+   * fdtd_set_design blends each cell's ADE coefficients between vacuum and
+   * the metal.  It must lie inside the absorption box, off the CPML. */
+  int design_box[6];
 } fdtd_params;
 
 typedef struct fdtd_sim fdtd_sim;   /* opaque */

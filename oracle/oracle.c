@@ -425,6 +425,19 @@ orc_sim* orc_create(const fdtd_params* pin, char* err) {
   s->mat = (int*)calloc(s->n, sizeof(int));
   for (int c = 0; c < 3; c++) s->matc[c] = (int*)calloc(s->n, sizeof(int));
   rasterise(s);
+  {
+    /* adjoint design region (no counterpart in the reference): dispersive
+     * for all three components, class `material` */
+    const int* b = p->design_box;
+    if (b[1] > b[0] && b[3] > b[2] && b[5] > b[4])
+      for (int c = 0; c < 3; c++)
+        for (int i = b[0]; i < b[1]; i++)
+          for (int j = b[2]; j < b[3]; j++)
+            for (int k = b[4]; k < b[5]; k++) {
+              s->matc[c][IDX(s, i, j, k)] = p->material;
+              s->mat[IDX(s, i, j, k)] = p->material;
+            }
+  }
   if (s->hydro) {
     /* the reference reads outside its arrays when metal touches the outer
      * planes (main.cu:1950-1980 wrap and i-1 = -1); that case is rejected */

@@ -1,0 +1,108 @@
+"""Reverse-time adjoint (fdtd_set_design / fdtd_forward / fdtd_backward):
+gradients of the absorbed power at three frequencies with respect to the
+per-cell blend rho of a design box and to the Drude omega_D and gamma,
+checked against central finite differences of the forward objective."""
+import numpy as np
+import pytest
+
+import fdtd_b200 as F
+import oracle as O
+from cases import make
+
+pytestmark = pytest.mark.gpu
+
+BOX = [14, 20, 14, 20, 15, 19]  # inside the absorption box of the 34^3 grid
+SEL = [2, 4, 6]
+GOLD = dict(metal_custom=1, eps_inf=1.1431, omega_D=1.3202e16, gamma_D=1.0805e14,
+            cp_A=(0.26698, 3.0834), cp_phi=(-1.2371, -1.0968),
+            cp_Omega=(3.8711e15, 4.1684e15), cp_Gamma=(4.4642e14, 2.3555e15))
+
+
+def design_sim(prec, **over):
+    return F.Sim(make(F, "vacuum", precision=prec, Tend=300, design_box=BOX, **over))
+
+
+def rho0():
+    rng = np.random.default_rng(1)
+    return rng.uniform(0, 1, (BOX[5] - BOX[4], BOX[3] - BOX[2], BOX[1] - BOX[0])).astype(np.float32)
+
+
+@pytest.fixture(scope="module")
+def fp64_grad():
+    s = design_sim(F.FDTD_FP64, **GOLD)
+    s.set_design(rho0())
+    L = s.forward(SEL, 50)
+    g, gp = s.backward()
+    return s, L, g, gp
+
+
+def test_rho_gradient_matches_central_differences(fp64_grad):
+    s, L, g, _ = fp64_grad
+    rho, h = rho0(), 1e-3
+    for c in [(0, 0, 0), (2, 3, 1), (3, 5, 5), (1, 2, 4)]:
+        r = rho.copy(); r[c] += h; s.set_design(r); lp = s.forward(SEL, 50)
+        r = rho.copy(); r[c] -= h; s.set_design(r); lm = s.forward(SEL, 50)
+        fd = (lp - lm) / (2 * h)
+        print(c, "fd", fd, "adjoint", g[c])
+        assert abs(fd - g[c]) <= 1e-3 * abs(fd), (c, fd, g[c])
+
+
+@pytest.mark.parametrize("k,name", [(0, "omega_D"), (1, "gamma_D")])
+def test_drude_parameter_gradient_matches_central_differences(fp64_grad, k, name):
+    _, L, _, gp = fp64_grad
+    v = GOLD[name]
+    h = v * 1e-4
+    vals = []
+    for x in (v + h, v - h):
+        s = design_sim(F.FDTD_FP64, **dict(GOLD, **{name: x}))
+        s.set_design(rho0())
+        vals.append(s.forward(SEL, 50))
+        s.close()
+    fd = (vals[0] - vals[1]) / (2 * h)
+    print(name, "fd", fd, "adjoint", gp[k])
+    assert abs(fd - gp[k]) <= 1e-3 * abs(fd)
+
+
+def test_fp32_adjoint_agrees_with_fp64(fp64_grad):
+    _, L64, g64, gp64 = fp64_grad
+    s = design_sim(F.FDTD_FP32, **GOLD)
+    s.set_design(rho0())
+    L = s.forward(SEL, 50)
+    g, gp = s.backward()
+    assert abs(L - L64) <= 1e-4 * abs(L64)
+    assert np.abs(g - g64).max() <= 1e-3 * np.abs(g64).max()
+    assert np.all(np.abs(gp - gp64) <= 1e-3 * np.abs(gp64))
+
+
+def test_checkpoint_interval_does_not_change_the_gradient(fp64_grad):
+    _, L, g, gp = fp64_grad
+    s = design_sim(F.FDTD_FP64, **GOLD)
+    s.set_design(rho0())
+    assert s.forward(SEL, 37) == pytest.approx(L, rel=1e-12)
+    g2, gp2 = s.backward()
+    np.testing.assert_allclose(g2, g, rtol=1e-5, atol=1e-6 * np.abs(g).max())
+    np.testing.assert_allclose(gp2, gp, rtol=1e-10)
+
+
+def test_full_metal_design_box_matches_oracle():
+    """rho = 1 everywhere: the forward is the metal box itself, which the
+    FP64 oracle (no adjoint) also rasterises from design_box."""
+    steps = 120
+    p = make(F, "vacuum", precision=F.FDTD_FP64, Tend=300, design_box=BOX)
+    s = F.Sim(p)
+    s.step(steps)
+    o = O.OracleSim(make(O, "vacuum", precision=1, Tend=300, design_box=BOX))
+    o.step(steps)
+    for c in range(6):
+        a, b = s.field(c), o.field(c)
+        scale = max(np.abs(b).max(), 1e-300)
+        assert np.abs(a - b).max() <= 1e-11 * scale, c
+
+
+def test_design_errors():
+    s = F.Sim(make(F, "vacuum", precision=F.FDTD_FP64))
+    with pytest.raises(F.FdtdError) as e:
+        s.forward(SEL, 50)
+    assert e.value.status == 5
+    with pytest.raises(F.FdtdError):
+        F.Sim(make(F, "vacuum", precision=F.FDTD_FP64, design_box=[2, 6, 2, 6, 2, 6]))
