@@ -167,6 +167,7 @@ static fdtd_status batch_build(fdtd_batch* b) {
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   CUDA_TRY(cudaFuncSetAttribute(e_pass_batch<T, kBatchTY, kBatchS, kBatchMinB>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CUDA_TRY(cudaFuncSetAttribute(dft_contract_batch<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDftSmem));
   int per_sm_h = 0, per_sm_e = 0, sms = 0;
   CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_h, h_pass_batch<T, kBatchTY, kBatchS, kBatchMinB>,
                                                          32 * kBatchTY, smem));
@@ -207,7 +208,7 @@ static void batch_enqueue_step(fdtd_batch* b, cudaStream_t st) {
     k++;
     if (++b->host_nsamp == kSampleBlock) {
       dft_twiddles_batch<T><<<dim3(b->g_tw, n), 256, 0, st>>>(d);
-      dft_contract_batch<T><<<dim3(b->g_c, n), 128, 0, st>>>(d);
+      dft_contract_batch<T><<<dim3(b->g_c, n), 128, kDftSmem, st>>>(d);
       dft_reset_batch<T><<<dim3(1, n), 1, 0, st>>>(d);
       k += 3;
       b->host_nsamp = 0;

@@ -702,6 +702,7 @@ static void staged_attributes() {
                        (int)staged_smem<T, TY, S>());
   FDTD_STAGED_VARIANTS(FDTD_ATTR)
 #undef FDTD_ATTR
+  cudaFuncSetAttribute(dft_contract<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDftSmem);
   done = true;
 }
 
@@ -957,7 +958,7 @@ template <typename T>
 static void launch_contract(fdtd_sim* s, cudaStream_t st) {
   const int ntw = 2 * kSampleBlock * s->dft.nf;
   dft_twiddles<<<(ntw + 255) / 256, 256, 0, st>>>(s->dft, s->clk, s->twiddles);
-  dft_contract<T><<<(unsigned)(s->dft.rows / kDftRows), 128, 0, st>>>(s->dft, (const T*)s->ring, s->clk,
+  dft_contract<T><<<(unsigned)(s->dft.rows / kDftRows), 128, kDftSmem, st>>>(s->dft, (const T*)s->ring, s->clk,
                                                                         s->twiddles);
   dft_reset_count<<<1, 1, 0, st>>>(s->clk);
   s->kernels += 3;

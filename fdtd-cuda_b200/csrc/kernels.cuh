@@ -717,15 +717,29 @@ __global__ void dft_twiddles(const __grid_constant__ DftView d, const DevClock* 
 // acc[f][r] += sum_s x[s][r] tw[h(r)][s][f] in FP64.  A CTA owns kDftRows
 // rows (all E or all H thanks to the padding) and walks every frequency in
 // tiles of kDftFreqs; each thread accumulates a 4-row x 4-frequency
-// micro-tile, so one shared load feeds several FMAs.
+// micro-tile, so one shared load feeds several FMAs.  The accumulators of
+// a tile are copied into shared memory with cp.async while the tile's FMAs
+// run, so their DRAM latency overlaps the arithmetic.
 constexpr int kDftRows = 128;
 constexpr int kDftFreqs = 16;
+// dynamic shared memory of the contraction: samples, twiddles, accumulators
+constexpr size_t kDftSmem = sizeof(double) * kSampleBlock * kDftRows + sizeof(double2) * kSampleBlock * kDftFreqs +
+                            2 * sizeof(double) * kDftFreqs * kDftRows;
+
+__device__ __forceinline__ void dft_cp_async16(void* dst, const void* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src));
+}
 
 template <typename T>
 __device__ __forceinline__ void dft_contract_body(const DftView& d, const T* ring, const DevClock* clk,
                                                   const double2* tw) {
-  __shared__ double xs[kSampleBlock][kDftRows];
-  __shared__ double2 ws[kSampleBlock][kDftFreqs];
+  extern __shared__ __align__(16) unsigned char dft_smem[];
+  double(*xs)[kDftRows] = reinterpret_cast<double(*)[kDftRows]>(dft_smem);
+  double2(*ws)[kDftFreqs] = reinterpret_cast<double2(*)[kDftFreqs]>(dft_smem + sizeof(double) * kSampleBlock * kDftRows);
+  double(*ar)[kDftRows] = reinterpret_cast<double(*)[kDftRows]>(
+      dft_smem + sizeof(double) * kSampleBlock * kDftRows + sizeof(double2) * kSampleBlock * kDftFreqs);
+  double(*ai)[kDftRows] = ar + kDftFreqs;
   const int nsamp = min(kSampleBlock, clk->nsamp);
   const long long r0 = (long long)blockIdx.x * kDftRows;
   if (r0 >= d.rows) return;  // batched launches size the grid for the largest simulation
@@ -743,7 +757,17 @@ __device__ __forceinline__ void dft_contract_body(const DftView& d, const T* rin
   const int rg = tid & 31, fg = tid >> 5;  // rows rg*4..+3, freqs fg*4..+3
   const double2* twh = tw + (size_t)h * kSampleBlock * d.nf;
   for (int f0 = 0; f0 < d.nf; f0 += kDftFreqs) {
-    __syncthreads();  // xs loaded / previous tile's ws consumed
+    __syncthreads();  // xs loaded / previous tile's ws and accumulators consumed
+    // this tile's accumulators, 16 bytes (two rows) per copy
+    for (int q = tid; q < kDftFreqs * kDftRows / 2; q += 128) {
+      const int fl = q / (kDftRows / 2), rr = 2 * (q - fl * (kDftRows / 2));
+      if (f0 + fl < d.nf) {
+        const size_t o = (size_t)(f0 + fl) * d.rows + r0 + rr;
+        dft_cp_async16(&ar[fl][rr], d.acc_re + o);
+        dft_cp_async16(&ai[fl][rr], d.acc_im + o);
+      }
+    }
+    asm volatile("cp.async.commit_group;\n" ::);
     for (int q = tid; q < kSampleBlock * kDftFreqs; q += 128) {
       const int sidx = q / kDftFreqs, fl = q - sidx * kDftFreqs;
       ws[sidx][fl] = (f0 + fl < d.nf) ? twh[(size_t)sidx * d.nf + f0 + fl] : make_double2(0.0, 0.0);
@@ -768,17 +792,22 @@ __device__ __forceinline__ void dft_contract_body(const DftView& d, const T* rin
         }
       }
     }
+    asm volatile("cp.async.wait_all;\n" ::);
+    __syncthreads();  // every thread's copies have landed
 #pragma unroll
     for (int b = 0; b < 4; b++) {
-      const int f = f0 + fg * 4 + b;
+      const int fl = fg * 4 + b, f = f0 + fl;
       if (f >= d.nf) continue;
       double* pr = d.acc_re + (size_t)f * d.rows + r0 + rg * 4;
       double* pi = d.acc_im + (size_t)f * d.rows + r0 + rg * 4;
-#pragma unroll
-      for (int a = 0; a < 4; a++) {
-        pr[a] += re[a][b];
-        pi[a] += im[a][b];
-      }
+      const double2 r01 = *reinterpret_cast<const double2*>(&ar[fl][rg * 4]);
+      const double2 r23 = *reinterpret_cast<const double2*>(&ar[fl][rg * 4 + 2]);
+      const double2 i01 = *reinterpret_cast<const double2*>(&ai[fl][rg * 4]);
+      const double2 i23 = *reinterpret_cast<const double2*>(&ai[fl][rg * 4 + 2]);
+      *reinterpret_cast<double2*>(pr) = make_double2(r01.x + re[0][b], r01.y + re[1][b]);
+      *reinterpret_cast<double2*>(pr + 2) = make_double2(r23.x + re[2][b], r23.y + re[3][b]);
+      *reinterpret_cast<double2*>(pi) = make_double2(i01.x + im[0][b], i01.y + im[1][b]);
+      *reinterpret_cast<double2*>(pi + 2) = make_double2(i23.x + im[2][b], i23.y + im[3][b]);
     }
   }
 }
