@@ -302,10 +302,11 @@ static fdtd_status build_views(fdtd_sim* s) {
       return at;
     };
     CpmlAxis<T>& ca = v.cp[a];
-    ca.be_N = put(t.be_N, Nc + 1); ca.ce_N = put(t.ce_N, Nc + 1);
-    ca.be_F = put(t.be_F, Nc + 1); ca.ce_F = put(t.ce_F, Nc + 1);
-    ca.bh_N = put(t.bh_N, Nc + 1); ca.ch_N = put(t.ch_N, Nc + 1);
-    ca.bh_F = put(t.bh_F, Nc + 1); ca.ch_F = put(t.ch_F, Nc + 1);
+    // near then far, each Nc+1 entries, so that one index walks both slabs
+    ca.be_N = put(t.be_N, Nc + 1); ca.be_F = put(t.be_F, Nc + 1);
+    ca.ce_N = put(t.ce_N, Nc + 1); ca.ce_F = put(t.ce_F, Nc + 1);
+    ca.bh_N = put(t.bh_N, Nc + 1); ca.bh_F = put(t.bh_F, Nc + 1);
+    ca.ch_N = put(t.ch_N, Nc + 1); ca.ch_F = put(t.ch_F, Nc + 1);
     std::vector<double> ik(N3[a]), ih(N3[a]);
     for (int i = 0; i < N3[a]; i++) { ik[i] = 1.0 / t.ked[i]; ih[i] = 1.0 / t.khd[i]; }
     ca.inv_ked = put(ik, N3[a]);
@@ -336,12 +337,14 @@ static fdtd_status build_views(fdtd_sim* s) {
       if (ax == 2) { cells_e = (size_t)(Nc + 1) * s->plane; cells_h = (size_t)Nc * s->plane; }
       else if (ax == 1) { cells_e = (size_t)s->NZ * (Nc + 1) * s->PX; cells_h = (size_t)s->NZ * Nc * s->PX; }
       else { cells_e = (size_t)s->NZ * s->NY * (Nc + 1); cells_h = (size_t)s->NZ * s->NY * Nc; }
-      T *a1, *a2, *a3, *a4;
+      // near slab then far slab in one allocation (the passes index both
+      // from the near pointer)
+      T *a1, *a3;
       cudaError_t e;
-      if ((e = s->alloc(&a1, cells_e, true)) != cudaSuccess || (e = s->alloc(&a2, cells_e, true)) != cudaSuccess ||
-          (e = s->alloc(&a3, cells_h, true)) != cudaSuccess || (e = s->alloc(&a4, cells_h, true)) != cudaSuccess)
+      if ((e = s->alloc(&a1, 2 * cells_e, true)) != cudaSuccess || (e = s->alloc(&a3, 2 * cells_h, true)) != cudaSuccess)
         return fail(FDTD_ERR_ALLOC, cudaGetErrorString(e));
-      v.psiE_N[c][slot] = a1; v.psiE_F[c][slot] = a2; v.psiH_N[c][slot] = a3; v.psiH_F[c][slot] = a4;
+      v.psiE_N[c][slot] = a1; v.psiE_F[c][slot] = a1 + cells_e;
+      v.psiH_N[c][slot] = a3; v.psiH_F[c][slot] = a3 + cells_h;
     }
   // TFSF
   TfsfView& tf = v.tf;

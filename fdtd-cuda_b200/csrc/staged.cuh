@@ -227,7 +227,9 @@ __device__ __forceinline__ void h_pass_tile(const SimView<T>& s, int kchunk, int
   if (pml_xy) { sx = slab_h(s.cp[0], i); sy = slab_h(s.cp[1], j); }
   const T idx_ = s.cp[0].inv_d, idy_ = s.cp[1].inv_d, idz_ = s.cp[2].inv_d;
   const int Ncz = s.cp[2].Nc, Fz = s.cp[2].F;
-  const size_t xstep = (size_t)NY * s.cp[0].Nc, ystep = (size_t)s.cp[1].Nc * PX;
+  // psi offsets in 32 bits; near and far slabs are contiguous (near first)
+  const unsigned xstep = (unsigned)NY * (unsigned)s.cp[0].Nc, ystep = (unsigned)s.cp[1].Nc * (unsigned)PX;
+  const unsigned plane32 = (unsigned)plane, jrow = (unsigned)j * (unsigned)PX + (unsigned)i;
   T* bx0 = nullptr;  // psi_hy(x) at plane 0
   T* bx1 = nullptr;  // psi_hz(x)
   T* by0 = nullptr;  // psi_hx(y)
@@ -242,34 +244,33 @@ __device__ __forceinline__ void h_pass_tile(const SimView<T>& s, int kchunk, int
     by0 = (sy.side == 1 ? s.psiH_N[0][0] : s.psiH_F[0][0]) + q;
     by1 = (sy.side == 1 ? s.psiH_N[2][1] : s.psiH_F[2][1]) + q;
   }
-  const size_t jrow = (size_t)j * PX + i;
+  T* const pz0 = s.psiH_N[0][1];  // psi_hx(z)
+  T* const pz1 = s.psiH_N[1][0];  // psi_hy(z)
+  // z-slab plane of the psi arrays (near 0..Nc-1, far Nc..) and of the
+  // bh/ch tables (near 0..Nc-1, far Nc+1..: the tables hold Nc+1 entries a
+  // side); -1 outside the slabs
+  auto zq = [&](int kk) -> int { return kk < Ncz ? kk : (kk >= Fz ? kk - Fz + Ncz : -1); };
+  unsigned ox = (unsigned)k0 * xstep, oy = (unsigned)k0 * ystep;  // x/y psi offsets of plane k
   // psi of the next plane, prefetched one plane ahead
   T nz0 = 0, nz1 = 0, nx0 = 0, nx1 = 0, ny0 = 0, ny1 = 0;
-  auto zside = [&](int kk, int& q) -> int {
-    if (kk < Ncz) { q = kk; return 1; }
-    if (kk >= Fz) { q = kk - Fz; return 2; }
-    q = 0;
-    return 0;
-  };
-  auto fetch = [&](int kk) {
+  auto fetch = [&](int kk, unsigned oxk, unsigned oyk) {
     if (!pml_xy || kk >= NZ - 1) return;
-    int q;
-    const int zs = zside(kk, q);
-    if (zs) {
-      const size_t off = (size_t)q * plane + jrow;
-      nz0 = (zs == 1 ? s.psiH_N[0][1] : s.psiH_F[0][1])[off];
-      nz1 = (zs == 1 ? s.psiH_N[1][0] : s.psiH_F[1][0])[off];
+    const int q = zq(kk);
+    if (q >= 0) {
+      const unsigned off = (unsigned)q * plane32 + jrow;
+      nz0 = pz0[off];
+      nz1 = pz1[off];
     }
-    if (sx.side) { nx0 = bx0[(size_t)kk * xstep]; nx1 = bx1[(size_t)kk * xstep]; }
-    if (sy.side) { ny0 = by0[(size_t)kk * ystep]; ny1 = by1[(size_t)kk * ystep]; }
+    if (sx.side) { nx0 = bx0[oxk]; nx1 = bx1[oxk]; }
+    if (sy.side) { ny0 = by0[oyk]; ny1 = by1[oyk]; }
   };
-  fetch(k0);
+  fetch(k0, ox, oy);
   for (int k = k0; k < k1;) {
 #pragma unroll
     for (int u = 0; u < S; u++) {
       if (k < k1) {
         const T cz0 = nz0, cz1 = nz1, cx0 = nx0, cx1 = nx1, cy0 = ny0, cy1 = ny1;
-        if (k + 1 < k1) fetch(k + 1);
+        if (k + 1 < k1) fetch(k + 1, ox + xstep, oy + ystep);
         cp_async_wait<S - 3>();  // planes up to k+1 have landed
         __syncthreads();
         // stage (u+S-1)%S held plane k-1, last read in the previous iteration
@@ -289,24 +290,22 @@ __device__ __forceinline__ void h_pass_tile(const SimView<T>& s, int kchunk, int
           T vy = chh * hown[TY * 32 + oo] + che * ((ez_i - ezk) * ikx - (exk1 - exk) * ikz);
           T vz = chh * hown[2 * TY * 32 + oo] + che * ((ex_j - exk) * iky - (ey_i - eyk) * ikx);
           if (pml_xy && hask) {
-            int q;
-            const int zs = zside(k, q);
-            if (zs) {
-              const size_t off = (size_t)q * plane + jrow;
-              const T b = ldg((zs == 1 ? s.cp[2].bh_N : s.cp[2].bh_F) + q);
-              const T c = ldg((zs == 1 ? s.cp[2].ch_N : s.cp[2].ch_F) + q);
-              vx += che * psi_apply((zs == 1 ? s.psiH_N[0][1] : s.psiH_F[0][1]) + off, cz0, b, c, eyk1 - eyk, idz_);
-              vy -= che * psi_apply((zs == 1 ? s.psiH_N[1][0] : s.psiH_F[1][0]) + off, cz1, b, c, exk1 - exk, idz_);
+            const int q = zq(k);
+            if (q >= 0) {
+              const unsigned off = (unsigned)q * plane32 + jrow;
+              const int qt = q < Ncz ? q : q + 1;  // table index (Nc+1 entries a side)
+              const T b = ldg(s.cp[2].bh_N + qt);
+              const T c = ldg(s.cp[2].ch_N + qt);
+              vx += che * psi_apply(pz0 + off, cz0, b, c, eyk1 - eyk, idz_);
+              vy -= che * psi_apply(pz1 + off, cz1, b, c, exk1 - exk, idz_);
             }
             if (sx.side) {
-              const size_t off = (size_t)k * xstep;
-              vy += che * psi_apply(bx0 + off, cx0, sx.b, sx.c, ez_i - ezk, idx_);
-              vz -= che * psi_apply(bx1 + off, cx1, sx.b, sx.c, ey_i - eyk, idx_);
+              vy += che * psi_apply(bx0 + ox, cx0, sx.b, sx.c, ez_i - ezk, idx_);
+              vz -= che * psi_apply(bx1 + ox, cx1, sx.b, sx.c, ey_i - eyk, idx_);
             }
             if (sy.side) {
-              const size_t off = (size_t)k * ystep;
-              vx -= che * psi_apply(by0 + off, cy0, sy.b, sy.c, ez_j - ezk, idy_);
-              vz += che * psi_apply(by1 + off, cy1, sy.b, sy.c, ex_j - exk, idy_);
+              vx -= che * psi_apply(by0 + oy, cy0, sy.b, sy.c, ez_j - ezk, idy_);
+              vz += che * psi_apply(by1 + oy, cy1, sy.b, sy.c, ex_j - exk, idy_);
             }
           }
           if (hasy && hask) *phx = vx;
@@ -314,6 +313,7 @@ __device__ __forceinline__ void h_pass_tile(const SimView<T>& s, int kchunk, int
           if (hasx && hasy) *phz = vz;
         }
         phx += plane; phy += plane; phz += plane; ikzp++;
+        if (PML) { ox += xstep; oy += ystep; }
         k++;
       }
     }
@@ -408,7 +408,9 @@ __device__ __forceinline__ void e_pass_tile(const SimView<T>& s, int kchunk, int
   }
   const T idx_ = s.cp[0].inv_d, idy_ = s.cp[1].inv_d, idz_ = s.cp[2].inv_d;
   const int Ncz = s.cp[2].Nc, Fz = s.cp[2].F;
-  const size_t xstep = (size_t)NY * (s.cp[0].Nc + 1), ystep = (size_t)(s.cp[1].Nc + 1) * PX;
+  // psi offsets in 32 bits; near and far slabs are contiguous (near first)
+  const unsigned xstep = (unsigned)NY * (unsigned)(s.cp[0].Nc + 1), ystep = (unsigned)(s.cp[1].Nc + 1) * (unsigned)PX;
+  const unsigned plane32 = (unsigned)plane, jrow = (unsigned)j * (unsigned)PX + (unsigned)i;
   T* bx0 = nullptr;  // psi_ey(x) at plane 0
   T* bx1 = nullptr;  // psi_ez(x)
   T* by0 = nullptr;  // psi_ex(y)
@@ -423,34 +425,32 @@ __device__ __forceinline__ void e_pass_tile(const SimView<T>& s, int kchunk, int
     by0 = (sy.side == 1 ? s.psiE_N[0][0] : s.psiE_F[0][0]) + q;
     by1 = (sy.side == 1 ? s.psiE_N[2][1] : s.psiE_F[2][1]) + q;
   }
-  const size_t jrow = (size_t)j * PX + i;
+  T* const pz0 = s.psiE_N[0][1];  // psi_ex(z)
+  T* const pz1 = s.psiE_N[1][0];  // psi_ey(z)
+  // z-slab index of a plane (near 0..Nc, far Nc+1..), -1 outside: indexes
+  // the psi planes and the be/ce tables alike
+  auto zq = [&](int kk) -> int { return kk <= Ncz ? kk : (kk >= Fz ? kk - Fz + Ncz + 1 : -1); };
+  unsigned ox = (unsigned)k0 * xstep, oy = (unsigned)k0 * ystep;  // x/y psi offsets of plane k
   T nz0 = 0, nz1 = 0, nx0 = 0, nx1 = 0, ny0 = 0, ny1 = 0;
-  auto zside = [&](int kk, int& q) -> int {
-    if (kk <= Ncz) { q = kk; return 1; }
-    if (kk >= Fz) { q = kk - Fz; return 2; }
-    q = 0;
-    return 0;
-  };
-  auto fetch = [&](int kk) {
+  auto fetch = [&](int kk, unsigned oxk, unsigned oyk) {
     if (!pml_xy || kk >= NZ - 1) return;
-    int q;
-    const int zs = zside(kk, q);
-    if (zs) {
-      const size_t off = (size_t)q * plane + jrow;
-      nz0 = (zs == 1 ? s.psiE_N[0][1] : s.psiE_F[0][1])[off];
-      nz1 = (zs == 1 ? s.psiE_N[1][0] : s.psiE_F[1][0])[off];
+    const int q = zq(kk);
+    if (q >= 0) {
+      const unsigned off = (unsigned)q * plane32 + jrow;
+      nz0 = pz0[off];
+      nz1 = pz1[off];
     }
-    if (sx.side) { nx0 = bx0[(size_t)kk * xstep]; nx1 = bx1[(size_t)kk * xstep]; }
-    if (sy.side) { ny0 = by0[(size_t)kk * ystep]; ny1 = by1[(size_t)kk * ystep]; }
+    if (sx.side) { nx0 = bx0[oxk]; nx1 = bx1[oxk]; }
+    if (sy.side) { ny0 = by0[oyk]; ny1 = by1[oyk]; }
   };
-  fetch(k0);
+  fetch(k0, ox, oy);
   T check = T(0);
   for (int k = k0; k < k1;) {
 #pragma unroll
     for (int u = 0; u < S; u++) {
       if (k < k1) {
         const T cz0 = nz0, cz1 = nz1, cx0 = nx0, cx1 = nx1, cy0 = ny0, cy1 = ny1;
-        if (k + 1 < k1) fetch(k + 1);
+        if (k + 1 < k1) fetch(k + 1, ox + xstep, oy + ystep);
         cp_async_wait<S - 3>();  // planes up to k have landed
         __syncthreads();
         // stage (u+S-1)%S held plane k-2, last read in the previous iteration
@@ -482,24 +482,21 @@ __device__ __forceinline__ void e_pass_tile(const SimView<T>& s, int kchunk, int
           const bool wy = coly && hasz && okz && !(m & 2);
           const bool wz = colz && okz && !(m & 4);
           if (pml_xy && okz) {
-            int q;
-            const int zs = zside(k, q);
-            if (zs) {
-              const size_t off = (size_t)q * plane + jrow;
-              const T b = ldg((zs == 1 ? s.cp[2].be_N : s.cp[2].be_F) + q);
-              const T c = ldg((zs == 1 ? s.cp[2].ce_N : s.cp[2].ce_F) + q);
-              if (wx) vx -= ceh * psi_apply((zs == 1 ? s.psiE_N[0][1] : s.psiE_F[0][1]) + off, cz0, b, c, hyk - hym, idz_);
-              if (wy) vy += ceh * psi_apply((zs == 1 ? s.psiE_N[1][0] : s.psiE_F[1][0]) + off, cz1, b, c, hxk - hxm, idz_);
+            const int q = zq(k);
+            if (q >= 0) {
+              const unsigned off = (unsigned)q * plane32 + jrow;
+              const T b = ldg(s.cp[2].be_N + q);  // be_N then be_F
+              const T c = ldg(s.cp[2].ce_N + q);  // ce_N then ce_F
+              if (wx) vx -= ceh * psi_apply(pz0 + off, cz0, b, c, hyk - hym, idz_);
+              if (wy) vy += ceh * psi_apply(pz1 + off, cz1, b, c, hxk - hxm, idz_);
             }
             if (sy.side) {
-              const size_t off = (size_t)k * ystep;
-              if (wx) vx += ceh * psi_apply(by0 + off, cy0, sy.b, sy.c, hzk - hz_j, idy_);
-              if (wz) vz -= ceh * psi_apply(by1 + off, cy1, sy.b, sy.c, hxk - hx_j, idy_);
+              if (wx) vx += ceh * psi_apply(by0 + oy, cy0, sy.b, sy.c, hzk - hz_j, idy_);
+              if (wz) vz -= ceh * psi_apply(by1 + oy, cy1, sy.b, sy.c, hxk - hx_j, idy_);
             }
             if (sx.side) {
-              const size_t off = (size_t)k * xstep;
-              if (wy) vy -= ceh * psi_apply(bx0 + off, cx0, sx.b, cx_ey, hzk - hz_i, idx_);
-              if (wz) vz += ceh * psi_apply(bx1 + off, cx1, sx.b, sx.c, hyk - hy_i, idx_);
+              if (wy) vy -= ceh * psi_apply(bx0 + ox, cx0, sx.b, cx_ey, hzk - hz_i, idx_);
+              if (wz) vz += ceh * psi_apply(bx1 + ox, cx1, sx.b, sx.c, hyk - hy_i, idx_);
             }
           }
           if (wx) { *pex = vx; check += vx; }
@@ -507,6 +504,7 @@ __device__ __forceinline__ void e_pass_tile(const SimView<T>& s, int kchunk, int
           if (wz) { *pez = vz; check += vz; }
         }
         pex += plane; pey += plane; pez += plane; ikzp++;
+        if (PML) { ox += xstep; oy += ystep; }
         k++;
       }
     }
