@@ -153,14 +153,26 @@ def pass_bytes(dims, params, esize, which):
 # ----------------------------------------------------------------------
 # the reference arm and the CPU baseline: the oracle port on host cores
 
-def cpu_sample(steps=8):
-    """Times the FP64 CPU restatement (oracle) on the same 256^3 workload for
-    a bounded number of time steps (DFT samples included at t = 0 and 4)."""
+def max_over_ranks(x, world, device):
+    """The largest of a per-rank value over all ranks (the step time of the
+    slowest replica), on the process group's device."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_sample(steps=8, grid=256, num_freq=201):
+    """Times the FP64 CPU restatement (oracle) on the same workload for a
+    bounded number of time steps (DFT samples included at t = 0 and 4)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     cores = os.cpu_count() or 1
     O.lib().orc_set_threads(cores)
-    p = workload_params(O, 1)
+    p = workload_params(O, 1, grid=grid, NUM_freq=num_freq)
     s = O.OracleSim(p, threads=cores)
     s.step(1)  # first step allocates the DFT accumulators
     t0 = time.perf_counter()
@@ -169,7 +181,7 @@ def cpu_sample(steps=8):
     cells = s.shape[0] * s.shape[1] * s.shape[2]
     return {"value": cells * steps / dt / 1e9, "unit": "Gcell-steps/s", "cores": cores,
             "kind": "port",
-            "sample": f"{steps} time steps of the 256^3 workload (FP64, incl. 2 DFT samples), "
+            "sample": f"{steps} time steps of the {grid}^3 workload (FP64, incl. 2 DFT samples), "
                       f"{dt:.1f} s"}
 
 
@@ -343,7 +355,7 @@ def ref_gpu_build(t1=40, t2=240):
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    cb = cpu_sample()
+    cb = cpu_sample(grid=args.grid, num_freq=args.num_freq)
     line = {
         "impl": "reference", "metric": METRIC, "value": cb["value"], "unit": cb["unit"],
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -392,9 +404,14 @@ def main():
     import torch
     import torch.distributed as dist
     if world > 1:
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", device_id=torch.device("cuda", local),
-                                timeout=__import__("datetime").timedelta(seconds=600))
+        # one process per GPU over NCCL; gloo where no GPU is present (the
+        # CPU-only reference arm and the harness tests)
+        timeout = __import__("datetime").timedelta(seconds=600)
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", device_id=torch.device("cuda", local), timeout=timeout)
+        else:
+            dist.init_process_group("gloo", timeout=timeout)
 
     if args.impl == "reference":
         run_reference(args, rank, world)
@@ -417,12 +434,8 @@ def main():
         if world > 1:
             dist.barrier()
 
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    def max_over_ranks_(x):
+        return max_over_ranks(x, world, "cuda")
 
     def timed_blocks(sim, k):
         st0 = sim.stats()
@@ -436,7 +449,7 @@ def main():
         e1.record(stream)
         torch.cuda.synchronize()
         barrier()
-        ms = max_over_ranks(e0.elapsed_time(e1))
+        ms = max_over_ranks_(e0.elapsed_time(e1))
         st1 = sim.stats()
         return ms, st1.kernels - st0.kernels
 
@@ -499,7 +512,7 @@ def main():
         stream.synchronize()
     w1 = time.perf_counter()
     barrier()
-    e2e_s = max_over_ranks(w1 - w0)
+    e2e_s = max_over_ranks_(w1 - w0)
     e2e = None if args.no_e2e else {"value": round(world * cells * BLOCK * args.steps / e2e_s / 1e9, 3),
            "unit": "Gcell-steps/s", "h2d_bytes_per_step": BLOCK * 8,
            "d2h_bytes_per_step": BLOCK * 3 * 8,
