@@ -89,3 +89,110 @@ __global__ void tfsf_e_faces(const SimView<T>* __restrict__ gv, const ShellCells
 }
 
 }  // namespace fdtd
+
+namespace fdtd {
+
+// TFSF corrections tabulated once at create: per face cell and component
+// with at least one correction, up to two (line index, weight, meta) terms
+// in the reference's order; meta = (sign > 0) | axis << 1 | component << 3.
+// Applying a term is the same arithmetic as tfsf_h / tfsf_e with the
+// projection and the truncation already done.
+struct TfsfTable {
+  int n;                      // groups
+  const unsigned* id;         // cell offset in the device layout
+  const unsigned char* cn;    // component | terms << 2
+  const int* idx[2];          // line index of the left interpolation point
+  const double* dp[2];        // interpolation weight of the right point
+  const unsigned char* meta[2];
+};
+
+// dense build: slot (q, c) of shell cell q and component c
+template <typename T>
+__global__ void tfsf_tabulate(const SimView<T>* __restrict__ gv, const ShellCells sh, int efield, unsigned* id,
+                              unsigned char* cn, int* idx0, int* idx1, double* dp0, double* dp1,
+                              unsigned char* m0, unsigned char* m1) {
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= sh.total()) return;
+  const SimView<T>& g = *gv;
+  int i, j, k;
+  sh.cell(q, i, j, k);
+  for (int c = 0; c < 3; c++) {
+    int nt = 0;
+    int ix[2] = {0, 0};
+    double w[2] = {0, 0};
+    unsigned char mm[2] = {0, 0};
+    auto rec = [&](int sg, int ax, int f, double d) {
+      if (nt < 2) {
+        if (efield) {  // hinc_at
+          const double d2 = d + 0.5;
+          const int n = (int)d2;
+          ix[nt] = g.tf.m0 - 1 + n;
+          w[nt] = d2 - n;
+        } else {  // einc_at
+          const int n = (int)d;
+          ix[nt] = g.tf.m0 + n;
+          w[nt] = d - n;
+        }
+        mm[nt] = (unsigned char)((sg > 0 ? 1 : 0) | (ax << 1) | (f << 3));
+      }
+      nt++;
+    };
+    if (efield) tfsf_e_walk(g, c, i, j, k, rec);
+    else tfsf_h_walk(g, c, i, j, k, rec);
+    const size_t o = (size_t)q * 3 + c;
+    id[o] = (unsigned)fidx(g.PX, g.plane, i, j, k);
+    cn[o] = (unsigned char)(c | (min(nt, 3) << 2));  // 3 terms would be a bug: flagged, not applied
+    idx0[o] = ix[0]; idx1[o] = ix[1];
+    dp0[o] = w[0]; dp1[o] = w[1];
+    m0[o] = mm[0]; m1[o] = mm[1];
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ T tfsf_term(const double* line, const float* dir, int idx, double dp, unsigned meta, T v,
+                                       T coef, const T* dd) {
+  const T x = (T)(((1 - dp) * line[idx] + dp * line[idx + 1]) * (double)dir[meta >> 3]);
+  const int ax = (meta >> 1) & 3;
+  if (meta & 1) v += coef * x / dd[ax];
+  else v -= coef * x / dd[ax];
+  return v;
+}
+
+template <typename T>
+__global__ void tfsf_h_apply(const __grid_constant__ SimView<T> s, const __grid_constant__ TfsfTable tb) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= tb.n) return;
+  const unsigned id = tb.id[g];
+  const unsigned cn = tb.cn[g];
+  const int c = cn & 3, nt = cn >> 2;
+  const T dd[3] = {s.dxyz[0], s.dxyz[1], s.dxyz[2]};
+  T v = s.H[c][id];
+  v = tfsf_term(s.e_inc, s.tf.fe, tb.idx[0][g], tb.dp[0][g], tb.meta[0][g], v, s.che, dd);
+  if (nt > 1) v = tfsf_term(s.e_inc, s.tf.fe, tb.idx[1][g], tb.dp[1][g], tb.meta[1][g], v, s.che, dd);
+  s.H[c][id] = v;
+}
+
+template <typename T>
+__global__ void tfsf_e_apply(const __grid_constant__ SimView<T> s, const __grid_constant__ TfsfTable tb) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= tb.n) return;
+  const unsigned id = tb.id[g];
+  const unsigned cn = tb.cn[g];
+  const int c = cn & 3, nt = cn >> 2;
+  const size_t plane = s.plane;
+  const int k = (int)(id / plane);
+  const int r = (int)(id - (size_t)k * plane);
+  const int j = r / s.PX, i = r - j * s.PX;
+  unsigned m = 0;
+  if (i >= s.mat_lo[0] && i < s.mat_hi[0] && j >= s.mat_lo[1] && j < s.mat_hi[1] && k >= s.mat_lo[2] &&
+      k < s.mat_hi[2])
+    m = s.mat[id];
+  const T ceh = s.ceh[m >> 3];
+  const T dd[3] = {s.dxyz[0], s.dxyz[1], s.dxyz[2]};
+  T v = s.E[c][id];
+  v = tfsf_term(s.h_inc, s.tf.fh, tb.idx[0][g], tb.dp[0][g], tb.meta[0][g], v, ceh, dd);
+  if (nt > 1) v = tfsf_term(s.h_inc, s.tf.fh, tb.idx[1][g], tb.dp[1][g], tb.meta[1][g], v, ceh, dd);
+  s.E[c][id] = v;
+}
+
+}  // namespace fdtd

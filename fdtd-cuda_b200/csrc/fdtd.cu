@@ -80,6 +80,7 @@ struct fdtd_sim {
   };
   std::vector<TileSet> tilesets;
   ShellCells shell_h, shell_e;
+  TfsfTable tf_h{}, tf_e{};  // tabulated TFSF corrections of the two shells
   const void* dview = nullptr;  // device copy of the view
   PassCfg hcfg, ecfg;
   bool tuned = false;
@@ -413,6 +414,70 @@ static fdtd_status build_views(fdtd_sim* s) {
 template <typename T>
 static fdtd_status tune_passes(fdtd_sim* s, bool time_variants);
 
+// Tabulates the TFSF corrections of one shell (tfsf_tabulate on the device,
+// so the projections round exactly as in the applying kernels), keeps the
+// (cell, component) groups that have terms and uploads them packed.
+template <typename T>
+static fdtd_status build_tfsf_table(fdtd_sim* s, const ShellCells& sh, int efield, TfsfTable& out) {
+  const long long nq = sh.total();
+  out = TfsfTable{};
+  if (nq <= 0) return FDTD_OK;
+  const size_t n = (size_t)nq * 3;
+  DevBuf b;
+  const size_t bytes = n * (4 + 1 + 4 + 4 + 8 + 8 + 1 + 1);
+  CUDA_TRY(b.alloc(bytes));
+  char* p = static_cast<char*>(b.p);
+  double* dp0 = reinterpret_cast<double*>(p);
+  double* dp1 = dp0 + n;
+  unsigned* id = reinterpret_cast<unsigned*>(dp1 + n);
+  int* i0 = reinterpret_cast<int*>(id + n);
+  int* i1 = i0 + n;
+  unsigned char* cn = reinterpret_cast<unsigned char*>(i1 + n);
+  unsigned char* m0 = cn + n;
+  unsigned char* m1 = m0 + n;
+  tfsf_tabulate<T><<<(unsigned)((nq + 127) / 128), 128>>>(static_cast<const SimView<T>*>(s->dview), sh, efield, id,
+                                                          cn, i0, i1, dp0, dp1, m0, m1);
+  CUDA_TRY(cudaGetLastError());
+  std::vector<char> h(bytes);
+  CUDA_TRY(cudaMemcpy(h.data(), b.p, bytes, cudaMemcpyDeviceToHost));
+  const double* hdp0 = reinterpret_cast<const double*>(h.data());
+  const double* hdp1 = hdp0 + n;
+  const unsigned* hid = reinterpret_cast<const unsigned*>(hdp1 + n);
+  const int* hi0 = reinterpret_cast<const int*>(hid + n);
+  const int* hi1 = hi0 + n;
+  const unsigned char* hcn = reinterpret_cast<const unsigned char*>(hi1 + n);
+  const unsigned char* hm0 = hcn + n;
+  const unsigned char* hm1 = hm0 + n;
+  std::vector<unsigned> cid;
+  std::vector<unsigned char> ccn, cm0, cm1;
+  std::vector<int> ci0, ci1;
+  std::vector<double> cd0, cd1;
+  for (size_t q = 0; q < n; q++) {
+    const int nt = hcn[q] >> 2;
+    if (nt == 0) continue;
+    if (nt > 2) return fail(FDTD_ERR_INVALID, "a TFSF face cell has more than two corrections");
+    cid.push_back(hid[q]); ccn.push_back(hcn[q]); cm0.push_back(hm0[q]); cm1.push_back(hm1[q]);
+    ci0.push_back(hi0[q]); ci1.push_back(hi1[q]); cd0.push_back(hdp0[q]); cd1.push_back(hdp1[q]);
+  }
+  const size_t m = cid.size();
+  out.n = (int)m;
+  if (m == 0) return FDTD_OK;
+  unsigned* did; unsigned char *dcn, *dm0, *dm1; int *di0, *di1; double *dd0, *dd1;
+  CUDA_TRY(s->alloc(&did, m)); CUDA_TRY(s->alloc(&dcn, m)); CUDA_TRY(s->alloc(&dm0, m)); CUDA_TRY(s->alloc(&dm1, m));
+  CUDA_TRY(s->alloc(&di0, m)); CUDA_TRY(s->alloc(&di1, m)); CUDA_TRY(s->alloc(&dd0, m)); CUDA_TRY(s->alloc(&dd1, m));
+  CUDA_TRY(cudaMemcpy(did, cid.data(), m * 4, cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(dcn, ccn.data(), m, cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(dm0, cm0.data(), m, cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(dm1, cm1.data(), m, cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(di0, ci0.data(), m * 4, cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(di1, ci1.data(), m * 4, cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(dd0, cd0.data(), m * 8, cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(dd1, cd1.data(), m * 8, cudaMemcpyHostToDevice));
+  out.id = did; out.cn = dcn; out.meta[0] = dm0; out.meta[1] = dm1;
+  out.idx[0] = di0; out.idx[1] = di1; out.dp[0] = dd0; out.dp[1] = dd1;
+  return FDTD_OK;
+}
+
 static fdtd_status create_impl(const fdtd_params* p, int device, fdtd_sim** out, bool tune = true) {
   auto s = std::make_unique<fdtd_sim>();
   if (const char* msg = setup_build(*p, s->su)) return fail(FDTD_ERR_INVALID, msg);
@@ -604,6 +669,12 @@ static fdtd_status create_impl(const fdtd_params* p, int device, fdtd_sim** out,
     s->shell_e.init(lo, hi);
   }
   fdtd_status st = s->fp64 ? build_views<double>(s.get()) : build_views<float>(s.get());
+  if (st != FDTD_OK) return st;
+  st = s->fp64 ? build_tfsf_table<double>(s.get(), s->shell_h, 0, s->tf_h)
+              : build_tfsf_table<float>(s.get(), s->shell_h, 0, s->tf_h);
+  if (st != FDTD_OK) return st;
+  st = s->fp64 ? build_tfsf_table<double>(s.get(), s->shell_e, 1, s->tf_e)
+              : build_tfsf_table<float>(s.get(), s->shell_e, 1, s->tf_e);
   if (st != FDTD_OK) return st;
   if (s->has_design)
     for (int c = 0; c < 3; c++) {
@@ -903,9 +974,8 @@ static fdtd_status tune_passes(fdtd_sim* s, bool time_variants) {
 template <typename T>
 static void launch_h(fdtd_sim* s, cudaStream_t st) {
   s->kernels += launch_h_cfg<T>(s, s->hcfg, st) - 1;
-  const SimView<T>* dv = static_cast<const SimView<T>*>(s->dview);
-  const long long nf = s->shell_h.total();
-  if (nf > 0) tfsf_h_faces<T><<<(unsigned)((nf + 255) / 256), 256, 0, st>>>(dv, s->shell_h);
+  const int nf = s->tf_h.n;
+  if (nf > 0) tfsf_h_apply<T><<<(unsigned)((nf + 255) / 256), 256, 0, st>>>(view<T>(s), s->tf_h);
   s->kernels += 1 + (nf > 0);
 }
 template <typename T>
@@ -918,10 +988,9 @@ static void launch_metal(fdtd_sim* s, cudaStream_t st);
 
 template <typename T>
 static void launch_e(fdtd_sim* s, cudaStream_t st) {
-  const SimView<T>* dv = static_cast<const SimView<T>*>(s->dview);
-  const long long nf = s->shell_e.total();
+  const int nf = s->tf_e.n;
   // E half of CORRECT_* before the update (main.cu:2798-2813)
-  if (nf > 0) tfsf_e_faces<T><<<(unsigned)((nf + 255) / 256), 256, 0, st>>>(dv, s->shell_e);
+  if (nf > 0) tfsf_e_apply<T><<<(unsigned)((nf + 255) / 256), 256, 0, st>>>(view<T>(s), s->tf_e);
   if (s->su.hydro) launch_metal<T>(s, st);  // UpdateHydroP* read E^n here
   s->kernels += launch_e_cfg<T>(s, s->ecfg, st) - 1;
   if (!s->su.hydro) launch_metal<T>(s, st);

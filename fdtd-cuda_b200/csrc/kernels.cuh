@@ -79,148 +79,143 @@ __device__ __forceinline__ double hinc_at(const double* h, int m0, double d) {
   return (1 - dp) * h[m0 - 1 + n] + dp * h[m0 + n];
 }
 
-// The H half of CORRECT_X/Y/Z applied to H component c at (i,j,k), in the
-// reference's kernel order X, Y, Z.  v is the freshly updated value.
-template <typename T>
-__device__ __forceinline__ T tfsf_h(const SimView<T>& s, int c, int i, int j, int k, T v) {
+// The H half of CORRECT_X/Y/Z for H component c at (i,j,k), in the
+// reference's kernel order X, Y, Z: fn(sign, axis, e_component, d) per
+// correction, d the projected distance on the incident line.  The applying
+// form adds sign * che * e_inc(d) fe / d_axis; the tabulating form records
+// the line index and interpolation weight.
+template <typename T, typename Fn>
+__device__ __forceinline__ void tfsf_h_walk(const SimView<T>& s, int c, int i, int j, int k, Fn&& fn) {
   const TfsfView& tf = s.tf;
   const int NX = s.NX, NY = s.NY, NZ = s.NZ;
   const int Tx = tf.Tx, Ty = tf.Ty, Tz = tf.Tz;
   const int di = 2 * (i - tf.i0), dj = 2 * (j - tf.j0), dk = 2 * (k - tf.k0);
-  const T che = s.che;
-  const T idx_ = s.cp[0].inv_d, idy_ = s.cp[1].inv_d, idz_ = s.cp[2].inv_d;
-  (void)idx_; (void)idy_; (void)idz_;
-  const T dx = s.dxyz[0], dy = s.dxyz[1], dz = s.dxyz[2];
   if (c == 0) {  // hx: CORRECT_Y then CORRECT_Z
     if (i >= Tx && i <= NX - Tx && k >= Tz && k < NZ - Tz) {
       if (j == Ty - 1) {  // source at j+1
-        T ez = (T)(einc_at(s.e_inc, tf.m0, tf_proj(tf, di, dj + 2, dk + 1)) * (double)tf.fe[2]);
-        v += che * ez / dy;
+        fn(+1, 1, 2, tf_proj(tf, di, dj + 2, dk + 1));
       } else if (j == NY - Ty) {
-        T ez = (T)(einc_at(s.e_inc, tf.m0, tf_proj(tf, di, dj, dk + 1)) * (double)tf.fe[2]);
-        v -= che * ez / dy;
+        fn(-1, 1, 2, tf_proj(tf, di, dj, dk + 1));
       }
     }
     if (i >= Tx && i <= NX - Tx && j >= Ty && j < NY - Ty) {
       if (k == Tz - 1) {
-        T ey = (T)(einc_at(s.e_inc, tf.m0, tf_proj(tf, di, dj + 1, dk + 2)) * (double)tf.fe[1]);
-        v -= che * ey / dz;
+        fn(-1, 2, 1, tf_proj(tf, di, dj + 1, dk + 2));
       } else if (k == NZ - Tz) {
-        T ey = (T)(einc_at(s.e_inc, tf.m0, tf_proj(tf, di, dj + 1, dk)) * (double)tf.fe[1]);
-        v += che * ey / dz;
+        fn(+1, 2, 1, tf_proj(tf, di, dj + 1, dk));
       }
     }
   } else if (c == 1) {  // hy: CORRECT_X then CORRECT_Z
     if (j >= Ty && j <= NY - Ty && k >= Tz && k < NZ - Tz) {
       if (i == Tx - 1) {
-        T ez = (T)(einc_at(s.e_inc, tf.m0, tf_proj(tf, di + 2, dj, dk + 1)) * (double)tf.fe[2]);
-        v -= che * ez / dx;
+        fn(-1, 0, 2, tf_proj(tf, di + 2, dj, dk + 1));
       } else if (i == NX - Tx) {
-        T ez = (T)(einc_at(s.e_inc, tf.m0, tf_proj(tf, di, dj, dk + 1)) * (double)tf.fe[2]);
-        v += che * ez / dx;
+        fn(+1, 0, 2, tf_proj(tf, di, dj, dk + 1));
       }
     }
     if (i >= Tx && i < NX - Tx && j >= Ty && j <= NY - Ty) {
       if (k == Tz - 1) {
-        T ex = (T)(einc_at(s.e_inc, tf.m0, tf_proj(tf, di + 1, dj, dk + 2)) * (double)tf.fe[0]);
-        v += che * ex / dz;
+        fn(+1, 2, 0, tf_proj(tf, di + 1, dj, dk + 2));
       } else if (k == NZ - Tz) {
-        T ex = (T)(einc_at(s.e_inc, tf.m0, tf_proj(tf, di + 1, dj, dk)) * (double)tf.fe[0]);
-        v -= che * ex / dz;
+        fn(-1, 2, 0, tf_proj(tf, di + 1, dj, dk));
       }
     }
   } else {  // hz: CORRECT_X then CORRECT_Y
     if (j >= Ty && j < NY - Ty && k >= Tz && k <= NZ - Tz) {
       if (i == Tx - 1) {
-        T ey = (T)(einc_at(s.e_inc, tf.m0, tf_proj(tf, di + 2, dj + 1, dk)) * (double)tf.fe[1]);
-        v += che * ey / dx;
+        fn(+1, 0, 1, tf_proj(tf, di + 2, dj + 1, dk));
       } else if (i == NX - Tx) {
-        T ey = (T)(einc_at(s.e_inc, tf.m0, tf_proj(tf, di, dj + 1, dk)) * (double)tf.fe[1]);
-        v -= che * ey / dx;
+        fn(-1, 0, 1, tf_proj(tf, di, dj + 1, dk));
       }
     }
     if (i >= Tx && i < NX - Tx && k >= Tz && k <= NZ - Tz) {
       if (j == Ty - 1) {
-        T ex = (T)(einc_at(s.e_inc, tf.m0, tf_proj(tf, di + 1, dj + 2, dk)) * (double)tf.fe[0]);
-        v -= che * ex / dy;
+        fn(-1, 1, 0, tf_proj(tf, di + 1, dj + 2, dk));
       } else if (j == NY - Ty) {
-        T ex = (T)(einc_at(s.e_inc, tf.m0, tf_proj(tf, di + 1, dj, dk)) * (double)tf.fe[0]);
-        v += che * ex / dy;
+        fn(+1, 1, 0, tf_proj(tf, di + 1, dj, dk));
       }
     }
   }
-  return v;
 }
 
-// The E half of CORRECT_X/Y/Z, added to E component c before its update
-// (the reference launches CORRECT_* before UPDATE_e*).  ceh is the cell's
-// E-on-H coefficient (the reference uses Cexh for ex and ey, Cezh for ez;
-// they are equal per cell).
-template <typename T>
-__device__ __forceinline__ T tfsf_e(const SimView<T>& s, int c, int i, int j, int k, T v, T ceh) {
+// The E half of CORRECT_X/Y/Z for E component c, added before its update
+// (the reference launches CORRECT_* before UPDATE_e*): fn(sign, axis,
+// h_component, d) per correction.
+template <typename T, typename Fn>
+__device__ __forceinline__ void tfsf_e_walk(const SimView<T>& s, int c, int i, int j, int k, Fn&& fn) {
   const TfsfView& tf = s.tf;
   const int NX = s.NX, NY = s.NY, NZ = s.NZ;
   const int Tx = tf.Tx, Ty = tf.Ty, Tz = tf.Tz;
   const int di = 2 * (i - tf.i0), dj = 2 * (j - tf.j0), dk = 2 * (k - tf.k0);
-  const T dx = s.dxyz[0], dy = s.dxyz[1], dz = s.dxyz[2];
   if (c == 0) {  // ex: CORRECT_Y then CORRECT_Z
     if (i >= Tx && i < NX - Tx && k >= Tz && k <= NZ - Tz) {
       if (j == Ty) {
-        T hz = (T)(hinc_at(s.h_inc, tf.m0, tf_proj(tf, di + 1, dj - 1, dk)) * (double)tf.fh[2]);
-        v -= ceh * hz / dy;
+        fn(-1, 1, 2, tf_proj(tf, di + 1, dj - 1, dk));
       } else if (j == NY - Ty) {
-        T hz = (T)(hinc_at(s.h_inc, tf.m0, tf_proj(tf, di + 1, dj + 1, dk)) * (double)tf.fh[2]);
-        v += ceh * hz / dy;
+        fn(+1, 1, 2, tf_proj(tf, di + 1, dj + 1, dk));
       }
     }
     if (i >= Tx && i < NX - Tx && j >= Ty && j <= NY - Ty) {
       if (k == Tz) {
-        T hy = (T)(hinc_at(s.h_inc, tf.m0, tf_proj(tf, di + 1, dj, dk - 1)) * (double)tf.fh[1]);
-        v += ceh * hy / dz;
+        fn(+1, 2, 1, tf_proj(tf, di + 1, dj, dk - 1));
       } else if (k == NZ - Tz) {
-        T hy = (T)(hinc_at(s.h_inc, tf.m0, tf_proj(tf, di + 1, dj, dk + 1)) * (double)tf.fh[1]);
-        v -= ceh * hy / dz;
+        fn(-1, 2, 1, tf_proj(tf, di + 1, dj, dk + 1));
       }
     }
   } else if (c == 1) {  // ey: CORRECT_X then CORRECT_Z
     if (j >= Ty && j < NY - Ty && k >= Tz && k <= NZ - Tz) {
       if (i == Tx) {
-        T hz = (T)(hinc_at(s.h_inc, tf.m0, tf_proj(tf, di - 1, dj + 1, dk)) * (double)tf.fh[2]);
-        v += ceh * hz / dx;
+        fn(+1, 0, 2, tf_proj(tf, di - 1, dj + 1, dk));
       } else if (i == NX - Tx) {
-        T hz = (T)(hinc_at(s.h_inc, tf.m0, tf_proj(tf, di + 1, dj + 1, dk)) * (double)tf.fh[2]);
-        v -= ceh * hz / dx;
+        fn(-1, 0, 2, tf_proj(tf, di + 1, dj + 1, dk));
       }
     }
     if (i >= Tx && i <= NX - Tx && j >= Ty && j < NY - Ty) {
       if (k == Tz) {
-        T hx = (T)(hinc_at(s.h_inc, tf.m0, tf_proj(tf, di, dj + 1, dk - 1)) * (double)tf.fh[0]);
-        v -= ceh * hx / dz;
+        fn(-1, 2, 0, tf_proj(tf, di, dj + 1, dk - 1));
       } else if (k == NZ - Tz) {
-        T hx = (T)(hinc_at(s.h_inc, tf.m0, tf_proj(tf, di, dj + 1, dk + 1)) * (double)tf.fh[0]);
-        v += ceh * hx / dz;
+        fn(+1, 2, 0, tf_proj(tf, di, dj + 1, dk + 1));
       }
     }
   } else {  // ez: CORRECT_X then CORRECT_Y
     if (j >= Ty && j <= NY - Ty && k >= Tz && k < NZ - Tz) {
       if (i == Tx) {
-        T hy = (T)(hinc_at(s.h_inc, tf.m0, tf_proj(tf, di - 1, dj, dk + 1)) * (double)tf.fh[1]);
-        v -= ceh * hy / dx;
+        fn(-1, 0, 1, tf_proj(tf, di - 1, dj, dk + 1));
       } else if (i == NX - Tx) {
-        T hy = (T)(hinc_at(s.h_inc, tf.m0, tf_proj(tf, di + 1, dj, dk + 1)) * (double)tf.fh[1]);
-        v += ceh * hy / dx;
+        fn(+1, 0, 1, tf_proj(tf, di + 1, dj, dk + 1));
       }
     }
     if (i >= Tx && i <= NX - Tx && k >= Tz && k < NZ - Tz) {
       if (j == Ty) {
-        T hx = (T)(hinc_at(s.h_inc, tf.m0, tf_proj(tf, di, dj - 1, dk + 1)) * (double)tf.fh[0]);
-        v += ceh * hx / dy;
+        fn(+1, 1, 0, tf_proj(tf, di, dj - 1, dk + 1));
       } else if (j == NY - Ty) {
-        T hx = (T)(hinc_at(s.h_inc, tf.m0, tf_proj(tf, di, dj + 1, dk + 1)) * (double)tf.fh[0]);
-        v -= ceh * hx / dy;
+        fn(-1, 1, 0, tf_proj(tf, di, dj + 1, dk + 1));
       }
     }
   }
+}
+
+
+template <typename T>
+__device__ __forceinline__ T tfsf_h(const SimView<T>& s, int c, int i, int j, int k, T v) {
+  const T dd[3] = {s.dxyz[0], s.dxyz[1], s.dxyz[2]};
+  const T che = s.che;
+  tfsf_h_walk(s, c, i, j, k, [&](int sg, int ax, int f, double d) {
+    const T x = (T)(einc_at(s.e_inc, s.tf.m0, d) * (double)s.tf.fe[f]);
+    if (sg > 0) v += che * x / dd[ax]; else v -= che * x / dd[ax];
+  });
+  return v;
+}
+
+// ceh is the cell's E-on-H coefficient (the reference uses Cexh for ex and
+// ey, Cezh for ez; they are equal per cell).
+template <typename T>
+__device__ __forceinline__ T tfsf_e(const SimView<T>& s, int c, int i, int j, int k, T v, T ceh) {
+  const T dd[3] = {s.dxyz[0], s.dxyz[1], s.dxyz[2]};
+  tfsf_e_walk(s, c, i, j, k, [&](int sg, int ax, int f, double d) {
+    const T x = (T)(hinc_at(s.h_inc, s.tf.m0, d) * (double)s.tf.fh[f]);
+    if (sg > 0) v += ceh * x / dd[ax]; else v -= ceh * x / dd[ax];
+  });
   return v;
 }
 
