@@ -6,12 +6,13 @@
 // clock); the batch adds, in device memory, one descriptor per member and
 // one list of (member, tile) work items for the Yee passes.  A time step of
 // the whole batch is
-//   h_pass_batch      persistent grid, tiles of all members from one queue
-//   tfsf_h_faces      one launch, blockIdx.y = member
+//   h_pass_batch      two persistent grids: the CPML-free tiles of all
+//                     members from one queue, the CPML edge tiles from another
+//   tfsf_h_apply      one launch, blockIdx.y = member
 //   line_step         one launch, one CTA per member
-//   tfsf_e_faces      one launch
+//   tfsf_e_apply      one launch
 //   (hydrodynamic members: their three dispersive kernels, per member)
-//   e_pass_batch      persistent grid, one queue
+//   e_pass_batch      two persistent grids as for H
 //   metal_e           one launch
 //   dft_sample        one launch every dft_every steps, blockIdx.z = member
 //   twiddles + contraction + reset, one launch each, every 32 samples
@@ -31,6 +32,7 @@ struct BatchSim {
   LineArgs line;
   DftView dft;
   ShellCells sh_h, sh_e;
+  TfsfTable tf_h, tf_e;
   T* ring;
   double2* tw;
   DevClock* clk;
@@ -38,14 +40,14 @@ struct BatchSim {
 };
 
 template <typename T>
-__global__ void tfsf_h_faces_batch(const BatchSim<T>* __restrict__ b) {
+__global__ void tfsf_h_apply_batch(const BatchSim<T>* __restrict__ b) {
   const BatchSim<T>& x = b[blockIdx.y];
-  tfsf_h_faces_body(x.v, x.sh_h);
+  tfsf_h_apply_body(x.v, x.tf_h);
 }
 template <typename T>
-__global__ void tfsf_e_faces_batch(const BatchSim<T>* __restrict__ b) {
+__global__ void tfsf_e_apply_batch(const BatchSim<T>* __restrict__ b) {
   const BatchSim<T>& x = b[blockIdx.y];
-  tfsf_e_faces_body(x.v, x.sh_e);
+  tfsf_e_apply_body(x.v, x.tf_e);
 }
 template <typename T>
 __global__ void __launch_bounds__(1024) line_step_batch(const BatchSim<T>* __restrict__ b) {
@@ -91,8 +93,8 @@ struct fdtd_batch {
   void* descs = nullptr;  // BatchSim<T>[n]
   void* views = nullptr;  // SimView<T>[n]
   int4* items = nullptr;  // (member, bx, by, bz)
-  int* queue = nullptr;   // [2] work counters of the H and E passes
-  int nitems = 0, grid_pass = 0;
+  int* queue = nullptr;   // [4] work counters: H edge, H interior, E edge, E interior
+  int nedge = 0, ninner = 0, grid_pass = 0, grid_inner = 0;
   unsigned g_fh = 0, g_fe = 0, g_m = 0, g_s = 0, g_tw = 0, g_c = 0;
   int t = 0, host_nsamp = 0, dft_every = 0, tend = 0;
   long long kernels = 0, graph_launches = 0, graph_kernels = 0;
@@ -119,7 +121,7 @@ static fdtd_status batch_build(fdtd_batch* b) {
   const int n = (int)b->sims.size();
   std::vector<BatchSim<T>> d(n);
   std::vector<SimView<T>> v(n);
-  std::vector<int4> items;
+  std::vector<int4> items, inner;
   for (int i = 0; i < n; i++) {
     fdtd_sim* s = b->sims[i].get();
     BatchSim<T>& x = d[i];
@@ -129,6 +131,8 @@ static fdtd_status batch_build(fdtd_batch* b) {
     x.dft = s->dft;
     x.sh_h = s->shell_h;
     x.sh_e = s->shell_e;
+    x.tf_h = s->tf_h;
+    x.tf_e = s->tf_e;
     x.ring = static_cast<T*>(s->ring);
     x.tw = s->twiddles;
     x.clk = s->clk;
@@ -136,12 +140,24 @@ static fdtd_status batch_build(fdtd_batch* b) {
     v[i] = x.v;
     const int nbx = (s->NX + 31) / 32, nby = (s->NY + kBatchTY - 1) / kBatchTY;
     const int nbz = (s->NZ + kBatchKChunk - 1) / kBatchKChunk;
+    // tiles that touch no CPML slab go to the PML-free queue (the same
+    // rule as build_tiles)
+    const int nb3[3] = {nbx, nby, nbz}, w3[3] = {32, kBatchTY, kBatchKChunk};
+    int lo[3], hi[3];
+    for (int a = 0; a < 3; a++) {
+      const int Nc = s->su.Nc[a], F = s->su.F[a];
+      lo[a] = (Nc + 1 + w3[a] - 1) / w3[a];
+      hi[a] = std::min(F >= w3[a] ? (F - w3[a]) / w3[a] + 1 : 0, nb3[a]);
+    }
     for (int bz = 0; bz < nbz; bz++)
       for (int by = 0; by < nby; by++)
-        for (int bx = 0; bx < nbx; bx++) items.push_back(make_int4(i, bx, by, bz));
+        for (int bx = 0; bx < nbx; bx++) {
+          const bool in = bx >= lo[0] && bx < hi[0] && by >= lo[1] && by < hi[1] && bz >= lo[2] && bz < hi[2];
+          (in ? inner : items).push_back(make_int4(i, bx, by, bz));
+        }
     auto blocks = [](long long cells, int per) { return (unsigned)((cells + per - 1) / per); };
-    b->g_fh = std::max(b->g_fh, blocks(s->shell_h.total(), 256));
-    b->g_fe = std::max(b->g_fe, blocks(s->shell_e.total(), 256));
+    b->g_fh = std::max(b->g_fh, blocks(s->tf_h.n, 256));
+    b->g_fe = std::max(b->g_fe, blocks(s->tf_e.n, 256));
     b->g_m = std::max(b->g_m, blocks((long long)s->nmetal[0] + s->nmetal[1] + s->nmetal[2], 128));
     int maxn = 0;
     for (int f = 0; f < 12; f++) maxn = std::max(maxn, s->dft.face[f].na * s->dft.face[f].nb);
@@ -153,28 +169,34 @@ static fdtd_status batch_build(fdtd_batch* b) {
   SimView<T>* dv;
   CUDA_TRY(b->alloc(&dd, n));
   CUDA_TRY(b->alloc(&dv, n));
+  b->nedge = (int)items.size();
+  b->ninner = (int)inner.size();
+  items.insert(items.end(), inner.begin(), inner.end());  // edge items first, then interior
   CUDA_TRY(b->alloc(&b->items, items.size()));
-  CUDA_TRY(b->alloc(&b->queue, 2));
+  CUDA_TRY(b->alloc(&b->queue, 4));
   CUDA_TRY(cudaMemcpy(dd, d.data(), n * sizeof(BatchSim<T>), cudaMemcpyHostToDevice));
   CUDA_TRY(cudaMemcpy(dv, v.data(), n * sizeof(SimView<T>), cudaMemcpyHostToDevice));
   CUDA_TRY(cudaMemcpy(b->items, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice));
   b->descs = dd;
   b->views = dv;
-  b->nitems = (int)items.size();
-  // persistent grid: every CTA slot of the GPU once
+
+  // persistent grids: every CTA slot of the GPU once
   const size_t smem = staged_smem<T, kBatchTY, kBatchS>();
-  CUDA_TRY(cudaFuncSetAttribute(h_pass_batch<T, kBatchTY, kBatchS, kBatchMinB>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  CUDA_TRY(cudaFuncSetAttribute(e_pass_batch<T, kBatchTY, kBatchS, kBatchMinB>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  CUDA_TRY(cudaFuncSetAttribute(dft_contract_batch<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDftSmem));
-  int per_sm_h = 0, per_sm_e = 0, sms = 0;
-  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_h, h_pass_batch<T, kBatchTY, kBatchS, kBatchMinB>,
-                                                         32 * kBatchTY, smem));
-  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_e, e_pass_batch<T, kBatchTY, kBatchS, kBatchMinB>,
-                                                         32 * kBatchTY, smem));
+  int sms = 0;
   CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
-  b->grid_pass = std::max(1, std::min(per_sm_h, per_sm_e)) * sms;
+  auto slots = [&](auto kern, int& out) -> fdtd_status {
+    CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per = 0;
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 32 * kBatchTY, smem));
+    out = std::max(out, std::max(1, per) * sms);
+    return FDTD_OK;
+  };
+  fdtd_status st;
+  if ((st = slots(h_pass_batch<T, kBatchTY, kBatchS, kBatchMinB, true>, b->grid_pass)) != FDTD_OK) return st;
+  if ((st = slots(e_pass_batch<T, kBatchTY, kBatchS, kBatchMinB, true>, b->grid_pass)) != FDTD_OK) return st;
+  if ((st = slots(h_pass_batch<T, kBatchTY, kBatchS, kBatchMinB, false>, b->grid_inner)) != FDTD_OK) return st;
+  if ((st = slots(e_pass_batch<T, kBatchTY, kBatchS, kBatchMinB, false>, b->grid_inner)) != FDTD_OK) return st;
+  CUDA_TRY(cudaFuncSetAttribute(dft_contract_batch<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDftSmem));
   return FDTD_OK;
 }
 
@@ -185,23 +207,39 @@ static void batch_enqueue_step(fdtd_batch* b, cudaStream_t st) {
   const SimView<T>* v = static_cast<const SimView<T>*>(b->views);
   const size_t smem = staged_smem<T, kBatchTY, kBatchS>();
   const dim3 pb(32, kBatchTY);
-  cudaMemsetAsync(b->queue, 0, 2 * sizeof(int), st);
-  h_pass_batch<T, kBatchTY, kBatchS, kBatchMinB><<<b->grid_pass, pb, smem, st>>>(v, b->items, b->nitems, b->queue,
-                                                                                kBatchKChunk);
-  int k = 1;
-  if (b->g_fh) { tfsf_h_faces_batch<T><<<dim3(b->g_fh, n), 256, 0, st>>>(d); k++; }
+  const int4* inner_items = b->items + b->nedge;
+  cudaMemsetAsync(b->queue, 0, 4 * sizeof(int), st);
+  int k = 0;
+  if (b->ninner) {
+    h_pass_batch<T, kBatchTY, kBatchS, kBatchMinB, false><<<b->grid_inner, pb, smem, st>>>(
+        v, inner_items, b->ninner, b->queue + 1, kBatchKChunk);
+    k++;
+  }
+  if (b->nedge) {
+    h_pass_batch<T, kBatchTY, kBatchS, kBatchMinB, true><<<b->grid_pass, pb, smem, st>>>(v, b->items, b->nedge,
+                                                                                       b->queue, kBatchKChunk);
+    k++;
+  }
+  if (b->g_fh) { tfsf_h_apply_batch<T><<<dim3(b->g_fh, n), 256, 0, st>>>(d); k++; }
   line_step_batch<T><<<dim3(1, n), 1024, 0, st>>>(d);
   k++;
-  if (b->g_fe) { tfsf_e_faces_batch<T><<<dim3(b->g_fe, n), 256, 0, st>>>(d); k++; }
+  if (b->g_fe) { tfsf_e_apply_batch<T><<<dim3(b->g_fe, n), 256, 0, st>>>(d); k++; }
   if (b->hydro)
     for (auto& s : b->sims) {
       const long long k0 = s->kernels;
       launch_metal<T>(s.get(), st);  // UpdateHydroP* read E^n here
       k += (int)(s->kernels - k0);
     }
-  e_pass_batch<T, kBatchTY, kBatchS, kBatchMinB><<<b->grid_pass, pb, smem, st>>>(v, b->items, b->nitems,
-                                                                                b->queue + 1, kBatchKChunk);
-  k++;
+  if (b->ninner) {
+    e_pass_batch<T, kBatchTY, kBatchS, kBatchMinB, false><<<b->grid_inner, pb, smem, st>>>(
+        v, inner_items, b->ninner, b->queue + 3, kBatchKChunk);
+    k++;
+  }
+  if (b->nedge) {
+    e_pass_batch<T, kBatchTY, kBatchS, kBatchMinB, true><<<b->grid_pass, pb, smem, st>>>(v, b->items, b->nedge,
+                                                                                       b->queue + 2, kBatchKChunk);
+    k++;
+  }
   if (!b->hydro && b->g_m) { metal_e_batch<T><<<dim3(b->g_m, n), 128, 0, st>>>(d); k++; }
   if (b->dft_every > 0 && b->t % b->dft_every == 0) {
     dft_sample_batch<T><<<dim3(b->g_s, 12, n), 256, 0, st>>>(d);

@@ -159,7 +159,7 @@ __device__ __forceinline__ T tfsf_term(const double* line, const float* dir, int
 }
 
 template <typename T>
-__global__ void tfsf_h_apply(const __grid_constant__ SimView<T> s, const __grid_constant__ TfsfTable tb) {
+__device__ __forceinline__ void tfsf_h_apply_body(const SimView<T>& s, const TfsfTable& tb) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= tb.n) return;
   const unsigned id = tb.id[g];
@@ -173,7 +173,7 @@ __global__ void tfsf_h_apply(const __grid_constant__ SimView<T> s, const __grid_
 }
 
 template <typename T>
-__global__ void tfsf_e_apply(const __grid_constant__ SimView<T> s, const __grid_constant__ TfsfTable tb) {
+__device__ __forceinline__ void tfsf_e_apply_body(const SimView<T>& s, const TfsfTable& tb) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= tb.n) return;
   const unsigned id = tb.id[g];
@@ -193,6 +193,15 @@ __global__ void tfsf_e_apply(const __grid_constant__ SimView<T> s, const __grid_
   v = tfsf_term(s.h_inc, s.tf.fh, tb.idx[0][g], tb.dp[0][g], tb.meta[0][g], v, ceh, dd);
   if (nt > 1) v = tfsf_term(s.h_inc, s.tf.fh, tb.idx[1][g], tb.dp[1][g], tb.meta[1][g], v, ceh, dd);
   s.E[c][id] = v;
+}
+
+template <typename T>
+__global__ void tfsf_h_apply(const __grid_constant__ SimView<T> s, const __grid_constant__ TfsfTable tb) {
+  tfsf_h_apply_body(s, tb);
+}
+template <typename T>
+__global__ void tfsf_e_apply(const __grid_constant__ SimView<T> s, const __grid_constant__ TfsfTable tb) {
+  tfsf_e_apply_body(s, tb);
 }
 
 }  // namespace fdtd

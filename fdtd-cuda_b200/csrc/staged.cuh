@@ -331,7 +331,7 @@ __global__ void __launch_bounds__(32 * TY, MINB) h_pass_s(const __grid_constant_
 // Batched form: a persistent grid that takes (simulation, tile) work items
 // from a queue shared by every simulation of a batch; the views live in
 // device memory, one per simulation.
-template <typename T, int TY, int S, int MINB>
+template <typename T, int TY, int S, int MINB, bool PML>
 __global__ void __launch_bounds__(32 * TY, MINB) h_pass_batch(const SimView<T>* __restrict__ views,
                                                            const int4* __restrict__ items, int nitems,
                                                            int* __restrict__ queue, int kchunk) {
@@ -343,7 +343,7 @@ __global__ void __launch_bounds__(32 * TY, MINB) h_pass_batch(const SimView<T>* 
     const int it = next;
     if (it >= nitems) return;
     const int4 w = items[it];  // (simulation, bx, by, bz)
-    h_pass_tile<T, TY, S, true>(views[w.x], kchunk, w.y, w.z, w.w);
+    h_pass_tile<T, TY, S, PML>(views[w.x], kchunk, w.y, w.z, w.w);
   }
 }
 
@@ -524,7 +524,7 @@ __global__ void __launch_bounds__(32 * TY, MINB) e_pass_s(const __grid_constant_
 // Batched form: a persistent grid that takes (simulation, tile) work items
 // from a queue shared by every simulation of a batch; the views live in
 // device memory, one per simulation.
-template <typename T, int TY, int S, int MINB>
+template <typename T, int TY, int S, int MINB, bool PML>
 __global__ void __launch_bounds__(32 * TY, MINB) e_pass_batch(const SimView<T>* __restrict__ views,
                                                            const int4* __restrict__ items, int nitems,
                                                            int* __restrict__ queue, int kchunk) {
@@ -536,7 +536,7 @@ __global__ void __launch_bounds__(32 * TY, MINB) e_pass_batch(const SimView<T>* 
     const int it = next;
     if (it >= nitems) return;
     const int4 w = items[it];  // (simulation, bx, by, bz)
-    e_pass_tile<T, TY, S, true>(views[w.x], kchunk, w.y, w.z, w.w);
+    e_pass_tile<T, TY, S, PML>(views[w.x], kchunk, w.y, w.z, w.w);
   }
 }
 
