@@ -584,7 +584,7 @@ def main():
                        "time_steps_per_step": BLOCK, "num_freq": d.num_freq,
                        "dispersive_cells": list(d.n_metal_cells),
                        "l2": "no flush: working set (403 MB of fields + 7 GB DFT) > 126 MB L2",
-                       "tuning": {k: getattr(tune, k) for k in ("h_staged", "h_stages", "h_minb", "h_ty", "h_kchunk", "e_staged", "e_stages", "e_minb", "e_ty", "e_kchunk", "h_ms", "e_ms")},
+                       "tuning": {k: getattr(tune, k) for k in ("h_stages", "h_minb", "h_ty", "h_kchunk", "h_eminb", "h_estages", "e_stages", "e_minb", "e_ty", "e_kchunk", "e_eminb", "e_estages", "h_ms", "e_ms")},
                        "parallelism": f"replicas x{world}"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "clocks": clk.summary(), "gpu_launches": launches, "fp64": fp64,

@@ -69,7 +69,10 @@ struct fdtd_sim {
   // launch shape of the E and H passes, chosen by tune_passes()
   // staged = shared-memory pipelined kernels (minb unused), else the plain
   // register z-march
-  struct PassCfg { int minb = 1, ty = 4, kchunk = 16, staged = 1, stages = 4; float ms = 0; };
+  // launch shape of one pass: tile height and z-chunk shared by its two
+  // launches, register cap (min CTAs/SM) and ring depth per launch
+  // (interior tiles: minb/stages, CPML edge tiles: eminb/estages)
+  struct PassCfg { int minb = 1, ty = 4, kchunk = 16, staged = 1, stages = 4, eminb = 1, estages = 4; float ms = 0; };
   // pass tiles for one (tile height, z-chunk): the interior box of tiles
   // that touch no CPML slab and the table of the others
   struct TileSet {
@@ -824,66 +827,64 @@ static const fdtd_sim::TileSet& tiles(const fdtd_sim* s, const fdtd_sim::PassCfg
   return s->tilesets.front();  // unreachable: every configuration is built at create
 }
 
+// One launch of a pass variant over a tile map (box grid or table).
+template <typename T, bool PML>
+static void launch_h_variant(fdtd_sim* s, int ty, int mb, int sg, dim3 g, const TileMap& tm, int kchunk,
+                             cudaStream_t st) {
+#define FDTD_LAUNCH(TY, MB, S)                                                                   \
+  if (ty == TY && mb == MB && sg == S) {                                                         \
+    h_pass_s<T, TY, S, MB, PML><<<g, dim3(32, TY), staged_smem<T, TY, S>(), st>>>(view<T>(s), kchunk, tm); \
+    return;                                                                                      \
+  }
+  FDTD_STAGED_VARIANTS(FDTD_LAUNCH)
+#undef FDTD_LAUNCH
+}
+template <typename T, bool PML>
+static void launch_e_variant(fdtd_sim* s, int ty, int mb, int sg, dim3 g, const TileMap& tm, int kchunk,
+                             cudaStream_t st) {
+#define FDTD_LAUNCH(TY, MB, S)                                                                   \
+  if (ty == TY && mb == MB && sg == S) {                                                         \
+    e_pass_s<T, TY, S, MB, PML><<<g, dim3(32, TY), staged_smem<T, TY, S>(), st>>>(view<T>(s), kchunk, tm); \
+    return;                                                                                      \
+  }
+  FDTD_STAGED_VARIANTS(FDTD_LAUNCH)
+#undef FDTD_LAUNCH
+}
+
 // Launches one pass as its interior box (PML-free) and its edge table, the
 // edge launch on the side stream so that the two overlap; returns the
 // number of launches.
+template <typename T, bool EPASS>
+static int launch_pass_cfg(fdtd_sim* s, const fdtd_sim::PassCfg& c, cudaStream_t st) {
+  const fdtd_sim::TileSet& ts = tiles(s, c);
+  const bool fork = ts.inner.x && ts.nedge;
+  cudaStream_t est = st;
+  if (fork) {
+    cudaEventRecord(s->fork_ev, st);
+    cudaStreamWaitEvent(s->side, s->fork_ev, 0);
+    est = s->side;
+  }
+  if (ts.nedge) {
+    if (EPASS) launch_e_variant<T, true>(s, c.ty, c.eminb, c.estages, dim3(ts.nedge), ts.edge_map, c.kchunk, est);
+    else launch_h_variant<T, true>(s, c.ty, c.eminb, c.estages, dim3(ts.nedge), ts.edge_map, c.kchunk, est);
+  }
+  if (ts.inner.x) {
+    if (EPASS) launch_e_variant<T, false>(s, c.ty, c.minb, c.stages, ts.inner, ts.inner_map, c.kchunk, st);
+    else launch_h_variant<T, false>(s, c.ty, c.minb, c.stages, ts.inner, ts.inner_map, c.kchunk, st);
+  }
+  if (fork) {
+    cudaEventRecord(s->join_ev, s->side);
+    cudaStreamWaitEvent(st, s->join_ev, 0);
+  }
+  return (ts.inner.x ? 1 : 0) + (ts.nedge ? 1 : 0);
+}
 template <typename T>
 static int launch_h_cfg(fdtd_sim* s, const fdtd_sim::PassCfg& c, cudaStream_t st) {
-  const fdtd_sim::TileSet& ts = tiles(s, c);
-  const dim3 b(32, c.ty);
-#define FDTD_LAUNCH(TY, MB, S)                                                                          \
-  if (c.ty == TY && c.minb == MB && c.stages == S) {                                                    \
-    const bool fork = ts.inner.x && ts.nedge;                                                           \
-    cudaStream_t est = st;                                                                              \
-    if (fork) {                                                                                         \
-      cudaEventRecord(s->fork_ev, st);                                                                  \
-      cudaStreamWaitEvent(s->side, s->fork_ev, 0);                                                      \
-      est = s->side;                                                                                    \
-    }                                                                                                   \
-    if (ts.nedge)                                                                                       \
-      h_pass_s<T, TY, S, MB, true><<<ts.nedge, b, staged_smem<T, TY, S>(), est>>>(view<T>(s), c.kchunk, \
-                                                                                   ts.edge_map);       \
-    if (ts.inner.x)                                                                                     \
-      h_pass_s<T, TY, S, MB, false><<<ts.inner, b, staged_smem<T, TY, S>(), st>>>(view<T>(s), c.kchunk, \
-                                                                                   ts.inner_map);      \
-    if (fork) {                                                                                         \
-      cudaEventRecord(s->join_ev, s->side);                                                             \
-      cudaStreamWaitEvent(st, s->join_ev, 0);                                                           \
-    }                                                                                                   \
-    return (ts.inner.x ? 1 : 0) + (ts.nedge ? 1 : 0);                                                   \
-  }
-  FDTD_STAGED_VARIANTS(FDTD_LAUNCH)
-#undef FDTD_LAUNCH
-  return 0;
+  return launch_pass_cfg<T, false>(s, c, st);
 }
 template <typename T>
 static int launch_e_cfg(fdtd_sim* s, const fdtd_sim::PassCfg& c, cudaStream_t st) {
-  const fdtd_sim::TileSet& ts = tiles(s, c);
-  const dim3 b(32, c.ty);
-#define FDTD_LAUNCH(TY, MB, S)                                                                          \
-  if (c.ty == TY && c.minb == MB && c.stages == S) {                                                    \
-    const bool fork = ts.inner.x && ts.nedge;                                                           \
-    cudaStream_t est = st;                                                                              \
-    if (fork) {                                                                                         \
-      cudaEventRecord(s->fork_ev, st);                                                                  \
-      cudaStreamWaitEvent(s->side, s->fork_ev, 0);                                                      \
-      est = s->side;                                                                                    \
-    }                                                                                                   \
-    if (ts.nedge)                                                                                       \
-      e_pass_s<T, TY, S, MB, true><<<ts.nedge, b, staged_smem<T, TY, S>(), est>>>(view<T>(s), c.kchunk, \
-                                                                                   ts.edge_map);       \
-    if (ts.inner.x)                                                                                     \
-      e_pass_s<T, TY, S, MB, false><<<ts.inner, b, staged_smem<T, TY, S>(), st>>>(view<T>(s), c.kchunk, \
-                                                                                   ts.inner_map);      \
-    if (fork) {                                                                                         \
-      cudaEventRecord(s->join_ev, s->side);                                                             \
-      cudaStreamWaitEvent(st, s->join_ev, 0);                                                           \
-    }                                                                                                   \
-    return (ts.inner.x ? 1 : 0) + (ts.nedge ? 1 : 0);                                                   \
-  }
-  FDTD_STAGED_VARIANTS(FDTD_LAUNCH)
-#undef FDTD_LAUNCH
-  return 0;
+  return launch_pass_cfg<T, true>(s, c, st);
 }
 
 // Autotuner: times every launch shape of the E and H passes on the zero
@@ -913,6 +914,8 @@ static fdtd_status tune_passes(fdtd_sim* s, bool time_variants) {
 #undef FDTD_KNOWN
     if (!known || def.kchunk < 1) return fail(FDTD_ERR_INVALID, "FDTD_PASS names a pass variant that is not built");
   }
+  def.eminb = def.minb;
+  def.estages = def.stages;
   s->hcfg = s->ecfg = def;
   {
     const fdtd_status st = build_tiles(s, def.ty, def.kchunk);
@@ -928,40 +931,63 @@ static fdtd_status tune_passes(fdtd_sim* s, bool time_variants) {
   CUDA_TRY(cudaEventCreate(&b));
   const char* venv = std::getenv("FDTD_TUNE_VERBOSE");
   const bool verbose = venv && venv[0] == '1';
-  std::vector<fdtd_sim::PassCfg> cands;
+  // per (tile height, z-chunk): the fastest interior variant and the
+  // fastest edge variant, each timed alone; the pair with the smallest sum
   const int variants[][3] = {{4, 1, 4}, {4, 6, 4}, {4, 8, 4}, {8, 3, 4}, {4, 6, 6}};
-  for (const auto& v : variants)
-    for (int kc : {8, 16, 32}) {
-      fdtd_sim::PassCfg c;
-      c.staged = 1; c.ty = v[0]; c.minb = v[1]; c.stages = v[2]; c.kchunk = kc;
-      // skip variants whose shared memory does not fit (FP64 at depth 6)
-      const size_t sm = sizeof(T) * (size_t)c.stages * (c.ty == 4 ? StageLayout<T, 4>::STAGE : StageLayout<T, 8>::STAGE);
-      if (kc <= 2 * s->NZ && sm * std::max(1, c.minb) <= 220 * 1024) {
-        const fdtd_status st = build_tiles(s, c.ty, c.kchunk);
-        if (st != FDTD_OK) return st;
-        cands.push_back(c);
-      }
-    }
   for (int pass = 0; pass < 2; pass++) {
     fdtd_sim::PassCfg best;
     best.ms = 1e30f;
-    for (fdtd_sim::PassCfg c : cands) {
-        {
-          auto go = [&]() { pass == 0 ? launch_h_cfg<T>(s, c, 0) : launch_e_cfg<T>(s, c, 0); };
-          go();
-          CUDA_TRY(cudaEventRecord(a));
-          for (int r = 0; r < 3; r++) go();
-          CUDA_TRY(cudaEventRecord(b));
-          CUDA_TRY(cudaEventSynchronize(b));
-          float ms;
-          CUDA_TRY(cudaEventElapsedTime(&ms, a, b));
-          c.ms = ms / 3;
-          if (verbose)
-            std::fprintf(stderr, "[fdtd tune] %s staged=%d minb=%d ty=%d kchunk=%d stages=%d %.4f ms\n",
-                         pass == 0 ? "H" : "E", c.staged, c.minb, c.ty, c.kchunk, c.stages, c.ms);
-          if (c.ms < best.ms) best = c;
+    for (int ty : {4, 8})
+      for (int kc : {8, 16, 32}) {
+        if (kc > 2 * s->NZ) continue;
+        const fdtd_status st = build_tiles(s, ty, kc);
+        if (st != FDTD_OK) return st;
+        fdtd_sim::PassCfg probe;
+        probe.ty = ty; probe.kchunk = kc;
+        const fdtd_sim::TileSet& ts = tiles(s, probe);
+        float bin = ts.inner.x ? 1e30f : 0.f, bed = ts.nedge ? 1e30f : 0.f;
+        int in_mb = 1, in_sg = 4, ed_mb = 1, ed_sg = 4;
+        bool any = false;
+        for (const auto& v : variants) {
+          if (v[0] != ty) continue;
+          const size_t sm = sizeof(T) * (size_t)v[2] * (ty == 4 ? StageLayout<T, 4>::STAGE : StageLayout<T, 8>::STAGE);
+          if (sm * std::max(1, v[1]) > 220 * 1024) continue;
+          any = true;
+          for (int part = 0; part < 2; part++) {
+            if (part == 0 ? !ts.inner.x : !ts.nedge) continue;
+            auto go = [&]() {
+              if (part == 0) {
+                if (pass == 0) launch_h_variant<T, false>(s, ty, v[1], v[2], ts.inner, ts.inner_map, kc, 0);
+                else launch_e_variant<T, false>(s, ty, v[1], v[2], ts.inner, ts.inner_map, kc, 0);
+              } else {
+                if (pass == 0) launch_h_variant<T, true>(s, ty, v[1], v[2], dim3(ts.nedge), ts.edge_map, kc, 0);
+                else launch_e_variant<T, true>(s, ty, v[1], v[2], dim3(ts.nedge), ts.edge_map, kc, 0);
+              }
+            };
+            go();
+            CUDA_TRY(cudaEventRecord(a));
+            for (int r = 0; r < 3; r++) go();
+            CUDA_TRY(cudaEventRecord(b));
+            CUDA_TRY(cudaEventSynchronize(b));
+            float ms;
+            CUDA_TRY(cudaEventElapsedTime(&ms, a, b));
+            ms /= 3;
+            if (verbose)
+              std::fprintf(stderr, "[fdtd tune] %s %s minb=%d ty=%d kchunk=%d stages=%d %.4f ms\n",
+                           pass == 0 ? "H" : "E", part == 0 ? "interior" : "edge", v[1], ty, kc, v[2], ms);
+            if (part == 0 && ms < bin) { bin = ms; in_mb = v[1]; in_sg = v[2]; }
+            if (part == 1 && ms < bed) { bed = ms; ed_mb = v[1]; ed_sg = v[2]; }
+          }
         }
-    }
+        if (!any) continue;
+        const float tot = bin + bed;
+        if (tot < best.ms) {
+          best = fdtd_sim::PassCfg();
+          best.staged = 1; best.ty = ty; best.kchunk = kc;
+          best.minb = in_mb; best.stages = in_sg; best.eminb = ed_mb; best.estages = ed_sg;
+          best.ms = tot;
+        }
+      }
     (pass == 0 ? s->hcfg : s->ecfg) = best;
   }
   cudaEventDestroy(a);
@@ -1491,6 +1517,8 @@ extern "C" fdtd_status fdtd_get_stats(const fdtd_sim* s, fdtd_stats* out) {
   out->h_ms = s->hcfg.ms; out->e_ms = s->ecfg.ms;
   out->h_staged = s->hcfg.staged; out->e_staged = s->ecfg.staged;
   out->h_stages = s->hcfg.stages; out->e_stages = s->ecfg.stages;
+  out->h_eminb = s->hcfg.eminb; out->h_estages = s->hcfg.estages;
+  out->e_eminb = s->ecfg.eminb; out->e_estages = s->ecfg.estages;
   return FDTD_OK;
 }
 

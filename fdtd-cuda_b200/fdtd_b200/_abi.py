@@ -101,4 +101,6 @@ class Stats(C.Structure):
                 ("e_minb", C.c_int), ("e_ty", C.c_int), ("e_kchunk", C.c_int),
                 ("h_ms", C.c_float), ("e_ms", C.c_float),
                 ("h_staged", C.c_int), ("e_staged", C.c_int),
-                ("h_stages", C.c_int), ("e_stages", C.c_int)]
+                ("h_stages", C.c_int), ("e_stages", C.c_int),
+                ("h_eminb", C.c_int), ("h_estages", C.c_int),
+                ("e_eminb", C.c_int), ("e_estages", C.c_int)]

@@ -323,6 +323,8 @@ typedef struct fdtd_stats {
   float h_ms, e_ms;
   int h_staged, e_staged;  /* 1 = shared-memory pipelined pass */
   int h_stages, e_stages;  /* its ring depth */
+  /* the same two for the launch over the CPML edge tiles */
+  int h_eminb, h_estages, e_eminb, e_estages;
 } fdtd_stats;
 fdtd_status fdtd_get_stats(const fdtd_sim* s, fdtd_stats* out);
 /* Measurement hook (no counterpart in the reference): runs one Yee pass
