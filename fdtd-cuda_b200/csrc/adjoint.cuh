@@ -378,5 +378,6 @@ __global__ void adj_partner(const __grid_constant__ DftView d, const int* __rest
 }
 
 __global__ void adj_step_back(int* step) { *step -= 1; }
+__global__ void adj_set_step(int* step, int n) { *step = n; }
 
 }  // namespace fdtd

@@ -36,6 +36,20 @@ struct fdtd_sim::Adjoint {
   double* grho[3] = {nullptr, nullptr, nullptr};
   double* gpar = nullptr;
   int* step = nullptr;
+  // graphs of one full segment: the recompute (DFT off, recording on) and
+  // the reverse sweep; replayed for every full segment
+  cudaGraphExec_t g_rec = nullptr, g_adj = nullptr;
+  cudaStream_t cap = nullptr;
+
+  void drop_graphs() {
+    if (g_rec) cudaGraphExecDestroy(g_rec);
+    if (g_adj) cudaGraphExecDestroy(g_adj);
+    g_rec = g_adj = nullptr;
+  }
+  ~Adjoint() {
+    drop_graphs();
+    if (cap) cudaStreamDestroy(cap);
+  }
 
   template <typename U>
   cudaError_t alloc(U** out, size_t count, bool zeroed_each_sweep) {
@@ -94,6 +108,8 @@ extern "C" fdtd_status fdtd_forward(fdtd_sim* s, const int* freq_idx, int nfreq,
   fdtd_sim::Adjoint& A = *s->adj;
   A.sel.assign(freq_idx, freq_idx + nfreq);
   A.forward_done = false;
+  A.drop_graphs();  // they hold the partner buffer and the segment length
+  if (A.ready && A.every != checkpoint_every) A.ready = false;  // the record depth follows the segment
   st = fdtd_reset(s);
   if (st != FDTD_OK) return st;
   CUDA_TRY(cudaSetDevice(s->device));
@@ -171,6 +187,8 @@ extern "C" fdtd_status fdtd_forward(fdtd_sim* s, const int* freq_idx, int nfreq,
 template <typename T>
 static fdtd_status adj_prepare(fdtd_sim* s) {
   fdtd_sim::Adjoint& A = *s->adj;
+  A.bufs.clear();  // a re-preparation (another checkpoint interval) starts afresh
+  A.zero.clear();
   AdjView<T> a;
   std::memset(&a, 0, sizeof(a));
   const size_t nc = s->ncell;
@@ -257,9 +275,26 @@ static fdtd_status adj_sweep(fdtd_sim* s) {
   for (int f = 0; f < 6; f++) maxn = std::max(maxn, s->dft.face[f].na * s->dft.face[f].nb);
   const double* fsel = static_cast<const double*>(A.fsel->p) + A.sel.size();
   const int total = A.tend + 1;
+  auto adj_step = [&](int n, cudaStream_t stream) {
+    if (n % every_dft == 0)
+      adj_source<T><<<dim3((maxn + 255) / 256, 6), 256, 0, stream>>>(view<T>(s), s->dft, a,
+                                                                      static_cast<const double2*>(A.P->p), fsel,
+                                                                      (int)A.sel.size(), s->dft.rows);
+    adj_e_coef<T><<<gc, 256, 0, stream>>>(view<T>(s), a);
+    if (ntot > 0)
+      adj_e_design<T><<<(ntot + 127) / 128, 128, 0, stream>>>(view<T>(s), m, a, static_cast<const T*>(A.rec),
+                                                              A.every);
+    adj_gather_h<T><<<gc, 256, 0, stream>>>(view<T>(s), a);
+    adj_h_coef<T><<<gc, 256, 0, stream>>>(view<T>(s), a);
+    adj_gather_e<T><<<gc, 256, 0, stream>>>(view<T>(s), a);
+    adj_step_back<<<1, 1, 0, stream>>>(A.step);
+    return 6 + (ntot > 0) + (n % every_dft == 0);
+  };
+  if (!A.cap) CUDA_TRY(cudaStreamCreateWithFlags(&A.cap, cudaStreamNonBlocking));
   fdtd_status st = FDTD_OK;
   for (int seg = A.nseg - 1; seg >= 0 && st == FDTD_OK; seg--) {
     const int n0 = seg * A.every, n1 = std::min(total, n0 + A.every);
+    const bool full = n1 - n0 == A.every;
     const char* src = static_cast<const char*>(A.ck->p) + (size_t)seg * A.ck_bytes;
     for (const auto& b : A.ck_bufs) {
       CUDA_TRY(cudaMemcpyAsync(b.first, src, b.second, cudaMemcpyDeviceToDevice, 0));
@@ -267,23 +302,42 @@ static fdtd_status adj_sweep(fdtd_sim* s) {
     }
     s->t = n0;
     s->host_nsamp = 0;
-    st = step_impl<T>(s, n1 - n0, 0);  // records the dispersive cells, row n % every
-    if (st != FDTD_OK) break;
-    const int last = n1 - 1;
-    CUDA_TRY(cudaMemcpyAsync(A.step, &last, sizeof(int), cudaMemcpyHostToDevice, 0));
-    CUDA_TRY(cudaStreamSynchronize(0));  // &last lives on this stack frame
-    for (int n = n1 - 1; n >= n0; n--) {
-      if (n % every_dft == 0)
-        adj_source<T><<<dim3((maxn + 255) / 256, 6), 256>>>(view<T>(s), s->dft, a,
-                                                             static_cast<const double2*>(A.P->p), fsel,
-                                                             (int)A.sel.size(), s->dft.rows);
-      adj_e_coef<T><<<gc, 256>>>(view<T>(s), a);
-      if (ntot > 0) adj_e_design<T><<<(ntot + 127) / 128, 128>>>(view<T>(s), m, a, static_cast<const T*>(A.rec), A.every);
-      adj_gather_h<T><<<gc, 256>>>(view<T>(s), a);
-      adj_h_coef<T><<<gc, 256>>>(view<T>(s), a);
-      adj_gather_e<T><<<gc, 256>>>(view<T>(s), a);
-      adj_step_back<<<1, 1>>>(A.step);
-      s->kernels += 6 + (ntot > 0) + (n % every_dft == 0);
+    // recompute: records the dispersive cells, row n % every
+    if (full) {
+      if (!A.g_rec) {
+        cudaGraph_t g;
+        const long long k0 = s->kernels;
+        CUDA_TRY(cudaStreamBeginCapture(A.cap, cudaStreamCaptureModeThreadLocal));
+        for (int q = 0; q < A.every; q++) enqueue_step<T>(s, A.cap);
+        CUDA_TRY(cudaStreamEndCapture(A.cap, &g));
+        s->kernels = k0;
+        s->t = n0;
+        const cudaError_t e = cudaGraphInstantiate(&A.g_rec, g, 0);
+        cudaGraphDestroy(g);
+        CUDA_TRY(e);
+      }
+      CUDA_TRY(cudaGraphLaunch(A.g_rec, 0));
+      s->t = n1;
+    } else {
+      st = step_impl<T>(s, n1 - n0, 0);
+      if (st != FDTD_OK) break;
+    }
+    adj_set_step<<<1, 1>>>(A.step, n1 - 1);
+    // the reverse sweep; a full segment starting on a DFT sample step has
+    // the same launch pattern every time
+    if (full && n0 % every_dft == 0) {
+      if (!A.g_adj) {
+        cudaGraph_t g;
+        CUDA_TRY(cudaStreamBeginCapture(A.cap, cudaStreamCaptureModeThreadLocal));
+        for (int n = n1 - 1; n >= n0; n--) adj_step(n, A.cap);
+        CUDA_TRY(cudaStreamEndCapture(A.cap, &g));
+        const cudaError_t e = cudaGraphInstantiate(&A.g_adj, g, 0);
+        cudaGraphDestroy(g);
+        CUDA_TRY(e);
+      }
+      CUDA_TRY(cudaGraphLaunch(A.g_adj, 0));
+    } else {
+      for (int n = n1 - 1; n >= n0; n--) s->kernels += adj_step(n, 0);
     }
     CUDA_TRY(cudaGetLastError());
   }

@@ -65,6 +65,7 @@ struct orc_sim {
   double C_E, C_E_1, C_E_2;
   double d1, d2, d3, d4, d5, dNL, N_EQ;
   double C1[2], C2[2], C3[2], C4[2], C5[2];
+  double* rho;  /* design blend per cell (NULL: plain metal), see orc_set_design */
   /* TFSF */
   double *e_inc, *h_inc, e1, e2;
   float fe[3], fh[3];        /* E/H incident direction factors (x,y,z) */
@@ -549,6 +550,7 @@ orc_sim* orc_create(const fdtd_params* pin, char* err) {
 
 void orc_destroy(orc_sim* s) {
   if (!s) return;
+  free(s->rho);
   for (int c = 0; c < 3; c++) {
     free(s->E[c]); free(s->H[c]); free(s->En[c]); free(s->En1[c]);
     free(s->Pcp[c]); free(s->Pcp_n[c]); free(s->Pcp_n1[c]);
@@ -570,6 +572,25 @@ void orc_destroy(orc_sim* s) {
   free(s->mat); free(s->e_inc); free(s->h_inc); free(s->freq); free(s->Einc);
   free(s->probe);
   free(s);
+}
+
+/* Design blend of the cells of params.design_box (x fastest in the box),
+ * the other dispersive cells keep rho = 1.  Returns 0, or -1 for a
+ * simulation without a design box or a wrong count. */
+int orc_set_design(orc_sim* s, const float* rho, size_t count) {
+  const int* b = s->p.design_box;
+  if (!(b[1] > b[0] && b[3] > b[2] && b[5] > b[4])) return -1;
+  const int bx = b[1] - b[0], by = b[3] - b[2], bz = b[5] - b[4];
+  if (count != (size_t)bx * by * bz) return -1;
+  if (!s->rho) {
+    s->rho = (double*)malloc(s->n * sizeof(double));
+    for (size_t q = 0; q < s->n; q++) s->rho[q] = 1.0;
+  }
+  for (int k = 0; k < bz; k++)
+    for (int j = 0; j < by; j++)
+      for (int i = 0; i < bx; i++)
+        s->rho[IDX(s, b[0] + i, b[2] + j, b[4] + k)] = rho[((size_t)k * by + j) * bx + i];
+  return 0;
 }
 
 void orc_set_float_dft(orc_sim* s, int on) { s->float_dft = on; }
@@ -980,16 +1001,29 @@ static void update_e_comp(orc_sim* s, int c) {
             CP1 += (s->d1 - 1) * s->Pd_n[c][id];
             CP3 += (s->d2) * s->Pd_n1[c][id];
             CPNL += s->dNL * 0.0;
+            /* adjoint design region (no counterpart in the reference): the
+             * coupling coefficients blend linearly between vacuum (rho = 0)
+             * and the metal (rho = 1); the pole dynamics stay the metal's */
+            double CE = s->C_E, CE1 = s->C_E_1, CE2 = s->C_E_2, D3 = s->d3, D4 = s->d4, D5 = s->d5;
+            double C3[2] = {s->C3[0], s->C3[1]}, C4[2] = {s->C4[0], s->C4[1]}, C5[2] = {s->C5[0], s->C5[1]};
+            if (s->rho) {
+              const double r = s->rho[id], vac = K_EP0;
+              CE = vac + r * (s->C_E - vac);
+              CE1 = vac + r * (s->C_E_1 - vac);
+              CE2 = r * s->C_E_2;
+              D3 = r * s->d3; D4 = r * s->d4; D5 = r * s->d5;
+              for (int q = 0; q < 2; q++) { C3[q] = r * s->C3[q]; C4[q] = r * s->C4[q]; C5[q] = r * s->C5[q]; }
+            }
             s->En1[c][id] = s->En[c][id];
             s->En[c][id] = E[id];
-            E[id] = (1 / s->C_E) * (s->dt * curl / s->z0 + s->C_E_1 * s->En[c][id] -
-                                    s->C_E_2 * s->En1[c][id] - CP1 - CP2 - CP3 - CP4 - CPNL);
+            E[id] = (1 / CE) * (s->dt * curl / s->z0 + CE1 * s->En[c][id] -
+                                CE2 * s->En1[c][id] - CP1 - CP2 - CP3 - CP4 - CPNL);
             double en = s->En[c][id], en1 = s->En1[c][id];
             double ncp[2];
             for (int q = 0; q < 2; q++)
-              ncp[q] = s->C1[q] * cpn[q] + s->C2[q] * cpn1[q] + s->C3[q] * E[id] + s->C4[q] * en + s->C5[q] * en1;
-            double npd = s->d1 * s->Pd_n[c][id] + s->d2 * s->Pd_n1[c][id] + s->d3 * E[id] + s->d4 * en +
-                         s->d5 * en1 + s->dNL * 0.0;
+              ncp[q] = s->C1[q] * cpn[q] + s->C2[q] * cpn1[q] + C3[q] * E[id] + C4[q] * en + C5[q] * en1;
+            double npd = s->d1 * s->Pd_n[c][id] + s->d2 * s->Pd_n1[c][id] + D3 * E[id] + D4 * en +
+                         D5 * en1 + s->dNL * 0.0;
             s->Pd_n1[c][id] = s->Pd_n[c][id];
             s->Pd_n[c][id] = npd;
             for (int q = 0; q < 2; q++) { cpn1[q] = cpn[q]; cpn[q] = ncp[q]; }

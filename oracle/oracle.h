@@ -32,6 +32,7 @@ int orc_load_input_txt(const char* path, fdtd_params* p);
 /* Returns NULL and fills err (256 bytes) on invalid parameters. */
 orc_sim* orc_create(const fdtd_params* p, char* err);
 void orc_destroy(orc_sim* s);
+int orc_set_design(orc_sim* s, const float* rho, size_t count);
 /* 1 = DFT accumulators and spectral post emulate the reference's float
  * accumulators and float-complex flux arithmetic (global_var.h:22,
  * Spectral.cu:414-418); 0 = FP64 throughout (default). */

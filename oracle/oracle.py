@@ -35,6 +35,7 @@ def lib():
         L.orc_create.argtypes = [P(Params), C.c_char_p]
         L.orc_create.restype = C.c_void_p
         L.orc_destroy.argtypes = [C.c_void_p]
+        L.orc_set_design.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.c_size_t]
         for f in ("orc_set_float_dft", "orc_set_dft_enabled"):
             getattr(L, f).argtypes = [C.c_void_p, C.c_int]
         L.orc_set_threads.argtypes = [C.c_int]
@@ -142,6 +143,11 @@ class OracleSim:
         if rc != 0:
             raise RuntimeError("no DFT data")
         return re + 1j * im
+
+    def set_design(self, rho):
+        """Blend per cell of params.design_box, shape (nz, ny, nx) of the box."""
+        rho = np.ascontiguousarray(rho, dtype=np.float32)
+        assert lib().orc_set_design(self.h, rho.ctypes.data_as(C.POINTER(C.c_float)), rho.size) == 0
 
     def spectra(self):
         out = np.empty((self.dims.num_freq, 19), np.float64)

@@ -106,3 +106,26 @@ def test_design_errors():
     assert e.value.status == 5
     with pytest.raises(F.FdtdError):
         F.Sim(make(F, "vacuum", precision=F.FDTD_FP64, design_box=[2, 6, 2, 6, 2, 6]))
+
+
+def test_adjoint_matches_oracle_gradient(fp64_grad):
+    """The FP64 oracle (the CPU restatement, with the same design blend)
+    gives the reference gradient by central differences on the objective it
+    computes itself; the GPU adjoint matches it, and the two forward
+    objectives agree."""
+    _, L, g, _ = fp64_grad
+
+    def oracle_objective(rho):
+        o = O.OracleSim(make(O, "vacuum", precision=1, Tend=300, design_box=BOX, **GOLD))
+        o.set_design(rho)
+        o.step(301)
+        return float(o.spectra()[SEL, 2].sum())
+
+    rho, h = rho0(), 1e-3
+    assert oracle_objective(rho) == pytest.approx(L, rel=1e-10)
+    for c in [(0, 0, 0), (3, 5, 5)]:
+        r = rho.copy(); r[c] += h; lp = oracle_objective(r)
+        r = rho.copy(); r[c] -= h; lm = oracle_objective(r)
+        fd = (lp - lm) / (2 * h)
+        print(c, "oracle fd", fd, "adjoint", g[c])
+        assert abs(fd - g[c]) <= 1e-3 * abs(fd)
