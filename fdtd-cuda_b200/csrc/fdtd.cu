@@ -144,6 +144,10 @@ struct fdtd_sim {
   // interior launch (fork/join by events, also inside graph capture)
   cudaStream_t side = nullptr;
   cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+  // second side stream: the dispersive-cell kernels run beside the E pass
+  // (they touch only dispersive components, which the pass skips)
+  cudaStream_t side2 = nullptr;
+  cudaEvent_t fork2_ev = nullptr, join2_ev = nullptr;
 
   void destroy_streams() {
     if (graph) cudaGraphExecDestroy(graph);
@@ -151,6 +155,9 @@ struct fdtd_sim {
     if (side) cudaStreamDestroy(side);
     if (fork_ev) cudaEventDestroy(fork_ev);
     if (join_ev) cudaEventDestroy(join_ev);
+    if (side2) cudaStreamDestroy(side2);
+    if (fork2_ev) cudaEventDestroy(fork2_ev);
+    if (join2_ev) cudaEventDestroy(join2_ev);
   }
 
   // buffers that fdtd_reset zeroes (fields, psi, dispersive state, DFT,
@@ -694,6 +701,9 @@ static fdtd_status create_impl(const fdtd_params* p, int device, fdtd_sim** out,
   L.clk = s->clk; L.probe = s->probe; L.probe_cap = s->probe_cap;
   L.dft_every = s->dft_on ? su.p.dft_every : 0;
   CUDA_TRY(cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking));
+  CUDA_TRY(cudaStreamCreateWithFlags(&s->side2, cudaStreamNonBlocking));
+  CUDA_TRY(cudaEventCreateWithFlags(&s->fork2_ev, cudaEventDisableTiming));
+  CUDA_TRY(cudaEventCreateWithFlags(&s->join2_ev, cudaEventDisableTiming));
   CUDA_TRY(cudaEventCreateWithFlags(&s->fork_ev, cudaEventDisableTiming));
   CUDA_TRY(cudaEventCreateWithFlags(&s->join_ev, cudaEventDisableTiming));
   CUDA_TRY(cudaDeviceSynchronize());
@@ -1017,9 +1027,21 @@ static void launch_e(fdtd_sim* s, cudaStream_t st) {
   const int nf = s->tf_e.n;
   // E half of CORRECT_* before the update (main.cu:2798-2813)
   if (nf > 0) tfsf_e_apply<T><<<(unsigned)((nf + 255) / 256), 256, 0, st>>>(view<T>(s), s->tf_e);
-  if (s->su.hydro) launch_metal<T>(s, st);  // UpdateHydroP* read E^n here
+  // The dispersive components (Drude + 2CP, hydrodynamic current) run on a
+  // second stream beside the E pass: the pass skips them, reads no
+  // dispersive E component and writes none, and the dispersive kernels read
+  // E^n of their own cells and the final H only.
+  const bool metal = s->nmetal[0] + s->nmetal[1] + s->nmetal[2] > 0;
+  if (metal) {
+    cudaEventRecord(s->fork2_ev, st);
+    cudaStreamWaitEvent(s->side2, s->fork2_ev, 0);
+    launch_metal<T>(s, s->side2);
+  }
   s->kernels += launch_e_cfg<T>(s, s->ecfg, st) - 1;
-  if (!s->su.hydro) launch_metal<T>(s, st);
+  if (metal) {
+    cudaEventRecord(s->join2_ev, s->side2);
+    cudaStreamWaitEvent(st, s->join2_ev, 0);
+  }
   s->kernels += 1 + (nf > 0);
 }
 
