@@ -270,6 +270,47 @@ def adjoint_params(mod, steps=4000, precision=None):
         precision=mod.FDTD_FP32 if precision is None else precision)
 
 
+def large_params(mod, precision=None):
+    """The large nonlocal workload: 384 x 384 x 256 grid, dx = 1 nm, 12-cell
+    CPML, a 3 x 3 array of gold nanodisks (30 nm diameter, 10 nm high, 60 nm
+    pitch) on a 20 nm dielectric slab (eps 2.25), hydrodynamic current,
+    plane wave at normal incidence, 5 wavelengths 600-900 nm, FP32 fields."""
+    return mod.default_params(
+        Tend=11999, dx=1e-9, dy=1e-9, dz=1e-9, NCELLX=384 - 25, NCELLY=384 - 25, NCELLZ=256 - 25,
+        NcpmlX=12, NcpmlY=12, NcpmlZ=12, material=3, first_medium=1, NUM_freq=5, WL_or_freq=1,
+        lam_min=600e-9, lam_max=900e-9, lam_0=750e-9, BandWidth=7e14, NONLOCAL=3, hydro_D=3.0,
+        fermi_velocity=1.39e6, geometry=2, disk_diameter=30e-9, disk_height=10e-9, pitch=60e-9,
+        disk_nx=3, disk_ny=3, slab_eps=2.25, slab_thickness=20e-9,
+        precision=mod.FDTD_FP32 if precision is None else precision)
+
+
+def large_bench(mod, torch, stream, sp, dev, blocks=2):
+    """Forward throughput of the large nonlocal workload over a bounded
+    number of 128-step blocks (the full run is 12000 steps), and the device
+    memory the simulation holds.  Its adjoint is not built: the
+    hydrodynamic model is nonlinear."""
+    free0, _ = torch.cuda.mem_get_info(dev)
+    s = mod.Sim(large_params(mod), device=dev)
+    free1, _ = torch.cuda.mem_get_info(dev)
+    s.step(BLOCK, sp)
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    ev[0].record(stream)
+    s.step(BLOCK * blocks, sp)
+    ev[1].record(stream)
+    torch.cuda.synchronize()
+    ms = ev[0].elapsed_time(ev[1])
+    s.check()
+    d = s.dims
+    cells = d.nx * d.ny * d.nz
+    out = {"value": round(cells * BLOCK * blocks / (ms / 1e3) / 1e9, 3), "unit": "Gcell-steps/s",
+           "grid": [d.nx, d.ny, d.nz], "time_steps": BLOCK * blocks,
+           "dispersive_cells": list(d.n_metal_cells), "device_bytes": int(free0 - free1),
+           "adjoint": "not built for the hydrodynamic model (nonlinear in the current and density)"}
+    s.close()
+    return out
+
+
 ADJOINT_FREQS = [0, 83, 235]
 
 
@@ -392,6 +433,7 @@ def main():
     ap.add_argument("--num-freq", type=int, default=201)
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-large", action="store_true")
     ap.add_argument("--batch-members", type=int, default=64)
     ap.add_argument("--batch-steps", type=int, default=3000)
     ap.add_argument("--no-ref-gpu", action="store_true",
@@ -561,6 +603,10 @@ def main():
                                   / (msr / 1e3) / 1e9, 3)
             sm.close()
 
+    large = None
+    if not args.no_large and args.grid == 256:
+        large = large_bench(F, torch, stream, sp, dev)
+
     adjoint = None
     if not args.no_adjoint and args.grid == 256:
         adjoint = adjoint_bench(F, torch, stream, dev)
@@ -589,6 +635,7 @@ def main():
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "clocks": clk.summary(), "gpu_launches": launches, "fp64": fp64,
             "reference_deck": refdeck, "batched": batched, "adjoint": adjoint,
+            "large_nonlocal": large,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

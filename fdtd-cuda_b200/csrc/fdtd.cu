@@ -293,6 +293,7 @@ static fdtd_status build_views(fdtd_sim* s) {
   v.mat = s->mat;
   for (int a = 0; a < 3; a++) { v.mat_lo[a] = s->mat_lo[a]; v.mat_hi[a] = s->mat_hi[a]; }
   for (int q = 0; q < kMaxClasses; q++) { v.cee[q] = (T)su.Cee; v.ceh[q] = (T)su.Ceh; }
+  v.ceh[1] = (T)su.Ceh_slab;  // class 1: the dielectric slab (Cee = 1: no conductivity)
   v.chh = (T)su.Chh; v.che = (T)su.Che;
   const double dxyz[3] = {su.p.dx, su.p.dy, su.p.dz};
   const int N3[3] = {s->NX, s->NY, s->NZ};
@@ -530,6 +531,9 @@ static fdtd_status create_impl(const fdtd_params* p, int device, fdtd_sim** out,
         for (int i = 0; i < s->NX; i++) {
           const size_t r = ((size_t)i * s->NY + j) * s->NZ + k;
           uint8_t b = 0;
+          // class 1: the dielectric slab (any component on the slab)
+          for (int c = 0; c < 3; c++)
+            if (su.matc[c][r] == kSlabMaterial) b = (uint8_t)(1u << 3);
           for (int c = 0; c < 3; c++)
             if (is_dispersive(su.matc[c][r])) {
               b |= (uint8_t)(1u << c);

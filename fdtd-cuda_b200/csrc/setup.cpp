@@ -265,6 +265,20 @@ static void rasterise(Setup& s) {
           }
           if (in) s.matc[c][at(i, j, k)] = mat;
         }
+  // dielectric slab under the disks (no counterpart in the reference, whose
+  // DIELECTRIC_SLAB is commented out, main.cu:2566): cell centres with z in
+  // [-slab_thickness, 0) of the disk frame, strictly inside the TFSF box in
+  // x and y (off its faces, where the incident field is added); metal wins
+  // where both apply
+  if (p.geometry == FDTD_GEOM_DISK_ARRAY && p.slab_thickness > 0 && p.slab_eps != 1.0)
+    for (int i = s.Nt[0] + 1; i < NX - s.Nt[0] - 1; i++)
+      for (int j = s.Nt[1] + 1; j < NY - s.Nt[1] - 1; j++)
+        for (int k = 0; k < NZ; k++) {
+          const double z = (k - cz) * p.dz;
+          if (!(z >= -p.slab_thickness && z < 0)) continue;
+          for (int c = 0; c < 3; c++)
+            if (!is_dispersive(s.matc[c][at(i, j, k)])) s.matc[c][at(i, j, k)] = kSlabMaterial;
+        }
 }
 
 const char* setup_build(const fdtd_params& pin, Setup& s) {
@@ -277,6 +291,8 @@ const char* setup_build(const fdtd_params& pin, Setup& s) {
   if (p.material != 2 && p.material != 3 && !p.metal_custom) return "material must be 2 (Ag) or 3 (Au)";
   if (p.dft_every < 1) return "dft_every must be >= 1";
   if (p.BandWidth <= 0) return "BandWidth must be > 0";
+  if (p.geometry == FDTD_GEOM_DISK_ARRAY && p.slab_thickness > 0 && !(p.slab_eps >= 1.0))
+    return "slab_eps must be >= 1";
   if (p.precision != FDTD_FP32 && p.precision != FDTD_FP64) return "precision must be FDTD_FP32 or FDTD_FP64";
   // SETUP_CONST (setup.cu:347-510)
   s.z0 = kZ0; s.ep0 = kEP0; s.mu0 = kMU0; s.c0 = kC0; s.pi = kPI; s.e0 = kE0; s.me = kME;
@@ -340,6 +356,7 @@ const char* setup_build(const fdtd_params& pin, Setup& s) {
   // DEF_UPDATE_COEFF_* with eps = EP0, mu = MU0, sigma = 0
   s.Cee = (1 - (s.dt * 0) / (2 * kEP0)) / (1 + (s.dt * 0) / (2 * kEP0));
   s.Ceh = (s.dt / (s.z0 * kEP0)) / ((1 + (s.dt * 0) / (2 * kEP0)));
+  s.Ceh_slab = (s.dt / (s.z0 * kEP0 * p.slab_eps)) / ((1 + (s.dt * 0) / (2 * kEP0 * p.slab_eps)));
   s.Chh = (1 - (s.dt * 0) / (2 * kMU0)) / (1 + (s.dt * 0) / (2 * kMU0));
   s.Che = (s.z0 * s.dt / kMU0) / (1 + (s.dt * 0) / (2 * kMU0));
   const double dxyz[3] = {p.dx, p.dy, p.dz};

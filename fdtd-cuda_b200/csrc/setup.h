@@ -28,6 +28,7 @@ struct Setup {
   bool hydro = false;
   // Yee coefficients (uniform medium: eps = EP0, mu = MU0, sigma = 0)
   double Cee = 1, Ceh = 0, Chh = 1, Che = 0;
+  double Ceh_slab = 0;  // E-on-H coefficient of the dielectric slab class (eps = slab_eps)
   CpmlTables cp[3];
   // ADE
   double C_E = 0, C_E_1 = 0, C_E_2 = 0, d1 = 0, d2 = 0, d3 = 0, d4 = 0, d5 = 0, dNL = 0, N_EQ = 0;
@@ -51,5 +52,7 @@ int read_input_txt(const char* path, fdtd_params* p);
 int write_input_txt(const char* path, const fdtd_params* p);
 
 inline bool is_dispersive(int v) { return v > 1 && v < 6; }
+// material value of the dielectric slab (non-dispersive, eps = slab_eps)
+constexpr int kSlabMaterial = 6;
 
 }  // namespace fdtd

@@ -56,6 +56,7 @@ struct orc_sim {
   int *mat, *matc[3];
   /* Yee coefficients (uniform: eps = EP0, mu = MU0, sigma = 0) */
   double Cee, Ceh, Chh, Che;
+  double Ceh_slab; /* dielectric slab class (material 6, eps = slab_eps) */
   /* CPML */
   double *ked[3], *khd[3];
   cpml_axis cp[3];
@@ -235,6 +236,20 @@ static void rasterise(orc_sim* s) {
             if (in) m[q][IDX(s, i, j, k)] = mat;
           }
         }
+    /* dielectric slab under the disks (the reference's DIELECTRIC_SLAB is
+     * commented out, main.cu:2566): cell centres with z in [-T, 0),
+     * strictly inside the TFSF box in x and y; metal wins */
+    if (p->geometry == FDTD_GEOM_DISK_ARRAY && p->slab_thickness > 0 && p->slab_eps != 1.0) {
+      double czs = NZ / 2;
+      for (int i = s->Nt[0] + 1; i < NX - s->Nt[0] - 1; i++)
+        for (int j = s->Nt[1] + 1; j < NY - s->Nt[1] - 1; j++)
+          for (int k = 0; k < NZ; k++) {
+            double z = (k - czs) * p->dz;
+            if (!(z >= -p->slab_thickness && z < 0)) continue;
+            for (int q = 0; q < 4; q++)
+              if (!(m[q][IDX(s, i, j, k)] > 1 && m[q][IDX(s, i, j, k)] < 6)) m[q][IDX(s, i, j, k)] = 6;
+          }
+    }
   } else if (p->geometry == FDTD_GEOM_REFERENCE && p->nano_sphere == 2) {
     double cz = p->dispersive_slab, cx = NX / 2, cy = NY / 2;
     for (int i = 0; i < NX; i++)
@@ -292,6 +307,20 @@ static void rasterise(orc_sim* s) {
             if (in) m[q][IDX(s, i, j, k)] = mat;
           }
         }
+    /* dielectric slab under the disks (the reference's DIELECTRIC_SLAB is
+     * commented out, main.cu:2566): cell centres with z in [-T, 0),
+     * strictly inside the TFSF box in x and y; metal wins */
+    if (p->geometry == FDTD_GEOM_DISK_ARRAY && p->slab_thickness > 0 && p->slab_eps != 1.0) {
+      double czs = NZ / 2;
+      for (int i = s->Nt[0] + 1; i < NX - s->Nt[0] - 1; i++)
+        for (int j = s->Nt[1] + 1; j < NY - s->Nt[1] - 1; j++)
+          for (int k = 0; k < NZ; k++) {
+            double z = (k - czs) * p->dz;
+            if (!(z >= -p->slab_thickness && z < 0)) continue;
+            for (int q = 0; q < 4; q++)
+              if (!(m[q][IDX(s, i, j, k)] > 1 && m[q][IDX(s, i, j, k)] < 6)) m[q][IDX(s, i, j, k)] = 6;
+          }
+    }
   }
 }
 
@@ -491,6 +520,7 @@ orc_sim* orc_create(const fdtd_params* pin, char* err) {
    * eps = EP0, mu = MU0, sigma = 0 (DEF_EPS/MU/SIGMA, setup.cu:1943-1997) */
   s->Cee = (1 - (s->dt * 0) / (2 * K_EP0)) / (1 + (s->dt * 0) / (2 * K_EP0));
   s->Ceh = (s->dt / (s->z0 * K_EP0)) / ((1 + (s->dt * 0) / (2 * K_EP0)));
+  s->Ceh_slab = (s->dt / (s->z0 * K_EP0 * s->p.slab_eps)) / ((1 + (s->dt * 0) / (2 * K_EP0 * s->p.slab_eps)));
   s->Chh = (1 - (s->dt * 0) / (2 * K_MU0)) / (1 + (s->dt * 0) / (2 * K_MU0));
   s->Che = (s->z0 * s->dt / K_MU0) / (1 + (s->dt * 0) / (2 * K_MU0));
   /* CPML; order X, Z, Y as SETUP_CPML does (setup.cu:513-533) */
@@ -1041,7 +1071,7 @@ static void update_e_comp(orc_sim* s, int c) {
             for (int q = 0; q < 2; q++) { cpn1[q] = cpn[q]; cpn[q] = ncp[q]; }
           }
         } else {
-          E[id] = s->Cee * E[id] + s->Ceh * curl;
+          E[id] = s->Cee * E[id] + (s->mat[id] == 6 ? s->Ceh_slab : s->Ceh) * curl;
         }
         /* CPML along the two transverse axes: for ex the z then y slabs
          * (main.cu:1294-1318); ey: z then x; ez: y then x. */
