@@ -4,6 +4,7 @@ Tolerances: FP64 fields and spectra within 1e-11 relative (norm-wise for
 fields: max |a - b| / max |b|); FP32 within the bounds stated per test.
 """
 import functools
+import os
 
 import numpy as np
 import pytest
@@ -202,3 +203,29 @@ def test_unbuilt_pass_variant_is_rejected(monkeypatch):
     with pytest.raises(F.FdtdError) as e:
         F.Sim(make(F, "vacuum", precision=F.FDTD_FP32))
     assert e.value.status == 1 and "not built" in str(e.value)
+
+
+def test_spectral_error_table():
+    """The error of every spectrum against the FP64 oracle, FP64 and FP32
+    builds: max over wavelengths of |this - oracle| / max |oracle| for the
+    scattering, absorption and extinction columns.  Written as a table to
+    the path in FDTD_PARITY_REPORT when set."""
+    rows = []
+    for name in sorted(CASES):
+        errs = {}
+        for prec, tag in ((F.FDTD_FP64, "f64"), (F.FDTD_FP32, "f32")):
+            s, o = spectra_pair(name, prec)
+            a, b = s.spectra(), o.spectra()
+            errs[tag] = [float(np.max(np.abs(a[:, c] - b[:, c])) / np.max(np.abs(b[:, c]))) for c in (1, 2, 3)]
+            s.close()
+        rows.append((name, errs))
+        if name != "vacuum":  # no particle: its spectra are leakage noise
+            assert max(errs["f64"]) < 1e-10, (name, errs)
+            assert max(errs["f32"]) < 2e-3, (name, errs)
+    path = os.environ.get("FDTD_PARITY_REPORT")
+    if path:
+        with open(path, "w") as f:
+            f.write("| case | FP64 sca | FP64 abs | FP64 ext | FP32 sca | FP32 abs | FP32 ext |\n")
+            f.write("|---|---|---|---|---|---|---|\n")
+            for name, e in rows:
+                f.write(f"| {name} | " + " | ".join("%.1e" % x for x in e["f64"] + e["f32"]) + " |\n")
