@@ -67,16 +67,19 @@ __global__ void dft_sample_batch(const BatchSim<T>* __restrict__ b) {
 template <typename T>
 __global__ void dft_twiddles_batch(const BatchSim<T>* __restrict__ b) {
   const BatchSim<T>& x = b[blockIdx.y];
-  dft_twiddles_body(x.dft, x.clk, x.tw);
+  dft_twiddles_body(x.dft, x.clk, x.tw, 0);
 }
 template <typename T>
 __global__ void __launch_bounds__(128) dft_contract_batch(const BatchSim<T>* __restrict__ b) {
   const BatchSim<T>& x = b[blockIdx.y];
-  dft_contract_body(x.dft, x.ring, x.clk, x.tw);
+  dft_contract_body(x.dft, x.ring, x.clk, x.tw, 0);
 }
+// a flush before the spectra are read goes through the member's own
+// contraction kernels (fdtd_spectral_finalize)
 template <typename T>
 __global__ void dft_reset_batch(const BatchSim<T>* __restrict__ b) {
-  b[blockIdx.y].clk->nsamp = 0;
+  DevClock* clk = b[blockIdx.y].clk;
+  if (dft_ring_ready(clk, 0)) clk->nsamp = 0;
 }
 
 }  // namespace fdtd
@@ -162,7 +165,7 @@ static fdtd_status batch_build(fdtd_batch* b) {
     int maxn = 0;
     for (int f = 0; f < 12; f++) maxn = std::max(maxn, s->dft.face[f].na * s->dft.face[f].nb);
     b->g_s = std::max(b->g_s, blocks(maxn, 256));
-    b->g_tw = std::max(b->g_tw, blocks(2LL * kSampleBlock * s->dft.nf, 256));
+    b->g_tw = std::max(b->g_tw, blocks(2LL * kRingSlots * s->dft.nf, 256));
     b->g_c = std::max(b->g_c, (unsigned)(s->dft.rows / kDftRows));
   }
   BatchSim<T>* dd;
@@ -196,7 +199,8 @@ static fdtd_status batch_build(fdtd_batch* b) {
   if ((st = slots(e_pass_batch<T, kBatchTY, kBatchS, kBatchMinB, true>, b->grid_pass)) != FDTD_OK) return st;
   if ((st = slots(h_pass_batch<T, kBatchTY, kBatchS, kBatchMinB, false>, b->grid_inner)) != FDTD_OK) return st;
   if ((st = slots(e_pass_batch<T, kBatchTY, kBatchS, kBatchMinB, false>, b->grid_inner)) != FDTD_OK) return st;
-  CUDA_TRY(cudaFuncSetAttribute(dft_contract_batch<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDftSmem));
+  CUDA_TRY(cudaFuncSetAttribute(dft_contract_batch<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)dft_smem_bytes<T>()));
   return FDTD_OK;
 }
 
@@ -245,8 +249,9 @@ static void batch_enqueue_step(fdtd_batch* b, cudaStream_t st) {
     dft_sample_batch<T><<<dim3(b->g_s, 12, n), 256, 0, st>>>(d);
     k++;
     if (++b->host_nsamp == kSampleBlock) {
+      // the members' rings fill together: these contract once they are full
       dft_twiddles_batch<T><<<dim3(b->g_tw, n), 256, 0, st>>>(d);
-      dft_contract_batch<T><<<dim3(b->g_c, n), 128, kDftSmem, st>>>(d);
+      dft_contract_batch<T><<<dim3(b->g_c, n), 128, dft_smem_bytes<T>(), st>>>(d);
       dft_reset_batch<T><<<dim3(1, n), 1, 0, st>>>(d);
       k += 3;
       b->host_nsamp = 0;

@@ -1,7 +1,8 @@
 // TFSF work of the time step, on the cells that need it only:
-//   tfsf_h_faces / tfsf_e_faces   CORRECT_X/Y/Z (main.cu:369-758) on the
-//                                 cells of the TFSF box faces: after the H
-//                                 update for H, before the E update for E
+//   tfsf_tabulate                 at create: the corrections of CORRECT_X/Y/Z
+//                                 (main.cu:369-758) on the TFSF box faces
+//   tfsf_h_apply / tfsf_e_apply   every step: after the H update for H,
+//                                 before the E update for E
 // Splitting these off keeps the Yee passes branch-free: x is the warp
 // dimension, so the x faces would otherwise make two warps of every row
 // execute the face code.
@@ -49,54 +50,12 @@ struct ShellCells {
   }
 };
 
-template <typename T>
-__device__ __forceinline__ void tfsf_h_faces_body(const SimView<T>& g, const ShellCells& sh) {
-  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= sh.total()) return;
-  int i, j, k;
-  sh.cell(q, i, j, k);
-  const size_t id = fidx(g.PX, g.plane, i, j, k);
-#pragma unroll
-  for (int c = 0; c < 3; c++) {
-    g.H[c][id] = tfsf_h(g, c, i, j, k, g.H[c][id]);
-  }
-}
-template <typename T>
-__global__ void tfsf_h_faces(const SimView<T>* __restrict__ gv, const ShellCells sh) {
-  tfsf_h_faces_body(*gv, sh);
-}
-
-template <typename T>
-__device__ __forceinline__ void tfsf_e_faces_body(const SimView<T>& g, const ShellCells& sh) {
-  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= sh.total()) return;
-  int i, j, k;
-  sh.cell(q, i, j, k);
-  const size_t id = fidx(g.PX, g.plane, i, j, k);
-  unsigned m = 0;
-  if (i >= g.mat_lo[0] && i < g.mat_hi[0] && j >= g.mat_lo[1] && j < g.mat_hi[1] && k >= g.mat_lo[2] &&
-      k < g.mat_hi[2])
-    m = g.mat[id];
-  const T ceh = g.ceh[m >> 3];
-#pragma unroll
-  for (int c = 0; c < 3; c++) {
-    g.E[c][id] = tfsf_e(g, c, i, j, k, g.E[c][id], ceh);
-  }
-}
-template <typename T>
-__global__ void tfsf_e_faces(const SimView<T>* __restrict__ gv, const ShellCells sh) {
-  tfsf_e_faces_body(*gv, sh);
-}
-
-}  // namespace fdtd
-
-namespace fdtd {
-
 // TFSF corrections tabulated once at create: per face cell and component
 // with at least one correction, up to two (line index, weight, meta) terms
 // in the reference's order; meta = (sign > 0) | axis << 1 | component << 3.
-// Applying a term is the same arithmetic as tfsf_h / tfsf_e with the
-// projection and the truncation already done.
+// Applying a term adds sign * coefficient * (interpolated incident value)
+// * (polarisation factor) / d_axis, the arithmetic of the walk forms in
+// kernels.cuh with the projection and the truncation already done.
 struct TfsfTable {
   int n;                      // groups
   const unsigned* id;         // cell offset in the device layout

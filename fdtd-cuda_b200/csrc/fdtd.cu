@@ -110,9 +110,9 @@ struct fdtd_sim {
   DftView dft;
   void* ring = nullptr;
   double* flux = nullptr;  // [12][nf]
-  double2* twiddles = nullptr;  // [2][kSampleBlock][nf]
+  double2* twiddles = nullptr;  // [2][kRingSlots][nf]
   bool dft_on = true;
-  int host_nsamp = 0;
+  int host_nsamp = 0;  // samples since the last contraction launch (launch period position)
   // views (one of them is used, by precision)
   SimView<float> vf;
   SimView<double> vd;
@@ -415,7 +415,7 @@ static fdtd_status build_views(fdtd_sim* s) {
   // DFT sample ring
   if (s->dft.rows > 0) {
     T* r;
-    cudaError_t e = s->alloc(&r, (size_t)kSampleBlock * s->dft.rows, true);
+    cudaError_t e = s->alloc(&r, (size_t)kRingSlots * s->dft.rows, true);
     if (e != cudaSuccess) return fail(FDTD_ERR_ALLOC, cudaGetErrorString(e));
     s->ring = r;
   }
@@ -671,7 +671,7 @@ static fdtd_status create_impl(const fdtd_params* p, int device, fdtd_sim** out,
         (e = s->alloc(&d.acc_im, (size_t)d.nf * d.rows, true)) != cudaSuccess)
       return fail(FDTD_ERR_ALLOC, std::string("DFT accumulators: ") + cudaGetErrorString(e));
     CUDA_TRY(s->alloc(&s->flux, (size_t)12 * d.nf));
-    CUDA_TRY(s->alloc(&s->twiddles, (size_t)2 * kSampleBlock * d.nf));
+    CUDA_TRY(s->alloc(&s->twiddles, (size_t)2 * kRingSlots * d.nf));
   }
   s->dft_on = su.p.StaticField == 0;
   // CPML slab cells and TFSF shells
@@ -793,7 +793,7 @@ static void staged_attributes() {
                        (int)staged_smem<T, TY, S>());
   FDTD_STAGED_VARIANTS(FDTD_ATTR)
 #undef FDTD_ATTR
-  cudaFuncSetAttribute(dft_contract<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDftSmem);
+  cudaFuncSetAttribute(dft_contract<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dft_smem_bytes<T>());
   done = true;
 }
 
@@ -1079,13 +1079,24 @@ static void launch_sample(fdtd_sim* s, cudaStream_t st) {
   s->kernels++;
 }
 template <typename T>
-static void launch_contract(fdtd_sim* s, cudaStream_t st) {
-  const int ntw = 2 * kSampleBlock * s->dft.nf;
-  dft_twiddles<<<(ntw + 255) / 256, 256, 0, st>>>(s->dft, s->clk, s->twiddles);
-  dft_contract<T><<<(unsigned)(s->dft.rows / kDftRows), 128, kDftSmem, st>>>(s->dft, (const T*)s->ring, s->clk,
-                                                                        s->twiddles);
-  dft_reset_count<<<1, 1, 0, st>>>(s->clk);
+static void launch_contract(fdtd_sim* s, cudaStream_t st, bool force) {
+  const int ntw = 2 * kRingSlots * s->dft.nf;
+  dft_twiddles<<<(ntw + 255) / 256, 256, 0, st>>>(s->dft, s->clk, s->twiddles, (int)force);
+  dft_contract<T><<<(unsigned)(s->dft.rows / kDftRows), 128, dft_smem_bytes<T>(), st>>>(
+      s->dft, (const T*)s->ring, s->clk, s->twiddles, (int)force);
+  dft_reset_count<<<1, 1, 0, st>>>(s->clk, (int)force);
   s->kernels += 3;
+}
+
+// One DFT sample of the step; every kSampleBlock samples the contraction
+// kernels are launched, and they contract once the ring is full.
+template <typename T>
+static void sample_and_contract(fdtd_sim* s, cudaStream_t st) {
+  launch_sample<T>(s, st);
+  if (++s->host_nsamp == kSampleBlock) {
+    launch_contract<T>(s, st, false);
+    s->host_nsamp = 0;
+  }
 }
 
 // One full step in the reference's order.  Host mirrors of the clock
@@ -1095,13 +1106,7 @@ static void enqueue_step(fdtd_sim* s, cudaStream_t st) {
   launch_h<T>(s, st);
   launch_line<T>(s, st);
   launch_e<T>(s, st);
-  if (s->line.dft_every > 0 && s->t % s->line.dft_every == 0) {
-    launch_sample<T>(s, st);
-    if (++s->host_nsamp == kSampleBlock) {
-      launch_contract<T>(s, st);
-      s->host_nsamp = 0;
-    }
-  }
+  if (s->line.dft_every > 0 && s->t % s->line.dft_every == 0) sample_and_contract<T>(s, st);
   s->t++;
 }
 
@@ -1187,11 +1192,7 @@ extern "C" fdtd_status fdtd_spectral_accumulate(fdtd_sim* s, void* stream) {
   CUDA_TRY(cudaSetDevice(s->device));
   cudaStream_t st = as_stream(stream);
   if (s->line.dft_every > 0 && s->t % s->line.dft_every == 0) {
-    if (s->fp64) launch_sample<double>(s, st); else launch_sample<float>(s, st);
-    if (++s->host_nsamp == kSampleBlock) {
-      if (s->fp64) launch_contract<double>(s, st); else launch_contract<float>(s, st);
-      s->host_nsamp = 0;
-    }
+    if (s->fp64) sample_and_contract<double>(s, st); else sample_and_contract<float>(s, st);
   }
   s->t++;
   CUDA_TRY(cudaGetLastError());
@@ -1247,11 +1248,12 @@ extern "C" fdtd_status fdtd_check(fdtd_sim* s) {
 // ---------------------------------------------------------------------
 // spectra
 
+// Contracts what the device ring holds (nothing when it is empty).
 static fdtd_status flush_dft(fdtd_sim* s) {
-  if (s->host_nsamp > 0) {
-    if (s->fp64) launch_contract<double>(s, 0); else launch_contract<float>(s, 0);
-    s->host_nsamp = 0;
+  if (s->dft.rows > 0 && s->line.dft_every > 0) {
+    if (s->fp64) launch_contract<double>(s, 0, true); else launch_contract<float>(s, 0, true);
   }
+  s->host_nsamp = 0;
   CUDA_TRY(cudaGetLastError());
   return FDTD_OK;
 }

@@ -19,7 +19,9 @@
 namespace fdtd {
 
 constexpr int kMaxClasses = 32;   // dielectric classes (bits 3..7)
-constexpr int kSampleBlock = 32;  // DFT samples per FP64 contraction
+constexpr int kSampleBlock = 32;  // DFT samples per launch period of the stepper
+constexpr int kRingSlots = 64;    // DFT samples per FP64 contraction (ring depth)
+static_assert(kRingSlots % kSampleBlock == 0, "the ring holds whole launch periods");
 
 // Step clock kept in device memory so captured graphs can be replayed.
 struct DevClock {
@@ -28,7 +30,7 @@ struct DevClock {
   int nonfinite;  // watchdog flag
   int samp_slot;  // ring slot of the current step's DFT sample
   double e1, e2;  // Mur history of the incident line ends (main.cu:2835-2838)
-  int samp_t[kSampleBlock];
+  int samp_t[kRingSlots];
 };
 
 // Per-axis CPML tables.  The E tables have Nc+1 entries, the H tables Nc.

@@ -1,17 +1,19 @@
 // CUDA kernels of the FDTD time step (sm_100a).
 //
 // One time step is:
-//   h_pass      fused UPDATE_hx/hy/hz + H CPML + H half of CORRECT_X/Y/Z
+//   h_pass      UPDATE_hx/hy/hz + H CPML (staged.cuh)
+//   tfsf_h      H half of CORRECT_X/Y/Z on the TFSF faces (boundary.cuh)
 //   line_step   UPDATE_h_inc + UPDATE_e_inc + Mur ends + source (1 CTA)
-//   e_pass      E half of CORRECT_*, UPDATE_ex/ey/ez for non-dispersive
-//               components + E CPML
-//   metal_*     dispersive (Drude + 2CP, hydrodynamic) cells, compact list
+//   tfsf_e      E half of CORRECT_X/Y/Z (boundary.cuh)
+//   e_pass      UPDATE_ex/ey/ez for non-dispersive components + E CPML
+//   metal_e / hydro_*   dispersive (Drude + 2CP, hydrodynamic) cells,
+//               compact lists
 //   dft_sample  every dft_every steps: gather the flux-plane tangential
 //               components into a sample ring
-//   dft_contract every kSampleBlock samples: FP64 contraction of the ring
-//               with the phasors into the accumulators
-// The E and H passes march along z with a 2-D (x, y) thread tile; the
-// z-neighbour is carried in registers, x and y neighbours come through L1.
+//   dft_contract once the ring holds kRingSlots samples: FP64 contraction
+//               of the ring with the phasors into the accumulators
+// This file holds the bodies of everything but the Yee passes and the TFSF
+// tables.
 #pragma once
 #include <cuda_runtime.h>
 #include <math.h>
@@ -81,9 +83,9 @@ __device__ __forceinline__ double hinc_at(const double* h, int m0, double d) {
 
 // The H half of CORRECT_X/Y/Z for H component c at (i,j,k), in the
 // reference's kernel order X, Y, Z: fn(sign, axis, e_component, d) per
-// correction, d the projected distance on the incident line.  The applying
-// form adds sign * che * e_inc(d) fe / d_axis; the tabulating form records
-// the line index and interpolation weight.
+// correction, d the projected distance on the incident line.  tfsf_tabulate
+// records the line index and interpolation weight of each correction; the
+// appliers add sign * che * e_inc(d) fe / d_axis.
 template <typename T, typename Fn>
 __device__ __forceinline__ void tfsf_h_walk(const SimView<T>& s, int c, int i, int j, int k, Fn&& fn) {
   const TfsfView& tf = s.tf;
@@ -195,38 +197,6 @@ __device__ __forceinline__ void tfsf_e_walk(const SimView<T>& s, int c, int i, i
   }
 }
 
-
-template <typename T>
-__device__ __forceinline__ T tfsf_h(const SimView<T>& s, int c, int i, int j, int k, T v) {
-  const T dd[3] = {s.dxyz[0], s.dxyz[1], s.dxyz[2]};
-  const T che = s.che;
-  tfsf_h_walk(s, c, i, j, k, [&](int sg, int ax, int f, double d) {
-    const T x = (T)(einc_at(s.e_inc, s.tf.m0, d) * (double)s.tf.fe[f]);
-    if (sg > 0) v += che * x / dd[ax]; else v -= che * x / dd[ax];
-  });
-  return v;
-}
-
-// ceh is the cell's E-on-H coefficient (the reference uses Cexh for ex and
-// ey, Cezh for ez; they are equal per cell).
-template <typename T>
-__device__ __forceinline__ T tfsf_e(const SimView<T>& s, int c, int i, int j, int k, T v, T ceh) {
-  const T dd[3] = {s.dxyz[0], s.dxyz[1], s.dxyz[2]};
-  tfsf_e_walk(s, c, i, j, k, [&](int sg, int ax, int f, double d) {
-    const T x = (T)(hinc_at(s.h_inc, s.tf.m0, d) * (double)s.tf.fh[f]);
-    if (sg > 0) v += ceh * x / dd[ax]; else v -= ceh * x / dd[ax];
-  });
-  return v;
-}
-
-__device__ __forceinline__ bool near_tfsf_h(const TfsfView& tf, int NX, int NY, int NZ, int i, int j, int k) {
-  return tf.on && (i == tf.Tx - 1 || i == NX - tf.Tx || j == tf.Ty - 1 || j == NY - tf.Ty ||
-                   k == tf.Tz - 1 || k == NZ - tf.Tz);
-}
-__device__ __forceinline__ bool near_tfsf_e(const TfsfView& tf, int NX, int NY, int NZ, int i, int j, int k) {
-  return tf.on && (i == tf.Tx || i == NX - tf.Tx || j == tf.Ty || j == NY - tf.Ty || k == tf.Tz ||
-                   k == NZ - tf.Tz);
-}
 
 // ---------------------------------------------------------------------
 // CPML psi helpers.  psi layouts: z slab [w][NY][PX], y slab [NZ][w][PX],
@@ -342,7 +312,7 @@ __device__ __forceinline__ void line_step_body(const LineArgs& a, const SimView<
     // t % 4 == 0, main.cu:2920)
     if (a.dft_every > 0 && t % a.dft_every == 0) {
       const int slot = a.clk->nsamp;
-      if (slot < kSampleBlock) {
+      if (slot < kRingSlots) {
         a.clk->samp_slot = slot;
         a.clk->samp_t[slot] = t;
         a.clk->nsamp = slot + 1;
@@ -421,7 +391,7 @@ __device__ __forceinline__ void metal_e_body(const SimView<T>& s, const MetalVie
   const size_t id = fidx(s.PX, s.plane, i, j, k);
   const unsigned mb = s.mat[id];
   const T ceh = s.ceh[mb >> 3];
-  // the E half of CORRECT_* has already been added by tfsf_e_faces
+  // the E half of CORRECT_* has already been added by tfsf_e_apply
   const T v = s.E[c][id];
   T da, db;
   const T curl = curl_h_at(s, c, i, j, k, &da, &db);
@@ -663,7 +633,7 @@ struct DftView {
 template <typename T>
 __device__ __forceinline__ void dft_sample_body(const SimView<T>& s, const DftView& d, T* ring, const DevClock* clk) {
   const int slot = clk->samp_slot;
-  if (slot < 0 || slot >= kSampleBlock) return;
+  if (slot < 0 || slot >= kRingSlots) return;
   const int f = blockIdx.y;
   const DftFace F = d.face[f];
   const int n = F.na * F.nb;
@@ -690,52 +660,81 @@ __global__ void dft_sample(const __grid_constant__ SimView<T> s, const __grid_co
 
 // Phasors of the samples waiting in the ring: tw[h][s][f] = exp(i 2 pi
 // (t_s + delta_h) dt freq[f]) with delta = 1 for E (sampled after the E
-// update) and 1/2 for H (main.cu:62-76).  [2][kSampleBlock][nf] of double2.
-__device__ __forceinline__ void dft_twiddles_body(const DftView& d, const DevClock* clk, double2* tw) {
+// update) and 1/2 for H (main.cu:62-76).  [2][kRingSlots][nf] of double2.
+// The stepper launches the contraction kernels every kSampleBlock samples.
+// Unless `force` is set (a flush before the spectra are read) they return
+// at once while the ring can take another kSampleBlock samples, so the
+// ring never overflows whatever the ring held when the launches began.
+__device__ __forceinline__ bool dft_ring_ready(const DevClock* clk, int force) {
+  return force || clk->nsamp > kRingSlots - kSampleBlock;
+}
+__device__ __forceinline__ void dft_twiddles_body(const DftView& d, const DevClock* clk, double2* tw, int force) {
+  if (!dft_ring_ready(clk, force)) return;
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= 2 * kSampleBlock * d.nf) return;
-  const int h = q / (kSampleBlock * d.nf);
-  const int r = q - h * kSampleBlock * d.nf;
+  if (q >= 2 * kRingSlots * d.nf) return;
+  const int h = q / (kRingSlots * d.nf);
+  const int r = q - h * kRingSlots * d.nf;
   const int sidx = r / d.nf, f = r - sidx * d.nf;
   double c = 0, sv = 0;
-  if (sidx < min(kSampleBlock, clk->nsamp)) {
+  if (sidx < min(kRingSlots, clk->nsamp)) {
     const int ts = clk->samp_t[sidx];
     const double ph = (double)(float)2.0 * 3.1415926535897932384626433832795 * (ts + (h ? 0.5 : 1.0)) * d.dt * d.freq[f];
     sincos(ph, &sv, &c);
   }
   tw[q] = make_double2(c, sv);
 }
-__global__ void dft_twiddles(const __grid_constant__ DftView d, const DevClock* clk, double2* tw) {
-  dft_twiddles_body(d, clk, tw);
+__global__ void dft_twiddles(const __grid_constant__ DftView d, const DevClock* clk, double2* tw, int force) {
+  dft_twiddles_body(d, clk, tw, force);
 }
 
-// acc[f][r] += sum_s x[s][r] tw[h(r)][s][f] in FP64.  A CTA owns kDftRows
-// rows (all E or all H thanks to the padding) and walks every frequency in
-// tiles of kDftFreqs; each thread accumulates a 4-row x 4-frequency
-// micro-tile, so one shared load feeds several FMAs.  The accumulators of
-// a tile are copied into shared memory with cp.async while the tile's FMAs
-// run, so their DRAM latency overlaps the arithmetic.
+// acc[f][r] += sum_s x[s][r] tw[h(r)][s][f] in FP64, as a real matrix
+// product on the FP64 tensor path (mma.sync m8n8k4 .f64): M = the real and
+// imaginary parts of the phasors of 8 frequencies, K = 4 samples, N = 8 rows.
+// A CTA owns kDftRows rows (all E or all H thanks to the padding) and walks
+// every frequency in tiles of kDftFreqs; each of its four warps owns 32 rows
+// of the tile, i.e. 2 frequency groups x {re, im} x 4 row groups = 16
+// accumulator fragments.  The samples of the CTA's rows are staged once in
+// shared memory, the phasors are read through L1 (a tile's phasors are 16
+// KB), and the accumulators of a tile are copied into shared memory with
+// cp.async while the tile's products run.  With
+// kRingSlots = 64 samples per contraction the accumulator traffic (one FP64
+// read and write per row and frequency) is spread over 64 samples.
 constexpr int kDftRows = 128;
 constexpr int kDftFreqs = 16;
-// dynamic shared memory of the contraction: samples, twiddles, accumulators
-constexpr size_t kDftSmem = sizeof(double) * kSampleBlock * kDftRows + sizeof(double2) * kSampleBlock * kDftFreqs +
-                            2 * sizeof(double) * kDftFreqs * kDftRows;
+constexpr int kDftXsPitch = kDftRows + 8;   // sample row pitch (elements): conflict-free B loads
+constexpr int kDftAccPitch = kDftRows + 4;  // accumulator row pitch (doubles)
+// dynamic shared memory of the contraction: samples (in the field type) and
+// accumulators; three CTAs fit an SM in FP32, two in FP64
+template <typename T>
+constexpr size_t dft_smem_bytes() {
+  return sizeof(T) * kRingSlots * kDftXsPitch + 2 * sizeof(double) * kDftFreqs * kDftAccPitch;
+}
 
 __device__ __forceinline__ void dft_cp_async16(void* dst, const void* src) {
   const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src));
 }
 
+// D = A B + D for one m8n8k4 FP64 fragment: a = A[lane/4][lane%4],
+// b = B[lane%4][lane/4], d = D[lane/4][2 (lane%4) + {0, 1}].
+__device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
 template <typename T>
 __device__ __forceinline__ void dft_contract_body(const DftView& d, const T* ring, const DevClock* clk,
-                                                  const double2* tw) {
+                                                  const double2* tw, int force) {
   extern __shared__ __align__(16) unsigned char dft_smem[];
-  double(*xs)[kDftRows] = reinterpret_cast<double(*)[kDftRows]>(dft_smem);
-  double2(*ws)[kDftFreqs] = reinterpret_cast<double2(*)[kDftFreqs]>(dft_smem + sizeof(double) * kSampleBlock * kDftRows);
-  double(*ar)[kDftRows] = reinterpret_cast<double(*)[kDftRows]>(
-      dft_smem + sizeof(double) * kSampleBlock * kDftRows + sizeof(double2) * kSampleBlock * kDftFreqs);
-  double(*ai)[kDftRows] = ar + kDftFreqs;
-  const int nsamp = min(kSampleBlock, clk->nsamp);
+  constexpr size_t kXs = sizeof(T) * kRingSlots * kDftXsPitch;
+  T(*xs)[kDftXsPitch] = reinterpret_cast<T(*)[kDftXsPitch]>(dft_smem);
+  double(*ar)[kDftAccPitch] = reinterpret_cast<double(*)[kDftAccPitch]>(dft_smem + kXs);
+  double(*ai)[kDftAccPitch] = ar + kDftFreqs;
+  if (!dft_ring_ready(clk, force)) return;
+  const int nsamp = min(kRingSlots, clk->nsamp);
+  if (nsamp == 0) return;  // an empty ring adds nothing
+  const int nk = (nsamp + 3) & ~3;  // K padded to whole m8n8k4 steps with zero samples
   const long long r0 = (long long)blockIdx.x * kDftRows;
   if (r0 >= d.rows) return;  // batched launches size the grid for the largest simulation
   // E or H rows: the tile lies inside one (face, component) block
@@ -745,14 +744,23 @@ __device__ __forceinline__ void dft_contract_body(const DftView& d, const T* rin
     if (r0 >= F.row0 && r0 < F.row0 + 4 * F.npad) { h = (r0 - F.row0) >= 2 * F.npad; break; }
   }
   const int tid = threadIdx.x;
-  for (int q = tid; q < kSampleBlock * kDftRows; q += 128) {
-    const int sidx = q / kDftRows, rr = q - sidx * kDftRows;
-    xs[sidx][rr] = sidx < nsamp ? (double)ring[(size_t)sidx * d.rows + r0 + rr] : 0.0;
+  // the samples of this CTA's rows, 16 bytes per copy (rows are padded to
+  // kDftRows, so every copy lies inside the ring); the K padding is zeroed
+  constexpr int kPer = 16 / sizeof(T);
+  for (int q = tid; q < nsamp * (kDftRows / kPer); q += 128) {
+    const int sidx = q / (kDftRows / kPer), rr = kPer * (q - sidx * (kDftRows / kPer));
+    dft_cp_async16(&xs[sidx][rr], ring + (size_t)sidx * d.rows + r0 + rr);
   }
-  const int rg = tid & 31, fg = tid >> 5;  // rows rg*4..+3, freqs fg*4..+3
-  const double2* twh = tw + (size_t)h * kSampleBlock * d.nf;
+  for (int q = tid; q < (nk - nsamp) * kDftRows; q += 128) xs[nsamp + q / kDftRows][q % kDftRows] = T(0);
+  asm volatile("cp.async.commit_group;\n" ::);
+  asm volatile("cp.async.wait_all;\n" ::);  // the barrier at the top of the tile loop publishes them
+  const int lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, q4 = lane & 3;  // fragment row group and thread-in-group
+  const int rw = warp * 32;                // this warp's rows within the tile
+  // phasors: slots past nsamp hold zeros (dft_twiddles writes every slot)
+  const double2* twh = tw + (size_t)h * kRingSlots * d.nf;
   for (int f0 = 0; f0 < d.nf; f0 += kDftFreqs) {
-    __syncthreads();  // xs loaded / previous tile's ws and accumulators consumed
+    __syncthreads();  // xs loaded / previous tile's accumulators consumed
     // this tile's accumulators, 16 bytes (two rows) per copy
     for (int q = tid; q < kDftFreqs * kDftRows / 2; q += 128) {
       const int fl = q / (kDftRows / 2), rr = 2 * (q - fl * (kDftRows / 2));
@@ -763,56 +771,61 @@ __device__ __forceinline__ void dft_contract_body(const DftView& d, const T* rin
       }
     }
     asm volatile("cp.async.commit_group;\n" ::);
-    for (int q = tid; q < kSampleBlock * kDftFreqs; q += 128) {
-      const int sidx = q / kDftFreqs, fl = q - sidx * kDftFreqs;
-      ws[sidx][fl] = (f0 + fl < d.nf) ? twh[(size_t)sidx * d.nf + f0 + fl] : make_double2(0.0, 0.0);
-    }
-    __syncthreads();
-    double re[4][4], im[4][4];
+    // A operands: this thread's two frequencies, clamped to the last one
+    // (the rows of frequencies past nf are computed and dropped)
+    const double2* tw0 = twh + min(f0 + g, d.nf - 1);
+    const double2* tw1 = twh + min(f0 + 8 + g, d.nf - 1);
+    // acc[fg][c][n]: frequency group fg, c = 0 re / 1 im, row group n
+    double acc[2][2][4][2];
 #pragma unroll
-    for (int a = 0; a < 4; a++)
+    for (int fg = 0; fg < 2; fg++)
 #pragma unroll
-      for (int b = 0; b < 4; b++) re[a][b] = im[a][b] = 0.0;
-    for (int sidx = 0; sidx < nsamp; sidx++) {
-      const double2 x01 = *reinterpret_cast<const double2*>(&xs[sidx][rg * 4]);
-      const double2 x23 = *reinterpret_cast<const double2*>(&xs[sidx][rg * 4 + 2]);
-      const double xv[4] = {x01.x, x01.y, x23.x, x23.y};
+      for (int c = 0; c < 2; c++)
 #pragma unroll
-      for (int b = 0; b < 4; b++) {
-        const double2 w = ws[sidx][fg * 4 + b];
+        for (int n = 0; n < 4; n++) acc[fg][c][n][0] = acc[fg][c][n][1] = 0.0;
+#pragma unroll 2
+    for (int s0 = 0; s0 < nk; s0 += 4) {
+      const double2 w0 = __ldg(tw0 + (size_t)(s0 + q4) * d.nf), w1 = __ldg(tw1 + (size_t)(s0 + q4) * d.nf);
+      double b[4];
 #pragma unroll
-        for (int a = 0; a < 4; a++) {
-          re[a][b] = fma(xv[a], w.x, re[a][b]);
-          im[a][b] = fma(xv[a], w.y, im[a][b]);
-        }
+      for (int n = 0; n < 4; n++) b[n] = (double)xs[s0 + q4][rw + 8 * n + g];
+#pragma unroll
+      for (int n = 0; n < 4; n++) {
+        dmma_8x8x4(acc[0][0][n][0], acc[0][0][n][1], w0.x, b[n]);
+        dmma_8x8x4(acc[0][1][n][0], acc[0][1][n][1], w0.y, b[n]);
+        dmma_8x8x4(acc[1][0][n][0], acc[1][0][n][1], w1.x, b[n]);
+        dmma_8x8x4(acc[1][1][n][0], acc[1][1][n][1], w1.y, b[n]);
       }
     }
     asm volatile("cp.async.wait_all;\n" ::);
     __syncthreads();  // every thread's copies have landed
 #pragma unroll
-    for (int b = 0; b < 4; b++) {
-      const int fl = fg * 4 + b, f = f0 + fl;
+    for (int fg = 0; fg < 2; fg++) {
+      const int fl = fg * 8 + g, f = f0 + fl;
       if (f >= d.nf) continue;
-      double* pr = d.acc_re + (size_t)f * d.rows + r0 + rg * 4;
-      double* pi = d.acc_im + (size_t)f * d.rows + r0 + rg * 4;
-      const double2 r01 = *reinterpret_cast<const double2*>(&ar[fl][rg * 4]);
-      const double2 r23 = *reinterpret_cast<const double2*>(&ar[fl][rg * 4 + 2]);
-      const double2 i01 = *reinterpret_cast<const double2*>(&ai[fl][rg * 4]);
-      const double2 i23 = *reinterpret_cast<const double2*>(&ai[fl][rg * 4 + 2]);
-      *reinterpret_cast<double2*>(pr) = make_double2(r01.x + re[0][b], r01.y + re[1][b]);
-      *reinterpret_cast<double2*>(pr + 2) = make_double2(r23.x + re[2][b], r23.y + re[3][b]);
-      *reinterpret_cast<double2*>(pi) = make_double2(i01.x + im[0][b], i01.y + im[1][b]);
-      *reinterpret_cast<double2*>(pi + 2) = make_double2(i23.x + im[2][b], i23.y + im[3][b]);
+#pragma unroll
+      for (int n = 0; n < 4; n++) {
+        const int rl = rw + 8 * n + 2 * q4;
+        const double2 pr = *reinterpret_cast<const double2*>(&ar[fl][rl]);
+        const double2 pi = *reinterpret_cast<const double2*>(&ai[fl][rl]);
+        const size_t o = (size_t)f * d.rows + r0 + rl;
+        *reinterpret_cast<double2*>(d.acc_re + o) = make_double2(pr.x + acc[fg][0][n][0], pr.y + acc[fg][0][n][1]);
+        *reinterpret_cast<double2*>(d.acc_im + o) = make_double2(pi.x + acc[fg][1][n][0], pi.y + acc[fg][1][n][1]);
+      }
     }
   }
 }
 template <typename T>
 __global__ void __launch_bounds__(128) dft_contract(const __grid_constant__ DftView d, const T* ring,
-                                                     const DevClock* clk, const double2* tw) {
-  dft_contract_body(d, ring, clk, tw);
+                                                     const DevClock* clk, const double2* tw, int force) {
+  dft_contract_body(d, ring, clk, tw, force);
 }
 
-__global__ void dft_reset_count(DevClock* clk) { clk->nsamp = 0; }
+// empties the ring after a contraction (the same condition as the
+// contraction kernels, which ran before it on the stream)
+__global__ void dft_reset_count(DevClock* clk, int force) {
+  if (dft_ring_ready(clk, force)) clk->nsamp = 0;
+}
 
 // Per (box-face, frequency): sum over the face of Re(cEx conj(HY) -
 // cEy conj(HX)) with the reference's component pairing

@@ -65,6 +65,24 @@ def test_batch_launches_do_not_grow_with_members():
     four.close()
 
 
+def test_batch_member_spectra_read_mid_run():
+    """Reading one member's spectra empties its sample ring only; the batch's
+    contraction launches then find the members' rings at different fill
+    levels, and each member contracts before its ring could overflow."""
+    params = [make(F, "sphere_au", precision=F.FDTD_FP64) for _ in range(2)]
+    b = F.Batch(params)
+    b.step(150)
+    b.spectra(0)
+    b.step(270)
+    alone = F.Sim(params[0])
+    alone.step(420)
+    ref = alone.spectra()
+    for i in (0, 1):
+        assert rel(b.spectra(i)[:, 1:4], ref[:, 1:4]) < 1e-12, i
+    alone.close()
+    b.close()
+
+
 def test_batch_hydro_members():
     params = [make(F, "hydro", precision=F.FDTD_FP64),
               make(F, "hydro", precision=F.FDTD_FP64, NCELLX=25, nano_sphere_radius=8e-9)]
