@@ -8,9 +8,8 @@
 // the whole batch is
 //   h_pass_batch      two persistent grids: the CPML-free tiles of all
 //                     members from one queue, the CPML edge tiles from another
-//   tfsf_h_apply      one launch, blockIdx.y = member
-//   line_step         one launch, one CTA per member
-//   tfsf_e_apply      one launch
+//   line_step         one launch, one CTA per member (double-buffered line E)
+//   tfsf_apply        both TFSF halves, one launch, blockIdx.y = member
 //   (hydrodynamic members: their three dispersive kernels, per member)
 //   e_pass_batch      two persistent grids as for H
 //   metal_e           one launch
@@ -40,14 +39,9 @@ struct BatchSim {
 };
 
 template <typename T>
-__global__ void tfsf_h_apply_batch(const BatchSim<T>* __restrict__ b) {
+__global__ void tfsf_apply_batch(const BatchSim<T>* __restrict__ b) {
   const BatchSim<T>& x = b[blockIdx.y];
-  tfsf_h_apply_body(x.v, x.tf_h);
-}
-template <typename T>
-__global__ void tfsf_e_apply_batch(const BatchSim<T>* __restrict__ b) {
-  const BatchSim<T>& x = b[blockIdx.y];
-  tfsf_e_apply_body(x.v, x.tf_e);
+  tfsf_apply_body(x.v, x.tf_h, x.tf_e, x.line);
 }
 template <typename T>
 __global__ void __launch_bounds__(1024) line_step_batch(const BatchSim<T>* __restrict__ b) {
@@ -98,7 +92,7 @@ struct fdtd_batch {
   int4* items = nullptr;  // (member, bx, by, bz)
   int* queue = nullptr;   // [4] work counters: H edge, H interior, E edge, E interior
   int nedge = 0, ninner = 0, grid_pass = 0, grid_inner = 0;
-  unsigned g_fh = 0, g_fe = 0, g_m = 0, g_s = 0, g_tw = 0, g_c = 0;
+  unsigned g_f = 0, g_m = 0, g_s = 0, g_tw = 0, g_c = 0;
   int t = 0, host_nsamp = 0, dft_every = 0, tend = 0;
   long long kernels = 0, graph_launches = 0, graph_kernels = 0;
   cudaGraphExec_t graph = nullptr;
@@ -159,8 +153,7 @@ static fdtd_status batch_build(fdtd_batch* b) {
           (in ? inner : items).push_back(make_int4(i, bx, by, bz));
         }
     auto blocks = [](long long cells, int per) { return (unsigned)((cells + per - 1) / per); };
-    b->g_fh = std::max(b->g_fh, blocks(s->tf_h.n, 256));
-    b->g_fe = std::max(b->g_fe, blocks(s->tf_e.n, 256));
+    b->g_f = std::max(b->g_f, blocks((long long)s->tf_h.n + s->tf_e.n, 256));
     b->g_m = std::max(b->g_m, blocks((long long)s->nmetal[0] + s->nmetal[1] + s->nmetal[2], 128));
     int maxn = 0;
     for (int f = 0; f < 12; f++) maxn = std::max(maxn, s->dft.face[f].na * s->dft.face[f].nb);
@@ -224,10 +217,11 @@ static void batch_enqueue_step(fdtd_batch* b, cudaStream_t st) {
                                                                                        b->queue, kBatchKChunk);
     k++;
   }
-  if (b->g_fh) { tfsf_h_apply_batch<T><<<dim3(b->g_fh, n), 256, 0, st>>>(d); k++; }
+  // the line step writes the line's other E buffer, so the fused TFSF launch
+  // after it still applies the H half with the line's E from before it
   line_step_batch<T><<<dim3(1, n), 1024, 0, st>>>(d);
   k++;
-  if (b->g_fe) { tfsf_e_apply_batch<T><<<dim3(b->g_fe, n), 256, 0, st>>>(d); k++; }
+  if (b->g_f) { tfsf_apply_batch<T><<<dim3(b->g_f, n), 256, 0, st>>>(d); k++; }
   if (b->hydro)
     for (auto& s : b->sims) {
       const long long k0 = s->kernels;

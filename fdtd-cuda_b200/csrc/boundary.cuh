@@ -117,24 +117,23 @@ __device__ __forceinline__ T tfsf_term(const double* line, const float* dir, int
   return v;
 }
 
+// Entry g of the H table: e_line is the incident line's E from before this
+// step's line update.
 template <typename T>
-__device__ __forceinline__ void tfsf_h_apply_body(const SimView<T>& s, const TfsfTable& tb) {
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= tb.n) return;
+__device__ __forceinline__ void tfsf_h_entry(const SimView<T>& s, const TfsfTable& tb, int g, const double* e_line) {
   const unsigned id = tb.id[g];
   const unsigned cn = tb.cn[g];
   const int c = cn & 3, nt = cn >> 2;
   const T dd[3] = {s.dxyz[0], s.dxyz[1], s.dxyz[2]};
   T v = s.H[c][id];
-  v = tfsf_term(s.e_inc, s.tf.fe, tb.idx[0][g], tb.dp[0][g], tb.meta[0][g], v, s.che, dd);
-  if (nt > 1) v = tfsf_term(s.e_inc, s.tf.fe, tb.idx[1][g], tb.dp[1][g], tb.meta[1][g], v, s.che, dd);
+  v = tfsf_term(e_line, s.tf.fe, tb.idx[0][g], tb.dp[0][g], tb.meta[0][g], v, s.che, dd);
+  if (nt > 1) v = tfsf_term(e_line, s.tf.fe, tb.idx[1][g], tb.dp[1][g], tb.meta[1][g], v, s.che, dd);
   s.H[c][id] = v;
 }
 
+// Entry g of the E table (the line's H after this step's line update).
 template <typename T>
-__device__ __forceinline__ void tfsf_e_apply_body(const SimView<T>& s, const TfsfTable& tb) {
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= tb.n) return;
+__device__ __forceinline__ void tfsf_e_entry(const SimView<T>& s, const TfsfTable& tb, int g) {
   const unsigned id = tb.id[g];
   const unsigned cn = tb.cn[g];
   const int c = cn & 3, nt = cn >> 2;
@@ -154,13 +153,41 @@ __device__ __forceinline__ void tfsf_e_apply_body(const SimView<T>& s, const Tfs
   s.E[c][id] = v;
 }
 
+// The halves as separate launches (the split per-half entry points) and
+// fused: the H entries write H face cells from the line's E, the E entries
+// write E face cells from the line's H, so one launch can run both once
+// the line step is done.  Thread g < th.n takes H entry g, the rest the E
+// entries.
 template <typename T>
-__global__ void tfsf_h_apply(const __grid_constant__ SimView<T> s, const __grid_constant__ TfsfTable tb) {
-  tfsf_h_apply_body(s, tb);
+__device__ __forceinline__ void tfsf_h_apply_body(const SimView<T>& s, const TfsfTable& tb, const LineArgs& line) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g < tb.n) tfsf_h_entry(s, tb, g, line_e_before(line, 0));
+}
+template <typename T>
+__device__ __forceinline__ void tfsf_e_apply_body(const SimView<T>& s, const TfsfTable& tb) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g < tb.n) tfsf_e_entry(s, tb, g);
+}
+template <typename T>
+__device__ __forceinline__ void tfsf_apply_body(const SimView<T>& s, const TfsfTable& th, const TfsfTable& te,
+                                                const LineArgs& line) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g < th.n) tfsf_h_entry(s, th, g, line_e_before(line, 1));
+  else if (g - th.n < te.n) tfsf_e_entry(s, te, g - th.n);
+}
+template <typename T>
+__global__ void tfsf_h_apply(const __grid_constant__ SimView<T> s, const __grid_constant__ TfsfTable tb,
+                             const __grid_constant__ LineArgs line) {
+  tfsf_h_apply_body(s, tb, line);
 }
 template <typename T>
 __global__ void tfsf_e_apply(const __grid_constant__ SimView<T> s, const __grid_constant__ TfsfTable tb) {
   tfsf_e_apply_body(s, tb);
+}
+template <typename T>
+__global__ void tfsf_apply(const __grid_constant__ SimView<T> s, const __grid_constant__ TfsfTable th,
+                           const __grid_constant__ TfsfTable te, const __grid_constant__ LineArgs line) {
+  tfsf_apply_body(s, th, te, line);
 }
 
 }  // namespace fdtd

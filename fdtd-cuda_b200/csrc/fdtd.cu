@@ -148,6 +148,7 @@ struct fdtd_sim {
   // (they touch only dispersive components, which the pass skips)
   cudaStream_t side2 = nullptr;
   cudaEvent_t fork2_ev = nullptr, join2_ev = nullptr;
+  cudaEvent_t fork3_ev = nullptr, join3_ev = nullptr;  // the line step beside the H pass
 
   void destroy_streams() {
     if (graph) cudaGraphExecDestroy(graph);
@@ -158,6 +159,8 @@ struct fdtd_sim {
     if (side2) cudaStreamDestroy(side2);
     if (fork2_ev) cudaEventDestroy(fork2_ev);
     if (join2_ev) cudaEventDestroy(join2_ev);
+    if (fork3_ev) cudaEventDestroy(fork3_ev);
+    if (join3_ev) cudaEventDestroy(join3_ev);
   }
 
   // buffers that fdtd_reset zeroes (fields, psi, dispersive state, DFT,
@@ -366,7 +369,6 @@ static fdtd_status build_views(fdtd_sim* s) {
   tf.sth = su.sth; tf.cth = su.cth; tf.sph = su.sph; tf.cph = su.cph;
   for (int c = 0; c < 3; c++) { tf.fe[c] = su.fe[c]; tf.fh[c] = su.fh[c]; }
   tf.dscale = su.p.dx / su.d1D;
-  v.e_inc = s->e_inc;
   v.h_inc = s->h_inc;
   v.nonfinite = &s->clk->nonfinite;
   // dispersive cells
@@ -514,7 +516,7 @@ static fdtd_status create_impl(const fdtd_params* p, int device, fdtd_sim** out,
     s->H[c] = b;
   }
   CUDA_TRY(s->alloc(&s->clk, 1, true));
-  CUDA_TRY(s->alloc(&s->e_inc, su.L, true));
+  CUDA_TRY(s->alloc(&s->e_inc, 2 * (size_t)su.L, true));  // two buffers, by step parity
   CUDA_TRY(s->alloc(&s->h_inc, su.L, true));
   CUDA_TRY(s->alloc(&s->pulse, su.pulse.size()));
   CUDA_TRY(cudaMemcpy(s->pulse, su.pulse.data(), su.pulse.size() * sizeof(double), cudaMemcpyHostToDevice));
@@ -708,6 +710,8 @@ static fdtd_status create_impl(const fdtd_params* p, int device, fdtd_sim** out,
   CUDA_TRY(cudaStreamCreateWithFlags(&s->side2, cudaStreamNonBlocking));
   CUDA_TRY(cudaEventCreateWithFlags(&s->fork2_ev, cudaEventDisableTiming));
   CUDA_TRY(cudaEventCreateWithFlags(&s->join2_ev, cudaEventDisableTiming));
+  CUDA_TRY(cudaEventCreateWithFlags(&s->fork3_ev, cudaEventDisableTiming));
+  CUDA_TRY(cudaEventCreateWithFlags(&s->join3_ev, cudaEventDisableTiming));
   CUDA_TRY(cudaEventCreateWithFlags(&s->fork_ev, cudaEventDisableTiming));
   CUDA_TRY(cudaEventCreateWithFlags(&s->join_ev, cudaEventDisableTiming));
   CUDA_TRY(cudaDeviceSynchronize());
@@ -1011,12 +1015,16 @@ static fdtd_status tune_passes(fdtd_sim* s, bool time_variants) {
   return FDTD_OK;
 }
 
+// The split per-half entry points (fdtd_update_h / _line / _e) launch the
+// H pass + the H half of CORRECT_*, the line, then the E half + the E pass.
 template <typename T>
 static void launch_h(fdtd_sim* s, cudaStream_t st) {
-  s->kernels += launch_h_cfg<T>(s, s->hcfg, st) - 1;
+  s->kernels += launch_h_cfg<T>(s, s->hcfg, st);
   const int nf = s->tf_h.n;
-  if (nf > 0) tfsf_h_apply<T><<<(unsigned)((nf + 255) / 256), 256, 0, st>>>(view<T>(s), s->tf_h);
-  s->kernels += 1 + (nf > 0);
+  if (nf > 0) {
+    tfsf_h_apply<T><<<(unsigned)((nf + 255) / 256), 256, 0, st>>>(view<T>(s), s->tf_h, s->line);
+    s->kernels++;
+  }
 }
 template <typename T>
 static void launch_line(fdtd_sim* s, cudaStream_t st) {
@@ -1025,12 +1033,32 @@ static void launch_line(fdtd_sim* s, cudaStream_t st) {
 }
 template <typename T>
 static void launch_metal(fdtd_sim* s, cudaStream_t st);
+template <typename T>
+static void launch_e_pass(fdtd_sim* s, cudaStream_t st);
 
 template <typename T>
 static void launch_e(fdtd_sim* s, cudaStream_t st) {
   const int nf = s->tf_e.n;
   // E half of CORRECT_* before the update (main.cu:2798-2813)
-  if (nf > 0) tfsf_e_apply<T><<<(unsigned)((nf + 255) / 256), 256, 0, st>>>(view<T>(s), s->tf_e);
+  if (nf > 0) {
+    tfsf_e_apply<T><<<(unsigned)((nf + 255) / 256), 256, 0, st>>>(view<T>(s), s->tf_e);
+    s->kernels++;
+  }
+  launch_e_pass<T>(s, st);
+}
+
+// The fused step's TFSF: both halves in one launch, after the line step.
+template <typename T>
+static void launch_tfsf(fdtd_sim* s, cudaStream_t st) {
+  const int nf = s->tf_h.n + s->tf_e.n;
+  if (nf > 0) {
+    tfsf_apply<T><<<(unsigned)((nf + 255) / 256), 256, 0, st>>>(view<T>(s), s->tf_h, s->tf_e, s->line);
+    s->kernels++;
+  }
+}
+
+template <typename T>
+static void launch_e_pass(fdtd_sim* s, cudaStream_t st) {
   // The dispersive components (Drude + 2CP, hydrodynamic current) run on a
   // second stream beside the E pass: the pass skips them, reads no
   // dispersive E component and writes none, and the dispersive kernels read
@@ -1041,12 +1069,11 @@ static void launch_e(fdtd_sim* s, cudaStream_t st) {
     cudaStreamWaitEvent(s->side2, s->fork2_ev, 0);
     launch_metal<T>(s, s->side2);
   }
-  s->kernels += launch_e_cfg<T>(s, s->ecfg, st) - 1;
+  s->kernels += launch_e_cfg<T>(s, s->ecfg, st);
   if (metal) {
     cudaEventRecord(s->join2_ev, s->side2);
     cudaStreamWaitEvent(st, s->join2_ev, 0);
   }
-  s->kernels += 1 + (nf > 0);
 }
 
 template <typename T>
@@ -1099,13 +1126,24 @@ static void sample_and_contract(fdtd_sim* s, cudaStream_t st) {
   }
 }
 
-// One full step in the reference's order.  Host mirrors of the clock
-// decide which optional kernels run; the kernels read t from the device.
+// One full step.  The 1-D line step runs on the second side stream beside
+// the H pass: it reads the line, E at the probe cell and the clock, none of
+// which the H pass touches, and writes the line's other E buffer, so the H
+// half of CORRECT_* still sees the line's E from before the update, as in
+// the reference's order (UPDATE_h*, CORRECT_* H, UPDATE_h_inc/e_inc,
+// CORRECT_* E, UPDATE_e*).  Both TFSF halves then run as one launch.  Host
+// mirrors of the clock decide which optional kernels run; the kernels read
+// t from the device.
 template <typename T>
 static void enqueue_step(fdtd_sim* s, cudaStream_t st) {
-  launch_h<T>(s, st);
-  launch_line<T>(s, st);
-  launch_e<T>(s, st);
+  cudaEventRecord(s->fork3_ev, st);
+  cudaStreamWaitEvent(s->side2, s->fork3_ev, 0);
+  launch_line<T>(s, s->side2);
+  s->kernels += launch_h_cfg<T>(s, s->hcfg, st);
+  cudaEventRecord(s->join3_ev, s->side2);
+  cudaStreamWaitEvent(st, s->join3_ev, 0);
+  launch_tfsf<T>(s, st);
+  launch_e_pass<T>(s, st);
   if (s->line.dft_every > 0 && s->t % s->line.dft_every == 0) sample_and_contract<T>(s, st);
   s->t++;
 }

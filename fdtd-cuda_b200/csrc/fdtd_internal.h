@@ -70,8 +70,8 @@ struct SimView {
   T* psiH_N[3][2]; T* psiH_F[3][2];
   T dxyz[3];
   TfsfView tf;
-  const double* e_inc;  // incident line (double in both precisions)
-  const double* h_inc;
+  const double* h_inc;  // incident line H (double in both precisions); the
+                        // line's E is double-buffered and passed per launch
   int* nonfinite;
   const SimView* self;  // a copy of this view in device memory (cold paths)
 };

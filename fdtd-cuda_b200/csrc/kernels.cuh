@@ -67,20 +67,6 @@ __device__ __forceinline__ double tf_proj(const TfsfView& tf, int hx2, int hy2, 
   return __dmul_rn(tf.dscale, d);
 }
 
-// Linear interpolation of the incident line at projected distance d
-// (truncation toward zero as the reference's (int) casts).
-__device__ __forceinline__ double einc_at(const double* e, int m0, double d) {
-  int n = (int)d;
-  double dp = d - n;
-  return (1 - dp) * e[m0 + n] + dp * e[m0 + n + 1];
-}
-__device__ __forceinline__ double hinc_at(const double* h, int m0, double d) {
-  double d2 = d + 0.5;
-  int n = (int)d2;
-  double dp = d2 - n;
-  return (1 - dp) * h[m0 - 1 + n] + dp * h[m0 + n];
-}
-
 // The H half of CORRECT_X/Y/Z for H component c at (i,j,k), in the
 // reference's kernel order X, Y, Z: fn(sign, axis, e_component, d) per
 // correction, d the projected distance on the incident line.  tfsf_tabulate
@@ -275,9 +261,15 @@ __device__ __forceinline__ void flag_nonfinite(const SimView<T>& s, T v) {
 // the Mur ends and the soft source that the reference applies on the host
 // (main.cu:2831-2859).  One CTA.  Advances the device clock and records the
 // probe (E after the previous step).
+//
+// The line's E is double-buffered: step t reads buffer t & 1 and writes
+// the other, so the H half of the TFSF correction (which needs the line's
+// E from before the update) can run after the line step, and the line step
+// can run beside the H pass.  The parity comes from the device clock, so
+// captured graphs replay correctly from either parity.
 
 struct LineArgs {
-  double* e_inc;
+  double* e_inc;        // [2][L]: the line's E, buffer t & 1 current at step t
   double* h_inc;
   int L, m0, src;
   double ch, ce, mur;
@@ -289,22 +281,36 @@ struct LineArgs {
   int dft_every;        // 0 = no DFT sampling
 };
 
+// E buffer of the line current at step parity `par` (the other one receives
+// the update)
+__device__ __forceinline__ double* line_e(const LineArgs& a, int par) {
+  return a.e_inc + (size_t)(par & 1) * a.L;
+}
+// The line's E from before the update of the current step, for a kernel
+// that runs before the line step of the step (after_line = 0: the clock
+// still holds the step) or after it (after_line = 1: the clock holds the
+// step + 1).
+__device__ __forceinline__ const double* line_e_before(const LineArgs& a, int after_line) {
+  return line_e(a, a.clk->t - after_line);
+}
+
 template <typename T>
 __device__ __forceinline__ void line_step_body(const LineArgs& a, const SimView<T>& s, size_t probe_id) {
   const int t = a.clk->t;
+  const double* ec = line_e(a, t);
+  double* e = line_e(a, t + 1);
   // probe: E after step t-1 (OUT.txt records it at the top of step t)
   if (threadIdx.x < 3 && t >= 1 && t - 1 < a.probe_cap)
     a.probe[3 * (size_t)(t - 1) + threadIdx.x] = (double)s.E[threadIdx.x][probe_id];
   for (int q = threadIdx.x; q < a.L - 1; q += blockDim.x)
-    a.h_inc[q] = a.h_inc[q] - a.ch * (a.e_inc[q + 1] - a.e_inc[q]);
+    a.h_inc[q] = a.h_inc[q] - a.ch * (ec[q + 1] - ec[q]);
   __syncthreads();
   for (int q = threadIdx.x + 1; q < a.L - 1; q += blockDim.x)
-    a.e_inc[q] = a.e_inc[q] - a.ce * (a.h_inc[q] - a.h_inc[q - 1]);
+    e[q] = ec[q] - a.ce * (a.h_inc[q] - a.h_inc[q - 1]);
   __syncthreads();
   if (threadIdx.x == 0) {
-    double* e = a.e_inc;
-    e[0] = a.clk->e1 + a.mur * (e[1] - e[0]);
-    e[a.L - 1] = a.clk->e2 + a.mur * (e[a.L - 2] - e[a.L - 1]);
+    e[0] = a.clk->e1 + a.mur * (e[1] - ec[0]);
+    e[a.L - 1] = a.clk->e2 + a.mur * (e[a.L - 2] - ec[a.L - 1]);
     a.clk->e1 = e[1];
     a.clk->e2 = e[a.L - 2];
     if (t < a.tmax) e[a.src] += a.pulse[t];
@@ -324,7 +330,8 @@ __device__ __forceinline__ void line_step_body(const LineArgs& a, const SimView<
   }
 }
 template <typename T>
-__global__ void __launch_bounds__(1024) line_step(const __grid_constant__ LineArgs a, const __grid_constant__ SimView<T> s, size_t probe_id) {
+__global__ void __launch_bounds__(1024) line_step(const __grid_constant__ LineArgs a, const __grid_constant__ SimView<T> s,
+                                                  size_t probe_id) {
   line_step_body(a, s, probe_id);
 }
 
@@ -718,9 +725,9 @@ __device__ __forceinline__ void dft_cp_async16(void* dst, const void* src) {
 // D = A B + D for one m8n8k4 FP64 fragment: a = A[lane/4][lane%4],
 // b = B[lane%4][lane/4], d = D[lane/4][2 (lane%4) + {0, 1}].
 __device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
-               : "+d"(d0), "+d"(d1)
-               : "d"(a), "d"(b));
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+      : "+d"(d0), "+d"(d1)
+      : "d"(a), "d"(b));
 }
 
 template <typename T>
