@@ -162,11 +162,23 @@ extern "C" fdtd_status fdtd_forward(fdtd_sim* s, const int* freq_idx, int nfreq,
     if (sphere) w[m] *= -1.0 / (su.pi * su.p.nano_sphere_radius * su.p.nano_sphere_radius);
     fs[m] = su.freq[A.sel[m]];
   }
-  auto Pb = std::make_unique<DevBuf>();
-  CUDA_TRY(Pb->alloc((size_t)nfreq * s->dft.rows * sizeof(double2)));
-  auto Fb = std::make_unique<DevBuf>();
-  CUDA_TRY(Fb->alloc((size_t)nfreq * (2 * sizeof(double) + sizeof(int))));
-  double* dw = static_cast<double*>(Fb->p);
+  // partner accumulators and the frequency list, kept across forwards (an
+  // allocation per forward would synchronise the device)
+  const size_t pbytes = (size_t)nfreq * s->dft.rows * sizeof(double2);
+  const size_t fbytes = (size_t)nfreq * (2 * sizeof(double) + sizeof(int));
+  if (!A.P || A.P->bytes < pbytes) {
+    A.P.reset();
+    auto b = std::make_unique<DevBuf>();
+    CUDA_TRY(b->alloc(pbytes));
+    A.P = std::move(b);
+  }
+  if (!A.fsel || A.fsel->bytes < fbytes) {
+    A.fsel.reset();
+    auto b = std::make_unique<DevBuf>();
+    CUDA_TRY(b->alloc(fbytes));
+    A.fsel = std::move(b);
+  }
+  double* dw = static_cast<double*>(A.fsel->p);
   double* dfs = dw + nfreq;
   int* dsel = reinterpret_cast<int*>(dfs + nfreq);
   CUDA_TRY(cudaMemcpy(dw, w.data(), nfreq * sizeof(double), cudaMemcpyHostToDevice));
@@ -174,12 +186,10 @@ extern "C" fdtd_status fdtd_forward(fdtd_sim* s, const int* freq_idx, int nfreq,
   CUDA_TRY(cudaMemcpy(dsel, A.sel.data(), nfreq * sizeof(int), cudaMemcpyHostToDevice));
   int maxn = 0;
   for (int f = 0; f < 6; f++) maxn = std::max(maxn, s->dft.face[f].na * s->dft.face[f].nb);
-  adj_partner<<<dim3((maxn + 255) / 256, 6, nfreq), 256>>>(s->dft, dsel, dw, nfreq, static_cast<double2*>(Pb->p),
+  adj_partner<<<dim3((maxn + 255) / 256, 6, nfreq), 256>>>(s->dft, dsel, dw, nfreq, static_cast<double2*>(A.P->p),
                                                           s->dft.rows);
   CUDA_TRY(cudaGetLastError());
   CUDA_TRY(cudaDeviceSynchronize());
-  A.P = std::move(Pb);
-  A.fsel = std::move(Fb);
   A.forward_done = true;
   return FDTD_OK;
 }

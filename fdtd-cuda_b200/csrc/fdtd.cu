@@ -72,7 +72,9 @@ struct fdtd_sim {
   // launch shape of one pass: tile height and z-chunk shared by its two
   // launches, register cap (min CTAs/SM) and ring depth per launch
   // (interior tiles: minb/stages, CPML edge tiles: eminb/estages)
-  struct PassCfg { int minb = 1, ty = 4, kchunk = 16, staged = 1, stages = 4, eminb = 1, estages = 4; float ms = 0; };
+  // pdl = 1: the edge and interior launches of a pass go on one stream
+  // with a programmatic dependency instead of on two streams
+  struct PassCfg { int minb = 1, ty = 4, kchunk = 16, staged = 1, stages = 4, eminb = 1, estages = 4, pdl = 0; float ms = 0; };
   // pass tiles for one (tile height, z-chunk): the interior box of tiles
   // that touch no CPML slab and the table of the others
   struct TileSet {
@@ -845,13 +847,25 @@ static const fdtd_sim::TileSet& tiles(const fdtd_sim* s, const fdtd_sim::PassCfg
   return s->tilesets.front();  // unreachable: every configuration is built at create
 }
 
-// One launch of a pass variant over a tile map (box grid or table).
+// One launch of a pass variant over a tile map (box grid or table); pdl =
+// true gives it a programmatic dependency on the launch before it on the
+// stream.
 template <typename T, bool PML>
 static void launch_h_variant(fdtd_sim* s, int ty, int mb, int sg, dim3 g, const TileMap& tm, int kchunk,
-                             cudaStream_t st) {
+                             cudaStream_t st, bool pdl = false) {
 #define FDTD_LAUNCH(TY, MB, S)                                                                   \
   if (ty == TY && mb == MB && sg == S) {                                                         \
-    h_pass_s<T, TY, S, MB, PML><<<g, dim3(32, TY), staged_smem<T, TY, S>(), st>>>(view<T>(s), kchunk, tm); \
+    if (pdl) {                                                                                   \
+      cudaLaunchConfig_t cfg = {};                                                               \
+      cfg.gridDim = g; cfg.blockDim = dim3(32, TY); cfg.dynamicSmemBytes = staged_smem<T, TY, S>(); cfg.stream = st; \
+      cudaLaunchAttribute at[1];                                                                 \
+      at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;                             \
+      at[0].val.programmaticStreamSerializationAllowed = 1;                                      \
+      cfg.attrs = at; cfg.numAttrs = 1;                                                          \
+      cudaLaunchKernelEx(&cfg, h_pass_s<T, TY, S, MB, PML>, view<T>(s), kchunk, tm);             \
+    } else {                                                                                     \
+      h_pass_s<T, TY, S, MB, PML><<<g, dim3(32, TY), staged_smem<T, TY, S>(), st>>>(view<T>(s), kchunk, tm); \
+    }                                                                                            \
     return;                                                                                      \
   }
   FDTD_STAGED_VARIANTS(FDTD_LAUNCH)
@@ -859,22 +873,43 @@ static void launch_h_variant(fdtd_sim* s, int ty, int mb, int sg, dim3 g, const 
 }
 template <typename T, bool PML>
 static void launch_e_variant(fdtd_sim* s, int ty, int mb, int sg, dim3 g, const TileMap& tm, int kchunk,
-                             cudaStream_t st) {
+                             cudaStream_t st, bool pdl = false) {
 #define FDTD_LAUNCH(TY, MB, S)                                                                   \
   if (ty == TY && mb == MB && sg == S) {                                                         \
-    e_pass_s<T, TY, S, MB, PML><<<g, dim3(32, TY), staged_smem<T, TY, S>(), st>>>(view<T>(s), kchunk, tm); \
+    if (pdl) {                                                                                   \
+      cudaLaunchConfig_t cfg = {};                                                               \
+      cfg.gridDim = g; cfg.blockDim = dim3(32, TY); cfg.dynamicSmemBytes = staged_smem<T, TY, S>(); cfg.stream = st; \
+      cudaLaunchAttribute at[1];                                                                 \
+      at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;                             \
+      at[0].val.programmaticStreamSerializationAllowed = 1;                                      \
+      cfg.attrs = at; cfg.numAttrs = 1;                                                          \
+      cudaLaunchKernelEx(&cfg, e_pass_s<T, TY, S, MB, PML>, view<T>(s), kchunk, tm);             \
+    } else {                                                                                     \
+      e_pass_s<T, TY, S, MB, PML><<<g, dim3(32, TY), staged_smem<T, TY, S>(), st>>>(view<T>(s), kchunk, tm); \
+    }                                                                                            \
     return;                                                                                      \
   }
   FDTD_STAGED_VARIANTS(FDTD_LAUNCH)
 #undef FDTD_LAUNCH
 }
 
-// Launches one pass as its interior box (PML-free) and its edge table, the
-// edge launch on the side stream so that the two overlap; returns the
-// number of launches.
+// Launches one pass as its interior box (PML-free) and its edge table so
+// that the two overlap: the edge launch on the side stream, or (c.pdl) the
+// edge launch then the interior launch with a programmatic dependency on
+// one stream; returns the number of launches.
 template <typename T, bool EPASS>
 static int launch_pass_cfg(fdtd_sim* s, const fdtd_sim::PassCfg& c, cudaStream_t st) {
   const fdtd_sim::TileSet& ts = tiles(s, c);
+  if (c.pdl && ts.inner.x && ts.nedge) {
+    if (EPASS) {
+      launch_e_variant<T, true>(s, c.ty, c.eminb, c.estages, dim3(ts.nedge), ts.edge_map, c.kchunk, st);
+      launch_e_variant<T, false>(s, c.ty, c.minb, c.stages, ts.inner, ts.inner_map, c.kchunk, st, true);
+    } else {
+      launch_h_variant<T, true>(s, c.ty, c.eminb, c.estages, dim3(ts.nedge), ts.edge_map, c.kchunk, st);
+      launch_h_variant<T, false>(s, c.ty, c.minb, c.stages, ts.inner, ts.inner_map, c.kchunk, st, true);
+    }
+    return 2;
+  }
   const bool fork = ts.inner.x && ts.nedge;
   cudaStream_t est = st;
   if (fork) {
@@ -934,6 +969,12 @@ static fdtd_status tune_passes(fdtd_sim* s, bool time_variants) {
   }
   def.eminb = def.minb;
   def.estages = def.stages;
+  // FDTD_PDL=0 / 1 fixes how the two launches of a pass overlap (two
+  // streams / one stream with a programmatic dependency) instead of timing
+  // both
+  const char* pdl_env = std::getenv("FDTD_PDL");
+  const int pdl_force = pdl_env && (pdl_env[0] == '0' || pdl_env[0] == '1') ? pdl_env[0] - '0' : -1;
+  if (pdl_force >= 0) def.pdl = pdl_force;
   s->hcfg = s->ecfg = def;
   {
     const fdtd_status st = build_tiles(s, def.ty, def.kchunk);
@@ -1007,6 +1048,33 @@ static fdtd_status tune_passes(fdtd_sim* s, bool time_variants) {
         }
       }
     (pass == 0 ? s->hcfg : s->ecfg) = best;
+    // the two launches together: on two streams, or on one stream with a
+    // programmatic dependency; the faster arrangement is kept
+    fdtd_sim::PassCfg& c = pass == 0 ? s->hcfg : s->ecfg;
+    if (pdl_force >= 0) {
+      c.pdl = pdl_force;
+      continue;
+    }
+    float both[2] = {0.f, 0.f};
+    for (int mode = 0; mode < 2; mode++) {
+      c.pdl = mode;
+      auto go = [&]() {
+        if (pass == 0) launch_pass_cfg<T, false>(s, c, 0);
+        else launch_pass_cfg<T, true>(s, c, 0);
+      };
+      go();
+      CUDA_TRY(cudaEventRecord(a));
+      for (int r = 0; r < 3; r++) go();
+      CUDA_TRY(cudaEventRecord(b));
+      CUDA_TRY(cudaEventSynchronize(b));
+      CUDA_TRY(cudaEventElapsedTime(&both[mode], a, b));
+      both[mode] /= 3;
+      if (verbose)
+        std::fprintf(stderr, "[fdtd tune] %s pass, %s: %.4f ms\n", pass == 0 ? "H" : "E",
+                     mode ? "one stream, programmatic dependency" : "two streams", both[mode]);
+    }
+    c.pdl = both[1] < both[0] ? 1 : 0;
+    c.ms = std::min(both[0], both[1]);
   }
   cudaEventDestroy(a);
   cudaEventDestroy(b);
@@ -1585,6 +1653,7 @@ extern "C" fdtd_status fdtd_get_stats(const fdtd_sim* s, fdtd_stats* out) {
   out->h_stages = s->hcfg.stages; out->e_stages = s->ecfg.stages;
   out->h_eminb = s->hcfg.eminb; out->h_estages = s->hcfg.estages;
   out->e_eminb = s->ecfg.eminb; out->e_estages = s->ecfg.estages;
+  out->h_pdl = s->hcfg.pdl; out->e_pdl = s->ecfg.pdl;
   return FDTD_OK;
 }
 

@@ -320,12 +320,24 @@ __device__ __forceinline__ void h_pass_tile(const SimView<T>& s, int kchunk, int
   }
   cp_async_wait<0>();
 }
+// Programmatic dependent launch of the two launches of a pass on one
+// stream (the CPML edge tiles, then the interior box): the first lets the
+// second start its CTAs as soon as all of its own are running, so the
+// second fills the first's tail, and the second waits, after its own work,
+// for the first to finish, so that its completion implies both.  The two
+// launches touch disjoint cells and read only the other field.  Both are
+// no-ops in a launch without a programmatic dependency.
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+
 template <typename T, int TY, int S, int MINB, bool PML>
 __global__ void __launch_bounds__(32 * TY, MINB) h_pass_s(const __grid_constant__ SimView<T> s, int kchunk,
                                                       const __grid_constant__ TileMap tm) {
+  pdl_launch_dependents();
   int bx, by, bz;
   tile_of(tm, bx, by, bz);
   h_pass_tile<T, TY, S, PML>(s, kchunk, bx, by, bz);
+  pdl_wait();
 }
 
 // Batched form: a persistent grid that takes (simulation, tile) work items
@@ -516,9 +528,11 @@ __device__ __forceinline__ void e_pass_tile(const SimView<T>& s, int kchunk, int
 template <typename T, int TY, int S, int MINB, bool PML>
 __global__ void __launch_bounds__(32 * TY, MINB) e_pass_s(const __grid_constant__ SimView<T> s, int kchunk,
                                                       const __grid_constant__ TileMap tm) {
+  pdl_launch_dependents();
   int bx, by, bz;
   tile_of(tm, bx, by, bz);
   e_pass_tile<T, TY, S, PML>(s, kchunk, bx, by, bz);
+  pdl_wait();
 }
 
 // Batched form: a persistent grid that takes (simulation, tile) work items

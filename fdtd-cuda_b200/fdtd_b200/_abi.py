@@ -103,4 +103,5 @@ class Stats(C.Structure):
                 ("h_staged", C.c_int), ("e_staged", C.c_int),
                 ("h_stages", C.c_int), ("e_stages", C.c_int),
                 ("h_eminb", C.c_int), ("h_estages", C.c_int),
-                ("e_eminb", C.c_int), ("e_estages", C.c_int)]
+                ("e_eminb", C.c_int), ("e_estages", C.c_int),
+                ("h_pdl", C.c_int), ("e_pdl", C.c_int)]

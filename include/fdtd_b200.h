@@ -325,6 +325,9 @@ typedef struct fdtd_stats {
   int h_stages, e_stages;  /* its ring depth */
   /* the same two for the launch over the CPML edge tiles */
   int h_eminb, h_estages, e_eminb, e_estages;
+  /* 1 = the two launches of the pass run on one stream with a programmatic
+   * dependency, 0 = on two streams */
+  int h_pdl, e_pdl;
 } fdtd_stats;
 fdtd_status fdtd_get_stats(const fdtd_sim* s, fdtd_stats* out);
 /* Measurement hook (no counterpart in the reference): runs one Yee pass

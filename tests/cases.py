@@ -28,6 +28,9 @@ CASES = {
     "fixes": dict(SMALL, fixes=7),
     "dimer": dict(SMALL, geometry=1, axis=0, rod_length=8e-9, rod_diameter=4e-9, gap=2e-9,
                   NCELLX=25, inc_phi_deg=90.0),
+    # 97 x 89 x 93 cells: large enough for the CPML-free interior box of pass
+    # tiles (the smaller cases have CPML edge tiles only)
+    "sphere_big": dict(SMALL, NCELLX=84, NCELLY=76, NCELLZ=80, nano_sphere_radius=12e-9),
     # 2x2 gold disks on a dielectric slab (eps 2.25)
     "disks_slab": dict(SMALL, geometry=2, disk_diameter=8e-9, disk_height=4e-9, pitch=12e-9,
                        disk_nx=2, disk_ny=2, slab_eps=2.25, slab_thickness=6e-9),
