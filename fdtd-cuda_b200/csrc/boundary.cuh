@@ -53,6 +53,9 @@ struct ShellCells {
 // TFSF corrections tabulated once at create: per face cell and component
 // with at least one correction, up to two (line index, weight, meta) terms
 // in the reference's order; meta = (sign > 0) | axis << 1 | component << 3.
+// A term whose polarisation factor is exactly zero (the incident field has
+// no such component, e.g. E_z and H_z of a wave along z) adds a signed zero
+// and is left out.
 // Applying a term adds sign * coefficient * (interpolated incident value)
 // * (polarisation factor) / d_axis, the arithmetic of the walk forms in
 // kernels.cuh with the projection and the truncation already done.
@@ -80,7 +83,9 @@ __global__ void tfsf_tabulate(const SimView<T>* __restrict__ gv, const ShellCell
     int ix[2] = {0, 0};
     double w[2] = {0, 0};
     unsigned char mm[2] = {0, 0};
+    const float* fac = efield ? g.tf.fh : g.tf.fe;
     auto rec = [&](int sg, int ax, int f, double d) {
+      if (fac[f] == 0.0f) return;
       if (nt < 2) {
         if (efield) {  // hinc_at
           const double d2 = d + 0.5;
