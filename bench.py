@@ -306,7 +306,59 @@ def large_bench(mod, torch, stream, sp, dev, blocks=2):
     out = {"value": round(cells * BLOCK * blocks / (ms / 1e3) / 1e9, 3), "unit": "Gcell-steps/s",
            "grid": [d.nx, d.ny, d.nz], "time_steps": BLOCK * blocks,
            "dispersive_cells": list(d.n_metal_cells), "device_bytes": int(free0 - free1),
-           "adjoint": "not built for the hydrodynamic model (nonlinear in the current and density)"}
+           "adjoint": "not built for the hydrodynamic model (nonlinear in the current and density); "
+                      "see adjoint_local for the same geometry with the local model"}
+    s.close()
+    out["adjoint_local"] = large_adjoint_bench(mod, torch, dev)
+    return out
+
+
+LARGE_DESIGN = [192 - 32, 192 + 32, 192 - 32, 192 + 32, 128, 138]  # 64 x 64 x 10 over the central disk
+LARGE_FREQS = [0, 1, 2, 3, 4]
+
+
+def large_adjoint_bench(mod, torch, dev, steps=2400, every=400):
+    """The adjoint at the large geometry with the local Drude+2CP model (the
+    hydrodynamic adjoint is not built): a 64 x 64 x 10 design region over
+    the central disk, rho ~ U[0, 1] from the seed, objective = AbsTot at the 5
+    wavelengths, checkpoints every 400 steps.  A bounded sample of the
+    12000-step run: `steps` steps; forward and backward throughput and the
+    device memory the checkpoints and adjoint state take."""
+    import numpy as np
+    p = large_params(mod)
+    p.NONLOCAL = 0
+    p.Tend = steps - 1
+    for a, v in enumerate(LARGE_DESIGN):
+        p.design_box[a] = v
+    b = LARGE_DESIGN
+    free0, _ = torch.cuda.mem_get_info(dev)
+    s = mod.Sim(p, device=dev)
+    rng = np.random.default_rng(BATCH_SEED)
+    s.set_design(rng.uniform(0, 1, (b[5] - b[4], b[3] - b[2], b[1] - b[0])))
+    free1, _ = torch.cuda.mem_get_info(dev)
+    s.forward(LARGE_FREQS, every)
+    free2, _ = torch.cuda.mem_get_info(dev)
+    s.backward()  # warm-up: buffers and the segment graphs
+    free3, _ = torch.cuda.mem_get_info(dev)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    L = s.forward(LARGE_FREQS, every)
+    t1 = time.perf_counter()
+    g, gp = s.backward()
+    t2 = time.perf_counter()
+    s.check()
+    d = s.dims
+    cs = d.nx * d.ny * d.nz * steps
+    out = {"grid": [d.nx, d.ny, d.nz], "design": [64, 64, 10], "time_steps": steps,
+           "full_run_steps": 12000, "checkpoint_every": every, "model": "local Drude+2CP",
+           "forward_s": round(t1 - t0, 3), "backward_s": round(t2 - t1, 3),
+           "ratio": round((t2 - t1) / (t1 - t0), 3),
+           "forward_gcell_steps_per_s": round(cs / (t1 - t0) / 1e9, 2),
+           "backward_gcell_steps_per_s": round(cs / (t2 - t1) / 1e9, 2),
+           "sim_bytes": int(free0 - free1), "checkpoint_bytes": int(free1 - free2),
+           "adjoint_state_bytes": int(free2 - free3),
+           "objective": L, "grad_rho_max": float(np.abs(g).max()),
+           "timing": "host wall clock around each blocking C-ABI call, after a warm-up pair"}
     s.close()
     return out
 

@@ -44,6 +44,7 @@ struct AdjView {
   // derivatives of the metal coefficients: [p] = d/d omega_D, d/d gamma
   T dCE[2], dCE1[2], dCE2[2], dd1[2], dd2[2], dd3[2], dd4[2], dd5[2];
   int* step;        // adjoint clock: the step being transposed
+  unsigned* flags;  // per cell: adj_flags_e | adj_flags_h << 16 (adj_build_flags)
 };
 
 // psi element of component c, slot q at cell (i, j, k) for slab axis ax;
@@ -379,5 +380,413 @@ __global__ void adj_partner(const __grid_constant__ DftView d, const int* __rest
 
 __global__ void adj_step_back(int* step) { *step -= 1; }
 __global__ void adj_set_step(int* step, int n) { *step = n; }
+
+// ---------------------------------------------------------------------
+// Fused form of the transposed Yee sub-steps.  Away from the CPML slabs and
+// the dispersive cells a difference coefficient is a fixed multiple of the
+// adjoint of the component that read the difference, so the gathers
+// compute it on the fly from that adjoint (read with a one-cell halo)
+// instead of from a coefficient array.  Only the slab cells (psi
+// recursions) and the dispersive cells keep their coefficients in the
+// arrays ("special" components, written by adj_e_slab / adj_h_slab and
+// adj_e_design before the gathers).  The scaling of a non-special E adjoint
+// by cee, which must follow every read of it by the H gather, moves into
+// the E gather of the same step.  The H scaling chh is 1 (no magnetic loss
+// in the reference's coefficients, setup.cu:2020), which the host checks
+// before taking this path.  Per step the two gathers each read one field
+// adjoint and update the other: 9 values per cell each, against 24 per
+// sub-step for coefficient arrays written then gathered.  Arithmetic and
+// summation order are those of adj_e_coef / adj_gather_h / adj_h_coef /
+// adj_gather_e, so both forms give the same values.
+
+// Cells of the thick shell n < lo[a] or n >= hi[a] along some axis a, each
+// once: the z slabs (whole planes), then the y slabs of the other planes,
+// then the x slabs of the other rows.
+struct SlabShell {
+  int N[3], lo[3], hi[3];
+  long long n0, n1, n2;
+  __host__ void init(const int n[3], const int l[3], const int h[3]) {
+    for (int a = 0; a < 3; a++) {
+      N[a] = n[a];
+      lo[a] = std::max(0, std::min(l[a], n[a]));
+      hi[a] = std::max(lo[a], std::min(h[a], n[a]));
+    }
+    const long long zc = lo[2] + (N[2] - hi[2]), yc = lo[1] + (N[1] - hi[1]), xc = lo[0] + (N[0] - hi[0]);
+    const long long mz = hi[2] - lo[2], my = hi[1] - lo[1];
+    n0 = zc * N[1] * N[0];
+    n1 = mz * yc * N[0];
+    n2 = mz * my * xc;
+  }
+  __host__ __device__ long long total() const { return n0 + n1 + n2; }
+  __device__ void cell(long long q, int& i, int& j, int& k) const {
+    if (q < n0) {
+      i = (int)(q % N[0]);
+      const long long r = q / N[0];
+      j = (int)(r % N[1]);
+      const int kk = (int)(r / N[1]);
+      k = kk < lo[2] ? kk : hi[2] + (kk - lo[2]);
+    } else if (q < n0 + n1) {
+      q -= n0;
+      i = (int)(q % N[0]);
+      const long long r = q / N[0];
+      const int yc = lo[1] + (N[1] - hi[1]);
+      const int jj = (int)(r % yc);
+      k = lo[2] + (int)(r / yc);
+      j = jj < lo[1] ? jj : hi[1] + (jj - lo[1]);
+    } else {
+      q -= n0 + n1;
+      const int xc = lo[0] + (N[0] - hi[0]), my = hi[1] - lo[1];
+      const int ii = (int)(q % xc);
+      const long long r = q / xc;
+      j = lo[1] + (int)(r % my);
+      k = lo[2] + (int)(r / my);
+      i = ii < lo[0] ? ii : hi[0] + (ii - lo[0]);
+    }
+  }
+};
+
+template <typename T>
+__device__ __forceinline__ unsigned adj_mat(const SimView<T>& s, int i, int j, int k, size_t id) {
+  return (i >= s.mat_lo[0] && i < s.mat_hi[0] && j >= s.mat_lo[1] && j < s.mat_hi[1] && k >= s.mat_lo[2] &&
+          k < s.mat_hi[2])
+             ? s.mat[id]
+             : 0u;
+}
+// active range of E component c (main.cu:1172, 1476, 1767) and of H
+// component h (the two other indices below N-1)
+template <typename T>
+__device__ __forceinline__ bool adj_e_act(const SimView<T>& s, int c, int i, int j, int k) {
+  const int ijk[3] = {i, j, k}, N[3] = {s.NX, s.NY, s.NZ};
+  bool act = true;
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    if (ijk[d] >= N[d] - 1) act = false;
+    if (d != c && ijk[d] < 1) act = false;
+  }
+  return act;
+}
+template <typename T>
+__device__ __forceinline__ bool adj_h_act(const SimView<T>& s, int h, int i, int j, int k) {
+  const int ijk[3] = {i, j, k}, N[3] = {s.NX, s.NY, s.NZ};
+  bool act = true;
+#pragma unroll
+  for (int d = 0; d < 3; d++)
+    if (d != h && ijk[d] >= N[d] - 1) act = false;
+  return act;
+}
+// slab membership as adj_psi decides it (E extent Nc+1, H extent Nc)
+template <typename T>
+__device__ __forceinline__ bool adj_in_slab(const SimView<T>& s, int ax, int n, bool e_extent) {
+  const CpmlAxis<T>& a = s.cp[ax];
+  return (e_extent ? n <= a.Nc : n < a.Nc) || n >= a.F;
+}
+// E component c keeps its coefficients in the arrays: dispersive, or
+// updated with a psi recursion in one of its two slots
+template <typename T>
+__device__ __forceinline__ bool adj_e_special(const SimView<T>& s, int c, int i, int j, int k, unsigned m) {
+  if (m & (1u << c)) return true;
+  if (!adj_e_act(s, c, i, j, k)) return false;
+  const int ijk[3] = {i, j, k};
+  const int a0 = (c + 1) % 3, a1 = (c + 2) % 3;
+  return adj_in_slab(s, a0, ijk[a0], true) || adj_in_slab(s, a1, ijk[a1], true);
+}
+template <typename T>
+__device__ __forceinline__ bool adj_h_special(const SimView<T>& s, int h, int i, int j, int k) {
+  if (!adj_h_act(s, h, i, j, k)) return false;
+  if (!(i < s.NX - 1 && j < s.NY - 1 && k < s.NZ - 1)) return false;  // CPML range (main.cu:829)
+  const int ijk[3] = {i, j, k};
+  const int a0 = (h + 1) % 3, a1 = (h + 2) % 3;
+  return adj_in_slab(s, a0, ijk[a0], false) || adj_in_slab(s, a1, ijk[a1], false);
+}
+
+// Per-cell flags of the gathers, evaluated once per cell: bit c = E (or H)
+// component c active, bit 3 + c = special; bits 8.. = the material byte.
+template <typename T>
+__device__ __forceinline__ unsigned adj_flags_e(const SimView<T>& s, int i, int j, int k, size_t id) {
+  const unsigned m = adj_mat(s, i, j, k, id);
+  const bool sl[3] = {adj_in_slab(s, 0, i, true), adj_in_slab(s, 1, j, true), adj_in_slab(s, 2, k, true)};
+  unsigned f = m << 8;
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    const bool act = adj_e_act(s, c, i, j, k);
+    const bool spec = (m & (1u << c)) || (act && (sl[(c + 1) % 3] || sl[(c + 2) % 3]));
+    f |= (act ? 1u << c : 0u) | (spec ? 8u << c : 0u);
+  }
+  return f;
+}
+template <typename T>
+__device__ __forceinline__ unsigned adj_flags_h(const SimView<T>& s, int i, int j, int k) {
+  const bool ok = i < s.NX - 1 && j < s.NY - 1 && k < s.NZ - 1;
+  const bool sl[3] = {adj_in_slab(s, 0, i, false), adj_in_slab(s, 1, j, false), adj_in_slab(s, 2, k, false)};
+  unsigned f = 0;
+#pragma unroll
+  for (int h = 0; h < 3; h++) {
+    const bool act = adj_h_act(s, h, i, j, k);
+    const bool spec = act && ok && (sl[(h + 1) % 3] || sl[(h + 2) % 3]);
+    f |= (act ? 1u << h : 0u) | (spec ? 8u << h : 0u);
+  }
+  return f;
+}
+
+// The flags of every cell, once per reverse sweep: E flags in the low
+// half (material byte in bits 8..15), H flags in bits 16..21.
+template <typename T>
+__global__ void adj_build_flags(const __grid_constant__ SimView<T> s, unsigned* __restrict__ flags) {
+  const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y, k = blockIdx.z;
+  if (i >= s.NX || j >= s.NY) return;
+  const size_t id = fidx(s.PX, s.plane, i, j, k);
+  flags[id] = adj_flags_e(s, i, j, k, id) | (adj_flags_h(s, i, j, k) << 16);
+}
+
+// Product rounded on its own (no contraction into a following add), as a
+// value stored to a coefficient array is.
+__device__ __forceinline__ float adj_mul(float x, float y) { return __fmul_rn(x, y); }
+__device__ __forceinline__ double adj_mul(double x, double y) { return __dmul_rn(x, y); }
+
+// Difference coefficient of E component c, slot sl (axis (c+1+sl)%3), at a
+// cell: from the arrays for a special component, else sg ceh ikd lambda_E
+// (H: sg che ikh lambda_H), from the cell's flags (adj_flags_e /
+// adj_flags_h); n = the cell's coordinate along the slot's axis.
+// lam is the component's adjoint at the cell, loaded by the caller ahead of
+// the flags so that the two loads overlap.
+template <typename T>
+__device__ __forceinline__ T adj_e_coef_f(const SimView<T>& s, const AdjView<T>& a, int c, int sl, int n, size_t id,
+                                          unsigned f, T lam) {
+  if (f & (8u << c)) return a.a[c][sl][id];
+  if (!(f & (1u << c))) return T(0);
+  const int ax = (c + 1 + sl) % 3;
+  const T sg = sl == 0 ? T(1) : T(-1);
+  return adj_mul(sg * s.ceh[(f >> 8) >> 3] * ldg(s.cp[ax].inv_ked + n), lam);
+}
+template <typename T>
+__device__ __forceinline__ T adj_h_coef_f(const SimView<T>& s, const AdjView<T>& a, int h, int sl, int n, size_t id,
+                                          unsigned f, T lam) {
+  if (f & (8u << h)) return a.a[h][sl][id];
+  if (!(f & (1u << h))) return T(0);
+  const int ax = (h + 1 + sl) % 3;
+  const T sg = sl == 0 ? T(-1) : T(1);
+  return adj_mul(sg * s.che * ldg(s.cp[ax].inv_khd + n), lam);
+}
+
+// E sub-step transposed at the special slab components (the dispersive ones
+// are adj_e_design's): coefficients, psi_E adjoints, lambda_E <- cee lambda_E.
+template <typename T>
+__global__ void adj_e_slab(const __grid_constant__ SimView<T> s, const __grid_constant__ AdjView<T> a,
+                           const SlabShell sh) {
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= sh.total()) return;
+  int i, j, k;
+  sh.cell(q, i, j, k);
+  const size_t id = fidx(s.PX, s.plane, i, j, k);
+  const unsigned m = adj_mat(s, i, j, k, id);
+  const T cee = s.cee[m >> 3], ceh = s.ceh[m >> 3];
+  const int ijk[3] = {i, j, k};
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    if ((m & (1u << c)) || !adj_e_special(s, c, i, j, k, m)) continue;
+    const T lam = a.lE[c][id];
+#pragma unroll
+    for (int sl = 0; sl < 2; sl++) {
+      const int ax = (c + 1 + sl) % 3;
+      const T sg = sl == 0 ? T(1) : T(-1);
+      const CpmlAxis<T>& cp = s.cp[ax];
+      T coef = sg * ceh * ldg(cp.inv_ked + ijk[ax]) * lam;
+      int qs;
+      T* lp = adj_psi(s, &a.lpE_N[c][sl], &a.lpE_F[c][sl], ax, true, i, j, k, &qs);
+      if (lp) {
+        T b, cc;
+        if (qs >= 0) {
+          b = ldg(cp.be_N + qs);
+          cc = ldg(((c == 1 && ax == 0) ? cp.ce_N_ey : cp.ce_N) + qs);
+        } else {
+          b = ldg(cp.be_F + (-1 - qs));
+          cc = ldg(cp.ce_F + (-1 - qs));
+        }
+        const T tot = *lp + sg * ceh * lam;
+        *lp = b * tot;
+        coef += cc * cp.inv_d * tot;
+      }
+      a.a[c][sl][id] = coef;
+    }
+    a.lE[c][id] = cee * lam;
+  }
+}
+
+// H sub-step transposed at the special slab components: coefficients and
+// psi_H adjoints (lambda_H <- chh lambda_H is the identity).
+template <typename T>
+__global__ void adj_h_slab(const __grid_constant__ SimView<T> s, const __grid_constant__ AdjView<T> a,
+                           const SlabShell sh) {
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= sh.total()) return;
+  int i, j, k;
+  sh.cell(q, i, j, k);
+  const size_t id = fidx(s.PX, s.plane, i, j, k);
+  const int ijk[3] = {i, j, k};
+  const T che = s.che;
+#pragma unroll
+  for (int h = 0; h < 3; h++) {
+    if (!adj_h_special(s, h, i, j, k)) continue;
+    const T lam = a.lH[h][id];
+#pragma unroll
+    for (int sl = 0; sl < 2; sl++) {
+      const int ax = (h + 1 + sl) % 3;
+      const T sg = sl == 0 ? T(-1) : T(1);
+      const CpmlAxis<T>& cp = s.cp[ax];
+      T coef = sg * che * ldg(cp.inv_khd + ijk[ax]) * lam;
+      int qs;
+      T* lp = adj_psi(s, &a.lpH_N[h][sl], &a.lpH_F[h][sl], ax, false, i, j, k, &qs);
+      if (lp) {
+        T b, cc;
+        if (qs >= 0) { b = ldg(cp.bh_N + qs); cc = ldg(cp.ch_N + qs); }
+        else { b = ldg(cp.bh_F + (-1 - qs)); cc = ldg(cp.ch_F + (-1 - qs)); }
+        const T tot = *lp + sg * che * lam;
+        *lp = b * tot;
+        coef += cc * cp.inv_d * tot;
+      }
+      a.a[h][sl][id] = coef;
+    }
+  }
+}
+
+// A block's cells [i0, i0 + 32) x [j0, j0 + 8) x {k}, widened by the halo
+// [lo_off, hi_off] on every axis, lie away from the CPML slabs (E extent),
+// off the grid boundary and outside the material box: every component
+// there is active, not special, with the background coefficients.
+template <typename T>
+__device__ __forceinline__ bool adj_block_simple(const SimView<T>& s, int i0, int j0, int k, int lo_off, int hi_off) {
+  const int lo[3] = {i0 + lo_off, j0 + lo_off, k + lo_off};
+  const int hi[3] = {i0 + 31 + hi_off, j0 + 7 + hi_off, k + hi_off};  // inclusive
+  bool inside = true, off_mat = false;
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    inside = inside && lo[a] >= s.cp[a].Nc + 1 && hi[a] < s.cp[a].F;
+    off_mat = off_mat || hi[a] < s.mat_lo[a] || lo[a] >= s.mat_hi[a];
+  }
+  return inside && off_mat;
+}
+
+// lambda_H += gather of the E-sub-step coefficients (adj_gather_h's sums),
+// the non-special coefficients computed from lambda_E of the cell and of
+// its +x, +y, +z neighbours.  Grid (x tiles of 32, y rows of 8, z).
+template <typename T>
+__global__ void __launch_bounds__(256) adj_gather_h_fused(const __grid_constant__ SimView<T> s,
+                                                          const __grid_constant__ AdjView<T> a) {
+  const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y, k = blockIdx.z;
+  const size_t sx = 1, sy = s.PX, sz = s.plane;
+  if (adj_block_simple(s, blockIdx.x * 32, blockIdx.y * 8, k, 0, 1)) {
+    // the same sums with every coefficient sg ceh0 ikd lambda_E
+    const size_t id = fidx(s.PX, s.plane, i, j, k);
+    const T ceh = s.ceh[0];
+    const T kx = ldg(s.cp[0].inv_ked + i), kx1 = ldg(s.cp[0].inv_ked + i + 1);
+    const T ky = ldg(s.cp[1].inv_ked + j), ky1 = ldg(s.cp[1].inv_ked + j + 1);
+    const T kz = ldg(s.cp[2].inv_ked + k), kz1 = ldg(s.cp[2].inv_ked + k + 1);
+    const T* ex = a.lE[0] + id;
+    const T* ey = a.lE[1] + id;
+    const T* ez = a.lE[2] + id;
+    const T ex0 = ex[0], ey0 = ey[0], ez0 = ez[0];
+    // Hx: Ey slot 0 (axis z, sg +1), Ez slot 1 (axis y, sg -1)
+    a.lH[0][id] += adj_mul(T(1) * ceh * kz, ey0) - adj_mul(T(1) * ceh * kz1, ey[sz]) +
+                   adj_mul(T(-1) * ceh * ky, ez0) - adj_mul(T(-1) * ceh * ky1, ez[sy]);
+    // Hy: Ex slot 1 (axis z, sg -1), Ez slot 0 (axis x, sg +1)
+    a.lH[1][id] += adj_mul(T(-1) * ceh * kz, ex0) - adj_mul(T(-1) * ceh * kz1, ex[sz]) +
+                   adj_mul(T(1) * ceh * kx, ez0) - adj_mul(T(1) * ceh * kx1, ez[sx]);
+    // Hz: Ex slot 0 (axis y, sg +1), Ey slot 1 (axis x, sg -1)
+    a.lH[2][id] += adj_mul(T(1) * ceh * ky, ex0) - adj_mul(T(1) * ceh * ky1, ex[sy]) +
+                   adj_mul(T(-1) * ceh * kx, ey0) - adj_mul(T(-1) * ceh * kx1, ey[sx]);
+    return;
+  }
+  if (i >= s.NX || j >= s.NY) return;
+  const size_t id = fidx(s.PX, s.plane, i, j, k);
+  const bool nx = i + 1 < s.NX, ny = j + 1 < s.NY, nz = k + 1 < s.NZ;
+  // neighbour offsets, 0 past the grid (the term is dropped there)
+  const size_t ox = nx ? sx : 0, oy = ny ? sy : 0, oz = nz ? sz : 0;
+  const T ex0 = a.lE[0][id], ey0 = a.lE[1][id], ez0 = a.lE[2][id];
+  const T exy = a.lE[0][id + oy], exz = a.lE[0][id + oz], eyx = a.lE[1][id + ox], eyz = a.lE[1][id + oz];
+  const T ezx = a.lE[2][id + ox], ezy = a.lE[2][id + oy];
+  const T h0 = a.lH[0][id], h1 = a.lH[1][id], h2 = a.lH[2][id];
+  const unsigned f0 = a.flags[id] & 0xffffu;
+  const unsigned fx = a.flags[id + ox] & 0xffffu, fy = a.flags[id + oy] & 0xffffu, fz = a.flags[id + oz] & 0xffffu;
+  // Hx: Ey slot 0 (z), Ez slot 1 (y)
+  a.lH[0][id] = h0 + (adj_e_coef_f(s, a, 1, 0, k, id, f0, ey0) -
+                      (nz ? adj_e_coef_f(s, a, 1, 0, k + 1, id + sz, fz, eyz) : T(0)) +
+                      adj_e_coef_f(s, a, 2, 1, j, id, f0, ez0) -
+                      (ny ? adj_e_coef_f(s, a, 2, 1, j + 1, id + sy, fy, ezy) : T(0)));
+  // Hy: Ex slot 1 (z), Ez slot 0 (x)
+  a.lH[1][id] = h1 + (adj_e_coef_f(s, a, 0, 1, k, id, f0, ex0) -
+                      (nz ? adj_e_coef_f(s, a, 0, 1, k + 1, id + sz, fz, exz) : T(0)) +
+                      adj_e_coef_f(s, a, 2, 0, i, id, f0, ez0) -
+                      (nx ? adj_e_coef_f(s, a, 2, 0, i + 1, id + sx, fx, ezx) : T(0)));
+  // Hz: Ex slot 0 (y), Ey slot 1 (x)
+  a.lH[2][id] = h2 + (adj_e_coef_f(s, a, 0, 0, j, id, f0, ex0) -
+                      (ny ? adj_e_coef_f(s, a, 0, 0, j + 1, id + sy, fy, exy) : T(0)) +
+                      adj_e_coef_f(s, a, 1, 1, i, id, f0, ey0) -
+                      (nx ? adj_e_coef_f(s, a, 1, 1, i + 1, id + sx, fx, eyx) : T(0)));
+}
+
+// lambda_E <- (non-special: cee) lambda_E + gather of the H-sub-step
+// coefficients (adj_gather_e's sums), the non-special ones computed from
+// lambda_H of the cell and of its -x, -y, -z neighbours.
+template <typename T>
+__global__ void __launch_bounds__(256) adj_gather_e_fused(const __grid_constant__ SimView<T> s,
+                                                          const __grid_constant__ AdjView<T> a) {
+  const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y, k = blockIdx.z;
+  const size_t sx = 1, sy = s.PX, sz = s.plane;
+  if (adj_block_simple(s, blockIdx.x * 32, blockIdx.y * 8, k, -1, 0)) {
+    // the same sums with every coefficient sg che ikh lambda_H, after
+    // lambda_E <- cee0 lambda_E
+    const size_t id = fidx(s.PX, s.plane, i, j, k);
+    const T che = s.che, cee = s.cee[0];
+    const T kx = ldg(s.cp[0].inv_khd + i), kxm = ldg(s.cp[0].inv_khd + i - 1);
+    const T ky = ldg(s.cp[1].inv_khd + j), kym = ldg(s.cp[1].inv_khd + j - 1);
+    const T kz = ldg(s.cp[2].inv_khd + k), kzm = ldg(s.cp[2].inv_khd + k - 1);
+    const T* hx = a.lH[0] + id;
+    const T* hy = a.lH[1] + id;
+    const T* hz = a.lH[2] + id;
+    const T hx0 = hx[0], hy0 = hy[0], hz0 = hz[0];
+    T l0 = adj_mul(cee, a.lE[0][id]), l1 = adj_mul(cee, a.lE[1][id]), l2 = adj_mul(cee, a.lE[2][id]);
+    // Ex: Hy slot 0 (axis z, sg -1), Hz slot 1 (axis y, sg +1)
+    l0 += adj_mul(T(-1) * che * kzm, hy[-(ptrdiff_t)sz]) - adj_mul(T(-1) * che * kz, hy0) +
+          adj_mul(T(1) * che * kym, hz[-(ptrdiff_t)sy]) - adj_mul(T(1) * che * ky, hz0);
+    // Ey: Hx slot 1 (axis z, sg +1), Hz slot 0 (axis x, sg -1)
+    l1 += adj_mul(T(1) * che * kzm, hx[-(ptrdiff_t)sz]) - adj_mul(T(1) * che * kz, hx0) +
+          adj_mul(T(-1) * che * kxm, hz[-(ptrdiff_t)sx]) - adj_mul(T(-1) * che * kx, hz0);
+    // Ez: Hx slot 0 (axis y, sg -1), Hy slot 1 (axis x, sg +1)
+    l2 += adj_mul(T(-1) * che * kym, hx[-(ptrdiff_t)sy]) - adj_mul(T(-1) * che * ky, hx0) +
+          adj_mul(T(1) * che * kxm, hy[-(ptrdiff_t)sx]) - adj_mul(T(1) * che * kx, hy0);
+    a.lE[0][id] = l0;
+    a.lE[1][id] = l1;
+    a.lE[2][id] = l2;
+    return;
+  }
+  if (i >= s.NX || j >= s.NY) return;
+  const size_t id = fidx(s.PX, s.plane, i, j, k);
+  const bool px = i > 0, py = j > 0, pz = k > 0;
+  // neighbour offsets, 0 before the grid (the term is dropped there)
+  const size_t ox = px ? sx : 0, oy = py ? sy : 0, oz = pz ? sz : 0;
+  T l[3] = {a.lE[0][id], a.lE[1][id], a.lE[2][id]};
+  const T hx0 = a.lH[0][id], hy0 = a.lH[1][id], hz0 = a.lH[2][id];
+  const T hxy = a.lH[0][id - oy], hxz = a.lH[0][id - oz], hyx = a.lH[1][id - ox], hyz = a.lH[1][id - oz];
+  const T hzx = a.lH[2][id - ox], hzy = a.lH[2][id - oy];
+  const unsigned fw = a.flags[id];
+  const unsigned fe = fw & 0xffffu;
+  const T cee = s.cee[(fe >> 8) >> 3];
+#pragma unroll
+  for (int c = 0; c < 3; c++)
+    if ((fe & (1u << c)) && !(fe & (8u << c))) l[c] = adj_mul(cee, l[c]);
+  const unsigned f0 = fw >> 16;
+  const unsigned fx = a.flags[id - ox] >> 16, fy = a.flags[id - oy] >> 16, fz = a.flags[id - oz] >> 16;
+  // Ex: Hy slot 0 (z), Hz slot 1 (y)
+  l[0] += (pz ? adj_h_coef_f(s, a, 1, 0, k - 1, id - sz, fz, hyz) : T(0)) - adj_h_coef_f(s, a, 1, 0, k, id, f0, hy0) +
+          (py ? adj_h_coef_f(s, a, 2, 1, j - 1, id - sy, fy, hzy) : T(0)) - adj_h_coef_f(s, a, 2, 1, j, id, f0, hz0);
+  // Ey: Hx slot 1 (z), Hz slot 0 (x)
+  l[1] += (pz ? adj_h_coef_f(s, a, 0, 1, k - 1, id - sz, fz, hxz) : T(0)) - adj_h_coef_f(s, a, 0, 1, k, id, f0, hx0) +
+          (px ? adj_h_coef_f(s, a, 2, 0, i - 1, id - sx, fx, hzx) : T(0)) - adj_h_coef_f(s, a, 2, 0, i, id, f0, hz0);
+  // Ez: Hx slot 0 (y), Hy slot 1 (x)
+  l[2] += (py ? adj_h_coef_f(s, a, 0, 0, j - 1, id - sy, fy, hxy) : T(0)) - adj_h_coef_f(s, a, 0, 0, j, id, f0, hx0) +
+          (px ? adj_h_coef_f(s, a, 1, 1, i - 1, id - sx, fx, hyx) : T(0)) - adj_h_coef_f(s, a, 1, 1, i, id, f0, hy0);
+#pragma unroll
+  for (int c = 0; c < 3; c++) a.lE[c][id] = l[c];
+}
 
 }  // namespace fdtd

@@ -240,6 +240,7 @@ static fdtd_status adj_prepare(fdtd_sim* s) {
   CUDA_TRY(A.alloc(&a.gpar, 2, true));
   A.gpar = a.gpar;
   CUDA_TRY(A.alloc(&a.step, 1, false));
+  CUDA_TRY(A.alloc(&a.flags, s->ncell, false));
   A.step = a.step;
   A.rec_slots = std::max(1LL, slots);
   T* rec;
@@ -285,11 +286,42 @@ static fdtd_status adj_sweep(fdtd_sim* s) {
   for (int f = 0; f < 6; f++) maxn = std::max(maxn, s->dft.face[f].na * s->dft.face[f].nb);
   const double* fsel = static_cast<const double*>(A.fsel->p) + A.sel.size();
   const int total = A.tend + 1;
+  // fused gathers (the default; FDTD_ADJ_FUSED=0 selects the coefficient
+  // arrays everywhere) need chh == 1
+  const char* fenv = std::getenv("FDTD_ADJ_FUSED");
+  const bool fused = s->su.Chh == 1.0 && !(fenv && fenv[0] == '0');
+  SlabShell she, shh;
+  {
+    const int n3[3] = {s->NX, s->NY, s->NZ};
+    int lo_e[3], lo_h[3], hi[3];
+    for (int ax = 0; ax < 3; ax++) {
+      lo_e[ax] = s->su.Nc[ax] + 1;
+      lo_h[ax] = s->su.Nc[ax];
+      hi[ax] = s->su.F[ax];
+    }
+    she.init(n3, lo_e, hi);
+    shh.init(n3, lo_h, hi);
+  }
+  const dim3 gtile((unsigned)((s->NX + 31) / 32), (unsigned)((s->NY + 7) / 8), (unsigned)s->NZ);
+  if (fused) adj_build_flags<T><<<gtile, dim3(32, 8)>>>(view<T>(s), a.flags);
   auto adj_step = [&](int n, cudaStream_t stream) {
     if (n % every_dft == 0)
       adj_source<T><<<dim3((maxn + 255) / 256, 6), 256, 0, stream>>>(view<T>(s), s->dft, a,
                                                                       static_cast<const double2*>(A.P->p), fsel,
                                                                       (int)A.sel.size(), s->dft.rows);
+    if (fused) {
+      if (she.total() > 0)
+        adj_e_slab<T><<<(unsigned)((she.total() + 255) / 256), 256, 0, stream>>>(view<T>(s), a, she);
+      if (ntot > 0)
+        adj_e_design<T><<<(ntot + 127) / 128, 128, 0, stream>>>(view<T>(s), m, a, static_cast<const T*>(A.rec),
+                                                                A.every);
+      adj_gather_h_fused<T><<<gtile, dim3(32, 8), 0, stream>>>(view<T>(s), a);
+      if (shh.total() > 0)
+        adj_h_slab<T><<<(unsigned)((shh.total() + 255) / 256), 256, 0, stream>>>(view<T>(s), a, shh);
+      adj_gather_e_fused<T><<<gtile, dim3(32, 8), 0, stream>>>(view<T>(s), a);
+      adj_step_back<<<1, 1, 0, stream>>>(A.step);
+      return 4 + (she.total() > 0) + (shh.total() > 0) + (ntot > 0) + (n % every_dft == 0);
+    }
     adj_e_coef<T><<<gc, 256, 0, stream>>>(view<T>(s), a);
     if (ntot > 0)
       adj_e_design<T><<<(ntot + 127) / 128, 128, 0, stream>>>(view<T>(s), m, a, static_cast<const T*>(A.rec),
