@@ -418,26 +418,29 @@ struct SlabShell {
     n2 = mz * my * xc;
   }
   __host__ __device__ long long total() const { return n0 + n1 + n2; }
-  __device__ void cell(long long q, int& i, int& j, int& k) const {
-    if (q < n0) {
-      i = (int)(q % N[0]);
-      const long long r = q / N[0];
-      j = (int)(r % N[1]);
-      const int kk = (int)(r / N[1]);
+  // 32-bit index arithmetic: the host takes this path only for shells of
+  // fewer than 2^32 cells
+  __device__ void cell(unsigned q, int& i, int& j, int& k) const {
+    const unsigned N0 = (unsigned)N[0], N1 = (unsigned)N[1];
+    if (q < (unsigned)n0) {
+      i = (int)(q % N0);
+      const unsigned r = q / N0;
+      j = (int)(r % N1);
+      const int kk = (int)(r / N1);
       k = kk < lo[2] ? kk : hi[2] + (kk - lo[2]);
-    } else if (q < n0 + n1) {
-      q -= n0;
-      i = (int)(q % N[0]);
-      const long long r = q / N[0];
-      const int yc = lo[1] + (N[1] - hi[1]);
+    } else if (q < (unsigned)(n0 + n1)) {
+      q -= (unsigned)n0;
+      i = (int)(q % N0);
+      const unsigned r = q / N0;
+      const unsigned yc = (unsigned)(lo[1] + (N[1] - hi[1]));
       const int jj = (int)(r % yc);
       k = lo[2] + (int)(r / yc);
       j = jj < lo[1] ? jj : hi[1] + (jj - lo[1]);
     } else {
-      q -= n0 + n1;
-      const int xc = lo[0] + (N[0] - hi[0]), my = hi[1] - lo[1];
+      q -= (unsigned)(n0 + n1);
+      const unsigned xc = (unsigned)(lo[0] + (N[0] - hi[0])), my = (unsigned)(hi[1] - lo[1]);
       const int ii = (int)(q % xc);
-      const long long r = q / xc;
+      const unsigned r = q / xc;
       j = lo[1] + (int)(r % my);
       k = lo[2] + (int)(r / my);
       i = ii < lo[0] ? ii : hi[0] + (ii - lo[0]);
@@ -573,8 +576,8 @@ __device__ __forceinline__ T adj_h_coef_f(const SimView<T>& s, const AdjView<T>&
 template <typename T>
 __global__ void adj_e_slab(const __grid_constant__ SimView<T> s, const __grid_constant__ AdjView<T> a,
                            const SlabShell sh) {
-  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= sh.total()) return;
+  const unsigned q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= (unsigned)sh.total()) return;
   int i, j, k;
   sh.cell(q, i, j, k);
   const size_t id = fidx(s.PX, s.plane, i, j, k);
@@ -617,8 +620,8 @@ __global__ void adj_e_slab(const __grid_constant__ SimView<T> s, const __grid_co
 template <typename T>
 __global__ void adj_h_slab(const __grid_constant__ SimView<T> s, const __grid_constant__ AdjView<T> a,
                            const SlabShell sh) {
-  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= sh.total()) return;
+  const unsigned q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= (unsigned)sh.total()) return;
   int i, j, k;
   sh.cell(q, i, j, k);
   const size_t id = fidx(s.PX, s.plane, i, j, k);

@@ -289,7 +289,7 @@ static fdtd_status adj_sweep(fdtd_sim* s) {
   // fused gathers (the default; FDTD_ADJ_FUSED=0 selects the coefficient
   // arrays everywhere) need chh == 1
   const char* fenv = std::getenv("FDTD_ADJ_FUSED");
-  const bool fused = s->su.Chh == 1.0 && !(fenv && fenv[0] == '0');
+  bool fused = s->su.Chh == 1.0 && !(fenv && fenv[0] == '0');
   SlabShell she, shh;
   {
     const int n3[3] = {s->NX, s->NY, s->NZ};
@@ -301,6 +301,7 @@ static fdtd_status adj_sweep(fdtd_sim* s) {
     }
     she.init(n3, lo_e, hi);
     shh.init(n3, lo_h, hi);
+    if (she.total() >= (1LL << 32) || shh.total() >= (1LL << 32)) fused = false;  // 32-bit shell indices
   }
   const dim3 gtile((unsigned)((s->NX + 31) / 32), (unsigned)((s->NY + 7) / 8), (unsigned)s->NZ);
   if (fused) adj_build_flags<T><<<gtile, dim3(32, 8)>>>(view<T>(s), a.flags);
