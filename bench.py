@@ -284,7 +284,7 @@ def large_params(mod, precision=None):
         precision=mod.FDTD_FP32 if precision is None else precision)
 
 
-def large_bench(mod, torch, stream, sp, dev, blocks=2):
+def large_bench(mod, torch, stream, sp, dev, blocks=2, adjoint_steps=2400):
     """Forward throughput of the large nonlocal workload over a bounded
     number of 128-step blocks (the full run is 12000 steps), and the device
     memory the simulation holds.  Its adjoint is not built: the
@@ -309,7 +309,7 @@ def large_bench(mod, torch, stream, sp, dev, blocks=2):
            "adjoint": "not built for the hydrodynamic model (nonlinear in the current and density); "
                       "see adjoint_local for the same geometry with the local model"}
     s.close()
-    out["adjoint_local"] = large_adjoint_bench(mod, torch, dev)
+    out["adjoint_local"] = large_adjoint_bench(mod, torch, dev, steps=adjoint_steps)
     return out
 
 
@@ -491,6 +491,8 @@ def main():
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-large", action="store_true")
+    ap.add_argument("--large-adjoint-steps", type=int, default=2400,
+                    help="time steps of the large-geometry adjoint sample (multiple of 400)")
     ap.add_argument("--batch-members", type=int, default=64)
     ap.add_argument("--batch-steps", type=int, default=3000)
     ap.add_argument("--no-ref-gpu", action="store_true",
@@ -662,7 +664,7 @@ def main():
 
     large = None
     if not args.no_large and args.grid == 256:
-        large = large_bench(F, torch, stream, sp, dev)
+        large = large_bench(F, torch, stream, sp, dev, adjoint_steps=args.large_adjoint_steps)
 
     adjoint = None
     if not args.no_adjoint and args.grid == 256:
