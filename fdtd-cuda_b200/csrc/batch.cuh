@@ -197,6 +197,24 @@ static fdtd_status batch_build(fdtd_batch* b) {
   return FDTD_OK;
 }
 
+// A launch with a programmatic dependency on the launch before it on the
+// stream (both persistent pass launches of a half step: the second fills
+// the tail of the first).
+template <typename... P, typename... A>
+static void launch_dependent(void (*kern)(P...), dim3 g, dim3 blk, size_t smem, cudaStream_t st, A&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = g;
+  cfg.blockDim = blk;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kern, std::forward<A>(args)...);
+}
+
 template <typename T>
 static void batch_enqueue_step(fdtd_batch* b, cudaStream_t st) {
   const int n = (int)b->sims.size();
@@ -207,14 +225,16 @@ static void batch_enqueue_step(fdtd_batch* b, cudaStream_t st) {
   const int4* inner_items = b->items + b->nedge;
   cudaMemsetAsync(b->queue, 0, 4 * sizeof(int), st);
   int k = 0;
-  if (b->ninner) {
-    h_pass_batch<T, kBatchTY, kBatchS, kBatchMinB, false><<<b->grid_inner, pb, smem, st>>>(
-        v, inner_items, b->ninner, b->queue + 1, kBatchKChunk);
-    k++;
-  }
+  // each pass: the CPML edge items, then the CPML-free items with a
+  // programmatic dependency (they touch disjoint cells)
   if (b->nedge) {
     h_pass_batch<T, kBatchTY, kBatchS, kBatchMinB, true><<<b->grid_pass, pb, smem, st>>>(v, b->items, b->nedge,
                                                                                        b->queue, kBatchKChunk);
+    k++;
+  }
+  if (b->ninner) {
+    launch_dependent(h_pass_batch<T, kBatchTY, kBatchS, kBatchMinB, false>, dim3(b->grid_inner), pb, smem, st, v,
+                     inner_items, b->ninner, b->queue + 1, (int)kBatchKChunk);
     k++;
   }
   // the line step writes the line's other E buffer, so the fused TFSF launch
@@ -228,14 +248,14 @@ static void batch_enqueue_step(fdtd_batch* b, cudaStream_t st) {
       launch_metal<T>(s.get(), st);  // UpdateHydroP* read E^n here
       k += (int)(s->kernels - k0);
     }
-  if (b->ninner) {
-    e_pass_batch<T, kBatchTY, kBatchS, kBatchMinB, false><<<b->grid_inner, pb, smem, st>>>(
-        v, inner_items, b->ninner, b->queue + 3, kBatchKChunk);
-    k++;
-  }
   if (b->nedge) {
     e_pass_batch<T, kBatchTY, kBatchS, kBatchMinB, true><<<b->grid_pass, pb, smem, st>>>(v, b->items, b->nedge,
                                                                                        b->queue + 2, kBatchKChunk);
+    k++;
+  }
+  if (b->ninner) {
+    launch_dependent(e_pass_batch<T, kBatchTY, kBatchS, kBatchMinB, false>, dim3(b->grid_inner), pb, smem, st, v,
+                     inner_items, b->ninner, b->queue + 3, (int)kBatchKChunk);
     k++;
   }
   if (!b->hydro && b->g_m) { metal_e_batch<T><<<dim3(b->g_m, n), 128, 0, st>>>(d); k++; }

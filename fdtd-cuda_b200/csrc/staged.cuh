@@ -348,12 +348,16 @@ __global__ void __launch_bounds__(32 * TY, MINB) h_pass_batch(const SimView<T>* 
                                                            const int4* __restrict__ items, int nitems,
                                                            int* __restrict__ queue, int kchunk) {
   __shared__ int next;
+  pdl_launch_dependents();  // the second launch of the pass may fill this one's tail
   for (;;) {
     __syncthreads();  // the previous item is finished with the stage ring and with next
     if (threadIdx.x == 0 && threadIdx.y == 0) next = atomicAdd(queue, 1);
     __syncthreads();
     const int it = next;
-    if (it >= nitems) return;
+    if (it >= nitems) {
+      pdl_wait();
+      return;
+    }
     const int4 w = items[it];  // (simulation, bx, by, bz)
     h_pass_tile<T, TY, S, PML>(views[w.x], kchunk, w.y, w.z, w.w);
   }
@@ -543,12 +547,16 @@ __global__ void __launch_bounds__(32 * TY, MINB) e_pass_batch(const SimView<T>* 
                                                            const int4* __restrict__ items, int nitems,
                                                            int* __restrict__ queue, int kchunk) {
   __shared__ int next;
+  pdl_launch_dependents();  // the second launch of the pass may fill this one's tail
   for (;;) {
     __syncthreads();  // the previous item is finished with the stage ring and with next
     if (threadIdx.x == 0 && threadIdx.y == 0) next = atomicAdd(queue, 1);
     __syncthreads();
     const int it = next;
-    if (it >= nitems) return;
+    if (it >= nitems) {
+      pdl_wait();
+      return;
+    }
     const int4 w = items[it];  // (simulation, bx, by, bz)
     e_pass_tile<T, TY, S, PML>(views[w.x], kchunk, w.y, w.z, w.w);
   }
