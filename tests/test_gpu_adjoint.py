@@ -97,6 +97,29 @@ def test_fused_gathers_match_coefficient_arrays(prec, monkeypatch):
     np.testing.assert_allclose(out[0][2], out[1][2], rtol=tol)
 
 
+def test_fused_gathers_plain_blocks_match_coefficient_arrays(monkeypatch):
+    """On a 97 x 89 x 93 grid the fused gathers take their flag-free path
+    in the blocks clear of the CPML slabs and the material box (the 34^3
+    grids above have none); it must agree with the coefficient arrays too."""
+    box = [40, 48, 40, 48, 44, 48]
+    out = []
+    for mode in ("1", "0"):
+        monkeypatch.setenv("FDTD_ADJ_FUSED", mode)
+        s = F.Sim(make(F, "sphere_big", precision=F.FDTD_FP64, nano_sphere=0, Tend=420,
+                       design_box=box, **GOLD))
+        rng = np.random.default_rng(3)
+        s.set_design(rng.uniform(0, 1, (box[5] - box[4], box[3] - box[2], box[1] - box[0])).astype(np.float32))
+        L = s.forward(SEL, 40)
+        g, gp = s.backward()
+        out.append((L, g, gp))
+        s.close()
+    assert out[0][0] == out[1][0]
+    g0, g1 = out[0][1], out[1][1]
+    assert np.abs(g1).max() > 0
+    assert np.abs(g0 - g1).max() <= 1e-12 * np.abs(g1).max()
+    np.testing.assert_allclose(out[0][2], out[1][2], rtol=1e-12)
+
+
 def test_checkpoint_interval_does_not_change_the_gradient(fp64_grad):
     _, L, g, gp = fp64_grad
     s = design_sim(F.FDTD_FP64, **GOLD)
