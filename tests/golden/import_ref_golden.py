@@ -5,7 +5,7 @@ small .npz fixtures:
                  reference's per-step printf (main.cu:2726), 7 digits
   scatabs_<t>    the 19-column ScatAbs.<t>.txt (Spectral.cu:1157-1174)
 
-    python tests/golden/import_ref_golden.py gpurun_out/ref_golden
+    python tests/golden/import_ref_golden.py <directory holding the reference's outputs>
 """
 import glob
 import os

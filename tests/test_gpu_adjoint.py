@@ -120,6 +120,29 @@ def test_fused_gathers_plain_blocks_match_coefficient_arrays(monkeypatch):
     np.testing.assert_allclose(out[0][2], out[1][2], rtol=1e-12)
 
 
+def test_autograd_wrapper_matches_backward_and_differences(fp64_grad):
+    """The torch.autograd.Function over fdtd_forward / fdtd_backward gives
+    the adjoint's gradient and agrees with differences of its own forward."""
+    import torch
+    from fdtd_b200.autograd import AbsorbedPower
+    _, L, g, gp = fp64_grad
+    s = design_sim(F.FDTD_FP64, **GOLD)
+    rho = torch.tensor(rho0(), dtype=torch.float64, requires_grad=True)
+    Lt = AbsorbedPower.apply(rho, s, SEL, 50)
+    assert Lt.item() == pytest.approx(L, rel=1e-12)
+    Lt.backward()
+    gt = rho.grad.numpy()
+    assert np.abs(gt - g).max() <= 1e-12 * np.abs(g).max()
+    np.testing.assert_allclose(s.last_param_grad, gp, rtol=1e-12)
+    h, c = 1e-3, (2, 3, 1)
+    with torch.no_grad():
+        r = rho.detach().clone(); r[c] += h; lp = AbsorbedPower.apply(r, s, SEL, 50).item()
+        r = rho.detach().clone(); r[c] -= h; lm = AbsorbedPower.apply(r, s, SEL, 50).item()
+    fd = (lp - lm) / (2 * h)
+    assert abs(fd - gt[c]) <= 1e-3 * abs(fd)
+    s.close()
+
+
 def test_checkpoint_interval_does_not_change_the_gradient(fp64_grad):
     _, L, g, gp = fp64_grad
     s = design_sim(F.FDTD_FP64, **GOLD)
