@@ -1,6 +1,7 @@
-"""Builds libfdtd_b200.so (the CUDA kernels and the C ABI) for sm_100a.
+"""Builds libfdtd_b200.so (the CUDA kernels and the C ABI) for sm_100a, and
+fdtd_runner, the reference's program as a C++ host over that ABI.
 
-The library is built in-tree next to this file so that it travels with the
+Both are built in-tree next to this file so that they travel with the
 repository; nvcc cross-compiles without a GPU.
 """
 import os
@@ -9,6 +10,7 @@ import subprocess
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(os.path.dirname(HERE), "csrc")
 LIB = os.path.join(HERE, "libfdtd_b200.so")
+RUNNER = os.path.join(HERE, "fdtd_runner")
 SOURCES = ["fdtd.cu", "setup.cpp"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
@@ -36,8 +38,20 @@ def needs_build():
     return any(os.path.getmtime(d) > t for d in deps)
 
 
+def build_runner(verbose=False):
+    """fdtd_runner: host C++ only, linked against the library found next to
+    it at run time."""
+    cmd = [os.environ.get("CXX", "g++"), "-O2", "-std=c++17", os.path.join(CSRC, "runner.cpp"),
+           "-L" + HERE, "-lfdtd_b200", "-Wl,-rpath,$ORIGIN", "-o", RUNNER + ".tmp"]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.check_call(cmd, cwd=CSRC)
+    os.replace(RUNNER + ".tmp", RUNNER)
+    return RUNNER
+
+
 def build(force=False, verbose=False, extra=()):
-    if not force and not needs_build():
+    if not force and not needs_build() and os.path.exists(RUNNER):
         return LIB
     srcs, _ = sources()
     cmd = [nvcc(), *NVCC_FLAGS, *extra, "-o", LIB + ".tmp", *srcs]
@@ -45,6 +59,7 @@ def build(force=False, verbose=False, extra=()):
         print(" ".join(cmd))
     subprocess.check_call(cmd, cwd=CSRC)
     os.replace(LIB + ".tmp", LIB)
+    build_runner(verbose)
     return LIB
 
 

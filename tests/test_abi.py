@@ -82,3 +82,19 @@ def test_plan_matches_oracle(name):
     assert list(d.sca_end) == list(od.sca_end)
     assert list(d.n_metal_cells) == list(od.n_metal_cells)
     assert d.dt == od.dt and d.delay == od.delay and d.width == od.width
+
+
+RUNNER = os.path.join(os.path.dirname(F.LIB_PATH), "fdtd_runner")
+
+
+def test_runner_usage_and_errors_without_gpu(tmp_path):
+    """fdtd_runner (the reference's program over the C ABI) is built next to
+    the library; its usage and input errors need no GPU."""
+    import subprocess
+    assert os.access(RUNNER, os.X_OK)
+    r = subprocess.run([RUNNER, "--help"], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0 and "usage" in r.stderr
+    r = subprocess.run([RUNNER, "--bogus"], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 2
+    r = subprocess.run([RUNNER, str(tmp_path / "missing.txt")], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 1 and "reading the input" in r.stderr

@@ -192,6 +192,35 @@ def test_watchdog_reports_nonfinite():
     assert e.value.status == 6
 
 
+def test_runner_writes_the_reference_outputs(tmp_path):
+    """fdtd_runner on an Input.txt deck writes OUT.txt (t*dt and E at the
+    centre at the top of every step) and ScatAbs.<Tend>.txt, matching the
+    same deck run through the Python binding.  The deck holds the
+    reference's Input.txt fields only, so the case uses the reference's
+    other constants."""
+    import subprocess
+    p = make(F, "sphere_ref", precision=F.FDTD_FP64, Tend=200)
+    deck = tmp_path / "Input.txt"
+    F.write_input_txt(str(deck), p)
+    runner = os.path.join(os.path.dirname(F.LIB_PATH), "fdtd_runner")
+    r = subprocess.run([runner, str(deck), "--out", str(tmp_path), "--fp64"], capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0, r.stderr
+    q = F.load_input_txt(str(deck))
+    q.precision = F.FDTD_FP64
+    s = F.Sim(q)
+    s.run()
+    rows = np.loadtxt(tmp_path / "ScatAbs.200.txt")
+    np.testing.assert_allclose(rows, s.spectra(), rtol=1e-6)
+    out = np.loadtxt(tmp_path / "OUT.txt")
+    assert out.shape == (201, 4)
+    probe = s.probe()
+    np.testing.assert_allclose(out[1:, 1:], probe[:200], rtol=1e-6, atol=1e-6 * np.abs(probe).max())
+    np.testing.assert_array_equal(out[0, 1:], 0.0)
+    np.testing.assert_allclose(out[:, 0], np.arange(201) * s.dims.dt, rtol=1e-6)
+    s.close()
+
+
 def test_scatabs_file_format(tmp_path):
     s = run_sim("sphere_au", 200, F.FDTD_FP64)
     path = tmp_path / "ScatAbs.200.txt"
