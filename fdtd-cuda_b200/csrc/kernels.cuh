@@ -195,30 +195,6 @@ __device__ __forceinline__ size_t slab_idx(const SimView<T>& s, int ax, int w, i
   return ((size_t)k * s.NY + j) * w + i;
 }
 
-// One psi recursion of an H component along axis ax, applied with sign sg
-// (UPDATE_h* CPML blocks, main.cu:829-861 and mirrors).
-template <typename T>
-__device__ __forceinline__ T cpml_h(const SimView<T>& s, int c, int slot, int ax, int i, int j, int k,
-                                    T diff, T v, T sg) {
-  const CpmlAxis<T>& a = s.cp[ax];
-  int q = ax == 0 ? i : ax == 1 ? j : k;
-  if (q < a.Nc) {
-    T* p = s.psiH_N[c][slot] + slab_idx(s, ax, a.Nc, i, j, k);
-    T ps = ldg(a.bh_N + q) * *p + ldg(a.ch_N + q) * diff * a.inv_d;
-    *p = ps;
-    v += sg * (s.che * ps);
-  }
-  if (q >= a.F) {
-    int q2 = q - a.F;
-    int ii = ax == 0 ? q2 : i, jj = ax == 1 ? q2 : j, kk = ax == 2 ? q2 : k;
-    T* p = s.psiH_F[c][slot] + slab_idx(s, ax, a.Nc, ii, jj, kk);
-    T ps = ldg(a.bh_F + q2) * *p + ldg(a.ch_F + q2) * diff * a.inv_d;
-    *p = ps;
-    v += sg * (s.che * ps);
-  }
-  return v;
-}
-
 // One psi recursion of an E component (UPDATE_e* CPML blocks,
 // main.cu:1294-1318 and mirrors).  near_lim is Nc+1 except Ez's near-y
 // slab, which the reference bounds by Nc (main.cu:1843).
