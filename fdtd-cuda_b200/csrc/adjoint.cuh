@@ -151,10 +151,11 @@ __global__ void adj_e_design(const __grid_constant__ SimView<T> s, const __grid_
     const T v = r[0], e1 = r[m.rec_slots], J = r[2 * m.rec_slots], Jm = r[3 * m.rec_slots],
             nv = r[4 * m.rec_slots];
     const T rho = m.rho[c] ? (T)m.rho[c][sl] : T(1);
-    const T CE = m.vac + rho * (m.C_E - m.vac), CE1 = m.vac + rho * (m.C_E_1 - m.vac), CE2 = rho * m.C_E_2;
-    const T D3 = rho * m.d3, D4 = rho * m.d4, D5 = rho * m.d5;
-    const T C3[2] = {rho * m.C3[0], rho * m.C3[1]}, C4[2] = {rho * m.C4[0], rho * m.C4[1]},
-            C5[2] = {rho * m.C5[0], rho * m.C5[1]};
+    const T CE = (T)(m.vac + rho * (m.C_E - m.vac)), CE1 = (T)(m.vac + rho * (m.C_E_1 - m.vac));
+    const T CE2 = (T)(rho * m.C_E_2);
+    const T D3 = (T)(rho * m.d3), D4 = (T)(rho * m.d4), D5 = (T)(rho * m.d5);
+    const T C3[2] = {(T)(rho * m.C3[0]), (T)(rho * m.C3[1])}, C4[2] = {(T)(rho * m.C4[0]), (T)(rho * m.C4[1])},
+            C5[2] = {(T)(rho * m.C5[0]), (T)(rho * m.C5[1])};
     const T lnv = a.lE[c][id];
     const T al = a.lJa[c][sl], be = a.lJb[c][sl], ep = a.lEh[c][sl];
     const T aq[2] = {a.lPa[c][0][sl], a.lPa[c][1][sl]}, bq[2] = {a.lPb[c][0][sl], a.lPb[c][1][sl]};

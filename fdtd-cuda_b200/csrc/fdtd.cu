@@ -392,15 +392,15 @@ static fdtd_status build_views(fdtd_sim* s) {
     }
     s->mstate = st;
   }
-  m.C_E = (T)su.C_E; m.C_E_1 = (T)su.C_E_1; m.C_E_2 = (T)su.C_E_2;
-  m.d1 = (T)su.d1; m.d2 = (T)su.d2; m.d3 = (T)su.d3; m.d4 = (T)su.d4; m.d5 = (T)su.d5; m.dNL = (T)su.dNL;
+  m.C_E = su.C_E; m.C_E_1 = su.C_E_1; m.C_E_2 = su.C_E_2;
+  m.d1 = su.d1; m.d2 = su.d2; m.d3 = su.d3; m.d4 = su.d4; m.d5 = su.d5; m.dNL = su.dNL;
   for (int q = 0; q < 2; q++) {
-    m.C1[q] = (T)su.C1[q]; m.C2[q] = (T)su.C2[q]; m.C3[q] = (T)su.C3[q]; m.C4[q] = (T)su.C4[q]; m.C5[q] = (T)su.C5[q];
+    m.C1[q] = su.C1[q]; m.C2[q] = su.C2[q]; m.C3[q] = su.C3[q]; m.C4[q] = su.C4[q]; m.C5[q] = su.C5[q];
   }
   m.dt = (T)su.dt; m.z0 = (T)su.z0; m.e0 = (T)su.e0; m.N_EQ = (T)su.N_EQ;
   m.inv_dx = (T)(1.0 / su.p.dx); m.inv_dy = (T)(1.0 / su.p.dy); m.inv_dz = (T)(1.0 / su.p.dz);
   m.hydro = su.hydro;
-  m.vac = (T)su.ep0;
+  m.vac = su.ep0;
   for (int c = 0; c < 3; c++) { m.rho[c] = nullptr; m.rec_off[c] = 0; }
   m.rec = nullptr;
   m.rec_rows = 1;

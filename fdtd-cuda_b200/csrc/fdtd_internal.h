@@ -87,7 +87,7 @@ struct MetalView {
   T* pd[3][3];          // Drude current ring (n, n-1, new) indexed by step
   T* nd[3][2];          // hydro density ring
   const float* rho[3];  // design blend per slot (null: plain metal coefficients)
-  T vac;                // vacuum C_E = C_E_1 = ep0, the rho = 0 end of the blend
+  double vac;           // vacuum C_E = C_E_1 = ep0, the rho = 0 end of the blend
   // forward record for the adjoint (null = off): per step row (t % rec_rows)
   // five values per slot, [row][value][rec_off[c] + slot], value = E^n,
   // E^{n-1}, J^n, J^{n-1}, E^{n+1}
@@ -97,10 +97,13 @@ struct MetalView {
   long long rec_slots;
   // hydrodynamic neighbour slots, 12 per cell (see hydro_neighbours)
   const int* nbr[3];
-  // coefficients
-  T C_E, C_E_1, C_E_2;
-  T d1, d2, d3, d4, d5, dNL;
-  T C1[2], C2[2], C3[2], C4[2], C5[2];
+  // ADE coefficients, FP64 in both builds: the CP pole recursions sit close
+  // to their stability limit, and rounding these to FP32 alone shifts the
+  // spectra by 1e-5 to 1e-4 of their peak.  The recursions run in FP64 and
+  // the state is stored in T.
+  double C_E, C_E_1, C_E_2;
+  double d1, d2, d3, d4, d5, dNL;
+  double C1[2], C2[2], C3[2], C4[2], C5[2];
   T dt, z0, e0, N_EQ;
   T inv_dx, inv_dy, inv_dz;
   int hydro;

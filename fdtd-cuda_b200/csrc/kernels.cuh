@@ -381,7 +381,8 @@ __device__ __forceinline__ void metal_e_body(const SimView<T>& s, const MetalVie
   const T pdn = m.pd[c][rn][sl], pdn1 = m.pd[c][rn1][sl];
   const T cpn0 = m.cpn[c][0][sl], cpn1_0 = m.cpn1[c][0][sl];
   const T cpn1 = m.cpn[c][1][sl], cpn1_1 = m.cpn1[c][1][sl];
-  T CP1 = T(0), CP2 = T(0), CP3 = T(0), CP4 = T(0);
+  // the ADE recursions in FP64 (the coefficients are FP64), the state in T
+  double CP1 = 0.0, CP2 = 0.0, CP3 = 0.0, CP4 = 0.0;
   CP1 += (m.d1 - 1) * pdn;
   CP3 += m.d2 * pdn1;
   CP2 += (m.C1[0] - 1) * cpn0;
@@ -392,10 +393,10 @@ __device__ __forceinline__ void metal_e_body(const SimView<T>& s, const MetalVie
   const T en = v;             // current E becomes e_n
   // coefficients coupling E to the poles; an adjoint design region blends
   // them linearly between vacuum (rho = 0) and the metal (rho = 1)
-  T CE = m.C_E, CE1 = m.C_E_1, CE2 = m.C_E_2, D3 = m.d3, D4 = m.d4, D5 = m.d5;
-  T C3[2] = {m.C3[0], m.C3[1]}, C4[2] = {m.C4[0], m.C4[1]}, C5[2] = {m.C5[0], m.C5[1]};
+  double CE = m.C_E, CE1 = m.C_E_1, CE2 = m.C_E_2, D3 = m.d3, D4 = m.d4, D5 = m.d5;
+  double C3[2] = {m.C3[0], m.C3[1]}, C4[2] = {m.C4[0], m.C4[1]}, C5[2] = {m.C5[0], m.C5[1]};
   if (m.rho[c]) {
-    const T r = (T)m.rho[c][sl];
+    const double r = (double)(T)m.rho[c][sl];
     CE = m.vac + r * (m.C_E - m.vac);
     CE1 = m.vac + r * (m.C_E_1 - m.vac);
     CE2 = r * m.C_E_2;
@@ -403,11 +404,12 @@ __device__ __forceinline__ void metal_e_body(const SimView<T>& s, const MetalVie
 #pragma unroll
     for (int q = 0; q < 2; q++) { C3[q] = r * m.C3[q]; C4[q] = r * m.C4[q]; C5[q] = r * m.C5[q]; }
   }
-  const T inv_CE = T(1) / CE;
-  T nv = inv_CE * (m.dt * curl / m.z0 + CE1 * en - CE2 * en1 - CP1 - CP2 - CP3 - CP4 - T(0));
-  const T ncp0 = m.C1[0] * cpn0 + m.C2[0] * cpn1_0 + C3[0] * nv + C4[0] * en + C5[0] * en1;
-  const T ncp1 = m.C1[1] * cpn1 + m.C2[1] * cpn1_1 + C3[1] * nv + C4[1] * en + C5[1] * en1;
-  const T npd = m.d1 * pdn + m.d2 * pdn1 + D3 * nv + D4 * en + D5 * en1 + m.dNL * T(0);
+  const double inv_CE = 1.0 / CE;
+  const double nvd = inv_CE * ((double)(m.dt * curl / m.z0) + CE1 * en - CE2 * en1 - CP1 - CP2 - CP3 - CP4 - 0.0);
+  const double ncp0 = m.C1[0] * cpn0 + m.C2[0] * cpn1_0 + C3[0] * nvd + C4[0] * en + C5[0] * en1;
+  const double ncp1 = m.C1[1] * cpn1 + m.C2[1] * cpn1_1 + C3[1] * nvd + C4[1] * en + C5[1] * en1;
+  const double npd = m.d1 * pdn + m.d2 * pdn1 + D3 * nvd + D4 * en + D5 * en1 + m.dNL * 0.0;
+  T nv = (T)nvd;
   if (m.rec) {
     T* r = m.rec + (size_t)(t % m.rec_rows) * 5 * m.rec_slots + m.rec_off[c] + sl;
     r[0] = en; r[m.rec_slots] = en1; r[2 * m.rec_slots] = pdn; r[3 * m.rec_slots] = pdn1; r[4 * m.rec_slots] = nv;
@@ -416,9 +418,9 @@ __device__ __forceinline__ void metal_e_body(const SimView<T>& s, const MetalVie
   m.en[c][sl] = en;
   m.cpn1[c][0][sl] = cpn0;
   m.cpn1[c][1][sl] = cpn1;
-  m.cpn[c][0][sl] = ncp0;
-  m.cpn[c][1][sl] = ncp1;
-  m.pd[c][rnew][sl] = npd;
+  m.cpn[c][0][sl] = (T)ncp0;
+  m.cpn[c][1][sl] = (T)ncp1;
+  m.pd[c][rnew][sl] = (T)npd;
   nv = cpml_e_all(s, c, i, j, k, da, db, nv, ceh);
   if (!isfinite((double)nv)) atomicOr(s.nonfinite, 1);
   s.E[c][id] = nv;
@@ -480,7 +482,9 @@ __device__ __forceinline__ T hydro_current(const MetalView<T>& m, int t, int sl,
   if (m.fix_cbrt) cb = (T)cbrt((double)ND1);
   else cb = (T)powf((float)ND1, (float)(1.0 / 3.0));
   const T pn = m.pd[c][t % 3][sl], pn1 = m.pd[c][(t + 2) % 3][sl];
-  return m.d1 * pn + m.d2 * pn1 + m.d3 * ev + m.d4 * en_prev + m.d5 * T(0) + m.dNL * (gd + gd2 / m.N_EQ) / cb;
+  // FP64 recursion (FP64 coefficients), rounded to the state type
+  return (T)(m.d1 * pn + m.d2 * pn1 + m.d3 * ev + m.d4 * en_prev + m.d5 * 0.0 +
+             m.dNL * (double)((gd + gd2 / m.N_EQ) / cb));
 }
 
 // Hydrodynamic E update of one cell of component c (UPDATE_e* hydro
@@ -524,23 +528,26 @@ __device__ __forceinline__ void hydro_e_cell(const SimView<T>& s, const MetalVie
   const T curl = curl_h_at(s, c, i, j, k, &da, &db);
   const T cpn0 = m.cpn[c][0][sl], cpn1_0 = m.cpn1[c][0][sl];
   const T cpn1 = m.cpn[c][1][sl], cpn1_1 = m.cpn1[c][1][sl];
-  T CP2 = T(0), CP4 = T(0);
+  // the ADE recursions in FP64 (the coefficients are FP64), the state in T
+  double CP2 = 0.0, CP4 = 0.0;
   CP2 += (m.C1[0] - 1) * cpn0;
   CP2 += (m.C1[1] - 1) * cpn1;
   CP4 += m.C2[0] * cpn1_0;
   CP4 += m.C2[1] * cpn1_1;
   const T en1 = m.en[c][sl];
   const T en = v;
-  const T inv_CE = T(1) / m.C_E;
-  T nv = inv_CE * (m.dt * curl / m.z0 + m.dt * jd * m.e0 * (m.N_EQ + nd) + m.C_E_1 * en - m.C_E_2 * en1 - CP2 - CP4);
-  const T ncp0 = m.C1[0] * cpn0 + m.C2[0] * cpn1_0 + m.C3[0] * nv + m.C4[0] * en + m.C5[0] * en1;
-  const T ncp1 = m.C1[1] * cpn1 + m.C2[1] * cpn1_1 + m.C3[1] * nv + m.C4[1] * en + m.C5[1] * en1;
+  const double inv_CE = 1.0 / m.C_E;
+  const double nvd = inv_CE * ((double)(m.dt * curl / m.z0 + m.dt * jd * m.e0 * (m.N_EQ + nd)) + m.C_E_1 * en -
+                               m.C_E_2 * en1 - CP2 - CP4);
+  const double ncp0 = m.C1[0] * cpn0 + m.C2[0] * cpn1_0 + m.C3[0] * nvd + m.C4[0] * en + m.C5[0] * en1;
+  const double ncp1 = m.C1[1] * cpn1 + m.C2[1] * cpn1_1 + m.C3[1] * nvd + m.C4[1] * en + m.C5[1] * en1;
+  T nv = (T)nvd;
   m.en1[c][sl] = en1;
   m.en[c][sl] = en;
   m.cpn1[c][0][sl] = cpn0;
   m.cpn1[c][1][sl] = cpn1;
-  m.cpn[c][0][sl] = ncp0;
-  m.cpn[c][1][sl] = ncp1;
+  m.cpn[c][0][sl] = (T)ncp0;
+  m.cpn[c][1][sl] = (T)ncp1;
   m.nd[c][(t + 1) & 1][sl] = nd;  // becomes "prev" after the parity flip
   nv = cpml_e_all(s, c, i, j, k, da, db, nv, ceh);
   if (!isfinite((double)nv)) atomicOr(s.nonfinite, 1);
