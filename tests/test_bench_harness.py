@@ -60,3 +60,21 @@ def test_reference_arm_under_torchrun_world2():
     assert d["impl"] == "reference" and d["n_gpus"] == 2
     assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["value"] == d["value"] > 0
     assert d["e2e"]["h2d_bytes_per_step"] == 0
+
+
+def test_roofline_numerator_of_the_headline():
+    """The algorithmic bytes of one E pass at 256^3 FP32 (the roofline's
+    numerator): 9 values per cell plus the psi read and write of the six
+    CPML slabs, from the host-side plan (no GPU)."""
+    sys.path.insert(0, ROOT)
+    import bench
+    import fdtd_b200 as F
+    p = bench.workload_params(F, F.FDTD_FP32)
+    d = F.plan(p)
+    assert (d.nx, d.ny, d.nz) == (256, 256, 256)
+    cells = 256 ** 3
+    e = bench.pass_bytes(d, p, 4, "e")
+    h = bench.pass_bytes(d, p, 4, "h")
+    assert e == cells * 9 * 4 + 3 * (2 * 2 * 13 * 256 * 256 * 2 * 4)
+    assert h == cells * 9 * 4 + 3 * (2 * 2 * 12 * 256 * 256 * 2 * 4)
+    assert e == 685768704
