@@ -397,7 +397,7 @@ static fdtd_status build_views(fdtd_sim* s) {
   for (int q = 0; q < 2; q++) {
     m.C1[q] = su.C1[q]; m.C2[q] = su.C2[q]; m.C3[q] = su.C3[q]; m.C4[q] = su.C4[q]; m.C5[q] = su.C5[q];
   }
-  m.dt = (T)su.dt; m.z0 = (T)su.z0; m.e0 = (T)su.e0; m.N_EQ = (T)su.N_EQ;
+  m.dt = su.dt; m.z0 = su.z0; m.e0 = su.e0; m.N_EQ = su.N_EQ;
   m.inv_dx = (T)(1.0 / su.p.dx); m.inv_dy = (T)(1.0 / su.p.dy); m.inv_dz = (T)(1.0 / su.p.dz);
   m.hydro = su.hydro;
   m.vac = su.ep0;

@@ -104,7 +104,9 @@ struct MetalView {
   double C_E, C_E_1, C_E_2;
   double d1, d2, d3, d4, d5, dNL;
   double C1[2], C2[2], C3[2], C4[2], C5[2];
-  T dt, z0, e0, N_EQ;
+  // the hydrodynamic E source dt J e0 (N_EQ + N) and the continuity update
+  // run in FP64 too (their constants are FP64)
+  double dt, z0, e0, N_EQ;
   T inv_dx, inv_dy, inv_dz;
   int hydro;
   int fix_cbrt;

@@ -509,7 +509,7 @@ __device__ __forceinline__ void hydro_e_cell(const SimView<T>& s, const MetalVie
     }
   }
   const T ndm1 = m.nd[c][(t + 1) & 1][sl];  // N^{n-1}
-  const T k2 = T(2) * m.dt * m.inv_dx;
+  const double k2 = 2.0 * m.dt * m.inv_dx;
   T nd;
   if (c == 0)
     nd = ndm1 - k2 * (T(0.5) * (N1[0] * V1[0] - N2[0] * V2[0]) + (N1[1] * V1[1] - N2[1] * V2[1]) +

@@ -116,9 +116,8 @@ def test_spectra_fp32(name):
         scale = np.max(np.abs(b[:, col]))
         errs.append(float(np.max(np.abs(a[:, col] - b[:, col])) / scale))
     print(name, "fp32 spectra errors (sca, abs)", errs)
-    # FP64 ADE coefficients: measured 3e-8 .. 1.1e-5 on these cases (the
-    # hydrodynamic scattering column is the largest)
-    assert max(errs) < 3e-5, errs
+    # FP64 dispersive-cell recursions: measured 3e-8 .. 7.7e-6 on these cases
+    assert max(errs) < 2e-5, errs
 
 
 def test_split_calls_equal_fused_step():
@@ -290,7 +289,7 @@ def test_spectral_error_table():
         rows.append((name, errs))
         if name != "vacuum":  # no particle: its spectra are leakage noise
             assert max(errs["f64"]) < 1e-10, (name, errs)
-            assert max(errs["f32"]) < 3e-5, (name, errs)  # measured at most 1.1e-5
+            assert max(errs["f32"]) < 2e-5, (name, errs)  # measured at most 9.4e-6
     path = os.environ.get("FDTD_PARITY_REPORT")
     if path:
         with open(path, "w") as f:
