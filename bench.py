@@ -51,6 +51,24 @@ def workload_params(mod, precision, grid=256, **over):
     return mod.default_params(**kw)
 
 
+def small_params(mod, precision, **over):
+    """The small plain configuration: 64^3 total grid (43 + 2 * 10 + 1),
+    dx = 2 nm, S = 0.5, a gold sphere of radius 10 nm at the centre
+    (Drude + 2CP gold), 10-cell CPML with kappa_max = 1, the TFSF box 8
+    cells inside the CPML, an x-polarised plane wave along +z whose pulse
+    (centred at 600 nm, bandwidth 3e15) spans 400-900 nm, 2000 time steps
+    and the 6-face DFT flux boxes at 101 wavelengths 400-900 nm."""
+    kw = dict(
+        Tend=1999, dx=2e-9, dy=2e-9, dz=2e-9, NCELLX=43, NCELLY=43, NCELLZ=43,
+        NcpmlX=10, NcpmlY=10, NcpmlZ=10, cpml_kappa_max=1.0, tfsf_inset=8,
+        nano_sphere=1, nano_sphere_radius=10e-9, material=3, first_medium=1,
+        NUM_freq=101, WL_or_freq=1, lam_min=400e-9, lam_max=900e-9, lam_0=600e-9,
+        BandWidth=3e15, inc_phi_deg=90.0, precision=precision,
+    )
+    kw.update(over)
+    return mod.default_params(**kw)
+
+
 # ----------------------------------------------------------------------
 # helpers
 
@@ -165,24 +183,59 @@ def max_over_ranks(x, world, device):
     return float(t.item())
 
 
-def cpu_sample(steps=8, grid=256, num_freq=201):
-    """Times the FP64 CPU restatement (oracle) on the same workload for a
-    bounded number of time steps (DFT samples included at t = 0 and 4)."""
+def cpu_model():
+    """The host CPU's model name (/proc/cpuinfo), or the platform string."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or platform.machine()
+
+
+def cpu_sample(steps=200, grid=256, num_freq=201):
+    """Times the FP64 CPU restatement (oracle) on the same workload over a
+    fixed window of time steps after the first (which allocates the DFT
+    accumulators); the window includes its DFT samples (every 4 steps)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     cores = os.cpu_count() or 1
     O.lib().orc_set_threads(cores)
     p = workload_params(O, 1, grid=grid, NUM_freq=num_freq)
     s = O.OracleSim(p, threads=cores)
-    s.step(1)  # first step allocates the DFT accumulators
+    s.step(1)
     t0 = time.perf_counter()
     s.step(steps)
     dt = time.perf_counter() - t0
     cells = s.shape[0] * s.shape[1] * s.shape[2]
     return {"value": cells * steps / dt / 1e9, "unit": "Gcell-steps/s", "cores": cores,
-            "kind": "port",
-            "sample": f"{steps} time steps of the {grid}^3 workload (FP64, incl. 2 DFT samples), "
-                      f"{dt:.1f} s"}
+            "kind": "port", "cpu": cpu_model(),
+            "sample": f"time steps 1-{steps} of the {grid}^3 workload (FP64, {steps // 4} DFT samples "
+                      f"at {num_freq} wavelengths), {dt:.1f} s"}
+
+
+def step_bytes(dims, params, st, esize):
+    """Algorithmic DRAM bytes of one whole time step, by kernel family:
+    the two Yee passes (pass_bytes), the TFSF table launch (per entry: the
+    31-byte table row and a read-modify-write of one field value), the
+    dispersive cells (per component and cell: 21 state and field values
+    and the 16-byte cell entry; hydrodynamic cells add the density ring and
+    the 48-byte neighbour list), the DFT sample (a field read and a ring
+    write per row every dft_every steps) and the DFT contraction (per
+    64 samples: the ring read and a read and write of the FP64 re/im
+    accumulators of every row and frequency)."""
+    out = {"e_pass": pass_bytes(dims, params, esize, "e"), "h_pass": pass_bytes(dims, params, esize, "h")}
+    out["tfsf"] = (st.tfsf_entries_h + st.tfsf_entries_e) * (31 + 2 * esize)
+    nd = sum(dims.n_metal_cells)
+    out["dispersive"] = nd * ((21 + (3 if dims.hydro else 0)) * esize + 16 + (48 if dims.hydro else 0))
+    every = max(params.dft_every, 1)
+    out["dft_sample"] = st.dft_rows * 2 * esize / every
+    out["dft_contract"] = st.dft_rows * (64 * esize + dims.num_freq * 32) / (64 * every)
+    out["total"] = sum(out.values())
+    return out
 
 
 BATCH_SEED = 20261203
@@ -284,7 +337,7 @@ def large_params(mod, precision=None):
         precision=mod.FDTD_FP32 if precision is None else precision)
 
 
-def large_bench(mod, torch, stream, sp, dev, blocks=2, adjoint_steps=2400):
+def large_bench(mod, torch, stream, sp, dev, blocks=2, adjoint_steps=12000):
     """Forward throughput of the large nonlocal workload over a bounded
     number of 128-step blocks (the full run is 12000 steps), and the device
     memory the simulation holds.  Its adjoint is not built: the
@@ -317,13 +370,14 @@ LARGE_DESIGN = [192 - 32, 192 + 32, 192 - 32, 192 + 32, 128, 138]  # 64 x 64 x 1
 LARGE_FREQS = [0, 1, 2, 3, 4]
 
 
-def large_adjoint_bench(mod, torch, dev, steps=2400, every=400):
-    """The adjoint at the large geometry with the local Drude+2CP model (the
-    hydrodynamic adjoint is not built): a 64 x 64 x 10 design region over
-    the central disk, rho ~ U[0, 1] from the seed, objective = AbsTot at the 5
-    wavelengths, checkpoints every 400 steps.  A bounded sample of the
-    12000-step run: `steps` steps; forward and backward throughput and the
-    device memory the checkpoints and adjoint state take."""
+def large_adjoint_bench(mod, torch, dev, steps=12000, every=400):
+    """The adjoint at the large geometry with the local Drude+2CP model: a
+    64 x 64 x 10 design region over the central disk, rho ~ U[0, 1] from
+    the seed, objective = the absorption cross-section summed over the 5
+    wavelengths, checkpoints every 400 steps, `steps` time steps (the whole
+    12000-step run by default: the pulse, delayed by 4908 steps, has passed
+    the disks); forward and backward throughput and the device memory the
+    checkpoints and adjoint state take."""
     import numpy as np
     p = large_params(mod)
     p.NONLOCAL = 0
@@ -388,15 +442,32 @@ def adjoint_bench(mod, torch, stream, dev, steps=4000, every=200):
         fw.append(t1 - t0)
         bw.append(t2 - t1)
     s.check()
+    s.close()
     f_s, b_s = statistics.median(fw), statistics.median(bw)
+    # a finite-difference check of one design cell: central differences
+    # (h = 1e-3) of the FP64 forward objective against the FP32 adjoint
+    q = adjoint_params(mod, steps, precision=mod.FDTD_FP64)
+    s64 = mod.Sim(q, device=dev)
+    rho = np.random.default_rng(BATCH_SEED).uniform(0, 1, (b[5] - b[4], b[3] - b[2], b[1] - b[0])).astype(np.float32)
+    cell = (8, 16, 16)
+    vals = []
+    for d in (1e-3, -1e-3):
+        r = rho.copy()
+        r[cell] += d
+        s64.set_design(r)
+        vals.append(s64.forward(ADJOINT_FREQS, every))
+    s64.close()
+    fd = (vals[0] - vals[1]) / 2e-3
     cells = (96 ** 3) * steps
     out = {"forward_s": round(f_s, 4), "backward_s": round(b_s, 4),
            "ratio": round(b_s / f_s, 3), "objective": L,
+           "objective_def": "absorption cross-section (m^2) summed over 550, 633, 785 nm",
            "grad_rho_max": float(np.abs(g).max()), "grad_params": [float(x) for x in gp],
+           "fd_check": {"cell": list(cell), "adjoint": float(g[cell]), "fd_fp64": fd,
+                        "rel": abs(float(g[cell]) - fd) / abs(fd)},
            "forward_gcell_steps_per_s": round(cells / f_s / 1e9, 2),
            "time_steps": steps, "checkpoint_every": every, "grid": 96, "design": [32, 32, 16],
            "timing": "host wall clock around each blocking C-ABI call, median of 3"}
-    s.close()
     return out
 
 
@@ -491,8 +562,8 @@ def main():
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-large", action="store_true")
-    ap.add_argument("--large-adjoint-steps", type=int, default=2400,
-                    help="time steps of the large-geometry adjoint sample (multiple of 400)")
+    ap.add_argument("--large-adjoint-steps", type=int, default=12000,
+                    help="time steps of the large-geometry adjoint run (multiple of 400)")
     ap.add_argument("--batch-members", type=int, default=64)
     ap.add_argument("--batch-steps", type=int, default=3000)
     ap.add_argument("--no-ref-gpu", action="store_true",
@@ -578,6 +649,9 @@ def main():
     alg_h = pass_bytes(d, p32, 4, "h")
     peak, peak_kind = measured_peak()
     achieved = alg / (kms["e_pass"] / 1e3) / 1e9
+    sb = step_bytes(d, p32, tune, 4)
+    step_ms = ms / args.steps / BLOCK
+    step_gbs = sb["total"] / (step_ms / 1e3) / 1e9
     roofline = {"bound": "hbm", "kernel": "e_pass_s<float> (Yee + CPML E pass, whole grid)",
                 "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4),
@@ -585,7 +659,12 @@ def main():
                 "alg_bytes_per_launch": alg, "launch_ms": round(kms["e_pass"], 4),
                 "peak_source": peak_kind,
                 "h_pass": {"launch_ms": round(kms["h_pass"], 4),
-                           "achieved": round(alg_h / (kms["h_pass"] / 1e3) / 1e9, 1)}}
+                           "achieved": round(alg_h / (kms["h_pass"] / 1e3) / 1e9, 1),
+                           "frac": round(alg_h / (kms["h_pass"] / 1e3) / 1e9 / peak, 4)},
+                "step": {"alg_bytes": {k: int(v) for k, v in sb.items()},
+                         "ms": round(step_ms, 5), "achieved": round(step_gbs, 1),
+                         "frac": round(step_gbs / peak, 4),
+                         "note": "all algorithmic bytes of one whole time step / (ms_per_step / 128)"}}
 
     # --- end to end through the public API with host buffers --------------
     # every bench step: pinned H2D of the block's source samples, the block,
@@ -696,6 +775,10 @@ def main():
             "reference_deck": refdeck, "batched": batched, "adjoint": adjoint,
             "large_nonlocal": large,
         }
+        if fp64 and cpu:
+            # FP64 on the GPU against the FP64 CPU restatement (the headline
+            # value is FP32)
+            fp64["vs_cpu_baseline"] = round(fp64["value"] / cpu["value"], 1)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()

@@ -15,9 +15,10 @@
 // F(p) and -a(p) to F(p - e)).  The dispersive (design) cells transpose
 // their ADE recursions locally and accumulate dL/drho and the Drude
 // parameter gradients from the forward values recorded during the segment
-// recompute.  Objective: the absorbed power (AbsTot column) summed over
-// chosen frequencies, a bilinear form of the DFT accumulators, whose
-// derivative enters at every DFT sample step.
+// recompute.  Objective: any linear combination of the ScatAbs table
+// (the totals and the 12 face fluxes at every frequency), each a bilinear
+// form of the DFT accumulators, whose derivative enters at every DFT
+// sample step.
 #pragma once
 #include "kernels.cuh"
 
@@ -41,6 +42,12 @@ struct AdjView {
   T* lEh[3];
   double* grho[3];  // dL/drho per slot
   double* gpar;     // [2]: dL/d omega_D, dL/d gamma
+  // hydrodynamic cells: adjoints of the current J and the density N of
+  // component c at time m in ring slot m % 3 (FP64, like their forward state)
+  double* lJ[3][3];
+  double* lN[3][3];
+  // hydrodynamic model: d/d gamma of d1, d2, d3, d4, dNL
+  double dgam[5];
   // derivatives of the metal coefficients: [p] = d/d omega_D, d/d gamma
   T dCE[2], dCE1[2], dCE2[2], dd1[2], dd2[2], dd3[2], dd4[2], dd5[2];
   int* step;        // adjoint clock: the step being transposed
@@ -215,6 +222,241 @@ __global__ void adj_e_design(const __grid_constant__ SimView<T> s, const __grid_
   }
 }
 
+// ---------------------------------------------------------------------
+// Hydrodynamic cells, transposed.  The forward step (kernels.cuh) is three
+// phases: hydro_p_ex computes J^{n+1} of every cell from J^n, J^{n-1},
+// E^n, E^{n-1} and the pressure term over the neighbour slots' J^n and
+// N^n, then the x cells' continuity and E update; hydro_e<1> and <2> do the
+// y and z cells, whose continuity reads the x (and y) neighbours' new J and
+// N.  Linearised about the recorded trajectory (MetalView::hrec, ::rec),
+// the reverse step runs adj_hydro_e<2>, <1>, <0> (E update and continuity
+// of each phase, in reverse order), then adj_hydro_j (the current update).
+// A slot's J or N adjoint receives terms from its neighbours, added with
+// FP64 atomics.  Design cells: J' = rho (update), N' = rho (update), the
+// coupling coefficients blended as in the local model.
+//
+// Neighbour slots per cell of component c and component a (nbr, 12 per
+// cell): a == c: +e_c, 0, -e_c, unused; a != c: +e_c, 0, +e_c - e_a, -e_a.
+
+template <typename T>
+__device__ __forceinline__ void adj_hydro_blend(const MetalView<T>& m, bool blend, double r, double& CE,
+                                                double& CE1, double& CE2, double C3[2], double C4[2],
+                                                double C5[2]) {
+  CE = m.C_E; CE1 = m.C_E_1; CE2 = m.C_E_2;
+#pragma unroll
+  for (int q = 0; q < 2; q++) { C3[q] = m.C3[q]; C4[q] = m.C4[q]; C5[q] = m.C5[q]; }
+  if (blend) {
+    CE = m.vac + r * (m.C_E - m.vac);
+    CE1 = m.vac + r * (m.C_E_1 - m.vac);
+    CE2 = r * m.C_E_2;
+#pragma unroll
+    for (int q = 0; q < 2; q++) { C3[q] = r * m.C3[q]; C4[q] = r * m.C4[q]; C5[q] = r * m.C5[q]; }
+  }
+}
+
+// The E update and the continuity of the cells of component c, transposed.
+template <typename T, int c>
+__global__ void adj_hydro_e(const __grid_constant__ SimView<T> s, const __grid_constant__ MetalView<T> m,
+                            const __grid_constant__ AdjView<T> a) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= m.n[c]) return;
+  const int4 e = m.cell[c][q];
+  const int sl = e.w;
+  const size_t id = fidx(s.PX, s.plane, e.x, e.y, e.z);
+  const int n = *a.step;
+  const int row = n % m.rec_rows;
+  const long long S = m.rec_slots;
+  const T* rec = m.rec + (size_t)row * 5 * S + m.rec_off[c] + sl;
+  const double v = (double)rec[0], e1 = (double)rec[S], nv = (double)rec[4 * S];
+  const double* h = m.hrec + (size_t)row * 6 * S;
+  const long long own = m.rec_off[c] + sl;
+  const double Jn1 = h[2 * S + own], Nm1 = h[3 * S + own], Nn1 = h[5 * S + own];
+  const bool blend = m.rho[c] != nullptr;
+  const double r = blend ? (double)m.rho[c][sl] : 1.0;
+  double CE, CE1, CE2, C3[2], C4[2], C5[2];
+  adj_hydro_blend(m, blend, r, CE, CE1, CE2, C3, C4, C5);
+  const int r1 = (n + 1) % 3, r0 = n % 3, rm = (n + 2) % 3;
+  // E update: nv = (dt/z0 curl + dt e0 J' (N_EQ + N') + CE1 v - CE2 e1 - sum (C1q-1) Pq + C2q Pqm) / CE
+  const double lnv = (double)a.lE[c][id];
+  const double aq[2] = {(double)a.lPa[c][0][sl], (double)a.lPa[c][1][sl]};
+  const double bq[2] = {(double)a.lPb[c][0][sl], (double)a.lPb[c][1][sl]};
+  const double ep = (double)a.lEh[c][sl];
+  const double mu = (lnv + C3[0] * aq[0] + C3[1] * aq[1]) / CE;
+  a.lE[c][id] = (T)(CE1 * mu + C4[0] * aq[0] + C4[1] * aq[1] + ep);
+  const int ijk[3] = {e.x, e.y, e.z};
+  const double f = m.dt / m.z0 * mu;
+#pragma unroll
+  for (int sq = 0; sq < 2; sq++) {
+    const int ax = (c + 1 + sq) % 3;
+    a.a[c][sq][id] = (T)((sq == 0 ? f : -f) * (double)ldg(s.cp[ax].inv_ked + ijk[ax]));
+  }
+#pragma unroll
+  for (int p = 0; p < 2; p++) {
+    a.lPa[c][p][sl] = (T)(bq[p] + m.C1[p] * aq[p] - (m.C1[p] - 1.0) * mu);
+    a.lPb[c][p][sl] = (T)(m.C2[p] * aq[p] - m.C2[p] * mu);
+  }
+  a.lEh[c][sl] = (T)(-CE2 * mu + C5[0] * aq[0] + C5[1] * aq[1]);
+  const double src = mu * m.dt * m.e0;
+  a.lJ[c][r1][sl] += src * (m.N_EQ + Nn1);
+  const double lNp = a.lN[c][r1][sl] + src * Jn1;  // complete: later phases have run
+  a.lN[c][r1][sl] = 0.0;
+  double g = mu * (-nv * (m.C_E - m.vac) + v * (m.C_E_1 - m.vac) - e1 * m.C_E_2);
+#pragma unroll
+  for (int p = 0; p < 2; p++) g += aq[p] * (nv * m.C3[p] + v * m.C4[p] + e1 * m.C5[p]);
+  // continuity: N' = r (N^{n-1} - k2 B), B over the neighbours' J and N at
+  // n + 1 for the components updated before c, at n for the others
+  const double rl = r * lNp;
+  a.lN[c][rm][sl] += rl;
+  const int* nb = m.nbr[c] + (size_t)q * 12;
+  double P[3][4], N[3][4];
+#pragma unroll
+  for (int b = 0; b < 3; b++) {
+    const int vj = b < c ? 2 : 1, vn = b < c ? 5 : 4;
+#pragma unroll
+    for (int x = 0; x < 4; x++) {
+      const int o = nb[b * 4 + x];
+      P[b][x] = o >= 0 ? h[vj * S + m.rec_off[b] + o] : 0.0;
+      N[b][x] = o >= 0 ? h[vn * S + m.rec_off[b] + o] : 0.0;
+    }
+  }
+  double V1[3], V2[3], N1[3], N2[3];
+#pragma unroll
+  for (int b = 0; b < 3; b++) {
+    if (b == c) {
+      V1[b] = P[b][0]; V2[b] = P[b][2]; N1[b] = N[b][0]; N2[b] = N[b][2];
+    } else {
+      V1[b] = 0.5 * (P[b][0] + P[b][1]);
+      V2[b] = 0.5 * (P[b][2] + P[b][3]);
+      N1[b] = 0.5 * (N[b][0] + N[b][1]);
+      N2[b] = 0.5 * (N[b][2] + N[b][3]);
+    }
+  }
+  const double k2 = 2.0 * m.dt * m.inv_dx;
+  double B = 0.0;
+  double dN1[3], dN2[3], dV1[3], dV2[3];  // dB / d(each averaged value)
+#pragma unroll
+  for (int b = 0; b < 3; b++) {
+    const double w = b == c ? 0.5 : 1.0;
+    if (c == 2 && b == 2) {
+      // the z form carries 0.5 (V1z - V2z) without the density factors
+      B += 0.5 * (V1[b] - V2[b]) + 0.5 * (V1[b] - V2[b]) * m.N_EQ;
+      dN1[b] = 0.0; dN2[b] = 0.0;
+      dV1[b] = 0.5 + 0.5 * m.N_EQ; dV2[b] = -(0.5 + 0.5 * m.N_EQ);
+    } else {
+      B += w * (N1[b] * V1[b] - N2[b] * V2[b]) + w * (V1[b] - V2[b]) * m.N_EQ;
+      dN1[b] = w * V1[b]; dN2[b] = -w * V2[b];
+      dV1[b] = w * (N1[b] + m.N_EQ); dV2[b] = -w * (N2[b] + m.N_EQ);
+    }
+  }
+  g += lNp * (Nm1 - k2 * B);
+  const double kk = -k2 * rl;
+#pragma unroll
+  for (int b = 0; b < 3; b++) {
+    const int ring = b < c ? r1 : r0;
+    double* lJb = a.lJ[b][ring];
+    double* lNb = a.lN[b][ring];
+    if (b == c) {
+      const int o0 = nb[b * 4 + 0], o2 = nb[b * 4 + 2];
+      if (o0 >= 0) { atomicAdd(lJb + o0, kk * dV1[b]); atomicAdd(lNb + o0, kk * dN1[b]); }
+      if (o2 >= 0) { atomicAdd(lJb + o2, kk * dV2[b]); atomicAdd(lNb + o2, kk * dN2[b]); }
+    } else {
+#pragma unroll
+      for (int x = 0; x < 4; x++) {
+        const int o = nb[b * 4 + x];
+        if (o < 0) continue;
+        const double dv = x < 2 ? dV1[b] : dV2[b], dn = x < 2 ? dN1[b] : dN2[b];
+        atomicAdd(lJb + o, 0.5 * kk * dv);
+        atomicAdd(lNb + o, 0.5 * kk * dn);
+      }
+    }
+  }
+  a.grho[c][sl] += g;
+}
+
+// The current update of every hydrodynamic cell, transposed:
+// J' = r (d1 J + d2 Jm + d3 E + d4 Em + dNL (gd + gd2 / N_EQ) / cb), gd and
+// gd2 the stencil sums of J and of J N over the neighbour slots at time n,
+// cb = (N_EQ + N)^(1/3) of the cell (the reference's FP32 powf is locally
+// constant in N; with the cube-root fix its derivative is kept).
+template <typename T>
+__global__ void adj_hydro_j(const __grid_constant__ SimView<T> s, const __grid_constant__ MetalView<T> m,
+                            const __grid_constant__ AdjView<T> a) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  int c = 0;
+  while (c < 3 && q >= m.n[c]) { q -= m.n[c]; c++; }
+  double gg = 0.0;
+  if (c < 3) {
+    const int4 e = m.cell[c][q];
+    const int sl = e.w;
+    const size_t id = fidx(s.PX, s.plane, e.x, e.y, e.z);
+    const int n = *a.step;
+    const int row = n % m.rec_rows;
+    const long long S = m.rec_slots;
+    const T* rec = m.rec + (size_t)row * 5 * S + m.rec_off[c] + sl;
+    const double v = (double)rec[0], e1 = (double)rec[S];
+    const double* h = m.hrec + (size_t)row * 6 * S;
+    const long long own = m.rec_off[c] + sl;
+    const double Jm = h[own], J = h[S + own];
+    const int r1 = (n + 1) % 3, r0 = n % 3, rm = (n + 2) % 3;
+    const double lJp = a.lJ[c][r1][sl];
+    a.lJ[c][r1][sl] = 0.0;
+    const bool blend = m.rho[c] != nullptr;
+    const double r = blend ? (double)m.rho[c][sl] : 1.0;
+    const double rl = r * lJp;
+    atomicAdd(a.lJ[c][r0] + sl, m.d1 * rl);
+    a.lJ[c][rm][sl] += m.d2 * rl;
+    a.lE[c][id] += (T)(m.d3 * rl);
+    a.lEh[c][sl] += (T)(m.d4 * rl);
+    // pressure term over the neighbour slots at time n
+    const int* nb = m.nbr[c] + (size_t)q * 12;
+    const double I3[3] = {m.inv_dx, m.inv_dy, m.inv_dz};
+    double wgt[3][4], P[3][4], N[3][4];
+#pragma unroll
+    for (int b = 0; b < 3; b++) {
+      const double kb = b == c ? I3[c] * I3[c] : I3[b < c ? b : c] * I3[b < c ? c : b];
+      if (b == c) { wgt[b][0] = kb; wgt[b][1] = -2.0 * kb; wgt[b][2] = kb; wgt[b][3] = 0.0; }
+      else { wgt[b][0] = kb; wgt[b][1] = -kb; wgt[b][2] = -kb; wgt[b][3] = kb; }
+#pragma unroll
+      for (int x = 0; x < 4; x++) {
+        const int o = nb[b * 4 + x];
+        P[b][x] = o >= 0 ? h[S + m.rec_off[b] + o] : 0.0;
+        N[b][x] = o >= 0 ? h[4 * S + m.rec_off[b] + o] : 0.0;
+      }
+    }
+    double gd = 0.0, gd2 = 0.0;
+#pragma unroll
+    for (int b = 0; b < 3; b++)
+#pragma unroll
+      for (int x = 0; x < 4; x++) { gd += wgt[b][x] * P[b][x]; gd2 += wgt[b][x] * P[b][x] * N[b][x]; }
+    const double ND1 = m.N_EQ + N[c][1];
+    const double cb = m.fix_cbrt ? cbrt(ND1) : (double)powf((float)ND1, (float)(1.0 / 3.0));
+    const double pr = (gd + gd2 / m.N_EQ) / cb;
+    const double gp = rl * m.dNL / cb;
+#pragma unroll
+    for (int b = 0; b < 3; b++)
+#pragma unroll
+      for (int x = 0; x < 4; x++) {
+        const int o = nb[b * 4 + x];
+        if (o < 0 || wgt[b][x] == 0.0) continue;
+        atomicAdd(a.lJ[b][r0] + o, gp * wgt[b][x] * (1.0 + N[b][x] / m.N_EQ));
+        atomicAdd(a.lN[b][r0] + o, gp * wgt[b][x] * P[b][x] / m.N_EQ);
+      }
+    if (m.fix_cbrt) atomicAdd(a.lN[c][r0] + sl, -rl * m.dNL * pr / (3.0 * ND1));
+    a.grho[c][sl] += lJp * (m.d1 * J + m.d2 * Jm + m.d3 * v + m.d4 * e1 + m.dNL * pr);
+    gg = rl * (a.dgam[0] * J + a.dgam[1] * Jm + a.dgam[2] * v + a.dgam[3] * e1 + a.dgam[4] * pr);
+  }
+  __shared__ double red[32];
+  for (int o = 16; o > 0; o >>= 1) gg += __shfl_down_sync(0xffffffffu, gg, o);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) red[w] = gg;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0;
+    for (int x = 0; x < (int)(blockDim.x >> 5); x++) t += red[x];
+    if (t != 0.0) atomicAdd(a.gpar + 1, t);
+  }
+}
+
 // lambda_H += gather of the E-sub-step coefficients: H component h is read
 // by the E components c != h through D = H_h(p) - H_h(p - e_ax), ax the
 // third axis.
@@ -312,15 +554,17 @@ __global__ void adj_gather_e(const __grid_constant__ SimView<T> s, const __grid_
   a.lE[2][id] += (py ? a.a[0][0][id - sy] : T(0)) - a.a[0][0][id] + (px ? a.a[1][1][id - sx] : T(0)) - a.a[1][1][id];
 }
 
-// Objective derivative at a DFT sample step n: for every absorption-box
-// face cell and tangential component, g = sum_m Re(P_m conj(w_m)) with
-// w_m = exp(i 2 pi (n + delta) dt f_m) (delta = 1 for E, 1/2 for H) and
-// P_m the weighted partner accumulator (adj_partner).
+// Objective derivative at a DFT sample step n: for every flux-face cell and
+// tangential component of the faces in face_mask (bit b*6+f: box b, face
+// f), g = sum_m Re(P_m conj(w_m)) with w_m = exp(i 2 pi (n + delta) dt f_m)
+// (delta = 1 for E, 1/2 for H) and P_m the weighted partner accumulator
+// (adj_partner).
 template <typename T>
 __global__ void adj_source(const __grid_constant__ SimView<T> s, const __grid_constant__ DftView d,
                            const __grid_constant__ AdjView<T> a, const double2* __restrict__ P,
-                           const double* __restrict__ fsel, int nsel, long long prows) {
-  const int f = blockIdx.y;  // absorption-box faces 0..5
+                           const double* __restrict__ fsel, int nsel, long long prows, unsigned face_mask) {
+  const int f = blockIdx.y;  // faces 0..11 (absorption box, then scattering box)
+  if (!((face_mask >> f) & 1u)) return;
   const DftFace F = d.face[f];
   const int nc = F.na * F.nb;
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
@@ -351,11 +595,13 @@ __global__ void adj_source(const __grid_constant__ SimView<T> s, const __grid_co
   }
 }
 
-// Weighted partner accumulators of the absorption-box rows for the chosen
-// frequencies: AbsTot = sum_f sgn_f dxy/|Einc|^2 sum Re(Ex conj(Hy) - Ey
-// conj(Hx)) (per face pairing), so d/d(sample of Ex) pairs with Hy, etc.
+// Weighted partner accumulators of the flux-face rows for the chosen
+// frequencies.  Face flux Q_f(m) = sum Re(Ex conj(Hy) - Ey conj(Hx)) (per
+// face pairing) is bilinear in the accumulators, so dQ/d(sample of Ex)
+// pairs with Hy, etc.; wface[m * 12 + f] = dL/dQ_f(m), zero for faces the
+// objective does not read.
 __global__ void adj_partner(const __grid_constant__ DftView d, const int* __restrict__ sel,
-                            const double* __restrict__ wsel, int nsel, double2* __restrict__ P, long long prows) {
+                            const double* __restrict__ wface, int nsel, double2* __restrict__ P, long long prows) {
   const int f = blockIdx.y;
   const int m = blockIdx.z;
   const DftFace F = d.face[f];
@@ -363,7 +609,7 @@ __global__ void adj_partner(const __grid_constant__ DftView d, const int* __rest
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= nc || m >= nsel) return;
   const int qx = F.ax == 1 ? 1 : 0, qy = F.ax == 1 ? 0 : 1;
-  const double K = ((f & 1) ? 1.0 : -1.0) * wsel[m];
+  const double K = wface[(size_t)m * 12 + f];
   const int fm = sel[m];
 #pragma unroll
   for (int cs = 0; cs < 4; cs++) {

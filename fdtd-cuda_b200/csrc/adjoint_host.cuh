@@ -20,17 +20,30 @@ struct fdtd_sim::Adjoint {
   size_t ck_bytes = 0;
   std::unique_ptr<DevBuf> ck;  // nseg * ck_bytes
   int every = 0, nseg = 0, tend = 0;
-  // objective
+  // objective: weights on the ScatAbs table (fdtd_forward's own, for
+  // fdtd_backward), the frequencies with a nonzero weight and the faces the
+  // objective reads (bit b*6+f)
+  std::vector<double> G;
   std::vector<int> sel;
+  unsigned face_mask = 0;
   double objective = 0;
-  bool forward_done = false;
-  std::unique_ptr<DevBuf> P, fsel;  // weighted partner accumulators, chosen frequencies
+  bool forward_done = false, has_objective = false;
+  std::unique_ptr<DevBuf> P, fsel;  // weighted partner accumulators; face weights, frequencies
+  bool obj_is_G = false;  // the partner accumulators are those of G
+  struct ObjSig {
+    int nsel = -1;
+    unsigned mask = 0;
+    const void* P = nullptr;
+    const void* fsel = nullptr;
+    bool operator==(const ObjSig& o) const { return nsel == o.nsel && mask == o.mask && P == o.P && fsel == o.fsel; }
+  } sig;
   // adjoint state (allocated on the first backward)
   bool ready = false;
   void* view = nullptr;  // AdjView<T> on the host, as bytes
   std::vector<char> view_bytes;
   std::vector<std::pair<void*, size_t>> zero;  // buffers zeroed before each sweep
   void* rec = nullptr;
+  double* hrec = nullptr;  // hydrodynamic cells' record (MetalView::hrec)
   long long rec_slots = 0;
   int rec_off[3] = {0, 0, 0};
   double* grho[3] = {nullptr, nullptr, nullptr};
@@ -89,32 +102,28 @@ extern "C" fdtd_status fdtd_set_design(fdtd_sim* s, const int box[6], const floa
 
 static fdtd_status adj_checks(fdtd_sim* s) {
   if (!s->has_design) return fail(FDTD_ERR_STATE, "the simulation was created without params.design_box");
-  if (s->su.hydro) return fail(FDTD_ERR_UNSUPPORTED, "the adjoint needs the local (non-hydrodynamic) model");
   if (s->pml_metal) return fail(FDTD_ERR_UNSUPPORTED, "the adjoint needs every dispersive cell outside the CPML");
   if (!s->dft_on || s->line.dft_every <= 0) return fail(FDTD_ERR_STATE, "the objective needs the DFT (StaticField = 0)");
   return FDTD_OK;
 }
 
-extern "C" fdtd_status fdtd_forward(fdtd_sim* s, const int* freq_idx, int nfreq, int checkpoint_every,
-                                    double* objective) {
-  if (!s || !freq_idx || nfreq <= 0 || checkpoint_every <= 0 || !objective)
-    return fail(FDTD_ERR_INVALID, "bad argument");
-  fdtd_status st = adj_checks(s);
-  if (st != FDTD_OK) return st;
-  const int nf = s->dft.nf;
-  for (int m = 0; m < nfreq; m++)
-    if (freq_idx[m] < 0 || freq_idx[m] >= nf) return fail(FDTD_ERR_INVALID, "frequency index out of range");
+// The checkpointed forward: every field, auxiliary state and accumulator
+// zeroed, then the whole time loop t = 0..Tend with a copy of the state
+// (without the DFT accumulators, the sample ring and the probe record) at
+// the start of every segment of checkpoint_every steps.  The DFT
+// accumulators of the run stay in place for the objective.
+static fdtd_status adj_forward_run(fdtd_sim* s, int checkpoint_every) {
   if (!s->adj) s->adj = std::make_unique<fdtd_sim::Adjoint>();
   fdtd_sim::Adjoint& A = *s->adj;
-  A.sel.assign(freq_idx, freq_idx + nfreq);
   A.forward_done = false;
-  A.drop_graphs();  // they hold the partner buffer and the segment length
-  if (A.ready && A.every != checkpoint_every) A.ready = false;  // the record depth follows the segment
-  st = fdtd_reset(s);
+  A.has_objective = false;
+  if (A.every != checkpoint_every) {
+    A.drop_graphs();  // they hold the segment length
+    A.ready = false;  // the record depth follows the segment
+  }
+  fdtd_status st = fdtd_reset(s);
   if (st != FDTD_OK) return st;
   CUDA_TRY(cudaSetDevice(s->device));
-  // checkpointed buffers: the state without the DFT accumulators, the
-  // sample ring and the probe record
   A.ck_bufs.clear();
   A.ck_bytes = 0;
   const void* skip[4] = {s->dft.acc_re, s->dft.acc_im, s->ring, s->probe};
@@ -145,27 +154,66 @@ extern "C" fdtd_status fdtd_forward(fdtd_sim* s, const int* freq_idx, int nfreq,
     if (st != FDTD_OK) return st;
   }
   CUDA_TRY(cudaDeviceSynchronize());
-  // objective: AbsTot (ScatAbs column 2) summed over the chosen frequencies
-  std::vector<double> rows((size_t)nf * 19);
-  st = fdtd_spectral_finalize(s, rows.data());
-  if (st != FDTD_OK) return st;
-  A.objective = 0;
-  for (int m : A.sel) A.objective += rows[(size_t)m * 19 + 2];
-  *objective = A.objective;
-  // d AbsTot / d(face flux sum) per chosen frequency (CalculateAbsScatt)
+  A.forward_done = true;
+  return FDTD_OK;
+}
+
+// The objective L = sum_m sum_c G[m][c] spectra[m][c] over the ScatAbs
+// table of fdtd_spectral_finalize.  Its columns are linear in the 12 face
+// fluxes Q_f(m) (flux_reduce) scaled by dxy / |E_inc(m)|^2:
+//   faces   col 4 + f = q_sca,f, col 10 + f = q_abs,f
+//   totals  col 1 = sum_f s_f q_sca,f (/ pi r^2 for the reference's
+//           sphere), col 2 = sum_f s_f q_abs,f (x -1 / pi r^2 for the
+//           sphere), col 3 = col 1 + col 2, with s_f = -1, +1 for the -, +
+//           face of each axis (Spectral.cu:1145-1168),
+// so dL/dQ_f(m) follows from G by the chain rule.  Frequencies whose
+// weights are all zero are dropped; the partner accumulators of the rest
+// are built for the reverse sweep.
+static fdtd_status adj_objective(fdtd_sim* s, const double* G) {
+  fdtd_sim::Adjoint& A = *s->adj;
+  const int nf = s->dft.nf;
   const Setup& su = s->su;
-  const bool sphere = su.p.geometry == FDTD_GEOM_REFERENCE && su.p.nano_sphere == 1;
-  std::vector<double> w(nfreq), fs(nfreq);
-  for (int m = 0; m < nfreq; m++) {
-    const double amp = std::abs(su.Einc[A.sel[m]]);
-    w[m] = su.p.dx * su.p.dy / (amp * amp);
-    if (sphere) w[m] *= -1.0 / (su.pi * su.p.nano_sphere_radius * su.p.nano_sphere_radius);
-    fs[m] = su.freq[A.sel[m]];
+  for (int m = 0; m < nf; m++) {
+    const double* g = G + (size_t)m * 19;
+    if (g[0] != 0.0 || g[16] != 0.0 || g[17] != 0.0 || g[18] != 0.0)
+      return fail(FDTD_ERR_INVALID, "dL_dspectra: columns 0 and 16-18 (wavelength, incident field) must be zero");
+    for (int c = 1; c < 16; c++)
+      if (!std::isfinite(g[c])) return fail(FDTD_ERR_INVALID, "dL_dspectra holds a non-finite value");
   }
-  // partner accumulators and the frequency list, kept across forwards (an
-  // allocation per forward would synchronise the device)
-  const size_t pbytes = (size_t)nfreq * s->dft.rows * sizeof(double2);
-  const size_t fbytes = (size_t)nfreq * (2 * sizeof(double) + sizeof(int));
+  const bool sphere = su.p.geometry == FDTD_GEOM_REFERENCE && su.p.nano_sphere == 1;
+  const double area = sphere ? su.pi * su.p.nano_sphere_radius * su.p.nano_sphere_radius : 1.0;
+  const double sca_scale = sphere ? 1.0 / area : 1.0, abs_scale = sphere ? -1.0 / area : 1.0;
+  const double dxy = su.p.dx * su.p.dy;
+  A.sel.clear();
+  std::vector<double> wface, fs;
+  unsigned mask = 0;
+  for (int m = 0; m < nf; m++) {
+    const double* g = G + (size_t)m * 19;
+    const double amp = std::abs(su.Einc[m]);
+    const double w = dxy / (amp * amp);
+    double k[12];
+    bool any = false;
+    for (int b = 0; b < 2; b++)
+      for (int f = 0; f < 6; f++) {
+        const double sf = (f & 1) ? 1.0 : -1.0;
+        const double v = b == 1 ? g[4 + f] + sf * (g[1] + g[3]) * sca_scale
+                                : g[10 + f] + sf * (g[2] + g[3]) * abs_scale;
+        k[b * 6 + f] = w * v;
+        if (v != 0.0) { any = true; mask |= 1u << (b * 6 + f); }
+      }
+    if (!any) continue;
+    A.sel.push_back(m);
+    wface.insert(wface.end(), k, k + 12);
+    fs.push_back(su.freq[m]);
+  }
+  const int nsel = (int)A.sel.size();
+  A.face_mask = mask;
+  A.has_objective = true;
+  if (nsel == 0) return FDTD_OK;
+  // partner accumulators and the frequency list, kept across calls (an
+  // allocation per call would synchronise the device)
+  const size_t pbytes = (size_t)nsel * s->dft.rows * sizeof(double2);
+  const size_t fbytes = (size_t)nsel * (13 * sizeof(double) + sizeof(int));
   if (!A.P || A.P->bytes < pbytes) {
     A.P.reset();
     auto b = std::make_unique<DevBuf>();
@@ -179,24 +227,75 @@ extern "C" fdtd_status fdtd_forward(fdtd_sim* s, const int* freq_idx, int nfreq,
     A.fsel = std::move(b);
   }
   double* dw = static_cast<double*>(A.fsel->p);
-  double* dfs = dw + nfreq;
-  int* dsel = reinterpret_cast<int*>(dfs + nfreq);
-  CUDA_TRY(cudaMemcpy(dw, w.data(), nfreq * sizeof(double), cudaMemcpyHostToDevice));
-  CUDA_TRY(cudaMemcpy(dfs, fs.data(), nfreq * sizeof(double), cudaMemcpyHostToDevice));
-  CUDA_TRY(cudaMemcpy(dsel, A.sel.data(), nfreq * sizeof(int), cudaMemcpyHostToDevice));
+  double* dfs = dw + (size_t)nsel * 12;
+  int* dsel = reinterpret_cast<int*>(dfs + nsel);
+  CUDA_TRY(cudaMemcpy(dw, wface.data(), wface.size() * sizeof(double), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(dfs, fs.data(), nsel * sizeof(double), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(dsel, A.sel.data(), nsel * sizeof(int), cudaMemcpyHostToDevice));
   int maxn = 0;
-  for (int f = 0; f < 6; f++) maxn = std::max(maxn, s->dft.face[f].na * s->dft.face[f].nb);
-  adj_partner<<<dim3((maxn + 255) / 256, 6, nfreq), 256>>>(s->dft, dsel, dw, nfreq, static_cast<double2*>(A.P->p),
-                                                          s->dft.rows);
+  for (int f = 0; f < 12; f++) maxn = std::max(maxn, s->dft.face[f].na * s->dft.face[f].nb);
+  adj_partner<<<dim3((maxn + 255) / 256, 12, nsel), 256>>>(s->dft, dsel, dw, nsel, static_cast<double2*>(A.P->p),
+                                                           s->dft.rows);
+  // the reverse-sweep graph holds the selection's size, face mask and
+  // buffers (their contents are read at replay)
+  const fdtd_sim::Adjoint::ObjSig sig{nsel, mask, A.P->p, A.fsel->p};
+  if (!(sig == A.sig)) A.drop_graphs();
+  A.sig = sig;
   CUDA_TRY(cudaGetLastError());
   CUDA_TRY(cudaDeviceSynchronize());
-  A.forward_done = true;
   return FDTD_OK;
+}
+
+extern "C" fdtd_status fdtd_forward_spectra(fdtd_sim* s, int checkpoint_every, double* out19) {
+  if (!s || checkpoint_every <= 0) return fail(FDTD_ERR_INVALID, "bad argument");
+  fdtd_status st = adj_checks(s);
+  if (st != FDTD_OK) return st;
+  st = adj_forward_run(s, checkpoint_every);
+  if (st != FDTD_OK) return st;
+  s->adj->G.clear();  // no objective of its own: fdtd_backward_spectra supplies one
+  if (out19) return fdtd_spectral_finalize(s, out19);
+  return FDTD_OK;
+}
+
+extern "C" fdtd_status fdtd_forward(fdtd_sim* s, const int* freq_idx, int nfreq, int checkpoint_every,
+                                    double* objective) {
+  if (!s || !freq_idx || nfreq <= 0 || checkpoint_every <= 0 || !objective)
+    return fail(FDTD_ERR_INVALID, "bad argument");
+  fdtd_status st = adj_checks(s);
+  if (st != FDTD_OK) return st;
+  const int nf = s->dft.nf;
+  for (int m = 0; m < nfreq; m++)
+    if (freq_idx[m] < 0 || freq_idx[m] >= nf) return fail(FDTD_ERR_INVALID, "frequency index out of range");
+  st = adj_forward_run(s, checkpoint_every);
+  if (st != FDTD_OK) return st;
+  std::vector<double> rows((size_t)nf * 19);
+  st = fdtd_spectral_finalize(s, rows.data());
+  if (st != FDTD_OK) return st;
+  // absorption cross-section sigma_abs(m) = P_abs / I_inc: the net inward
+  // flux through the absorption box, -sum_f s_f q_abs,f (positive for an
+  // absorbing structure whatever the geometry)
+  fdtd_sim::Adjoint& A = *s->adj;
+  A.G.assign((size_t)nf * 19, 0.0);
+  double L = 0;
+  for (int q = 0; q < nfreq; q++) {
+    const int m = freq_idx[q];
+    for (int f = 0; f < 6; f++) {
+      const double w = (f & 1) ? -1.0 : 1.0;
+      A.G[(size_t)m * 19 + 10 + f] += w;
+      L += w * rows[(size_t)m * 19 + 10 + f];
+    }
+  }
+  A.objective = L;
+  *objective = L;
+  st = adj_objective(s, A.G.data());
+  A.obj_is_G = st == FDTD_OK;
+  return st;
 }
 
 template <typename T>
 static fdtd_status adj_prepare(fdtd_sim* s) {
   fdtd_sim::Adjoint& A = *s->adj;
+  A.drop_graphs();  // they hold the buffers released here
   A.bufs.clear();  // a re-preparation (another checkpoint interval) starts afresh
   A.zero.clear();
   AdjView<T> a;
@@ -237,6 +336,13 @@ static fdtd_status adj_prepare(fdtd_sim* s) {
     A.rec_off[c] = (int)slots;
     slots += s->nmetal[c];
   }
+  if (su.hydro) {
+    for (int c = 0; c < 3; c++)
+      for (int r = 0; r < 3; r++) {
+        CUDA_TRY(A.alloc(&a.lJ[c][r], std::max(1, s->nmetal[c]), true));
+        CUDA_TRY(A.alloc(&a.lN[c][r], std::max(1, s->nmetal[c]), true));
+      }
+  }
   CUDA_TRY(A.alloc(&a.gpar, 2, true));
   A.gpar = a.gpar;
   CUDA_TRY(A.alloc(&a.step, 1, false));
@@ -246,6 +352,12 @@ static fdtd_status adj_prepare(fdtd_sim* s) {
   T* rec;
   CUDA_TRY(A.alloc(&rec, (size_t)A.every * 5 * A.rec_slots, false));
   A.rec = rec;
+  A.hrec = nullptr;
+  if (su.hydro) {
+    double* hr;
+    CUDA_TRY(A.alloc(&hr, (size_t)A.every * 6 * A.rec_slots, false));
+    A.hrec = hr;
+  }
   // derivatives of the metal's coupling and dynamics coefficients with
   // respect to omega_D and gamma (ade_coefficients, non-hydrodynamic form)
   const double dt = su.dt, wD = su.wD, gam = su.gam;
@@ -260,6 +372,13 @@ static fdtd_status adj_prepare(fdtd_sim* s) {
     a.dd3[p] = (T)dd3[p]; a.dd4[p] = (T)dd4[p]; a.dd5[p] = (T)dd5[p];
     a.dCE[p] = (T)dd3[p]; a.dCE1[p] = (T)(-dd4[p]); a.dCE2[p] = (T)dd5[p];
   }
+  // hydrodynamic model: gamma enters d1..d4 and dNL through dd (omega_D does
+  // not enter; the equilibrium density N_EQ is its own constant)
+  a.dgam[0] = -su.d1 * g1 / dd;
+  a.dgam[1] = g1 * (1.0 - su.d2) / dd;
+  a.dgam[2] = -su.d3 * g1 / dd;
+  a.dgam[3] = -su.d4 * g1 / dd;
+  a.dgam[4] = -su.dNL * g1 / dd;
   A.view_bytes.assign(reinterpret_cast<const char*>(&a), reinterpret_cast<const char*>(&a) + sizeof(a));
   A.ready = true;
   return FDTD_OK;
@@ -272,6 +391,7 @@ static fdtd_status adj_sweep(fdtd_sim* s) {
   for (const auto& z : A.zero) CUDA_TRY(cudaMemset(z.first, 0, z.second));
   MetalView<T>& m = mview<T>(s);
   m.rec = static_cast<T*>(A.rec);
+  m.hrec = A.hrec;
   m.rec_rows = A.every;
   m.rec_slots = A.rec_slots;
   for (int c = 0; c < 3; c++) m.rec_off[c] = A.rec_off[c];
@@ -283,8 +403,9 @@ static fdtd_status adj_sweep(fdtd_sim* s) {
   const unsigned gc = (unsigned)((ncell + 255) / 256);
   const int ntot = s->nmetal[0] + s->nmetal[1] + s->nmetal[2];
   int maxn = 0;
-  for (int f = 0; f < 6; f++) maxn = std::max(maxn, s->dft.face[f].na * s->dft.face[f].nb);
-  const double* fsel = static_cast<const double*>(A.fsel->p) + A.sel.size();
+  for (int f = 0; f < 12; f++) maxn = std::max(maxn, s->dft.face[f].na * s->dft.face[f].nb);
+  const int nsel = (int)A.sel.size();
+  const double* fsel = static_cast<const double*>(A.fsel->p) + (size_t)nsel * 12;
   const int total = A.tend + 1;
   // fused gathers (the default; FDTD_ADJ_FUSED=0 selects the coefficient
   // arrays everywhere) need chh == 1
@@ -305,33 +426,45 @@ static fdtd_status adj_sweep(fdtd_sim* s) {
   }
   const dim3 gtile((unsigned)((s->NX + 31) / 32), (unsigned)((s->NY + 7) / 8), (unsigned)s->NZ);
   if (fused) adj_build_flags<T><<<gtile, dim3(32, 8)>>>(view<T>(s), a.flags);
+  // the dispersive cells' transposed update: the local model in one
+  // launch; the hydrodynamic model as its three phases in reverse order,
+  // then the current update
+  const bool hydro = s->su.hydro;
+  auto launch_design = [&](cudaStream_t stream) -> int {
+    if (!hydro) {
+      adj_e_design<T><<<(ntot + 127) / 128, 128, 0, stream>>>(view<T>(s), m, a, static_cast<const T*>(A.rec), A.every);
+      return 1;
+    }
+    int k = 0;
+    if (s->nmetal[2] > 0) { adj_hydro_e<T, 2><<<(s->nmetal[2] + 127) / 128, 128, 0, stream>>>(view<T>(s), m, a); k++; }
+    if (s->nmetal[1] > 0) { adj_hydro_e<T, 1><<<(s->nmetal[1] + 127) / 128, 128, 0, stream>>>(view<T>(s), m, a); k++; }
+    if (s->nmetal[0] > 0) { adj_hydro_e<T, 0><<<(s->nmetal[0] + 127) / 128, 128, 0, stream>>>(view<T>(s), m, a); k++; }
+    adj_hydro_j<T><<<(ntot + 127) / 128, 128, 0, stream>>>(view<T>(s), m, a);
+    return k + 1;
+  };
   auto adj_step = [&](int n, cudaStream_t stream) {
     if (n % every_dft == 0)
-      adj_source<T><<<dim3((maxn + 255) / 256, 6), 256, 0, stream>>>(view<T>(s), s->dft, a,
-                                                                      static_cast<const double2*>(A.P->p), fsel,
-                                                                      (int)A.sel.size(), s->dft.rows);
+      adj_source<T><<<dim3((maxn + 255) / 256, 12), 256, 0, stream>>>(view<T>(s), s->dft, a,
+                                                                       static_cast<const double2*>(A.P->p), fsel,
+                                                                       nsel, s->dft.rows, A.face_mask);
     if (fused) {
       if (she.total() > 0)
         adj_e_slab<T><<<(unsigned)((she.total() + 255) / 256), 256, 0, stream>>>(view<T>(s), a, she);
-      if (ntot > 0)
-        adj_e_design<T><<<(ntot + 127) / 128, 128, 0, stream>>>(view<T>(s), m, a, static_cast<const T*>(A.rec),
-                                                                A.every);
+      const int kd = ntot > 0 ? launch_design(stream) : 0;
       adj_gather_h_fused<T><<<gtile, dim3(32, 8), 0, stream>>>(view<T>(s), a);
       if (shh.total() > 0)
         adj_h_slab<T><<<(unsigned)((shh.total() + 255) / 256), 256, 0, stream>>>(view<T>(s), a, shh);
       adj_gather_e_fused<T><<<gtile, dim3(32, 8), 0, stream>>>(view<T>(s), a);
       adj_step_back<<<1, 1, 0, stream>>>(A.step);
-      return 4 + (she.total() > 0) + (shh.total() > 0) + (ntot > 0) + (n % every_dft == 0);
+      return 4 + (she.total() > 0) + (shh.total() > 0) + kd + (n % every_dft == 0);
     }
     adj_e_coef<T><<<gc, 256, 0, stream>>>(view<T>(s), a);
-    if (ntot > 0)
-      adj_e_design<T><<<(ntot + 127) / 128, 128, 0, stream>>>(view<T>(s), m, a, static_cast<const T*>(A.rec),
-                                                              A.every);
+    const int kd = ntot > 0 ? launch_design(stream) : 0;
     adj_gather_h<T><<<gc, 256, 0, stream>>>(view<T>(s), a);
     adj_h_coef<T><<<gc, 256, 0, stream>>>(view<T>(s), a);
     adj_gather_e<T><<<gc, 256, 0, stream>>>(view<T>(s), a);
     adj_step_back<<<1, 1, 0, stream>>>(A.step);
-    return 6 + (ntot > 0) + (n % every_dft == 0);
+    return 5 + kd + (n % every_dft == 0);
   };
   if (!A.cap) CUDA_TRY(cudaStreamCreateWithFlags(&A.cap, cudaStreamNonBlocking));
   fdtd_status st = FDTD_OK;
@@ -385,21 +518,22 @@ static fdtd_status adj_sweep(fdtd_sim* s) {
     CUDA_TRY(cudaGetLastError());
   }
   m.rec = nullptr;
+  m.hrec = nullptr;
   s->line.dft_every = every_dft;
   s->use_graphs = graphs;
   CUDA_TRY(cudaDeviceSynchronize());
   return st;
 }
 
-extern "C" fdtd_status fdtd_backward(fdtd_sim* s, float* dL_drho, size_t count, double* dL_dparams) {
-  if (!s) return fail(FDTD_ERR_INVALID, "null argument");
-  fdtd_status st = adj_checks(s);
-  if (st != FDTD_OK) return st;
-  if (!s->adj || !s->adj->forward_done) return fail(FDTD_ERR_STATE, "fdtd_backward needs a completed fdtd_forward");
+static fdtd_status adj_backward(fdtd_sim* s, float* dL_drho, size_t count, double* dL_dparams) {
   if (dL_drho && count != s->dslot[0].size()) return fail(FDTD_ERR_INVALID, "count must be the design box's cell count");
-  CUDA_TRY(cudaSetDevice(s->device));
-  CUDA_TRY(cudaDeviceSynchronize());
   fdtd_sim::Adjoint& A = *s->adj;
+  if (A.sel.empty()) {  // the objective reads no field: every gradient is zero
+    if (dL_drho) std::fill(dL_drho, dL_drho + count, 0.0f);
+    if (dL_dparams) dL_dparams[0] = dL_dparams[1] = 0.0;
+    return FDTD_OK;
+  }
+  fdtd_status st;
   if (!A.ready) {
     st = s->fp64 ? adj_prepare<double>(s) : adj_prepare<float>(s);
     if (st != FDTD_OK) return st;
@@ -421,4 +555,36 @@ extern "C" fdtd_status fdtd_backward(fdtd_sim* s, float* dL_drho, size_t count, 
   }
   if (dL_dparams) CUDA_TRY(cudaMemcpy(dL_dparams, A.gpar, 2 * sizeof(double), cudaMemcpyDeviceToHost));
   return FDTD_OK;
+}
+
+extern "C" fdtd_status fdtd_backward(fdtd_sim* s, float* dL_drho, size_t count, double* dL_dparams) {
+  if (!s) return fail(FDTD_ERR_INVALID, "null argument");
+  fdtd_status st = adj_checks(s);
+  if (st != FDTD_OK) return st;
+  if (!s->adj || !s->adj->forward_done) return fail(FDTD_ERR_STATE, "fdtd_backward needs a completed fdtd_forward");
+  if (s->adj->G.empty()) return fail(FDTD_ERR_STATE, "fdtd_backward needs the objective of fdtd_forward "
+                                                     "(after fdtd_forward_spectra use fdtd_backward_spectra)");
+  CUDA_TRY(cudaSetDevice(s->device));
+  CUDA_TRY(cudaDeviceSynchronize());
+  if (!s->adj->has_objective || !s->adj->obj_is_G) {
+    st = adj_objective(s, s->adj->G.data());
+    if (st != FDTD_OK) return st;
+    s->adj->obj_is_G = true;
+  }
+  return adj_backward(s, dL_drho, count, dL_dparams);
+}
+
+extern "C" fdtd_status fdtd_backward_spectra(fdtd_sim* s, const double* dL_dspectra, float* dL_drho, size_t count,
+                                             double* dL_dparams) {
+  if (!s || !dL_dspectra) return fail(FDTD_ERR_INVALID, "null argument");
+  fdtd_status st = adj_checks(s);
+  if (st != FDTD_OK) return st;
+  if (!s->adj || !s->adj->forward_done)
+    return fail(FDTD_ERR_STATE, "fdtd_backward_spectra needs a completed fdtd_forward_spectra or fdtd_forward");
+  CUDA_TRY(cudaSetDevice(s->device));
+  CUDA_TRY(cudaDeviceSynchronize());
+  s->adj->obj_is_G = false;
+  st = adj_objective(s, dL_dspectra);
+  if (st != FDTD_OK) return st;
+  return adj_backward(s, dL_drho, count, dL_dparams);
 }

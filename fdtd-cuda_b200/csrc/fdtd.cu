@@ -106,7 +106,6 @@ struct fdtd_sim {
   // dispersive cells
   int nmetal[3] = {0, 0, 0};
   int4* mcell[3] = {nullptr, nullptr, nullptr};
-  void* mstate = nullptr;  // SoA state
   int* nbr[3] = {nullptr, nullptr, nullptr};  // hydrodynamic neighbour slots
   // DFT
   DftView dft;
@@ -377,20 +376,22 @@ static fdtd_status build_views(fdtd_sim* s) {
   for (int c = 0; c < 3; c++) { m.n[c] = s->nmetal[c]; m.cell[c] = s->mcell[c]; }
   size_t maxn = std::max(s->nmetal[0], std::max(s->nmetal[1], s->nmetal[2]));
   if (maxn > 0) {
-    // per component: en, en1, cpn[2], cpn1[2], pd[3], nd[2] = 11 arrays
+    // per component: en, en1 in T; cpn[2], cpn1[2], pd[3], nd[2] in FP64
     T* st;
-    cudaError_t e = s->alloc(&st, (size_t)3 * 11 * maxn, true);
+    double* sd;
+    cudaError_t e = s->alloc(&st, (size_t)3 * 2 * maxn, true);
+    if (e == cudaSuccess) e = s->alloc(&sd, (size_t)3 * 9 * maxn, true);
     if (e != cudaSuccess) return fail(FDTD_ERR_ALLOC, cudaGetErrorString(e));
     for (int c = 0; c < 3; c++) {
-      T* b = st + (size_t)c * 11 * maxn;
+      T* b = st + (size_t)c * 2 * maxn;
+      double* d = sd + (size_t)c * 9 * maxn;
       m.en[c] = b; m.en1[c] = b + maxn;
-      m.cpn[c][0] = b + 2 * maxn; m.cpn[c][1] = b + 3 * maxn;
-      m.cpn1[c][0] = b + 4 * maxn; m.cpn1[c][1] = b + 5 * maxn;
-      m.pd[c][0] = b + 6 * maxn; m.pd[c][1] = b + 7 * maxn; m.pd[c][2] = b + 8 * maxn;
-      m.nd[c][0] = b + 9 * maxn; m.nd[c][1] = b + 10 * maxn;
+      m.cpn[c][0] = d; m.cpn[c][1] = d + maxn;
+      m.cpn1[c][0] = d + 2 * maxn; m.cpn1[c][1] = d + 3 * maxn;
+      m.pd[c][0] = d + 4 * maxn; m.pd[c][1] = d + 5 * maxn; m.pd[c][2] = d + 6 * maxn;
+      m.nd[c][0] = d + 7 * maxn; m.nd[c][1] = d + 8 * maxn;
       m.nbr[c] = s->nbr[c];
     }
-    s->mstate = st;
   }
   m.C_E = su.C_E; m.C_E_1 = su.C_E_1; m.C_E_2 = su.C_E_2;
   m.d1 = su.d1; m.d2 = su.d2; m.d3 = su.d3; m.d4 = su.d4; m.d5 = su.d5; m.dNL = su.dNL;
@@ -398,11 +399,12 @@ static fdtd_status build_views(fdtd_sim* s) {
     m.C1[q] = su.C1[q]; m.C2[q] = su.C2[q]; m.C3[q] = su.C3[q]; m.C4[q] = su.C4[q]; m.C5[q] = su.C5[q];
   }
   m.dt = su.dt; m.z0 = su.z0; m.e0 = su.e0; m.N_EQ = su.N_EQ;
-  m.inv_dx = (T)(1.0 / su.p.dx); m.inv_dy = (T)(1.0 / su.p.dy); m.inv_dz = (T)(1.0 / su.p.dz);
+  m.inv_dx = 1.0 / su.p.dx; m.inv_dy = 1.0 / su.p.dy; m.inv_dz = 1.0 / su.p.dz;
   m.hydro = su.hydro;
   m.vac = su.ep0;
   for (int c = 0; c < 3; c++) { m.rho[c] = nullptr; m.rec_off[c] = 0; }
   m.rec = nullptr;
+  m.hrec = nullptr;
   m.rec_rows = 1;
   m.rec_slots = 0;
   m.fix_cbrt = (su.p.fixes & FDTD_FIX_HYDRO_CBRT) ? 1 : 0;
@@ -1552,9 +1554,12 @@ extern "C" fdtd_status fdtd_snapshot_plane(fdtd_sim* s, int comp, int axis, int 
 // copied back); the scratch is one per device, shared by every simulation
 // in the process, so calls that overlap in time on the same device (from
 // several host threads, or on streams that run concurrently) race on it and
-// must be serialised by the caller.  The first call on each device resolves
-// the scratch address with cudaGetSymbolAddress and should come before any
-// stream capture is begun.
+// must be serialised by the caller.  Every call synchronises its stream
+// (also for a device destination), so it cannot run inside a stream
+// capture.  The first call on each device resolves the scratch address
+// with cudaGetSymbolAddress and keeps it for the life of the process; a
+// cudaDeviceReset would leave the kept address stale, so the library must
+// not be used across one.
 constexpr size_t kPlaneScratchCells = (size_t)1 << 20;  // 8 MiB of doubles
 static __device__ __align__(256) double g_plane_scratch[kPlaneScratchCells];
 
@@ -1654,6 +1659,11 @@ extern "C" fdtd_status fdtd_get_stats(const fdtd_sim* s, fdtd_stats* out) {
   out->h_eminb = s->hcfg.eminb; out->h_estages = s->hcfg.estages;
   out->e_eminb = s->ecfg.eminb; out->e_estages = s->ecfg.estages;
   out->h_pdl = s->hcfg.pdl; out->e_pdl = s->ecfg.pdl;
+  out->tfsf_entries_h = s->tf_h.n;
+  out->tfsf_entries_e = s->tf_e.n;
+  long long rows = 0;
+  for (int f = 0; f < s->dft.nfaces; f++) rows += 4LL * s->dft.face[f].na * s->dft.face[f].nb;
+  out->dft_rows = rows;
   return FDTD_OK;
 }
 

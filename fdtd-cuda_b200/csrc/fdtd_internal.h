@@ -81,11 +81,15 @@ template <typename T>
 struct MetalView {
   int n[3];             // cells per component
   const int4* cell[3];  // (i, j, k, slot) per entry
-  // state, SoA per component: slot-major arrays
+  // state, SoA per component: slot-major arrays.  The E history is in the
+  // field type (it holds copies of field values); the polarisations, the
+  // Drude current and the hydrodynamic density are FP64 in both builds:
+  // rounding them to FP32 alone shifts the absorption spectra by 1e-5 of
+  // their peak
   T* en[3]; T* en1[3];
-  T* cpn[3][2]; T* cpn1[3][2];
-  T* pd[3][3];          // Drude current ring (n, n-1, new) indexed by step
-  T* nd[3][2];          // hydro density ring
+  double* cpn[3][2]; double* cpn1[3][2];
+  double* pd[3][3];     // Drude current ring (n, n-1, new) indexed by step
+  double* nd[3][2];     // hydro density ring
   const float* rho[3];  // design blend per slot (null: plain metal coefficients)
   double vac;           // vacuum C_E = C_E_1 = ep0, the rho = 0 end of the blend
   // forward record for the adjoint (null = off): per step row (t % rec_rows)
@@ -95,6 +99,9 @@ struct MetalView {
   int rec_rows;
   int rec_off[3];
   long long rec_slots;
+  // hydrodynamic cells: six FP64 values per slot and row, [row][value]
+  // [rec_off[c] + slot], value = J^{n-1}, J^n, J^{n+1}, N^{n-1}, N^n, N^{n+1}
+  double* hrec;
   // hydrodynamic neighbour slots, 12 per cell (see hydro_neighbours)
   const int* nbr[3];
   // ADE coefficients, FP64 in both builds: the CP pole recursions sit close
@@ -107,7 +114,7 @@ struct MetalView {
   // the hydrodynamic E source dt J e0 (N_EQ + N) and the continuity update
   // run in FP64 too (their constants are FP64)
   double dt, z0, e0, N_EQ;
-  T inv_dx, inv_dy, inv_dz;
+  double inv_dx, inv_dy, inv_dz;
   int hydro;
   int fix_cbrt;
 };

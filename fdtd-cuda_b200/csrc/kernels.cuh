@@ -25,6 +25,21 @@ namespace fdtd {
 template <typename T>
 __device__ __forceinline__ T ldg(const T* p) { return __ldg(p); }
 
+// Arithmetic with its rounding fixed: products, differences and fused
+// multiply-adds that the compiler may neither contract nor split.  The Yee
+// passes are written with these, so that a cell's update rounds the same
+// in every launch form (the CPML-free or the CPML-edge instantiation, any
+// tile shape, the batched work queue).
+__device__ __forceinline__ float rmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double rmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float rsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double rsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float rfma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double rfma(double a, double b, double c) { return __fma_rn(a, b, c); }
+// a * x - b * y with the first product fused
+template <typename T>
+__device__ __forceinline__ T rcurl(T x, T a, T y, T b) { return rfma(x, a, -rmul(y, b)); }
+
 __device__ __forceinline__ size_t fidx(int PX, size_t plane, int i, int j, int k) {
   return (size_t)k * plane + (size_t)j * PX + i;
 }
@@ -378,10 +393,10 @@ __device__ __forceinline__ void metal_e_body(const SimView<T>& s, const MetalVie
   const T v = s.E[c][id];
   T da, db;
   const T curl = curl_h_at(s, c, i, j, k, &da, &db);
-  const T pdn = m.pd[c][rn][sl], pdn1 = m.pd[c][rn1][sl];
-  const T cpn0 = m.cpn[c][0][sl], cpn1_0 = m.cpn1[c][0][sl];
-  const T cpn1 = m.cpn[c][1][sl], cpn1_1 = m.cpn1[c][1][sl];
-  // the ADE recursions in FP64 (the coefficients are FP64), the state in T
+  const double pdn = m.pd[c][rn][sl], pdn1 = m.pd[c][rn1][sl];
+  const double cpn0 = m.cpn[c][0][sl], cpn1_0 = m.cpn1[c][0][sl];
+  const double cpn1 = m.cpn[c][1][sl], cpn1_1 = m.cpn1[c][1][sl];
+  // the ADE recursions and their state in FP64, the fields in T
   double CP1 = 0.0, CP2 = 0.0, CP3 = 0.0, CP4 = 0.0;
   CP1 += (m.d1 - 1) * pdn;
   CP3 += m.d2 * pdn1;
@@ -412,15 +427,15 @@ __device__ __forceinline__ void metal_e_body(const SimView<T>& s, const MetalVie
   T nv = (T)nvd;
   if (m.rec) {
     T* r = m.rec + (size_t)(t % m.rec_rows) * 5 * m.rec_slots + m.rec_off[c] + sl;
-    r[0] = en; r[m.rec_slots] = en1; r[2 * m.rec_slots] = pdn; r[3 * m.rec_slots] = pdn1; r[4 * m.rec_slots] = nv;
+    r[0] = en; r[m.rec_slots] = en1; r[2 * m.rec_slots] = (T)pdn; r[3 * m.rec_slots] = (T)pdn1; r[4 * m.rec_slots] = nv;
   }
   m.en1[c][sl] = en1;
   m.en[c][sl] = en;
   m.cpn1[c][0][sl] = cpn0;
   m.cpn1[c][1][sl] = cpn1;
-  m.cpn[c][0][sl] = (T)ncp0;
-  m.cpn[c][1][sl] = (T)ncp1;
-  m.pd[c][rnew][sl] = (T)npd;
+  m.cpn[c][0][sl] = ncp0;
+  m.cpn[c][1][sl] = ncp1;
+  m.pd[c][rnew][sl] = npd;
   nv = cpml_e_all(s, c, i, j, k, da, db, nv, ceh);
   if (!isfinite((double)nv)) atomicOr(s.nonfinite, 1);
   s.E[c][id] = nv;
@@ -437,7 +452,7 @@ __global__ void metal_e(const __grid_constant__ SimView<T> s, const __grid_const
 // +e_c - e_a and -e_a.  cphase: components below it have already rotated
 // in this step (the reference launches UPDATE_ex, _ey, _ez in turn).
 template <typename T, int c, int cphase>
-__device__ __forceinline__ void hydro_neighbours(const MetalView<T>& m, int q, int t, T P[3][4], T N[3][4]) {
+__device__ __forceinline__ void hydro_neighbours(const MetalView<T>& m, int q, int t, double P[3][4], double N[3][4]) {
   const int* nb = m.nbr[c] + (size_t)q * 12;
 #pragma unroll
   for (int a = 0; a < 3; a++) {
@@ -446,8 +461,8 @@ __device__ __forceinline__ void hydro_neighbours(const MetalView<T>& m, int q, i
 #pragma unroll
     for (int x = 0; x < 4; x++) {
       const int sl = nb[a * 4 + x];
-      P[a][x] = sl >= 0 ? m.pd[a][rp][sl] : T(0);
-      N[a][x] = sl >= 0 ? m.nd[a][rn][sl] : T(0);
+      P[a][x] = sl >= 0 ? m.pd[a][rp][sl] : 0.0;
+      N[a][x] = sl >= 0 ? m.nd[a][rn][sl] : 0.0;
     }
   }
 }
@@ -457,34 +472,33 @@ __device__ __forceinline__ void hydro_neighbours(const MetalView<T>& m, int q, i
 // the pressure term d_NL (grad div J + grad div (N J) / N_EQ) / (N_EQ +
 // N)^(1/3).  Convection and Lorentz terms are off in the reference.
 template <typename T, int c>
-__device__ __forceinline__ T hydro_current(const MetalView<T>& m, int t, int sl, const T P[3][4], const T N[3][4],
-                                           T ev, T en_prev) {
-  const T IX = m.inv_dx, IY = m.inv_dy, IZ = m.inv_dz;
-  const T I3[3] = {IX, IY, IZ};
+__device__ __forceinline__ double hydro_current(const MetalView<T>& m, int t, int sl, const double P[3][4],
+                                                const double N[3][4], T ev, T en_prev) {
+  const double IX = m.inv_dx, IY = m.inv_dy, IZ = m.inv_dz;
+  const double I3[3] = {IX, IY, IZ};
   // the two other components in the reference's summation order, with
   // their mixed-derivative coefficients
   constexpr int a1 = c == 0 ? 1 : (c == 1 ? 0 : 1), a2 = c == 0 ? 2 : (c == 1 ? 2 : 0);
-  const T k1 = c == 2 ? IZ * IY : I3[c < a1 ? c : a1] * I3[c < a1 ? a1 : c];
-  const T k2 = I3[c < a2 ? c : a2] * I3[c < a2 ? a2 : c];
-  const T Ic = I3[c];
-  T PN[3][4];
+  const double k1 = c == 2 ? IZ * IY : I3[c < a1 ? c : a1] * I3[c < a1 ? a1 : c];
+  const double k2 = I3[c < a2 ? c : a2] * I3[c < a2 ? a2 : c];
+  const double Ic = I3[c];
+  double PN[3][4];
 #pragma unroll
   for (int a = 0; a < 3; a++)
 #pragma unroll
     for (int x = 0; x < 4; x++) PN[a][x] = P[a][x] * N[a][x];
-  const T gd2 = Ic * Ic * (PN[c][0] - T(2) * PN[c][1] + PN[c][2]) +
-                k1 * (PN[a1][0] - PN[a1][1] - PN[a1][2] + PN[a1][3]) +
-                k2 * (PN[a2][0] - PN[a2][1] - PN[a2][2] + PN[a2][3]);
-  const T gd = Ic * Ic * (P[c][0] - T(2) * P[c][1] + P[c][2]) + k1 * (P[a1][0] - P[a1][1] - P[a1][2] + P[a1][3]) +
-               k2 * (P[a2][0] - P[a2][1] - P[a2][2] + P[a2][3]);
-  const T ND1 = m.N_EQ + N[c][1];
-  T cb;
-  if (m.fix_cbrt) cb = (T)cbrt((double)ND1);
-  else cb = (T)powf((float)ND1, (float)(1.0 / 3.0));
-  const T pn = m.pd[c][t % 3][sl], pn1 = m.pd[c][(t + 2) % 3][sl];
-  // FP64 recursion (FP64 coefficients), rounded to the state type
-  return (T)(m.d1 * pn + m.d2 * pn1 + m.d3 * ev + m.d4 * en_prev + m.d5 * 0.0 +
-             m.dNL * (double)((gd + gd2 / m.N_EQ) / cb));
+  const double gd2 = Ic * Ic * (PN[c][0] - 2.0 * PN[c][1] + PN[c][2]) +
+                     k1 * (PN[a1][0] - PN[a1][1] - PN[a1][2] + PN[a1][3]) +
+                     k2 * (PN[a2][0] - PN[a2][1] - PN[a2][2] + PN[a2][3]);
+  const double gd = Ic * Ic * (P[c][0] - 2.0 * P[c][1] + P[c][2]) + k1 * (P[a1][0] - P[a1][1] - P[a1][2] + P[a1][3]) +
+                    k2 * (P[a2][0] - P[a2][1] - P[a2][2] + P[a2][3]);
+  const double ND1 = m.N_EQ + N[c][1];
+  double cb;
+  if (m.fix_cbrt) cb = cbrt(ND1);
+  else cb = (double)powf((float)ND1, (float)(1.0 / 3.0));
+  const double pn = m.pd[c][t % 3][sl], pn1 = m.pd[c][(t + 2) % 3][sl];
+  return m.d1 * pn + m.d2 * pn1 + m.d3 * (double)ev + m.d4 * (double)en_prev + m.d5 * 0.0 +
+         m.dNL * ((gd + gd2 / m.N_EQ) / cb);
 }
 
 // Hydrodynamic E update of one cell of component c (UPDATE_e* hydro
@@ -492,43 +506,49 @@ __device__ __forceinline__ T hydro_current(const MetalView<T>& m, int t, int sl,
 // perturbation, then E with the current source e0 (N_EQ + N) J.
 template <typename T, int c>
 __device__ __forceinline__ void hydro_e_cell(const SimView<T>& s, const MetalView<T>& m, int t, int4 e,
-                                             const T P[3][4], const T N[3][4], T jd) {
+                                             const double P[3][4], const double N[3][4], double jd) {
   const int i = e.x, j = e.y, k = e.z, sl = e.w;
   const size_t id = fidx(s.PX, s.plane, i, j, k);
   const T ceh = s.ceh[s.mat[id] >> 3];
-  T V1[3], V2[3], N1[3], N2[3];
+  double V1[3], V2[3], N1[3], N2[3];
 #pragma unroll
   for (int a = 0; a < 3; a++) {
     if (a == c) {
       V1[a] = P[a][0]; V2[a] = P[a][2]; N1[a] = N[a][0]; N2[a] = N[a][2];
     } else {
-      V1[a] = T(0.5) * (P[a][0] + P[a][1]);
-      V2[a] = T(0.5) * (P[a][2] + P[a][3]);
-      N1[a] = T(0.5) * (N[a][0] + N[a][1]);
-      N2[a] = T(0.5) * (N[a][2] + N[a][3]);
+      V1[a] = 0.5 * (P[a][0] + P[a][1]);
+      V2[a] = 0.5 * (P[a][2] + P[a][3]);
+      N1[a] = 0.5 * (N[a][0] + N[a][1]);
+      N2[a] = 0.5 * (N[a][2] + N[a][3]);
     }
   }
-  const T ndm1 = m.nd[c][(t + 1) & 1][sl];  // N^{n-1}
+  const double ndm1 = m.nd[c][(t + 1) & 1][sl];  // N^{n-1}
   const double k2 = 2.0 * m.dt * m.inv_dx;
-  T nd;
+  // an adjoint design cell scales its current and density updates and
+  // blends its coupling coefficients by rho (rho = 0: a vacuum cell with
+  // J = N = 0, as the neighbours of a non-dispersive cell see it)
+  const bool blend = m.rho[c] != nullptr;
+  const double r = blend ? (double)m.rho[c][sl] : 1.0;
+  double nd;
   if (c == 0)
-    nd = ndm1 - k2 * (T(0.5) * (N1[0] * V1[0] - N2[0] * V2[0]) + (N1[1] * V1[1] - N2[1] * V2[1]) +
+    nd = ndm1 - k2 * (0.5 * (N1[0] * V1[0] - N2[0] * V2[0]) + (N1[1] * V1[1] - N2[1] * V2[1]) +
                       (N1[2] * V1[2] - N2[2] * V2[2]) +
-                      (T(0.5) * (V1[0] - V2[0]) + (V1[1] - V2[1]) + (V1[2] - V2[2])) * m.N_EQ);
+                      (0.5 * (V1[0] - V2[0]) + (V1[1] - V2[1]) + (V1[2] - V2[2])) * m.N_EQ);
   else if (c == 1)
-    nd = ndm1 - k2 * ((N1[0] * V1[0] - N2[0] * V2[0]) + T(0.5) * (N1[1] * V1[1] - N2[1] * V2[1]) +
+    nd = ndm1 - k2 * ((N1[0] * V1[0] - N2[0] * V2[0]) + 0.5 * (N1[1] * V1[1] - N2[1] * V2[1]) +
                       (N1[2] * V1[2] - N2[2] * V2[2]) +
-                      ((V1[0] - V2[0]) + T(0.5) * (V1[1] - V2[1]) + (V1[2] - V2[2])) * m.N_EQ);
+                      ((V1[0] - V2[0]) + 0.5 * (V1[1] - V2[1]) + (V1[2] - V2[2])) * m.N_EQ);
   else
     nd = ndm1 - k2 * ((N1[0] * V1[0] - N2[0] * V2[0]) + (N1[1] * V1[1] - N2[1] * V2[1]) +
-                      T(0.5) * (V1[2] - V2[2]) +
-                      ((V1[0] - V2[0]) + (V1[1] - V2[1]) + T(0.5) * (V1[2] - V2[2])) * m.N_EQ);
+                      0.5 * (V1[2] - V2[2]) +
+                      ((V1[0] - V2[0]) + (V1[1] - V2[1]) + 0.5 * (V1[2] - V2[2])) * m.N_EQ);
+  if (blend) nd = r * nd;
   const T v = s.E[c][id];
   T da, db;
   const T curl = curl_h_at(s, c, i, j, k, &da, &db);
-  const T cpn0 = m.cpn[c][0][sl], cpn1_0 = m.cpn1[c][0][sl];
-  const T cpn1 = m.cpn[c][1][sl], cpn1_1 = m.cpn1[c][1][sl];
-  // the ADE recursions in FP64 (the coefficients are FP64), the state in T
+  const double cpn0 = m.cpn[c][0][sl], cpn1_0 = m.cpn1[c][0][sl];
+  const double cpn1 = m.cpn[c][1][sl], cpn1_1 = m.cpn1[c][1][sl];
+  // the ADE recursions and their state in FP64, the fields in T
   double CP2 = 0.0, CP4 = 0.0;
   CP2 += (m.C1[0] - 1) * cpn0;
   CP2 += (m.C1[1] - 1) * cpn1;
@@ -536,18 +556,32 @@ __device__ __forceinline__ void hydro_e_cell(const SimView<T>& s, const MetalVie
   CP4 += m.C2[1] * cpn1_1;
   const T en1 = m.en[c][sl];
   const T en = v;
-  const double inv_CE = 1.0 / m.C_E;
-  const double nvd = inv_CE * ((double)(m.dt * curl / m.z0 + m.dt * jd * m.e0 * (m.N_EQ + nd)) + m.C_E_1 * en -
-                               m.C_E_2 * en1 - CP2 - CP4);
-  const double ncp0 = m.C1[0] * cpn0 + m.C2[0] * cpn1_0 + m.C3[0] * nvd + m.C4[0] * en + m.C5[0] * en1;
-  const double ncp1 = m.C1[1] * cpn1 + m.C2[1] * cpn1_1 + m.C3[1] * nvd + m.C4[1] * en + m.C5[1] * en1;
+  double CE = m.C_E, CE1 = m.C_E_1, CE2 = m.C_E_2;
+  double C3[2] = {m.C3[0], m.C3[1]}, C4[2] = {m.C4[0], m.C4[1]}, C5[2] = {m.C5[0], m.C5[1]};
+  if (blend) {
+    CE = m.vac + r * (m.C_E - m.vac);
+    CE1 = m.vac + r * (m.C_E_1 - m.vac);
+    CE2 = r * m.C_E_2;
+#pragma unroll
+    for (int q = 0; q < 2; q++) { C3[q] = r * m.C3[q]; C4[q] = r * m.C4[q]; C5[q] = r * m.C5[q]; }
+  }
+  const double inv_CE = 1.0 / CE;
+  const double nvd = inv_CE * ((m.dt * (double)curl / m.z0 + m.dt * jd * m.e0 * (m.N_EQ + nd)) + CE1 * en -
+                               CE2 * en1 - CP2 - CP4);
+  const double ncp0 = m.C1[0] * cpn0 + m.C2[0] * cpn1_0 + C3[0] * nvd + C4[0] * en + C5[0] * en1;
+  const double ncp1 = m.C1[1] * cpn1 + m.C2[1] * cpn1_1 + C3[1] * nvd + C4[1] * en + C5[1] * en1;
   T nv = (T)nvd;
+  if (m.rec) {
+    T* rr = m.rec + (size_t)(t % m.rec_rows) * 5 * m.rec_slots + m.rec_off[c] + sl;
+    rr[0] = en; rr[m.rec_slots] = en1; rr[4 * m.rec_slots] = nv;
+  }
+  if (m.hrec) m.hrec[((size_t)(t % m.rec_rows) * 6 + 5) * m.rec_slots + m.rec_off[c] + sl] = nd;
   m.en1[c][sl] = en1;
   m.en[c][sl] = en;
   m.cpn1[c][0][sl] = cpn0;
   m.cpn1[c][1][sl] = cpn1;
-  m.cpn[c][0][sl] = (T)ncp0;
-  m.cpn[c][1][sl] = (T)ncp1;
+  m.cpn[c][0][sl] = ncp0;
+  m.cpn[c][1][sl] = ncp1;
   m.nd[c][(t + 1) & 1][sl] = nd;  // becomes "prev" after the parity flip
   nv = cpml_e_all(s, c, i, j, k, da, db, nv, ceh);
   if (!isfinite((double)nv)) atomicOr(s.nonfinite, 1);
@@ -557,10 +591,22 @@ __device__ __forceinline__ void hydro_e_cell(const SimView<T>& s, const MetalVie
 template <typename T, int c>
 __device__ __forceinline__ void hydro_p_cell(const SimView<T>& s, const MetalView<T>& m, int t, int q) {
   const int4 e = m.cell[c][q];
-  T P[3][4], N[3][4];
+  double P[3][4], N[3][4];
   hydro_neighbours<T, c, 0>(m, q, t, P, N);
   const size_t id = fidx(s.PX, s.plane, e.x, e.y, e.z);
-  const T jd = hydro_current<T, c>(m, t, e.w, P, N, s.E[c][id], m.en[c][e.w]);
+  double jd = hydro_current<T, c>(m, t, e.w, P, N, s.E[c][id], m.en[c][e.w]);
+  if (m.rho[c]) jd *= (double)m.rho[c][e.w];  // adjoint design cell (see hydro_e_cell)
+  if (m.hrec) {
+    // J^{n-1}, J^n, J^{n+1}, N^{n-1}, N^n of the slot; N^{n+1} follows in
+    // hydro_e_cell
+    double* h = m.hrec + (size_t)(t % m.rec_rows) * 6 * m.rec_slots + m.rec_off[c] + e.w;
+    const long long S = m.rec_slots;
+    h[0] = m.pd[c][(t + 2) % 3][e.w];
+    h[S] = m.pd[c][t % 3][e.w];
+    h[2 * S] = jd;
+    h[3 * S] = m.nd[c][(t + 1) & 1][e.w];
+    h[4 * S] = m.nd[c][t & 1][e.w];
+  }
   m.pd[c][(t + 1) % 3][e.w] = jd;
   if (c == 0) hydro_e_cell<T, 0>(s, m, t, e, P, N, jd);
 }
@@ -589,7 +635,7 @@ __global__ void hydro_e(const __grid_constant__ SimView<T> s, const __grid_const
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= m.n[c]) return;
   const int4 e = m.cell[c][q];
-  T P[3][4], N[3][4];
+  double P[3][4], N[3][4];
   hydro_neighbours<T, c, c>(m, q, t, P, N);
   hydro_e_cell<T, c>(s, m, t, e, P, N, m.pd[c][(t + 1) % 3][e.w]);
 }

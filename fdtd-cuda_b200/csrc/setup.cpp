@@ -371,7 +371,6 @@ const char* setup_build(const fdtd_params& pin, Setup& s) {
     const int* b = p.design_box;
     if (b[1] > b[0] || b[3] > b[2] || b[5] > b[4]) {
       if (!(b[1] > b[0] && b[3] > b[2] && b[5] > b[4])) return "design_box is empty along one axis";
-      if (s.hydro) return "the design region needs the local (non-hydrodynamic) model";
       if (p.first_medium != 1) return "the design region blends towards vacuum: first_medium must be 1";
       for (int a = 0; a < 3; a++)
         if (b[2 * a] < s.absS[a] + 1 || b[2 * a + 1] > s.absE[a] - 1)

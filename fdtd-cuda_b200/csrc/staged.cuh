@@ -59,7 +59,7 @@ __device__ __forceinline__ SlabAt<T> slab_h(const CpmlAxis<T>& a, int n) {
 // 1294-1318); stores and returns the new psi
 template <typename T>
 __device__ __forceinline__ T psi_apply(T* p, T old, T b, T c, T diff, T inv_d) {
-  const T ps = b * old + c * diff * inv_d;
+  const T ps = rfma(b, old, rmul(rmul(c, diff), inv_d));
   *p = ps;
   return ps;
 }
@@ -286,9 +286,9 @@ __device__ __forceinline__ void h_pass_tile(const SimView<T>& s, int kchunk, int
           const T exk1 = en[o], eyk1 = en[FH + o];
           const T ikz = ldg(ikzp);
           const bool hask = k + 1 < NZ;
-          T vx = chh * hown[oo] + che * ((eyk1 - eyk) * ikz - (ez_j - ezk) * iky);
-          T vy = chh * hown[TY * 32 + oo] + che * ((ez_i - ezk) * ikx - (exk1 - exk) * ikz);
-          T vz = chh * hown[2 * TY * 32 + oo] + che * ((ex_j - exk) * iky - (ey_i - eyk) * ikx);
+          T vx = rfma(che, rcurl(rsub(eyk1, eyk), ikz, rsub(ez_j, ezk), iky), rmul(chh, hown[oo]));
+          T vy = rfma(che, rcurl(rsub(ez_i, ezk), ikx, rsub(exk1, exk), ikz), rmul(chh, hown[TY * 32 + oo]));
+          T vz = rfma(che, rcurl(rsub(ex_j, exk), iky, rsub(ey_i, eyk), ikx), rmul(chh, hown[2 * TY * 32 + oo]));
           if (pml_xy && hask) {
             const int q = zq(k);
             if (q >= 0) {
@@ -296,16 +296,16 @@ __device__ __forceinline__ void h_pass_tile(const SimView<T>& s, int kchunk, int
               const int qt = q < Ncz ? q : q + 1;  // table index (Nc+1 entries a side)
               const T b = ldg(s.cp[2].bh_N + qt);
               const T c = ldg(s.cp[2].ch_N + qt);
-              vx += che * psi_apply(pz0 + off, cz0, b, c, eyk1 - eyk, idz_);
-              vy -= che * psi_apply(pz1 + off, cz1, b, c, exk1 - exk, idz_);
+              vx = rfma(che, psi_apply(pz0 + off, cz0, b, c, rsub(eyk1, eyk), idz_), vx);
+              vy = rfma(-che, psi_apply(pz1 + off, cz1, b, c, rsub(exk1, exk), idz_), vy);
             }
             if (sx.side) {
-              vy += che * psi_apply(bx0 + ox, cx0, sx.b, sx.c, ez_i - ezk, idx_);
-              vz -= che * psi_apply(bx1 + ox, cx1, sx.b, sx.c, ey_i - eyk, idx_);
+              vy = rfma(che, psi_apply(bx0 + ox, cx0, sx.b, sx.c, rsub(ez_i, ezk), idx_), vy);
+              vz = rfma(-che, psi_apply(bx1 + ox, cx1, sx.b, sx.c, rsub(ey_i, eyk), idx_), vz);
             }
             if (sy.side) {
-              vx -= che * psi_apply(by0 + oy, cy0, sy.b, sy.c, ez_j - ezk, idy_);
-              vz += che * psi_apply(by1 + oy, cy1, sy.b, sy.c, ex_j - exk, idy_);
+              vx = rfma(-che, psi_apply(by0 + oy, cy0, sy.b, sy.c, rsub(ez_j, ezk), idy_), vx);
+              vz = rfma(che, psi_apply(by1 + oy, cy1, sy.b, sy.c, rsub(ex_j, exk), idy_), vz);
             }
           }
           if (hasy && hask) *phx = vx;
@@ -491,9 +491,9 @@ __device__ __forceinline__ void e_pass_tile(const SimView<T>& s, int kchunk, int
               ceh = s.ceh[m >> 3];
             }
           }
-          T vx = cee * eown[oo] + ceh * ((hzk - hz_j) * iky - (hyk - hym) * ikz);
-          T vy = cee * eown[TY * 32 + oo] + ceh * ((hxk - hxm) * ikz - (hzk - hz_i) * ikx);
-          T vz = cee * eown[2 * TY * 32 + oo] + ceh * ((hyk - hy_i) * ikx - (hxk - hx_j) * iky);
+          T vx = rfma(ceh, rcurl(rsub(hzk, hz_j), iky, rsub(hyk, hym), ikz), rmul(cee, eown[oo]));
+          T vy = rfma(ceh, rcurl(rsub(hxk, hxm), ikz, rsub(hzk, hz_i), ikx), rmul(cee, eown[TY * 32 + oo]));
+          T vz = rfma(ceh, rcurl(rsub(hyk, hy_i), ikx, rsub(hxk, hx_j), iky), rmul(cee, eown[2 * TY * 32 + oo]));
           const bool wx = colx && hasz && okz && !(m & 1);
           const bool wy = coly && hasz && okz && !(m & 2);
           const bool wz = colz && okz && !(m & 4);
@@ -503,16 +503,16 @@ __device__ __forceinline__ void e_pass_tile(const SimView<T>& s, int kchunk, int
               const unsigned off = (unsigned)q * plane32 + jrow;
               const T b = ldg(s.cp[2].be_N + q);  // be_N then be_F
               const T c = ldg(s.cp[2].ce_N + q);  // ce_N then ce_F
-              if (wx) vx -= ceh * psi_apply(pz0 + off, cz0, b, c, hyk - hym, idz_);
-              if (wy) vy += ceh * psi_apply(pz1 + off, cz1, b, c, hxk - hxm, idz_);
+              if (wx) vx = rfma(-ceh, psi_apply(pz0 + off, cz0, b, c, rsub(hyk, hym), idz_), vx);
+              if (wy) vy = rfma(ceh, psi_apply(pz1 + off, cz1, b, c, rsub(hxk, hxm), idz_), vy);
             }
             if (sy.side) {
-              if (wx) vx += ceh * psi_apply(by0 + oy, cy0, sy.b, sy.c, hzk - hz_j, idy_);
-              if (wz) vz -= ceh * psi_apply(by1 + oy, cy1, sy.b, sy.c, hxk - hx_j, idy_);
+              if (wx) vx = rfma(ceh, psi_apply(by0 + oy, cy0, sy.b, sy.c, rsub(hzk, hz_j), idy_), vx);
+              if (wz) vz = rfma(-ceh, psi_apply(by1 + oy, cy1, sy.b, sy.c, rsub(hxk, hx_j), idy_), vz);
             }
             if (sx.side) {
-              if (wy) vy -= ceh * psi_apply(bx0 + ox, cx0, sx.b, cx_ey, hzk - hz_i, idx_);
-              if (wz) vz += ceh * psi_apply(bx1 + ox, cx1, sx.b, sx.c, hyk - hy_i, idx_);
+              if (wy) vy = rfma(-ceh, psi_apply(bx0 + ox, cx0, sx.b, cx_ey, rsub(hzk, hz_i), idx_), vy);
+              if (wz) vz = rfma(ceh, psi_apply(bx1 + ox, cx1, sx.b, sx.c, rsub(hyk, hy_i), idx_), vz);
             }
           }
           if (wx) { *pex = vx; check += vx; }

@@ -34,7 +34,8 @@ EXPORTS = [
     "fdtd_batch_create", "fdtd_batch_run", "fdtd_batch_spectra", "fdtd_batch_destroy",
     "fdtd_batch_step", "fdtd_batch_sim", "fdtd_batch_get_stats",
     "fdtd_plan", "fdtd_rasterise", "fdtd_coefficients", "fdtd_get_probe_range",
-    "fdtd_set_source", "fdtd_get_stats", "fdtd_time_kernel",
+    "fdtd_set_source", "fdtd_get_stats", "fdtd_time_kernel", "fdtd_forward_spectra",
+    "fdtd_backward_spectra",
 ]
 
 
@@ -86,6 +87,8 @@ def lib():
         "fdtd_set_design": (C.c_int, [vp, P(C.c_int), P(C.c_float), sz]),
         "fdtd_forward": (C.c_int, [vp, P(C.c_int), C.c_int, C.c_int, dp]),
         "fdtd_backward": (C.c_int, [vp, P(C.c_float), sz, dp]),
+        "fdtd_forward_spectra": (C.c_int, [vp, C.c_int, dp]),
+        "fdtd_backward_spectra": (C.c_int, [vp, dp, P(C.c_float), sz, dp]),
         "fdtd_batch_create": (C.c_int, [P(Params), C.c_int, C.c_int, P(vp)]),
         "fdtd_batch_run": (C.c_int, [vp, vp]),
         "fdtd_batch_spectra": (C.c_int, [vp, C.c_int, dp]),
@@ -274,7 +277,8 @@ class Sim:
 
     def forward(self, freq_idx, checkpoint_every=200):
         """Runs t = 0..Tend from zero fields with checkpoints; returns the
-        objective (AbsTot summed over freq_idx)."""
+        objective: the absorption cross-section (m^2, positive for an
+        absorbing structure) summed over freq_idx."""
         idx = (C.c_int * len(freq_idx))(*[int(x) for x in freq_idx])
         out = C.c_double()
         _check(lib().fdtd_forward(self.h, idx, len(freq_idx), int(checkpoint_every), C.byref(out)))
@@ -286,6 +290,26 @@ class Sim:
         g = np.empty((b[5] - b[4], b[3] - b[2], b[1] - b[0]), np.float32)
         gp = np.empty(2)
         _check(lib().fdtd_backward(self.h, g.ctypes.data_as(C.POINTER(C.c_float)), g.size, _dp(gp)))
+        return g, gp
+
+    def forward_spectra(self, checkpoint_every=200):
+        """Runs t = 0..Tend from zero fields with checkpoints; returns the
+        ScatAbs table (NUM_freq x 19) of the run."""
+        out = np.empty((self.dims.num_freq, 19))
+        _check(lib().fdtd_forward_spectra(self.h, int(checkpoint_every), _dp(out)))
+        return out
+
+    def backward_spectra(self, dL_dspectra):
+        """dL/drho (box shape) and dL/d(omega_D, gamma) of the last forward
+        for the objective whose gradient with respect to the ScatAbs table
+        is dL_dspectra (NUM_freq x 19; columns 0 and 16-18 zero)."""
+        G = np.ascontiguousarray(dL_dspectra, dtype=np.float64)
+        assert G.shape == (self.dims.num_freq, 19), G.shape
+        b = list(self.params.design_box)
+        g = np.empty((b[5] - b[4], b[3] - b[2], b[1] - b[0]), np.float32)
+        gp = np.empty(2)
+        _check(lib().fdtd_backward_spectra(self.h, _dp(G), g.ctypes.data_as(C.POINTER(C.c_float)), g.size,
+                                           _dp(gp)))
         return g, gp
 
     def time_kernel(self, which, reps=20, stream=None):

@@ -104,4 +104,6 @@ class Stats(C.Structure):
                 ("h_stages", C.c_int), ("e_stages", C.c_int),
                 ("h_eminb", C.c_int), ("h_estages", C.c_int),
                 ("e_eminb", C.c_int), ("e_estages", C.c_int),
-                ("h_pdl", C.c_int), ("e_pdl", C.c_int)]
+                ("h_pdl", C.c_int), ("e_pdl", C.c_int),
+                ("tfsf_entries_h", C.c_longlong), ("tfsf_entries_e", C.c_longlong),
+                ("dft_rows", C.c_longlong)]

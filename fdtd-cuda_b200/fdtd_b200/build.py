@@ -12,9 +12,14 @@ CSRC = os.path.join(os.path.dirname(HERE), "csrc")
 LIB = os.path.join(HERE, "libfdtd_b200.so")
 RUNNER = os.path.join(HERE, "fdtd_runner")
 SOURCES = ["fdtd.cu", "setup.cpp"]
+# -fmad=false: no multiply-add contraction chosen by the compiler.  A kernel
+# body shared by two launch forms (one simulation, a batch) then rounds the
+# same in both, and the arithmetic follows the order written, as in the FP64
+# oracle (built with -ffp-contract=off).  The Yee passes spell their fused
+# multiply-adds out with intrinsics, which this flag does not touch.
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
-    "-Xcompiler", "-fPIC,-O2", "-shared", "--expt-relaxed-constexpr",
+    "-Xcompiler", "-fPIC,-O2", "-shared", "--expt-relaxed-constexpr", "-fmad=false",
 ]
 
 

@@ -290,12 +290,15 @@ fdtd_status fdtd_snapshot_plane(fdtd_sim* s, int comp, int axis, int index,
                                 double* dst, size_t count, void* stream);
 /* The same plane as fdtd_snapshot_plane, with no memory allocation of any
  * kind: the plane is gathered into a fixed scratch array in the library's
- * static device memory and copied to dst (host or device) on `stream`; the
- * call returns once the copy is done.  No counterpart in the reference.
- * Limit: count <= 1048576 cells (FDTD_ERR_INVALID beyond).  The scratch is
- * one per device and shared by all simulations: calls that overlap in time
- * on one device race and must be serialised by the caller.  Make the first
- * call on each device before beginning any stream capture. */
+ * static device memory and copied to dst (host or device) on `stream`.
+ * No counterpart in the reference.  Every call synchronises `stream` before
+ * it returns, whatever dst is, so it cannot be used while a stream is being
+ * captured into a CUDA graph.  Limit: count <= 1048576 cells
+ * (FDTD_ERR_INVALID beyond).  The scratch is one per device and shared by
+ * all simulations: calls that overlap in time on one device race and must
+ * be serialised by the caller.  The scratch's device address is looked up
+ * on the first call on each device and kept for the life of the process:
+ * the library must not be used across a cudaDeviceReset. */
 fdtd_status fdtd_snapshot_plane_static(fdtd_sim* s, int comp, int axis,
                                        int index, double* dst, size_t count,
                                        void* stream);
@@ -328,6 +331,10 @@ typedef struct fdtd_stats {
   /* 1 = the two launches of the pass run on one stream with a programmatic
    * dependency, 0 = on two streams */
   int h_pdl, e_pdl;
+  /* sizes of the step's work beside the passes, for traffic accounting:
+   * TFSF table entries of the H and E shells, and DFT rows (one per
+   * tangential component and flux-face cell, padding excluded) */
+  long long tfsf_entries_h, tfsf_entries_e, dft_rows;
 } fdtd_stats;
 fdtd_status fdtd_get_stats(const fdtd_sim* s, fdtd_stats* out);
 /* Measurement hook (no counterpart in the reference): runs one Yee pass
@@ -354,12 +361,32 @@ fdtd_status fdtd_get_material(fdtd_sim* s, uint8_t* out, size_t count);
  * per-cell ADE update with linearly blended coefficients. */
 fdtd_status fdtd_set_design(fdtd_sim* s, const int box[6], const float* rho,
                             size_t count);
-/* Objective: sum over the listed frequency indices of the absorbed power
- * (AbsTot column).  Forward with checkpoints every K steps. */
+/* Forward with checkpoints: zeroes the state, runs t = 0..Tend and keeps a
+ * copy of the state every checkpoint_every steps for the reverse sweep.
+ * out19 (NUM_freq x 19, may be NULL) gets the ScatAbs table of
+ * fdtd_spectral_finalize. */
+fdtd_status fdtd_forward_spectra(fdtd_sim* s, int checkpoint_every,
+                                 double* out19);
+/* Reverse-time adjoint of the last forward, with segment recompute, for
+ * the objective whose gradient with respect to the ScatAbs table is
+ * dL_dspectra (NUM_freq x 19, row major): any weighted sum of the
+ * scattering, absorption and extinction columns and of the 12 face
+ * fluxes (columns 1-15; columns 0 and 16-18 do not depend on the fields
+ * and must be zero).  dL_drho (may be NULL) has the design box's cell
+ * count; dL_dparams (may be NULL) gets d/d(omega_D), d/d(gamma_D). */
+fdtd_status fdtd_backward_spectra(fdtd_sim* s, const double* dL_dspectra,
+                                  float* dL_drho, size_t count,
+                                  double* dL_dparams);
+/* The absorbed-power objective: fdtd_forward_spectra, then objective =
+ * sum over the listed frequency indices of the absorption cross-section
+ * sigma_abs = P_abs / I_inc (m^2), the net inward flux through the
+ * absorption box, -sum_f s_f q_abs,f over its faces (ScatAbs columns
+ * 10-15, s_f = -1 / +1 on the - / + face of each axis).  It is positive
+ * for an absorbing structure; the reference's AbsTot column is
+ * -sigma_abs for every geometry but its sphere (Spectral.cu:1163-1168). */
 fdtd_status fdtd_forward(fdtd_sim* s, const int* freq_idx, int nfreq,
                          int checkpoint_every, double* objective);
-/* Reverse-time adjoint with segment recompute.  dL_drho has the design
- * box's cell count; dL_dparams gets d/d(omega_D), d/d(gamma_D). */
+/* fdtd_backward_spectra for the objective of the last fdtd_forward. */
 fdtd_status fdtd_backward(fdtd_sim* s, float* dL_drho, size_t count,
                           double* dL_dparams);
 

@@ -47,6 +47,7 @@ struct orc_sim {
   int t;
   int hydro;
   int float_dft, dft_on;
+  unsigned char* dft_sel;     /* per frequency: accumulate (NULL = all) */
   /* fields, reference layout */
   double *E[3], *H[3];
   double *En[3], *En1[3];     /* e*_n, e*_n_1 */
@@ -581,6 +582,7 @@ orc_sim* orc_create(const fdtd_params* pin, char* err) {
 void orc_destroy(orc_sim* s) {
   if (!s) return;
   free(s->rho);
+  free(s->dft_sel);
   for (int c = 0; c < 3; c++) {
     free(s->E[c]); free(s->H[c]); free(s->En[c]); free(s->En1[c]);
     free(s->Pcp[c]); free(s->Pcp_n[c]); free(s->Pcp_n1[c]);
@@ -625,6 +627,17 @@ int orc_set_design(orc_sim* s, const float* rho, size_t count) {
 
 void orc_set_float_dft(orc_sim* s, int on) { s->float_dft = on; }
 void orc_set_dft_enabled(orc_sim* s, int on) { s->dft_on = on; }
+int orc_set_dft_freqs(orc_sim* s, const int* idx, int n) {
+  free(s->dft_sel);
+  s->dft_sel = NULL;
+  if (!idx || n <= 0) return 0;
+  s->dft_sel = (unsigned char*)calloc((size_t)s->NF, 1);
+  for (int q = 0; q < n; q++) {
+    if (idx[q] < 0 || idx[q] >= s->NF) return -1;
+    s->dft_sel[idx[q]] = 1;
+  }
+  return 0;
+}
 int orc_time(const orc_sim* s) { return s->t; }
 
 /* ------------------------------------------------------------------ */
@@ -934,6 +947,9 @@ static void hydro_p(orc_sim* s) {
           s->Pd[c][id] = s->d1 * P[c][id] + s->d2 * s->Pd_n1[c][id] + s->d3 * s->E[c][id] +
                          s->d4 * s->En[c][id] + s->d5 * (0.0 + (s->mu0 * s->e0 / s->me) * 0.0 / s->z0) +
                          s->dNL * (gd + gd2 / NEQ) / cb;
+          /* adjoint design region (no counterpart in the reference): the
+           * current and density updates scale by rho (update_e_comp) */
+          if (s->rho) s->Pd[c][id] *= s->rho[id];
         }
       }
 #undef A
@@ -1059,15 +1075,29 @@ static void update_e_comp(orc_sim* s, int c) {
             for (int q = 0; q < 2; q++) { cpn1[q] = cpn[q]; cpn[q] = ncp[q]; }
           } else {
             double nd = hydro_nd(s, c, i, j, k);
+            /* adjoint design region (no counterpart in the reference): a
+             * design cell scales its current (hydro_p) and density updates
+             * by rho and blends its coupling coefficients as in the local
+             * model, so that rho = 0 is a vacuum cell with J = N = 0 */
+            double CE = s->C_E, CE1 = s->C_E_1, CE2 = s->C_E_2;
+            double C3[2] = {s->C3[0], s->C3[1]}, C4[2] = {s->C4[0], s->C4[1]}, C5[2] = {s->C5[0], s->C5[1]};
+            if (s->rho) {
+              const double r = s->rho[id], vac = K_EP0;
+              nd = r * nd;
+              CE = vac + r * (s->C_E - vac);
+              CE1 = vac + r * (s->C_E_1 - vac);
+              CE2 = r * s->C_E_2;
+              for (int q = 0; q < 2; q++) { C3[q] = r * s->C3[q]; C4[q] = r * s->C4[q]; C5[q] = r * s->C5[q]; }
+            }
             dnd[id] = nd;
             s->En1[c][id] = s->En[c][id];
             s->En[c][id] = E[id];
-            E[id] = (1 / s->C_E) * (s->dt * curl / s->z0 + s->dt * s->Pd[c][id] * s->e0 * (s->N_EQ + nd) +
-                                    s->C_E_1 * s->En[c][id] - s->C_E_2 * s->En1[c][id] - CP2 - CP4);
+            E[id] = (1 / CE) * (s->dt * curl / s->z0 + s->dt * s->Pd[c][id] * s->e0 * (s->N_EQ + nd) +
+                                CE1 * s->En[c][id] - CE2 * s->En1[c][id] - CP2 - CP4);
             double en = s->En[c][id], en1 = s->En1[c][id];
             double ncp[2];
             for (int q = 0; q < 2; q++)
-              ncp[q] = s->C1[q] * cpn[q] + s->C2[q] * cpn1[q] + s->C3[q] * E[id] + s->C4[q] * en + s->C5[q] * en1;
+              ncp[q] = s->C1[q] * cpn[q] + s->C2[q] * cpn1[q] + C3[q] * E[id] + C4[q] * en + C5[q] * en1;
             for (int q = 0; q < 2; q++) { cpn1[q] = cpn[q]; cpn[q] = ncp[q]; }
           }
         } else {
@@ -1142,6 +1172,7 @@ static void dft_accumulate(orc_sim* s) {
   int t = s->t;
 #pragma omp parallel for schedule(dynamic)
   for (int m = 0; m < s->NF; m++) {
+    if (s->dft_sel && !s->dft_sel[m]) continue;
     double ph_e = (double)(float)2.0 * s->pi * (t + 1.0) * s->dt * s->freq[m];
     double ph_h = (double)(float)2.0 * s->pi * (t + 0.5) * s->dt * s->freq[m];
     double cre = cos(ph_e), cim = sin(ph_e), hre = cos(ph_h), him = sin(ph_h);

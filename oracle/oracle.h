@@ -39,6 +39,11 @@ int orc_set_design(orc_sim* s, const float* rho, size_t count);
 void orc_set_float_dft(orc_sim* s, int on);
 /* 0 disables DFT accumulation (CPU-baseline timing of the field update). */
 void orc_set_dft_enabled(orc_sim* s, int on);
+/* Accumulate the DFT at the listed frequency indices only (n = 0: all);
+ * the other frequencies keep zero accumulators.  Each frequency's
+ * accumulators are independent, so the listed ones are unchanged: a
+ * test-time saving for objectives that read a few frequencies. */
+int orc_set_dft_freqs(orc_sim* s, const int* idx, int n);
 void orc_set_threads(int n);
 
 /* One full reference time step t (main.cu:2724-2934); advances t. */

@@ -39,6 +39,7 @@ def lib():
         for f in ("orc_set_float_dft", "orc_set_dft_enabled"):
             getattr(L, f).argtypes = [C.c_void_p, C.c_int]
         L.orc_set_threads.argtypes = [C.c_int]
+        L.orc_set_dft_freqs.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.c_int]
         L.orc_step.argtypes = [C.c_void_p]
         L.orc_run.argtypes = [C.c_void_p, C.c_int]
         L.orc_time.argtypes = [C.c_void_p]
@@ -99,6 +100,11 @@ class OracleSim:
         if getattr(self, "h", None):
             lib().orc_destroy(self.h)
             self.h = None
+
+    def set_dft_freqs(self, idx):
+        """Accumulate the DFT at these frequency indices only."""
+        arr = (C.c_int * len(idx))(*[int(x) for x in idx])
+        assert lib().orc_set_dft_freqs(self.h, arr, len(idx)) == 0
 
     def step(self, n=1):
         lib().orc_run(self.h, n)

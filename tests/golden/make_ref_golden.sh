@@ -5,7 +5,8 @@
 set -euo pipefail
 HERE="$(cd "$(dirname "$0")" && pwd)"
 ROOT="$(cd "$HERE/../.." && pwd)"
-OUT="${1:-$ROOT/gpurun_out/ref_golden}"
+if [ $# -lt 1 ]; then echo "usage: $0 <output directory>" >&2; exit 2; fi
+OUT="$1"
 BIN="$ROOT/oracle/_ref/fdtd_ref"
 test -x "$BIN"
 python "$HERE/ref_cases.py" "$OUT"

@@ -1,7 +1,9 @@
-"""Reverse-time adjoint (fdtd_set_design / fdtd_forward / fdtd_backward):
-gradients of the absorbed power at three frequencies with respect to the
-per-cell blend rho of a design box and to the Drude omega_D and gamma,
-checked against central finite differences of the forward objective."""
+"""Reverse-time adjoint (fdtd_set_design / fdtd_forward / fdtd_backward and
+the general fdtd_forward_spectra / fdtd_backward_spectra): gradients of the
+absorption cross-section at three frequencies, and of weighted sums of the
+ScatAbs table, with respect to the per-cell blend rho of a design box and
+to the Drude omega_D and gamma, checked against central finite differences
+of the forward objective."""
 import numpy as np
 import pytest
 
@@ -16,6 +18,15 @@ SEL = [2, 4, 6]
 GOLD = dict(metal_custom=1, eps_inf=1.1431, omega_D=1.3202e16, gamma_D=1.0805e14,
             cp_A=(0.26698, 3.0834), cp_phi=(-1.2371, -1.0968),
             cp_Omega=(3.8711e15, 4.1684e15), cp_Gamma=(4.4642e14, 2.3555e15))
+
+
+# absorption cross-section from the ScatAbs face columns 10-15: the net
+# inward flux, -sum_f s_f q_abs,f with s_f = -1, +1 on the -, + faces
+SIGMA_ABS = np.array([1.0, -1.0, 1.0, -1.0, 1.0, -1.0])
+
+
+def sigma_abs(table, sel):
+    return float(np.sum(table[sel][:, 10:16] @ SIGMA_ABS))
 
 
 def design_sim(prec, **over):
@@ -188,7 +199,7 @@ def test_adjoint_matches_oracle_gradient(fp64_grad):
         o = O.OracleSim(make(O, "vacuum", precision=1, Tend=300, design_box=BOX, **GOLD))
         o.set_design(rho)
         o.step(301)
-        return float(o.spectra()[SEL, 2].sum())
+        return sigma_abs(o.spectra(), SEL)
 
     rho, h = rho0(), 1e-3
     assert oracle_objective(rho) == pytest.approx(L, rel=1e-10)
@@ -198,3 +209,101 @@ def test_adjoint_matches_oracle_gradient(fp64_grad):
         fd = (lp - lm) / (2 * h)
         print(c, "oracle fd", fd, "adjoint", g[c])
         assert abs(fd - g[c]) <= 1e-3 * abs(fd)
+
+
+def test_objective_is_the_positive_absorption_cross_section(fp64_grad):
+    """fdtd_forward's objective is sigma_abs summed over the frequencies:
+    -AbsTot for a geometry other than the reference's sphere, and positive
+    for the absorbing design box."""
+    s, L, _, _ = fp64_grad
+    s.set_design(rho0())
+    table = s.forward_spectra(50)
+    assert sigma_abs(table, SEL) == pytest.approx(L, rel=1e-12)
+    assert -float(table[SEL, 2].sum()) == pytest.approx(L, rel=1e-12)
+    assert L > 0
+
+
+def test_backward_spectra_of_the_same_objective_matches_backward(fp64_grad):
+    s, L, g, gp = fp64_grad
+    s.set_design(rho0())
+    s.forward_spectra(50)
+    G = np.zeros((s.dims.num_freq, 19))
+    G[SEL, 10:16] = SIGMA_ABS
+    g2, gp2 = s.backward_spectra(G)
+    np.testing.assert_allclose(g2, g, rtol=1e-12, atol=1e-12 * np.abs(g).max())
+    np.testing.assert_allclose(gp2, gp, rtol=1e-12)
+
+
+def weighted_objective(table):
+    """A mixed objective over the ScatAbs table: scattering, absorption and
+    extinction at different frequencies and weights, and two face fluxes
+    of the scattering box."""
+    return (2.0 * table[1, 1] - 0.5 * table[3, 2] + 1.5 * table[5, 3] + 0.7 * table[7, 6]
+            - 1.3 * table[2, 9] + table[4, 12])
+
+
+def weighted_G(nf):
+    G = np.zeros((nf, 19))
+    G[1, 1] = 2.0
+    G[3, 2] = -0.5
+    G[5, 3] = 1.5
+    G[7, 6] = 0.7
+    G[2, 9] = -1.3
+    G[4, 12] = 1.0
+    return G
+
+
+@pytest.mark.parametrize("name", ["vacuum", "sphere_au"])
+def test_general_objective_matches_central_differences(name):
+    """dL/drho and dL/d(omega_D, gamma) of a weighted sum of ScatAbs
+    columns (totals and faces of both boxes) against central differences.
+    sphere_au uses the reference's sphere normalisation (pi r^2) of the
+    totals."""
+    p = make(F, name, precision=F.FDTD_FP64, Tend=300, design_box=BOX, **GOLD)
+    if name == "sphere_au":
+        p.nano_sphere_radius = 4e-9
+        for a, v in enumerate([13, 16, 13, 16, 13, 16]):
+            p.design_box[a] = v
+    s = F.Sim(p)
+    b = list(p.design_box)
+    rng = np.random.default_rng(7)
+    rho = rng.uniform(0, 1, (b[5] - b[4], b[3] - b[2], b[1] - b[0])).astype(np.float32)
+    s.set_design(rho)
+    L = weighted_objective(s.forward_spectra(50))
+    g, gp = s.backward_spectra(weighted_G(s.dims.num_freq))
+    h = 1e-3
+    for c in [(0, 0, 0), (1, 2, 1)]:
+        r = rho.copy(); r[c] += h; s.set_design(r); lp = weighted_objective(s.forward_spectra(50))
+        r = rho.copy(); r[c] -= h; s.set_design(r); lm = weighted_objective(s.forward_spectra(50))
+        fd = (lp - lm) / (2 * h)
+        print(name, c, "L", L, "fd", fd, "adjoint", g[c])
+        assert abs(fd - g[c]) <= 1e-3 * abs(fd), (c, fd, g[c])
+    s.close()
+    for k, pname in enumerate(("omega_D", "gamma_D")):
+        v = GOLD[pname]
+        hv = v * 1e-4
+        vals = []
+        for x in (v + hv, v - hv):
+            setattr(p, pname, x)
+            q = F.Sim(p)
+            q.set_design(rho)
+            vals.append(weighted_objective(q.forward_spectra(50)))
+            q.close()
+        setattr(p, pname, v)
+        fd = (vals[0] - vals[1]) / (2 * hv)
+        print(name, pname, "fd", fd, "adjoint", gp[k])
+        assert abs(fd - gp[k]) <= 1e-3 * abs(fd), (pname, fd, gp[k])
+
+
+def test_backward_spectra_rejects_field_free_columns(fp64_grad):
+    s = fp64_grad[0]
+    s.set_design(rho0())
+    s.forward_spectra(50)
+    G = np.zeros((s.dims.num_freq, 19))
+    G[0, 0] = 1.0
+    with pytest.raises(F.FdtdError) as e:
+        s.backward_spectra(G)
+    assert e.value.status == 1
+    with pytest.raises(F.FdtdError) as e:  # forward_spectra has no objective of its own
+        s.backward()
+    assert e.value.status == 5

@@ -31,24 +31,23 @@ def family_errors(sa, sb):
 
 @pytest.mark.parametrize("prec", [F.FDTD_FP32, F.FDTD_FP64])
 def test_batch_matches_sequential(prec):
+    """Bit-identical: the batched passes run the same per-cell arithmetic
+    (fixed-rounding operations, so neither the tile shape nor the CPML-free
+    or CPML-edge instantiation changes a result), and every other kernel of
+    the step is the same body launched over all members."""
     params = [make(F, name, precision=prec, **over) for name, over in MEMBERS]
     steps = 300  # two graph periods of 128 plus an eager tail
     b = F.Batch(params)
     b.step(steps)
-    tol = 1e-12 if prec == F.FDTD_FP64 else 2e-6
     for i, p in enumerate(params):
         alone = F.Sim(p)
         alone.step(steps)
         m = b.sim(i)
         assert m.t == alone.t == steps
-        errs = family_errors(m, alone)
-        print(i, "field errors", errs)
-        assert max(errs) < tol, (i, errs)
-        pa, pb = m.probe(), alone.probe()
-        assert pa.shape == pb.shape
-        assert rel(pa, pb) < tol * 10
-        sa, sb = b.spectra(i), alone.spectra()
-        assert rel(sa[:, 1:4], sb[:, 1:4]) < (1e-10 if prec == F.FDTD_FP64 else 1e-4)
+        for c in range(6):
+            np.testing.assert_array_equal(m.field(c), alone.field(c), err_msg=f"member {i} component {c}")
+        np.testing.assert_array_equal(m.probe(), alone.probe())
+        np.testing.assert_array_equal(b.spectra(i), alone.spectra())
         alone.close()
     kernels, graphs = b.stats()
     assert graphs == 2 and kernels > 0
