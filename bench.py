@@ -358,11 +358,9 @@ def large_bench(mod, torch, stream, sp, dev, blocks=2, adjoint_steps=12000):
     cells = d.nx * d.ny * d.nz
     out = {"value": round(cells * BLOCK * blocks / (ms / 1e3) / 1e9, 3), "unit": "Gcell-steps/s",
            "grid": [d.nx, d.ny, d.nz], "time_steps": BLOCK * blocks,
-           "dispersive_cells": list(d.n_metal_cells), "device_bytes": int(free0 - free1),
-           "adjoint": "not built for the hydrodynamic model (nonlinear in the current and density); "
-                      "see adjoint_local for the same geometry with the local model"}
+           "dispersive_cells": list(d.n_metal_cells), "device_bytes": int(free0 - free1)}
     s.close()
-    out["adjoint_local"] = large_adjoint_bench(mod, torch, dev, steps=adjoint_steps)
+    out["adjoint"] = large_adjoint_bench(mod, torch, dev, steps=adjoint_steps)
     return out
 
 
@@ -371,16 +369,16 @@ LARGE_FREQS = [0, 1, 2, 3, 4]
 
 
 def large_adjoint_bench(mod, torch, dev, steps=12000, every=400):
-    """The adjoint at the large geometry with the local Drude+2CP model: a
-    64 x 64 x 10 design region over the central disk, rho ~ U[0, 1] from
-    the seed, objective = the absorption cross-section summed over the 5
+    """The adjoint at the large geometry with the hydrodynamic model: a
+    64 x 64 x 10 design region over the central disk (its cells blend
+    between vacuum and the hydrodynamic metal), rho ~ U[0, 1] from the
+    seed, objective = the absorption cross-section summed over the 5
     wavelengths, checkpoints every 400 steps, `steps` time steps (the whole
     12000-step run by default: the pulse, delayed by 4908 steps, has passed
     the disks); forward and backward throughput and the device memory the
     checkpoints and adjoint state take."""
     import numpy as np
     p = large_params(mod)
-    p.NONLOCAL = 0
     p.Tend = steps - 1
     for a, v in enumerate(LARGE_DESIGN):
         p.design_box[a] = v
@@ -404,7 +402,7 @@ def large_adjoint_bench(mod, torch, dev, steps=12000, every=400):
     d = s.dims
     cs = d.nx * d.ny * d.nz * steps
     out = {"grid": [d.nx, d.ny, d.nz], "design": [64, 64, 10], "time_steps": steps,
-           "full_run_steps": 12000, "checkpoint_every": every, "model": "local Drude+2CP",
+           "full_run_steps": 12000, "checkpoint_every": every, "model": "hydrodynamic (Drude+2CP + nonlocal current)",
            "forward_s": round(t1 - t0, 3), "backward_s": round(t2 - t1, 3),
            "ratio": round((t2 - t1) / (t1 - t0), 3),
            "forward_gcell_steps_per_s": round(cs / (t1 - t0) / 1e9, 2),
