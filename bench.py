@@ -282,6 +282,7 @@ def batch_bench(mod, torch, stream, sp, dev, n, steps):
     torch.cuda.synchronize()
     t_batch = ev[0].elapsed_time(ev[1]) / 1e3
     launches = b.stats()[0]
+    tuning = b.tuning()
     for i in range(n):
         b.sim(i).check()
     cells = sum(p.NCELLX + 21 for p in params)
@@ -303,7 +304,8 @@ def batch_bench(mod, torch, stream, sp, dev, n, steps):
             "speedup": round(t_seq / t_batch, 2), "members": n, "time_steps": steps,
             "batched_s": round(t_batch, 3), "sequential_s": round(t_seq, 3),
             "batched_gcell_steps_per_s": round(total / t_batch / 1e9, 2),
-            "edges": [min(edges), max(edges)], "seed": BATCH_SEED, "gpu_launches": launches}
+            "edges": [min(edges), max(edges)], "seed": BATCH_SEED, "gpu_launches": launches,
+            "tuning": tuning}
 
 
 def adjoint_params(mod, steps=4000, precision=None):
@@ -512,11 +514,23 @@ def ref_gpu_build(t1=40, t2=240):
             shutil.rmtree(d, ignore_errors=True)
     cells = 256 ** 3
     rate = cells * (t2 - t1) / max(walls[1] - walls[0], 1e-9) / 1e9
-    return {"value": round(rate, 4), "unit": "Gcell-steps/s", "dtype": "f64",
-            "deck": "256^3, Au sphere r = 10 nm, hydrodynamic model, 12-cell CPML, "
-                    "201 wavelengths, dx = 1 nm",
-            "method": f"wall time of {t2} minus {t1} time steps of the whole program",
-            "wall_s": [round(w, 3) for w in walls]}
+    out = {"value": round(rate, 4), "unit": "Gcell-steps/s", "dtype": "f64",
+           "deck": "256^3, Au sphere r = 10 nm, hydrodynamic model, 12-cell CPML, "
+                   "201 wavelengths, dx = 1 nm",
+           "method": f"wall time of {t2} minus {t1} time steps of the whole program",
+           "wall_s": [round(w, 3) for w in walls]}
+    # kernel time alone, from an ncu launch list of the same program on the
+    # same deck (profiles/reference_cuda_kernels_256.md)
+    try:
+        with open(os.path.join(ROOT, "profiles", "reference_kernels.json")) as f:
+            k = json.load(f)
+        out["kernel_only"] = {"value": round(cells / (k["kernel_ms_per_step"] / 1e3) / 1e9, 4),
+                              "unit": "Gcell-steps/s", "kernel_ms_per_step": k["kernel_ms_per_step"],
+                              "source": "profiles/reference_cuda_kernels_256.md (ncu gpu__time_duration.sum, "
+                                        f"{k['steps']} time steps)"}
+    except (OSError, ValueError, KeyError):
+        pass
+    return out
 
 
 def run_reference(args, rank, world):
@@ -566,7 +580,18 @@ def main():
     ap.add_argument("--batch-steps", type=int, default=3000)
     ap.add_argument("--no-ref-gpu", action="store_true",
                     help="reference arm: skip timing the reference's own CUDA build")
+    ap.add_argument("--write-ref-deck", metavar="DIR",
+                    help="write the reference-geometry deck (Input.txt, videofiles/) into DIR and exit: "
+                         "the working directory for running or profiling the reference's own build")
+    ap.add_argument("--ref-tend", type=int, default=40, help="Tend of the deck --write-ref-deck writes")
     args = ap.parse_args()
+    if args.write_ref_deck:
+        sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+        from ref_cases import deck
+        os.makedirs(os.path.join(args.write_ref_deck, "videofiles"), exist_ok=True)
+        with open(os.path.join(args.write_ref_deck, "Input.txt"), "w") as f:
+            f.write(deck(ref_deck_case(args.ref_tend)))
+        return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -21,6 +21,7 @@
 // sample step.
 #pragma once
 #include "kernels.cuh"
+#include "staged.cuh"
 
 namespace fdtd {
 
@@ -919,12 +920,25 @@ __device__ __forceinline__ bool adj_block_simple(const SimView<T>& s, int i0, in
 // lambda_H += gather of the E-sub-step coefficients (adj_gather_h's sums),
 // the non-special coefficients computed from lambda_E of the cell and of
 // its +x, +y, +z neighbours.  Grid (x tiles of 32, y rows of 8, z).
+// Block (x tile of 32, y row of 8, plane) of a fused gather: the launch
+// grid itself, or entry blockIdx.x of a table (the blocks the staged
+// gathers leave).
+__device__ __forceinline__ int3 adj_block(const int4* table) {
+  if (table) {
+    const int4 b = table[blockIdx.x];
+    return make_int3(b.x, b.y, b.z);
+  }
+  return make_int3((int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z);
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256) adj_gather_h_fused(const __grid_constant__ SimView<T> s,
-                                                          const __grid_constant__ AdjView<T> a) {
-  const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y, k = blockIdx.z;
+                                                          const __grid_constant__ AdjView<T> a,
+                                                          const int4* __restrict__ table) {
+  const int3 bk = adj_block(table);
+  const int i = bk.x * 32 + threadIdx.x, j = bk.y * 8 + threadIdx.y, k = bk.z;
   const size_t sx = 1, sy = s.PX, sz = s.plane;
-  if (adj_block_simple(s, blockIdx.x * 32, blockIdx.y * 8, k, 0, 1)) {
+  if (adj_block_simple(s, bk.x * 32, bk.y * 8, k, 0, 1)) {
     // the same sums with every coefficient sg ceh0 ikd lambda_E
     const size_t id = fidx(s.PX, s.plane, i, j, k);
     const T ceh = s.ceh[0];
@@ -979,10 +993,12 @@ __global__ void __launch_bounds__(256) adj_gather_h_fused(const __grid_constant_
 // lambda_H of the cell and of its -x, -y, -z neighbours.
 template <typename T>
 __global__ void __launch_bounds__(256) adj_gather_e_fused(const __grid_constant__ SimView<T> s,
-                                                          const __grid_constant__ AdjView<T> a) {
-  const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y, k = blockIdx.z;
+                                                          const __grid_constant__ AdjView<T> a,
+                                                          const int4* __restrict__ table) {
+  const int3 bk = adj_block(table);
+  const int i = bk.x * 32 + threadIdx.x, j = bk.y * 8 + threadIdx.y, k = bk.z;
   const size_t sx = 1, sy = s.PX, sz = s.plane;
-  if (adj_block_simple(s, blockIdx.x * 32, blockIdx.y * 8, k, -1, 0)) {
+  if (adj_block_simple(s, bk.x * 32, bk.y * 8, k, -1, 0)) {
     // the same sums with every coefficient sg che ikh lambda_H, after
     // lambda_E <- cee0 lambda_E
     const size_t id = fidx(s.PX, s.plane, i, j, k);
@@ -1037,6 +1053,161 @@ __global__ void __launch_bounds__(256) adj_gather_e_fused(const __grid_constant_
           (px ? adj_h_coef_f(s, a, 1, 1, i - 1, id - sx, fx, hyx) : T(0)) - adj_h_coef_f(s, a, 1, 1, i, id, f0, hy0);
 #pragma unroll
   for (int c = 0; c < 3; c++) a.lE[c][id] = l[c];
+}
+
+// ---------------------------------------------------------------------
+// Staged z-march form of the fused gathers over the "simple" tiles: a CTA
+// owns a 32 x 8 tile and a z-chunk whose cells, with the one-cell halo they
+// read, lie away from the CPML slabs and outside the material box (every
+// coefficient is sg ceh0 ik lambda_E, or sg che ik lambda_H).  The adjoint
+// planes stream through the shared-memory ring of the forward passes
+// (staged.cuh), with the same data movement: adj_gather_h reads lambda_E at
+// planes k and k + 1 with the +x and +y halo and updates lambda_H, as the H
+// pass reads E and updates H; adj_gather_e reads lambda_H at k - 1 and k
+// with the -x and -y halo and updates lambda_E, as the E pass.  Each
+// difference term is the product and sum order of the fused gathers.  The
+// host builds the tile table (adj_staged_tiles) and hands the remaining
+// blocks to the fused gathers.
+constexpr int kAdjTY = 8, kAdjS = 4, kAdjKC = 16;
+
+template <typename T>
+__global__ void __launch_bounds__(32 * kAdjTY) adj_gather_h_staged(const __grid_constant__ SimView<T> s,
+                                                                   const __grid_constant__ AdjView<T> a,
+                                                                   const int4* __restrict__ tiles) {
+  constexpr int TY = kAdjTY, S = kAdjS;
+  using L = StageLayout<T, TY>;
+  constexpr unsigned SB = L::STAGE * sizeof(T);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const T* sm = reinterpret_cast<const T*>(smem_raw);
+  const unsigned sbase = (unsigned)__cvta_generic_to_shared(smem_raw);
+  const int4 tl = tiles[blockIdx.x];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int i0 = tl.x * 32, j0 = tl.y * TY;
+  const int i = i0 + tx, j = j0 + ty;
+  const int NY = s.NY, NZ = s.NZ, PX = s.PX;
+  const size_t plane = s.plane;
+  const int k0 = tl.z * kAdjKC, k1 = min(NZ, k0 + kAdjKC);
+  CopyTasks<T, TY> tasks;
+  tasks.init(sbase, a.lE[0], a.lE[1], a.lE[2], a.lH[0], a.lH[1], a.lH[2], NY, PX, plane, k0, i0, j0, 0, 0);
+  int pnext = k0;
+#pragma unroll
+  for (int q = 0; q < S - 1; q++) {
+    tasks.issue(q * SB, pnext++, NZ, a.lE[0], plane);
+    cp_async_commit();
+  }
+  const T ceh = s.ceh[0];
+  const T kx = ldg(s.cp[0].inv_ked + i), kx1 = ldg(s.cp[0].inv_ked + i + 1);
+  const T ky = ldg(s.cp[1].inv_ked + j), ky1 = ldg(s.cp[1].inv_ked + j + 1);
+  const T* __restrict__ kzp = s.cp[2].inv_ked + k0;
+  const size_t id0 = fidx(PX, plane, i, j, k0);
+  T* __restrict__ phx = a.lH[0] + id0;
+  T* __restrict__ phy = a.lH[1] + id0;
+  T* __restrict__ phz = a.lH[2] + id0;
+  const int o = ty * L::HW + tx, oo = ty * 32 + tx;
+  constexpr int FH = (TY + 1) * L::HW;
+  for (int k = k0; k < k1;) {
+#pragma unroll
+    for (int u = 0; u < S; u++) {
+      if (k < k1) {
+        cp_async_wait<S - 3>();  // planes up to k+1 have landed
+        __syncthreads();
+        tasks.issue(((u + S - 1) % S) * SB, pnext++, NZ, a.lE[0], plane);
+        cp_async_commit();
+        const T* eh = sm + u * L::STAGE;
+        const T* en = sm + ((u + 1) % S) * L::STAGE;
+        const T* hown = eh + L::HALO;
+        const T ex0 = eh[o], ey0 = eh[FH + o], ez0 = eh[2 * FH + o];
+        const T ex_y = eh[o + L::HW], ez_y = eh[2 * FH + o + L::HW];
+        const T ey_x = eh[FH + o + 1], ez_x = eh[2 * FH + o + 1];
+        const T ex_z = en[o], ey_z = en[FH + o];
+        const T kz = ldg(kzp), kz1 = ldg(kzp + 1);
+        // Hx: Ey slot 0 (axis z, sg +1), Ez slot 1 (axis y, sg -1)
+        *phx = hown[oo] + (adj_mul(T(1) * ceh * kz, ey0) - adj_mul(T(1) * ceh * kz1, ey_z) +
+                           adj_mul(T(-1) * ceh * ky, ez0) - adj_mul(T(-1) * ceh * ky1, ez_y));
+        // Hy: Ex slot 1 (axis z, sg -1), Ez slot 0 (axis x, sg +1)
+        *phy = hown[TY * 32 + oo] + (adj_mul(T(-1) * ceh * kz, ex0) - adj_mul(T(-1) * ceh * kz1, ex_z) +
+                                     adj_mul(T(1) * ceh * kx, ez0) - adj_mul(T(1) * ceh * kx1, ez_x));
+        // Hz: Ex slot 0 (axis y, sg +1), Ey slot 1 (axis x, sg -1)
+        *phz = hown[2 * TY * 32 + oo] + (adj_mul(T(1) * ceh * ky, ex0) - adj_mul(T(1) * ceh * ky1, ex_y) +
+                                         adj_mul(T(-1) * ceh * kx, ey0) - adj_mul(T(-1) * ceh * kx1, ey_x));
+        phx += plane; phy += plane; phz += plane; kzp++;
+        k++;
+      }
+    }
+  }
+  cp_async_wait<0>();
+}
+
+template <typename T>
+__global__ void __launch_bounds__(32 * kAdjTY) adj_gather_e_staged(const __grid_constant__ SimView<T> s,
+                                                                   const __grid_constant__ AdjView<T> a,
+                                                                   const int4* __restrict__ tiles) {
+  constexpr int TY = kAdjTY, S = kAdjS;
+  using L = StageLayout<T, TY>;
+  constexpr unsigned SB = L::STAGE * sizeof(T);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const T* sm = reinterpret_cast<const T*>(smem_raw);
+  const unsigned sbase = (unsigned)__cvta_generic_to_shared(smem_raw);
+  const int4 tl = tiles[blockIdx.x];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int i0 = tl.x * 32, j0 = tl.y * TY;
+  const int i = i0 + tx, j = j0 + ty;
+  const int NY = s.NY, NZ = s.NZ, PX = s.PX;
+  const size_t plane = s.plane;
+  const int k0 = tl.z * kAdjKC, k1 = min(NZ, k0 + kAdjKC);
+  CopyTasks<T, TY> tasks;
+  tasks.init(sbase, a.lH[0], a.lH[1], a.lH[2], a.lE[0], a.lE[1], a.lE[2], NY, PX, plane, k0 - 1, i0, j0, -1, -L::CH);
+  int pnext = k0 - 1;
+#pragma unroll
+  for (int q = 0; q < S - 1; q++) {
+    tasks.issue(q * SB, pnext++, NZ, a.lH[0], plane);
+    cp_async_commit();
+  }
+  const T che = s.che, cee = s.cee[0];
+  const T kx = ldg(s.cp[0].inv_khd + i), kxm = ldg(s.cp[0].inv_khd + i - 1);
+  const T ky = ldg(s.cp[1].inv_khd + j), kym = ldg(s.cp[1].inv_khd + j - 1);
+  const T* __restrict__ kzp = s.cp[2].inv_khd + k0;
+  const size_t id0 = fidx(PX, plane, i, j, k0);
+  T* __restrict__ pex = a.lE[0] + id0;
+  T* __restrict__ pey = a.lE[1] + id0;
+  T* __restrict__ pez = a.lE[2] + id0;
+  const int o = (ty + 1) * L::HW + tx + L::CH, oo = ty * 32 + tx;
+  constexpr int FH = (TY + 1) * L::HW;
+  for (int k = k0; k < k1;) {
+#pragma unroll
+    for (int u = 0; u < S; u++) {
+      if (k < k1) {
+        cp_async_wait<S - 3>();  // planes up to k have landed
+        __syncthreads();
+        tasks.issue(((u + S - 1) % S) * SB, pnext++, NZ, a.lH[0], plane);
+        cp_async_commit();
+        const T* cur = sm + ((u + 1) % S) * L::STAGE;
+        const T* prv = sm + u * L::STAGE;
+        const T* eown = cur + L::HALO;
+        const T hx0 = cur[o], hy0 = cur[FH + o], hz0 = cur[2 * FH + o];
+        const T hx_y = cur[o - L::HW], hz_y = cur[2 * FH + o - L::HW];
+        const T hy_x = cur[FH + o - 1], hz_x = cur[2 * FH + o - 1];
+        const T hx_z = prv[o], hy_z = prv[FH + o];
+        const T kz = ldg(kzp), kzm = ldg(kzp - 1);
+        T l0 = adj_mul(cee, eown[oo]), l1 = adj_mul(cee, eown[TY * 32 + oo]), l2 = adj_mul(cee, eown[2 * TY * 32 + oo]);
+        // Ex: Hy slot 0 (axis z, sg -1), Hz slot 1 (axis y, sg +1)
+        l0 += adj_mul(T(-1) * che * kzm, hy_z) - adj_mul(T(-1) * che * kz, hy0) +
+              adj_mul(T(1) * che * kym, hz_y) - adj_mul(T(1) * che * ky, hz0);
+        // Ey: Hx slot 1 (axis z, sg +1), Hz slot 0 (axis x, sg -1)
+        l1 += adj_mul(T(1) * che * kzm, hx_z) - adj_mul(T(1) * che * kz, hx0) +
+              adj_mul(T(-1) * che * kxm, hz_x) - adj_mul(T(-1) * che * kx, hz0);
+        // Ez: Hx slot 0 (axis y, sg -1), Hy slot 1 (axis x, sg +1)
+        l2 += adj_mul(T(-1) * che * kym, hx_y) - adj_mul(T(-1) * che * ky, hx0) +
+              adj_mul(T(1) * che * kxm, hy_x) - adj_mul(T(1) * che * kx, hy0);
+        *pex = l0;
+        *pey = l1;
+        *pez = l2;
+        pex += plane; pey += plane; pez += plane; kzp++;
+        k++;
+      }
+    }
+  }
+  cp_async_wait<0>();
 }
 
 }  // namespace fdtd

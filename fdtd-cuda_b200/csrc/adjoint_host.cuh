@@ -49,6 +49,11 @@ struct fdtd_sim::Adjoint {
   double* grho[3] = {nullptr, nullptr, nullptr};
   double* gpar = nullptr;
   int* step = nullptr;
+  // staged-gather tiles (adj_gather_*_staged) and the blocks the fused
+  // gathers take, per gather (0 = H, 1 = E)
+  std::unique_ptr<DevBuf> gtab[2][2];
+  int ntile[2] = {0, 0}, nleft[2] = {0, 0};
+  bool tabs = false;
   // graphs of one full segment: the recompute (DFT off, recording on) and
   // the reverse sweep; replayed for every full segment
   cudaGraphExec_t g_rec = nullptr, g_adj = nullptr;
@@ -396,8 +401,9 @@ static fdtd_status adj_sweep(fdtd_sim* s) {
   m.rec_slots = A.rec_slots;
   for (int c = 0; c < 3; c++) m.rec_off[c] = A.rec_off[c];
   const int every_dft = s->line.dft_every;
-  const bool graphs = s->use_graphs;
+  const bool graphs = s->use_graphs, snaps = s->snap_on;
   s->line.dft_every = 0;  // the recompute needs no DFT samples
+  s->snap_on = false;     // nor snapshots
   s->use_graphs = false;
   const long long ncell = (long long)s->NX * s->NY * s->NZ;
   const unsigned gc = (unsigned)((ncell + 255) / 256);
@@ -426,6 +432,77 @@ static fdtd_status adj_sweep(fdtd_sim* s) {
   }
   const dim3 gtile((unsigned)((s->NX + 31) / 32), (unsigned)((s->NY + 7) / 8), (unsigned)s->NZ);
   if (fused) adj_build_flags<T><<<gtile, dim3(32, 8)>>>(view<T>(s), a.flags);
+  // staged tiles: 32 x kAdjTY x kAdjKC boxes whose cells and halo (+1 for
+  // the H gather, -1 for the E gather) are simple (adj_block_simple); the
+  // fused gathers take every other 32 x 8 block, one plane each
+  const char* senv = std::getenv("FDTD_ADJ_STAGED");
+  const bool staged = fused && !(senv && senv[0] == '0');
+  if (staged && !A.tabs) {
+    static_assert(kAdjTY == 8, "the staged tiles and the fused gathers' blocks share the 32 x 8 xy grid");
+    const int nbx = (s->NX + 31) / 32, nby = (s->NY + 7) / 8, nbz = (s->NZ + kAdjKC - 1) / kAdjKC;
+    for (int g = 0; g < 2; g++) {
+      const int lo_off = g == 0 ? 0 : -1, hi_off = g == 0 ? 1 : 0;
+      std::vector<int4> tiles, left;
+      std::vector<char> cover((size_t)nbx * nby * nbz, 0);
+      for (int bz = 0; bz < nbz; bz++)
+        for (int by = 0; by < nby; by++)
+          for (int bx = 0; bx < nbx; bx++) {
+            const int lo[3] = {bx * 32 + lo_off, by * 8 + lo_off, bz * kAdjKC + lo_off};
+            const int hi[3] = {bx * 32 + 31 + hi_off, by * 8 + 7 + hi_off,
+                               std::min(s->NZ, (bz + 1) * kAdjKC) - 1 + hi_off};
+            bool inside = true, off_mat = false;
+            for (int ax = 0; ax < 3; ax++) {
+              inside = inside && lo[ax] >= s->su.Nc[ax] + 1 && hi[ax] < s->su.F[ax];
+              off_mat = off_mat || hi[ax] < s->mat_lo[ax] || lo[ax] >= s->mat_hi[ax];
+            }
+            if (inside && off_mat) {
+              tiles.push_back(make_int4(bx, by, bz, 0));
+              cover[((size_t)bz * nby + by) * nbx + bx] = 1;
+            }
+          }
+      for (int k = 0; k < s->NZ; k++)
+        for (int by = 0; by < nby; by++)
+          for (int bx = 0; bx < nbx; bx++)
+            if (!cover[((size_t)(k / kAdjKC) * nby + by) * nbx + bx]) left.push_back(make_int4(bx, by, k, 0));
+      for (int q = 0; q < 2; q++) {
+        const std::vector<int4>& v = q == 0 ? tiles : left;
+        auto b = std::make_unique<DevBuf>();
+        CUDA_TRY(b->alloc(std::max<size_t>(1, v.size()) * sizeof(int4)));
+        if (!v.empty()) CUDA_TRY(cudaMemcpy(b->p, v.data(), v.size() * sizeof(int4), cudaMemcpyHostToDevice));
+        A.gtab[g][q] = std::move(b);
+      }
+      A.ntile[g] = (int)tiles.size();
+      A.nleft[g] = (int)left.size();
+    }
+    const int smem = (int)(kAdjS * StageLayout<T, kAdjTY>::STAGE * sizeof(T));
+    CUDA_TRY(cudaFuncSetAttribute(adj_gather_h_staged<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    CUDA_TRY(cudaFuncSetAttribute(adj_gather_e_staged<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    A.tabs = true;
+  }
+  const size_t gsmem = kAdjS * StageLayout<T, kAdjTY>::STAGE * sizeof(T);
+  // one gather: the staged tiles and the fused blocks (disjoint outputs,
+  // inputs they do not write); returns the launches
+  auto gather = [&](int g, cudaStream_t stream) -> int {
+    if (!staged) {
+      if (g == 0) adj_gather_h_fused<T><<<gtile, dim3(32, 8), 0, stream>>>(view<T>(s), a, nullptr);
+      else adj_gather_e_fused<T><<<gtile, dim3(32, 8), 0, stream>>>(view<T>(s), a, nullptr);
+      return 1;
+    }
+    int k = 0;
+    const int4* tt = static_cast<const int4*>(A.gtab[g][0]->p);
+    const int4* lt = static_cast<const int4*>(A.gtab[g][1]->p);
+    if (A.ntile[g]) {
+      if (g == 0) adj_gather_h_staged<T><<<A.ntile[g], dim3(32, kAdjTY), gsmem, stream>>>(view<T>(s), a, tt);
+      else adj_gather_e_staged<T><<<A.ntile[g], dim3(32, kAdjTY), gsmem, stream>>>(view<T>(s), a, tt);
+      k++;
+    }
+    if (A.nleft[g]) {
+      if (g == 0) adj_gather_h_fused<T><<<A.nleft[g], dim3(32, 8), 0, stream>>>(view<T>(s), a, lt);
+      else adj_gather_e_fused<T><<<A.nleft[g], dim3(32, 8), 0, stream>>>(view<T>(s), a, lt);
+      k++;
+    }
+    return k;
+  };
   // the dispersive cells' transposed update: the local model in one
   // launch; the hydrodynamic model as its three phases in reverse order,
   // then the current update
@@ -451,12 +528,12 @@ static fdtd_status adj_sweep(fdtd_sim* s) {
       if (she.total() > 0)
         adj_e_slab<T><<<(unsigned)((she.total() + 255) / 256), 256, 0, stream>>>(view<T>(s), a, she);
       const int kd = ntot > 0 ? launch_design(stream) : 0;
-      adj_gather_h_fused<T><<<gtile, dim3(32, 8), 0, stream>>>(view<T>(s), a);
+      const int kg = gather(0, stream);
       if (shh.total() > 0)
         adj_h_slab<T><<<(unsigned)((shh.total() + 255) / 256), 256, 0, stream>>>(view<T>(s), a, shh);
-      adj_gather_e_fused<T><<<gtile, dim3(32, 8), 0, stream>>>(view<T>(s), a);
+      const int kg2 = gather(1, stream);
       adj_step_back<<<1, 1, 0, stream>>>(A.step);
-      return 4 + (she.total() > 0) + (shh.total() > 0) + kd + (n % every_dft == 0);
+      return 1 + kg + kg2 + (she.total() > 0) + (shh.total() > 0) + kd + (n % every_dft == 0);
     }
     adj_e_coef<T><<<gc, 256, 0, stream>>>(view<T>(s), a);
     const int kd = ntot > 0 ? launch_design(stream) : 0;
@@ -521,6 +598,7 @@ static fdtd_status adj_sweep(fdtd_sim* s) {
   m.hrec = nullptr;
   s->line.dft_every = every_dft;
   s->use_graphs = graphs;
+  s->snap_on = snaps;
   CUDA_TRY(cudaDeviceSynchronize());
   return st;
 }

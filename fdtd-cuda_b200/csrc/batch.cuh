@@ -78,9 +78,18 @@ __global__ void dft_reset_batch(const BatchSim<T>* __restrict__ b) {
 
 }  // namespace fdtd
 
-// The batch shares one pass launch shape: 32 x 4 tiles, 4-stage ring, six
-// CTAs per SM, 16-plane z-chunks.
-constexpr int kBatchTY = 4, kBatchS = 4, kBatchMinB = 6, kBatchKChunk = 16;
+// Pass launch shapes of the batch.  Work items are 32 x 4 tiles (TY = 4 for
+// every launch, so that the CPML-edge and CPML-free item lists partition
+// the cells); each size bucket of members has its own z-chunk, carried by
+// its items; the edge and the interior launch of each pass have their own
+// kernel variant (register cap MINB and ring depth S).  fdtd_batch_create
+// times the choices (batch_tune).
+constexpr int kBatchTY = 4;
+#define FDTD_BATCH_VARIANTS(X) X(1, 4) X(6, 4) X(8, 4) X(6, 6)
+constexpr int kBatchVariants = 4;
+static const int kBatchVar[kBatchVariants][2] = {{1, 4}, {6, 4}, {8, 4}, {6, 6}};  // (MINB, S)
+constexpr int kBatchBucket = 16;  // members bucketed by their largest edge, 16 cells a bucket
+constexpr int kBatchMaxBuckets = FDTD_BATCH_MAX_BUCKETS;
 
 struct fdtd_batch {
   int device = 0;
@@ -89,9 +98,21 @@ struct fdtd_batch {
   std::vector<std::unique_ptr<DevBuf>> bufs;
   void* descs = nullptr;  // BatchSim<T>[n]
   void* views = nullptr;  // SimView<T>[n]
-  int4* items = nullptr;  // (member, bx, by, bz)
+  int4* items = nullptr;  // (member | z-chunk << 20, bx, by, bz): edge items, then interior items
   int* queue = nullptr;   // [4] work counters: H edge, H interior, E edge, E interior
-  int nedge = 0, ninner = 0, grid_pass = 0, grid_inner = 0;
+  int nedge = 0, ninner = 0;
+  size_t items_cap = 0;
+  // size buckets and the z-chunk of each; member -> bucket
+  int nbuckets = 0;
+  int bucket_lo[kBatchMaxBuckets] = {}, bucket_members[kBatchMaxBuckets] = {}, bucket_kc[kBatchMaxBuckets] = {};
+  float bucket_ms[kBatchMaxBuckets] = {};
+  std::vector<int> member_bucket;
+  // kernel variant (index into kBatchVar) and persistent grid per launch:
+  // [pass H / E][edge / interior]
+  int var[2][2] = {{1, 1}, {1, 1}};
+  int grid[2][2] = {{0, 0}, {0, 0}};
+  int sms = 0;
+  bool tuned = false;
   unsigned g_f = 0, g_m = 0, g_s = 0, g_tw = 0, g_c = 0;
   int t = 0, host_nsamp = 0, dft_every = 0, tend = 0;
   long long kernels = 0, graph_launches = 0, graph_kernels = 0;
@@ -112,6 +133,26 @@ struct fdtd_batch {
     return cudaSuccess;
   }
 };
+
+// Work items of member i with z-chunk kc: the tiles that touch no CPML slab
+// go to `inner` (the rule of build_tiles), the others to `edge`.
+static void batch_member_items(const fdtd_sim* s, int i, int kc, std::vector<int4>& edge, std::vector<int4>& inner) {
+  const int nbx = (s->NX + 31) / 32, nby = (s->NY + kBatchTY - 1) / kBatchTY, nbz = (s->NZ + kc - 1) / kc;
+  const int nb3[3] = {nbx, nby, nbz}, w3[3] = {32, kBatchTY, kc};
+  int lo[3], hi[3];
+  for (int a = 0; a < 3; a++) {
+    const int Nc = s->su.Nc[a], F = s->su.F[a];
+    lo[a] = (Nc + 1 + w3[a] - 1) / w3[a];
+    hi[a] = std::min(F >= w3[a] ? (F - w3[a]) / w3[a] + 1 : 0, nb3[a]);
+  }
+  const int tag = i | (kc << 20);
+  for (int bz = 0; bz < nbz; bz++)
+    for (int by = 0; by < nby; by++)
+      for (int bx = 0; bx < nbx; bx++) {
+        const bool in = bx >= lo[0] && bx < hi[0] && by >= lo[1] && by < hi[1] && bz >= lo[2] && bz < hi[2];
+        (in ? inner : edge).push_back(make_int4(tag, bx, by, bz));
+      }
+}
 
 template <typename T>
 static fdtd_status batch_build(fdtd_batch* b) {
@@ -135,23 +176,6 @@ static fdtd_status batch_build(fdtd_batch* b) {
     x.clk = s->clk;
     x.probe_id = s->probe_id;
     v[i] = x.v;
-    const int nbx = (s->NX + 31) / 32, nby = (s->NY + kBatchTY - 1) / kBatchTY;
-    const int nbz = (s->NZ + kBatchKChunk - 1) / kBatchKChunk;
-    // tiles that touch no CPML slab go to the PML-free queue (the same
-    // rule as build_tiles)
-    const int nb3[3] = {nbx, nby, nbz}, w3[3] = {32, kBatchTY, kBatchKChunk};
-    int lo[3], hi[3];
-    for (int a = 0; a < 3; a++) {
-      const int Nc = s->su.Nc[a], F = s->su.F[a];
-      lo[a] = (Nc + 1 + w3[a] - 1) / w3[a];
-      hi[a] = std::min(F >= w3[a] ? (F - w3[a]) / w3[a] + 1 : 0, nb3[a]);
-    }
-    for (int bz = 0; bz < nbz; bz++)
-      for (int by = 0; by < nby; by++)
-        for (int bx = 0; bx < nbx; bx++) {
-          const bool in = bx >= lo[0] && bx < hi[0] && by >= lo[1] && by < hi[1] && bz >= lo[2] && bz < hi[2];
-          (in ? inner : items).push_back(make_int4(i, bx, by, bz));
-        }
     auto blocks = [](long long cells, int per) { return (unsigned)((cells + per - 1) / per); };
     b->g_f = std::max(b->g_f, blocks((long long)s->tf_h.n + s->tf_e.n, 256));
     b->g_m = std::max(b->g_m, blocks((long long)s->nmetal[0] + s->nmetal[1] + s->nmetal[2], 128));
@@ -165,35 +189,97 @@ static fdtd_status batch_build(fdtd_batch* b) {
   SimView<T>* dv;
   CUDA_TRY(b->alloc(&dd, n));
   CUDA_TRY(b->alloc(&dv, n));
-  b->nedge = (int)items.size();
-  b->ninner = (int)inner.size();
-  items.insert(items.end(), inner.begin(), inner.end());  // edge items first, then interior
-  CUDA_TRY(b->alloc(&b->items, items.size()));
   CUDA_TRY(b->alloc(&b->queue, 4));
   CUDA_TRY(cudaMemcpy(dd, d.data(), n * sizeof(BatchSim<T>), cudaMemcpyHostToDevice));
   CUDA_TRY(cudaMemcpy(dv, v.data(), n * sizeof(SimView<T>), cudaMemcpyHostToDevice));
-  CUDA_TRY(cudaMemcpy(b->items, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice));
   b->descs = dd;
   b->views = dv;
-
-  // persistent grids: every CTA slot of the GPU once
-  const size_t smem = staged_smem<T, kBatchTY, kBatchS>();
-  int sms = 0;
-  CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
-  auto slots = [&](auto kern, int& out) -> fdtd_status {
-    CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int per = 0;
-    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 32 * kBatchTY, smem));
-    out = std::max(out, std::max(1, per) * sms);
-    return FDTD_OK;
-  };
-  fdtd_status st;
-  if ((st = slots(h_pass_batch<T, kBatchTY, kBatchS, kBatchMinB, true>, b->grid_pass)) != FDTD_OK) return st;
-  if ((st = slots(e_pass_batch<T, kBatchTY, kBatchS, kBatchMinB, true>, b->grid_pass)) != FDTD_OK) return st;
-  if ((st = slots(h_pass_batch<T, kBatchTY, kBatchS, kBatchMinB, false>, b->grid_inner)) != FDTD_OK) return st;
-  if ((st = slots(e_pass_batch<T, kBatchTY, kBatchS, kBatchMinB, false>, b->grid_inner)) != FDTD_OK) return st;
+  // size buckets by the largest edge, z-chunk 16 until tuned
+  b->member_bucket.assign(n, 0);
+  std::vector<int> key(n);
+  for (int i = 0; i < n; i++) {
+    const fdtd_sim* s = b->sims[i].get();
+    key[i] = (std::max(s->NX, std::max(s->NY, s->NZ)) - 1) / kBatchBucket;
+  }
+  std::vector<int> keys(key);
+  std::sort(keys.begin(), keys.end());
+  keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
+  if ((int)keys.size() > kBatchMaxBuckets) {  // merge the largest ones into the last bucket
+    keys.resize(kBatchMaxBuckets);
+  }
+  b->nbuckets = (int)keys.size();
+  for (int q = 0; q < b->nbuckets; q++) {
+    b->bucket_lo[q] = keys[q] * kBatchBucket + 1;
+    b->bucket_kc[q] = 16;
+    b->bucket_members[q] = 0;
+  }
+  for (int i = 0; i < n; i++) {
+    int q = (int)(std::lower_bound(keys.begin(), keys.end(), key[i]) - keys.begin());
+    q = std::min(q, b->nbuckets - 1);
+    b->member_bucket[i] = q;
+    b->bucket_members[q]++;
+  }
+  CUDA_TRY(cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, b->device));
+  // every batch pass variant may take more than 48 KB of shared memory
+#define FDTD_BATCH_ATTR(MB, S)                                                                                  \
+  CUDA_TRY(cudaFuncSetAttribute(h_pass_batch<T, kBatchTY, S, MB, true>,                                         \
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)staged_smem<T, kBatchTY, S>())); \
+  CUDA_TRY(cudaFuncSetAttribute(h_pass_batch<T, kBatchTY, S, MB, false>,                                        \
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)staged_smem<T, kBatchTY, S>())); \
+  CUDA_TRY(cudaFuncSetAttribute(e_pass_batch<T, kBatchTY, S, MB, true>,                                         \
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)staged_smem<T, kBatchTY, S>())); \
+  CUDA_TRY(cudaFuncSetAttribute(e_pass_batch<T, kBatchTY, S, MB, false>,                                        \
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)staged_smem<T, kBatchTY, S>()));
+  FDTD_BATCH_VARIANTS(FDTD_BATCH_ATTR)
+#undef FDTD_BATCH_ATTR
   CUDA_TRY(cudaFuncSetAttribute(dft_contract_batch<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)dft_smem_bytes<T>()));
+  return FDTD_OK;
+}
+
+// Persistent grid of one pass launch: every CTA slot of the GPU once.
+template <typename T, bool EPASS, bool PML>
+static int batch_grid(fdtd_batch* b, int var) {
+  int per = 0;
+  const int mb = kBatchVar[var][0], sg = kBatchVar[var][1];
+#define FDTD_BATCH_OCC(MB, S)                                                                                   \
+  if (mb == MB && sg == S) {                                                                                     \
+    if (EPASS)                                                                                                  \
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, e_pass_batch<T, kBatchTY, S, MB, PML>, 32 * kBatchTY,  \
+                                                    staged_smem<T, kBatchTY, S>());                             \
+    else                                                                                                        \
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, h_pass_batch<T, kBatchTY, S, MB, PML>, 32 * kBatchTY,  \
+                                                    staged_smem<T, kBatchTY, S>());                             \
+  }
+  FDTD_BATCH_VARIANTS(FDTD_BATCH_OCC)
+#undef FDTD_BATCH_OCC
+  return std::max(1, per) * b->sms;
+}
+
+// The item lists for the current per-bucket z-chunks, uploaded (edge items
+// first, then interior items).
+static fdtd_status batch_upload_items(fdtd_batch* b, const std::vector<int>* only_bucket_members = nullptr) {
+  std::vector<int4> edge, inner;
+  const int n = (int)b->sims.size();
+  for (int i = 0; i < n; i++) {
+    if (only_bucket_members && std::find(only_bucket_members->begin(), only_bucket_members->end(), i) ==
+                                   only_bucket_members->end())
+      continue;
+    batch_member_items(b->sims[i].get(), i, b->bucket_kc[b->member_bucket[i]], edge, inner);
+  }
+  b->nedge = (int)edge.size();
+  b->ninner = (int)inner.size();
+  edge.insert(edge.end(), inner.begin(), inner.end());
+  if (edge.empty()) return FDTD_OK;
+  // one buffer, kept and grown: the graph of the step holds its address
+  static_assert(sizeof(int4) == 16, "int4 items");
+  if (!b->items || b->items_cap < edge.size()) {
+    int4* d;
+    CUDA_TRY(b->alloc(&d, edge.size()));
+    b->items = d;
+    b->items_cap = edge.size();
+  }
+  CUDA_TRY(cudaMemcpy(b->items, edge.data(), edge.size() * sizeof(int4), cudaMemcpyHostToDevice));
   return FDTD_OK;
 }
 
@@ -215,28 +301,56 @@ static void launch_dependent(void (*kern)(P...), dim3 g, dim3 blk, size_t smem, 
   cudaLaunchKernelEx(&cfg, kern, std::forward<A>(args)...);
 }
 
+// One persistent pass launch of variant `var` over items [off, off + n),
+// counting its work from queue; pdl = a programmatic dependency on the
+// launch before it on the stream.
+template <typename T, bool EPASS, bool PML>
+static void batch_pass_launch(fdtd_batch* b, int var, int grid, int off, int n, int* queue, cudaStream_t st,
+                              bool pdl) {
+  const SimView<T>* v = static_cast<const SimView<T>*>(b->views);
+  const int4* items = b->items + off;
+  const int mb = kBatchVar[var][0], sg = kBatchVar[var][1];
+#define FDTD_BATCH_LAUNCH(MB, S)                                                                              \
+  if (mb == MB && sg == S) {                                                                                   \
+    const size_t smem = staged_smem<T, kBatchTY, S>();                                                        \
+    if (EPASS) {                                                                                              \
+      if (pdl) launch_dependent(e_pass_batch<T, kBatchTY, S, MB, PML>, dim3(grid), dim3(32, kBatchTY), smem,  \
+                                st, v, items, n, queue);                                                      \
+      else e_pass_batch<T, kBatchTY, S, MB, PML><<<grid, dim3(32, kBatchTY), smem, st>>>(v, items, n, queue); \
+    } else {                                                                                                  \
+      if (pdl) launch_dependent(h_pass_batch<T, kBatchTY, S, MB, PML>, dim3(grid), dim3(32, kBatchTY), smem,  \
+                                st, v, items, n, queue);                                                      \
+      else h_pass_batch<T, kBatchTY, S, MB, PML><<<grid, dim3(32, kBatchTY), smem, st>>>(v, items, n, queue); \
+    }                                                                                                         \
+  }
+  FDTD_BATCH_VARIANTS(FDTD_BATCH_LAUNCH)
+#undef FDTD_BATCH_LAUNCH
+}
+
+// One pass of every member: the CPML edge items, then the CPML-free items
+// with a programmatic dependency (they touch disjoint cells); returns the
+// number of launches.
+template <typename T, bool EPASS>
+static int batch_pass(fdtd_batch* b, int* queue, cudaStream_t st) {
+  const int p = EPASS ? 1 : 0;
+  int k = 0;
+  if (b->nedge) {
+    batch_pass_launch<T, EPASS, true>(b, b->var[p][0], b->grid[p][0], 0, b->nedge, queue, st, false);
+    k++;
+  }
+  if (b->ninner) {
+    batch_pass_launch<T, EPASS, false>(b, b->var[p][1], b->grid[p][1], b->nedge, b->ninner, queue + 1, st, true);
+    k++;
+  }
+  return k;
+}
+
 template <typename T>
 static void batch_enqueue_step(fdtd_batch* b, cudaStream_t st) {
   const int n = (int)b->sims.size();
   const BatchSim<T>* d = static_cast<const BatchSim<T>*>(b->descs);
-  const SimView<T>* v = static_cast<const SimView<T>*>(b->views);
-  const size_t smem = staged_smem<T, kBatchTY, kBatchS>();
-  const dim3 pb(32, kBatchTY);
-  const int4* inner_items = b->items + b->nedge;
   cudaMemsetAsync(b->queue, 0, 4 * sizeof(int), st);
-  int k = 0;
-  // each pass: the CPML edge items, then the CPML-free items with a
-  // programmatic dependency (they touch disjoint cells)
-  if (b->nedge) {
-    h_pass_batch<T, kBatchTY, kBatchS, kBatchMinB, true><<<b->grid_pass, pb, smem, st>>>(v, b->items, b->nedge,
-                                                                                       b->queue, kBatchKChunk);
-    k++;
-  }
-  if (b->ninner) {
-    launch_dependent(h_pass_batch<T, kBatchTY, kBatchS, kBatchMinB, false>, dim3(b->grid_inner), pb, smem, st, v,
-                     inner_items, b->ninner, b->queue + 1, (int)kBatchKChunk);
-    k++;
-  }
+  int k = batch_pass<T, false>(b, b->queue, st);
   // the line step writes the line's other E buffer, so the fused TFSF launch
   // after it still applies the H half with the line's E from before it
   line_step_batch<T><<<dim3(1, n), 1024, 0, st>>>(d);
@@ -248,16 +362,7 @@ static void batch_enqueue_step(fdtd_batch* b, cudaStream_t st) {
       launch_metal<T>(s.get(), st);  // UpdateHydroP* read E^n here
       k += (int)(s->kernels - k0);
     }
-  if (b->nedge) {
-    e_pass_batch<T, kBatchTY, kBatchS, kBatchMinB, true><<<b->grid_pass, pb, smem, st>>>(v, b->items, b->nedge,
-                                                                                       b->queue + 2, kBatchKChunk);
-    k++;
-  }
-  if (b->ninner) {
-    launch_dependent(e_pass_batch<T, kBatchTY, kBatchS, kBatchMinB, false>, dim3(b->grid_inner), pb, smem, st, v,
-                     inner_items, b->ninner, b->queue + 3, (int)kBatchKChunk);
-    k++;
-  }
+  k += batch_pass<T, true>(b, b->queue + 2, st);
   if (!b->hydro && b->g_m) { metal_e_batch<T><<<dim3(b->g_m, n), 128, 0, st>>>(d); k++; }
   if (b->dft_every > 0 && b->t % b->dft_every == 0) {
     dft_sample_batch<T><<<dim3(b->g_s, 12, n), 256, 0, st>>>(d);
@@ -273,6 +378,93 @@ static void batch_enqueue_step(fdtd_batch* b, cudaStream_t st) {
   }
   b->kernels += k;
   b->t++;
+}
+
+// Mean device time of `reps` runs of both passes (H and E, each its edge
+// and interior launch) over the current item lists, after one untimed run.
+// On the zero state the passes leave the fields at zero.
+template <typename T>
+static fdtd_status batch_time_passes(fdtd_batch* b, int reps, float* ms) {
+  cudaEvent_t e0, e1;
+  CUDA_TRY(cudaEventCreate(&e0));
+  CUDA_TRY(cudaEventCreate(&e1));
+  auto go = [&]() {
+    cudaMemsetAsync(b->queue, 0, 4 * sizeof(int), 0);
+    batch_pass<T, false>(b, b->queue, 0);
+    batch_pass<T, true>(b, b->queue + 2, 0);
+  };
+  go();
+  cudaEventRecord(e0, 0);
+  for (int r = 0; r < reps; r++) go();
+  cudaEventRecord(e1, 0);
+  cudaError_t e = cudaEventSynchronize(e1);
+  float t = 0.f;
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&t, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (e != cudaSuccess) return fail(FDTD_ERR_CUDA, std::string("batch tuning: ") + cudaGetErrorString(e));
+  *ms = t / reps;
+  return FDTD_OK;
+}
+
+// The autotuner of the batch's passes (no counterpart in the reference):
+// per size bucket the z-chunk (8, 16 or 32 planes) with the bucket's
+// members alone, then per launch (H / E pass, edge / interior items) the
+// kernel variant over the whole batch.  FDTD_TUNE=0, or a batch under 2^20
+// cells, keeps z-chunk 16 and variant (MINB 6, S 4) everywhere.
+template <typename T>
+static fdtd_status batch_tune(fdtd_batch* b) {
+  for (int p = 0; p < 2; p++)
+    for (int q = 0; q < 2; q++) b->var[p][q] = 1;
+  auto grids = [&]() {
+    b->grid[0][0] = batch_grid<T, false, true>(b, b->var[0][0]);
+    b->grid[0][1] = batch_grid<T, false, false>(b, b->var[0][1]);
+    b->grid[1][0] = batch_grid<T, true, true>(b, b->var[1][0]);
+    b->grid[1][1] = batch_grid<T, true, false>(b, b->var[1][1]);
+  };
+  grids();
+  long long cells = 0;
+  for (const auto& s : b->sims) cells += s->ncell;
+  const char* env = std::getenv("FDTD_TUNE");
+  fdtd_status st;
+  if ((env && env[0] == '0') || cells < (1LL << 20)) return batch_upload_items(b);
+  const int n = (int)b->sims.size();
+  // z-chunk per bucket, its members alone
+  for (int q = 0; q < b->nbuckets; q++) {
+    std::vector<int> mem;
+    for (int i = 0; i < n; i++)
+      if (b->member_bucket[i] == q) mem.push_back(i);
+    float best = 1e30f;
+    int best_kc = 16;
+    for (int kc : {8, 16, 32}) {
+      b->bucket_kc[q] = kc;
+      if ((st = batch_upload_items(b, &mem)) != FDTD_OK) return st;
+      float ms;
+      if ((st = batch_time_passes<T>(b, 3, &ms)) != FDTD_OK) return st;
+      if (ms < best) { best = ms; best_kc = kc; }
+    }
+    b->bucket_kc[q] = best_kc;
+    b->bucket_ms[q] = best;
+  }
+  if ((st = batch_upload_items(b)) != FDTD_OK) return st;
+  // the variant of each launch, the others held
+  for (int p = 0; p < 2; p++)
+    for (int e = 0; e < 2; e++) {
+      float best = 1e30f;
+      int best_v = b->var[p][e];
+      for (int v = 0; v < kBatchVariants; v++) {
+        b->var[p][e] = v;
+        grids();
+        float ms;
+        if ((st = batch_time_passes<T>(b, 3, &ms)) != FDTD_OK) return st;
+        if (ms < best) { best = ms; best_v = v; }
+      }
+      b->var[p][e] = best_v;
+      grids();
+    }
+  b->tuned = true;
+  CUDA_TRY(cudaGetLastError());
+  return FDTD_OK;
 }
 
 template <typename T>
@@ -340,7 +532,9 @@ static fdtd_status batch_create_impl(const fdtd_params* ps, int n, int device, f
                                     "DFT sampling period and Tend (member " + std::to_string(i) + ")");
     }
   }
-  const fdtd_status st = b->fp64 ? batch_build<double>(b.get()) : batch_build<float>(b.get());
+  fdtd_status st = b->fp64 ? batch_build<double>(b.get()) : batch_build<float>(b.get());
+  if (st != FDTD_OK) return st;
+  st = b->fp64 ? batch_tune<double>(b.get()) : batch_tune<float>(b.get());
   if (st != FDTD_OK) return st;
   CUDA_TRY(cudaDeviceSynchronize());
   *out = b.release();
@@ -383,6 +577,28 @@ extern "C" fdtd_status fdtd_batch_get_stats(const fdtd_batch* b, long long* kern
   if (!b) return fail(FDTD_ERR_INVALID, "null argument");
   if (kernels) *kernels = b->kernels;
   if (graph_launches) *graph_launches = b->graph_launches;
+  return FDTD_OK;
+}
+
+extern "C" fdtd_status fdtd_batch_get_tuning(const fdtd_batch* b, fdtd_batch_tuning* out) {
+  if (!b || !out) return fail(FDTD_ERR_INVALID, "null argument");
+  std::memset(out, 0, sizeof(*out));
+  out->tuned = b->tuned ? 1 : 0;
+  out->nbuckets = b->nbuckets;
+  for (int q = 0; q < b->nbuckets; q++) {
+    out->edge_lo[q] = b->bucket_lo[q];
+    out->edge_hi[q] = q + 1 < b->nbuckets ? b->bucket_lo[q + 1] - 1 : INT_MAX;
+    out->members[q] = b->bucket_members[q];
+    out->kchunk[q] = b->bucket_kc[q];
+    out->bucket_ms[q] = b->bucket_ms[q];
+  }
+  out->tile_x = 32;
+  out->tile_y = kBatchTY;
+  for (int p = 0; p < 2; p++)
+    for (int e = 0; e < 2; e++) {
+      out->minb[p][e] = kBatchVar[b->var[p][e]][0];
+      out->stages[p][e] = kBatchVar[b->var[p][e]][1];
+    }
   return FDTD_OK;
 }
 

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -17,6 +18,7 @@
 #include "staged.cuh"
 #include "boundary.cuh"
 #include "adjoint.cuh"
+#include "snapshot.cuh"
 #include "setup.h"
 
 using namespace fdtd;
@@ -130,6 +132,12 @@ struct fdtd_sim {
   int graph_len = 0;
   cudaStream_t graph_stream = nullptr;
   bool use_graphs = true;
+
+  // snapshots taken by the stepper (fdtd_snapshots_enable / _drain):
+  // records [snap_first, produced) exist, [snap_drained, produced) wait
+  SnapArgs snap{};
+  bool snap_on = false;
+  long long snap_first = 0, snap_drained = 0;
 
   // adjoint design region (fdtd_set_design / fdtd_forward / fdtd_backward)
   bool has_design = false;
@@ -756,6 +764,7 @@ extern "C" fdtd_status fdtd_reset(fdtd_sim* s) {
   for (const auto& b : s->state) CUDA_TRY(cudaMemset(b.first, 0, b.second));
   s->t = 0;
   s->host_nsamp = 0;
+  s->snap_first = s->snap_drained = 0;
   return FDTD_OK;
 }
 
@@ -1215,11 +1224,24 @@ static void enqueue_step(fdtd_sim* s, cudaStream_t st) {
   launch_tfsf<T>(s, st);
   launch_e_pass<T>(s, st);
   if (s->line.dft_every > 0 && s->t % s->line.dft_every == 0) sample_and_contract<T>(s, st);
+  if (s->snap_on) {
+    const int n = std::max(s->snap.rows * s->snap.cols, std::max(s->snap.aux_len, s->snap.line_len));
+    snap_gather<T><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(view<T>(s), mview<T>(s), s->line, s->snap);
+    s->kernels++;
+  }
   s->t++;
+}
+
+// Snapshot records the steps [0, t) have produced (every t_skip-th step).
+static long long snap_produced(const fdtd_sim* s, long long t) {
+  return t > 0 ? (t - 1) / s->snap.t_skip + 1 : 0;
 }
 
 template <typename T>
 static fdtd_status step_impl(fdtd_sim* s, int nsteps, cudaStream_t st) {
+  if (s->snap_on && snap_produced(s, (long long)s->t + nsteps) - s->snap_drained > s->snap.cap)
+    return fail(FDTD_ERR_STATE, "the snapshot ring would overflow: drain it (fdtd_snapshots_drain) or step fewer "
+                                "steps at a time");
   const int every = s->line.dft_every > 0 ? s->line.dft_every : 1;
   const int G = every * kSampleBlock;  // launch pattern period
   int done = 0;
@@ -1679,6 +1701,105 @@ extern "C" fdtd_status fdtd_get_material(fdtd_sim* s, uint8_t* out, size_t count
         for (int c = 0; c < 3; c++) b |= (uint8_t)(is_dispersive(s->su.matc[c][r]) << c);
         out[r] = b;
       }
+  return FDTD_OK;
+}
+
+// ---------------------------------------------------------------------
+// snapshots (snapshot.cuh)
+
+extern "C" fdtd_status fdtd_snapshots_enable(fdtd_sim* s, int mode, int capacity, fdtd_snapshot_layout* out) {
+  if (!s) return fail(FDTD_ERR_INVALID, "null argument");
+  if (mode < 0 || mode > 3) return fail(FDTD_ERR_INVALID, "mode must be 0 (off) or Snap_in 1, 2 or 3");
+  CUDA_TRY(cudaSetDevice(s->device));
+  CUDA_TRY(cudaDeviceSynchronize());
+  // a captured step graph holds the step's launches: capture it again
+  if (s->graph) {
+    cudaGraphExecDestroy(s->graph);
+    s->graph = nullptr;
+  }
+  s->snap_on = false;
+  if (mode == 0) {
+    if (out) std::memset(out, 0, sizeof(*out));
+    return FDTD_OK;
+  }
+  if (capacity <= 0) return fail(FDTD_ERR_INVALID, "capacity must be positive");
+  const fdtd_params& p = s->su.p;
+  if (p.t_skip <= 0 || p.y_skip <= 0 || p.z_skip <= 0) return fail(FDTD_ERR_INVALID, "t_skip, y_skip, z_skip must be positive");
+  SnapArgs a{};
+  a.mode = mode;
+  a.t_skip = p.t_skip; a.y_skip = p.y_skip; a.z_skip = p.z_skip;
+  a.xc = s->NX / 2;
+  a.rows = (s->NY + p.y_skip - 1) / p.y_skip;
+  a.cols = (s->NZ + p.z_skip - 1) / p.z_skip;
+  a.off_plane = a.off_plane2 = a.off_aux = a.off_line = -1;
+  int rec = 1;  // the step index
+  if (mode == 1 || mode == 3) {
+    a.aux_len = (s->NZ + p.z_skip - 1) / p.z_skip;
+    a.line_len = (s->line.L + p.z_skip - 1) / p.z_skip;
+    a.off_aux = rec; rec += a.aux_len;
+    a.off_line = rec; rec += a.line_len;
+  }
+  if (mode == 3) { a.off_plane = rec; rec += a.rows * a.cols; }
+  if (mode == 2) {
+    a.off_plane = rec; rec += a.rows * a.cols;
+    a.off_plane2 = rec; rec += a.rows * a.cols;
+    // dispersive slot of every plane cell per component
+    std::vector<int> ps((size_t)a.rows * a.cols * 3, -1);
+    for (int c = 0; c < 3; c++) {
+      if (s->nmetal[c] == 0) continue;
+      std::vector<int4> cells(s->nmetal[c]);
+      CUDA_TRY(cudaMemcpy(cells.data(), s->mcell[c], cells.size() * sizeof(int4), cudaMemcpyDeviceToHost));
+      for (const int4& e : cells)
+        if (e.x == a.xc && e.y % p.y_skip == 0 && e.z % p.z_skip == 0)
+          ps[((size_t)(e.y / p.y_skip) * a.cols + e.z / p.z_skip) * 3 + c] = e.w;
+    }
+    int* d;
+    CUDA_TRY(s->alloc(&d, ps.size()));
+    CUDA_TRY(cudaMemcpy(d, ps.data(), ps.size() * sizeof(int), cudaMemcpyHostToDevice));
+    a.pslot = d;
+  }
+  a.rec = rec;
+  a.cap = capacity;
+  double* ring;
+  CUDA_TRY(s->alloc(&ring, (size_t)rec * capacity));
+  a.ring = ring;
+  s->snap = a;
+  s->snap_on = true;
+  s->snap_first = s->snap_drained = snap_produced(s, s->t);
+  if (out) {
+    out->mode = mode;
+    out->t_skip = a.t_skip;
+    out->plane_rows = mode >= 2 ? a.rows : 0;
+    out->plane_cols = mode >= 2 ? a.cols : 0;
+    out->aux_len = mode != 2 ? a.aux_len : 0;
+    out->line_len = mode != 2 ? a.line_len : 0;
+    out->off_plane = a.off_plane; out->off_plane2 = a.off_plane2;
+    out->off_aux = a.off_aux; out->off_line = a.off_line;
+    out->record = rec;
+    out->capacity = capacity;
+  }
+  return FDTD_OK;
+}
+
+extern "C" fdtd_status fdtd_snapshots_drain(fdtd_sim* s, double* host, int max_records, int* n, void* stream) {
+  if (!s || !host || !n || max_records < 0) return fail(FDTD_ERR_INVALID, "bad argument");
+  if (!s->snap_on) return fail(FDTD_ERR_STATE, "snapshots are not enabled");
+  CUDA_TRY(cudaSetDevice(s->device));
+  const long long have = snap_produced(s, s->t) - s->snap_drained;
+  const int m = (int)std::min<long long>(have, max_records);
+  cudaStream_t st = as_stream(stream);
+  const SnapArgs& a = s->snap;
+  int done = 0;
+  while (done < m) {
+    const long long r = s->snap_drained + done;
+    const int slot = (int)(r % a.cap);
+    const int run = std::min(m - done, a.cap - slot);  // contiguous up to the ring's end
+    CUDA_TRY(cudaMemcpyAsync(host + (size_t)done * a.rec, a.ring + (size_t)slot * a.rec,
+                             (size_t)run * a.rec * sizeof(double), cudaMemcpyDeviceToHost, st));
+    done += run;
+  }
+  s->snap_drained += m;
+  *n = m;
   return FDTD_OK;
 }
 

@@ -1,17 +1,30 @@
 // fdtd_runner -- the reference's program (main.cu main()) as a C++ host
 // over the C ABI: read Input.txt (READ_DATA_FILE, setup.cu:10-133), set up
-// and run t = 0 .. Tend (main.cu:2724-3175), write the centre-probe record
-// OUT.txt (main.cu:2722-2732: t*dt, ex, ey, ez at the top of every step)
-// and the spectra ScatAbs.<Tend>.txt (CalculateAbsScatt, Spectral.cu).
+// and run t = 0 .. Tend (main.cu:2724-3175), and write what the reference
+// writes:
+//   OUT.txt              the centre probe (main.cu:2722-2732: t*dt, ex, ey,
+//                        ez at the top of every step)
+//   ScatAbs.<t>.txt      the spectra (CalculateAbsScatt, Spectral.cu) after
+//                        every step t with t % (Tend/10) == 0
+//                        (main.cu:3042-3172; at Tend only when Tend < 10)
+//   aux_sim.<n>.txt, aux_sim.<n>_2.txt, videofiles/YZ_sim.<n>.txt,
+//   videofiles/YZ_sim.<n>_N.txt
+//                        the snapshots of Snap_in 1, 2, 3 every t_skip
+//                        steps (main.cu:2948-2991, snapshot.cu), taken on
+//                        the device and drained while the run goes on; n
+//                        counts every file group written, as the
+//                        reference's snapshot_count does
 //
 //   fdtd_runner [Input.txt] [--out DIR] [--fp32 | --fp64] [--device N]
 //
 // Exit status: 0 on success, 1 on a library error (its text on stderr), 2
 // on bad arguments, 3 when the watchdog saw a non-finite field ("NAN
 // Detected" ends OUT.txt, as in the reference).
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <filesystem>
 #include <string>
 #include <vector>
 
@@ -22,13 +35,55 @@ namespace {
 void usage() {
   std::fprintf(stderr,
                "usage: fdtd_runner [Input.txt] [--out DIR] [--fp32 | --fp64] [--device N]\n"
-               "  runs the reference's time loop on the GPU and writes OUT.txt and\n"
-               "  ScatAbs.<Tend>.txt into DIR (default: the current directory)\n");
+               "  runs the reference's time loop on the GPU and writes OUT.txt, ScatAbs.<t>.txt\n"
+               "  every Tend/10 steps and the Snap_in snapshots into DIR (default: the current\n"
+               "  directory)\n");
 }
 
 int fail(const char* what) {
   std::fprintf(stderr, "fdtd_runner: %s: %s\n", what, fdtd_last_error());
   return 1;
+}
+
+// A one-value-per-line column (SNAPSHOT_1D).
+bool write_column(const std::string& path, const double* v, int n) {
+  FILE* f = std::fopen(path.c_str(), "w");
+  if (!f) return false;
+  for (int i = 0; i < n; i++) std::fprintf(f, "%e\n", v[i]);
+  std::fclose(f);
+  return true;
+}
+
+// A plane, one row per line, values separated by a space (SNAPSHOT_2D).
+bool write_plane(const std::string& path, const double* v, int rows, int cols) {
+  FILE* f = std::fopen(path.c_str(), "w");
+  if (!f) return false;
+  for (int r = 0; r < rows; r++) {
+    for (int c = 0; c < cols; c++) std::fprintf(f, "%e ", v[(size_t)r * cols + c]);
+    std::fprintf(f, "\n");
+  }
+  std::fclose(f);
+  return true;
+}
+
+// The files of one snapshot record, named with the reference's counter.
+bool write_snapshot(const std::string& out, const fdtd_snapshot_layout& L, const double* r, int& count) {
+  const std::string vf = out + "/videofiles/YZ_sim.";
+  auto aux = [&]() {
+    const std::string b = out + "/aux_sim." + std::to_string(count);
+    const bool ok = write_column(b + ".txt", r + L.off_aux, L.aux_len) &&
+                    write_column(b + "_2.txt", r + L.off_line, L.line_len);
+    count++;
+    return ok;
+  };
+  auto plane = [&](int off, const char* suffix) {
+    const bool ok = write_plane(vf + std::to_string(count) + suffix + ".txt", r + off, L.plane_rows, L.plane_cols);
+    count++;
+    return ok;
+  };
+  if (L.mode == 1) return aux();
+  if (L.mode == 2) return plane(L.off_plane, "") && plane(L.off_plane2, "_N");
+  return aux() && plane(L.off_plane, "");
 }
 
 }  // namespace
@@ -62,9 +117,62 @@ int main(int argc, char** argv) {
   if (precision >= 0) p.precision = precision;
   fdtd_sim* sim = nullptr;
   if (fdtd_create(&p, device, &sim) != FDTD_OK) return fail("setting up");
-  if (fdtd_run(sim, nullptr) != FDTD_OK) {
-    fdtd_destroy(sim);
-    return fail("running");
+  // snapshots: taken on the device, drained after every chunk of steps
+  fdtd_snapshot_layout lay{};
+  const bool snaps = p.Snap_in >= 1 && p.Snap_in <= 3;
+  const int cap = 130;  // a 128-step block of t_skip = 1 records between drains
+  std::vector<double> recs;
+  int snap_count = 0;
+  if (snaps) {
+    if (fdtd_snapshots_enable(sim, p.Snap_in, cap, &lay) != FDTD_OK) {
+      fdtd_destroy(sim);
+      return fail("enabling snapshots");
+    }
+    std::error_code ec;
+    std::filesystem::create_directories(out + "/videofiles", ec);
+    recs.resize((size_t)cap * lay.record);
+  }
+  // the time loop in chunks that end at every spectra dump and before the
+  // snapshot ring fills
+  const int total = p.Tend + 1;
+  const int period = p.Tend / 10;
+  std::vector<int> dumps;
+  for (int t = 0; t <= p.Tend; t++)
+    if (period > 0 ? t % period == 0 : t == p.Tend) dumps.push_back(t);
+  std::vector<std::string> written;
+  int done = 0;
+  size_t next_dump = 0;
+  while (done < total) {
+    int stop = total;
+    if (next_dump < dumps.size()) stop = std::min(stop, dumps[next_dump] + 1);
+    if (snaps) stop = std::min(stop, done + (cap - 1) * lay.t_skip);
+    if (fdtd_step(sim, stop - done, nullptr) != FDTD_OK) {
+      fdtd_destroy(sim);
+      return fail("running");
+    }
+    done = stop;
+    if (snaps) {
+      int n = 0;
+      if (fdtd_snapshots_drain(sim, recs.data(), cap, &n, nullptr) != FDTD_OK || fdtd_check(sim) == FDTD_ERR_CUDA) {
+        fdtd_destroy(sim);
+        return fail("draining snapshots");
+      }
+      for (int q = 0; q < n; q++)
+        if (!write_snapshot(out, lay, recs.data() + (size_t)q * lay.record, snap_count)) {
+          std::fprintf(stderr, "fdtd_runner: cannot write snapshot files under %s\n", out.c_str());
+          fdtd_destroy(sim);
+          return 1;
+        }
+    }
+    if (next_dump < dumps.size() && done == dumps[next_dump] + 1) {
+      const std::string sca = out + "/ScatAbs." + std::to_string(dumps[next_dump]) + ".txt";
+      if (fdtd_write_scatabs(sim, sca.c_str()) != FDTD_OK) {
+        fdtd_destroy(sim);
+        return fail("writing the spectra");
+      }
+      written.push_back(sca);
+      next_dump++;
+    }
   }
   const fdtd_status chk = fdtd_check(sim);
   fdtd_dims d;
@@ -98,13 +206,9 @@ int main(int argc, char** argv) {
     fdtd_destroy(sim);
     return 3;
   }
-  const std::string sca = out + "/ScatAbs." + std::to_string(p.Tend) + ".txt";
-  if (fdtd_write_scatabs(sim, sca.c_str()) != FDTD_OK) {
-    fdtd_destroy(sim);
-    return fail("writing the spectra");
-  }
-  std::printf("fdtd_runner: %d x %d x %d cells, %d steps, %s; wrote %s and %s\n", d.nx, d.ny, d.nz, p.Tend + 1,
-              p.precision == FDTD_FP64 ? "FP64" : "FP32", out_path.c_str(), sca.c_str());
+  std::printf("fdtd_runner: %d x %d x %d cells, %d steps, %s; wrote %s, %zu spectra (last %s), %d snapshot files\n",
+              d.nx, d.ny, d.nz, p.Tend + 1, p.precision == FDTD_FP64 ? "FP64" : "FP32", out_path.c_str(),
+              written.size(), written.empty() ? "-" : written.back().c_str(), snap_count);
   fdtd_destroy(sim);
   return 0;
 }

@@ -342,11 +342,12 @@ __global__ void __launch_bounds__(32 * TY, MINB) h_pass_s(const __grid_constant_
 
 // Batched form: a persistent grid that takes (simulation, tile) work items
 // from a queue shared by every simulation of a batch; the views live in
-// device memory, one per simulation.
+// device memory, one per simulation, and every item carries the z-chunk of
+// its simulation's size bucket.
 template <typename T, int TY, int S, int MINB, bool PML>
 __global__ void __launch_bounds__(32 * TY, MINB) h_pass_batch(const SimView<T>* __restrict__ views,
                                                            const int4* __restrict__ items, int nitems,
-                                                           int* __restrict__ queue, int kchunk) {
+                                                           int* __restrict__ queue) {
   __shared__ int next;
   pdl_launch_dependents();  // the second launch of the pass may fill this one's tail
   for (;;) {
@@ -358,8 +359,8 @@ __global__ void __launch_bounds__(32 * TY, MINB) h_pass_batch(const SimView<T>* 
       pdl_wait();
       return;
     }
-    const int4 w = items[it];  // (simulation, bx, by, bz)
-    h_pass_tile<T, TY, S, PML>(views[w.x], kchunk, w.y, w.z, w.w);
+    const int4 w = items[it];  // (simulation | z-chunk << 20, bx, by, bz)
+    h_pass_tile<T, TY, S, PML>(views[w.x & 0xFFFFF], w.x >> 20, w.y, w.z, w.w);
   }
 }
 
@@ -541,11 +542,12 @@ __global__ void __launch_bounds__(32 * TY, MINB) e_pass_s(const __grid_constant_
 
 // Batched form: a persistent grid that takes (simulation, tile) work items
 // from a queue shared by every simulation of a batch; the views live in
-// device memory, one per simulation.
+// device memory, one per simulation, and every item carries the z-chunk of
+// its simulation's size bucket.
 template <typename T, int TY, int S, int MINB, bool PML>
 __global__ void __launch_bounds__(32 * TY, MINB) e_pass_batch(const SimView<T>* __restrict__ views,
                                                            const int4* __restrict__ items, int nitems,
-                                                           int* __restrict__ queue, int kchunk) {
+                                                           int* __restrict__ queue) {
   __shared__ int next;
   pdl_launch_dependents();  // the second launch of the pass may fill this one's tail
   for (;;) {
@@ -557,8 +559,8 @@ __global__ void __launch_bounds__(32 * TY, MINB) e_pass_batch(const SimView<T>* 
       pdl_wait();
       return;
     }
-    const int4 w = items[it];  // (simulation, bx, by, bz)
-    e_pass_tile<T, TY, S, PML>(views[w.x], kchunk, w.y, w.z, w.w);
+    const int4 w = items[it];  // (simulation | z-chunk << 20, bx, by, bz)
+    e_pass_tile<T, TY, S, PML>(views[w.x & 0xFFFFF], w.x >> 20, w.y, w.z, w.w);
   }
 }
 

@@ -12,7 +12,7 @@ import numpy as np
 from ._abi import (FACE_COMPONENTS, FDTD_FP32, FDTD_FP64, FDTD_KERNEL_E_PASS,
                    FDTD_KERNEL_H_PASS, FIX_BH_X_F,
                    FIX_CE_EY_XN, FIX_HYDRO_CBRT, GEOM_DISK_ARRAY, GEOM_REFERENCE, GEOM_ROD_DIMER,
-                   GEOM_SPHERE, STATUS, Dims, Params, Stats)
+                   GEOM_SPHERE, STATUS, BatchTuning, Dims, Params, SnapshotLayout, Stats)
 
 __all__ = ["Params", "Dims", "Sim", "Batch", "FdtdError", "lib", "default_params", "load_input_txt",
            "FDTD_FP32", "FDTD_FP64", "GEOM_REFERENCE", "GEOM_ROD_DIMER", "GEOM_DISK_ARRAY",
@@ -35,7 +35,7 @@ EXPORTS = [
     "fdtd_batch_step", "fdtd_batch_sim", "fdtd_batch_get_stats",
     "fdtd_plan", "fdtd_rasterise", "fdtd_coefficients", "fdtd_get_probe_range",
     "fdtd_set_source", "fdtd_get_stats", "fdtd_time_kernel", "fdtd_forward_spectra",
-    "fdtd_backward_spectra",
+    "fdtd_backward_spectra", "fdtd_snapshots_enable", "fdtd_snapshots_drain", "fdtd_batch_get_tuning",
 ]
 
 
@@ -103,6 +103,9 @@ def lib():
         "fdtd_set_source": (C.c_int, [vp, C.c_int, C.c_int, vp, vp]),
         "fdtd_get_stats": (C.c_int, [vp, P(Stats)]),
         "fdtd_time_kernel": (C.c_int, [vp, C.c_int, C.c_int, vp, dp]),
+        "fdtd_snapshots_enable": (C.c_int, [vp, C.c_int, C.c_int, P(SnapshotLayout)]),
+        "fdtd_snapshots_drain": (C.c_int, [vp, vp, C.c_int, P(C.c_int), vp]),
+        "fdtd_batch_get_tuning": (C.c_int, [vp, P(BatchTuning)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -260,6 +263,38 @@ class Sim:
         """Async H2D of soft-source samples for steps [t0, t0+n)."""
         _check(lib().fdtd_set_source(self.h, t0, n, src_ptr, stream))
 
+    def enable_snapshots(self, mode, capacity=64):
+        """Snapshots taken by the stepper every t_skip steps
+        (fdtd_snapshots_enable); mode is the reference's Snap_in (0 off)."""
+        lay = SnapshotLayout()
+        _check(lib().fdtd_snapshots_enable(self.h, int(mode), int(capacity), C.byref(lay)))
+        self.snap_layout = lay
+        return lay
+
+    def drain_snapshots(self, max_records=None):
+        """The records taken since the last drain, as dicts with t and the
+        parts of the mode (plane, plane2, aux, line)."""
+        lay = self.snap_layout
+        m = lay.capacity if max_records is None else int(max_records)
+        buf = np.empty((max(m, 1), lay.record))
+        n = C.c_int()
+        _check(lib().fdtd_snapshots_drain(self.h, buf.ctypes.data, m, C.byref(n), None))
+        lib().fdtd_check(self.h)  # synchronising call: the copy has landed
+        out = []
+        for r in buf[: n.value]:
+            d = {"t": int(r[0])}
+            shp = (lay.plane_rows, lay.plane_cols)
+            if lay.off_plane >= 0:
+                d["plane"] = r[lay.off_plane:lay.off_plane + shp[0] * shp[1]].reshape(shp).copy()
+            if lay.off_plane2 >= 0:
+                d["plane2"] = r[lay.off_plane2:lay.off_plane2 + shp[0] * shp[1]].reshape(shp).copy()
+            if lay.off_aux >= 0:
+                d["aux"] = r[lay.off_aux:lay.off_aux + lay.aux_len].copy()
+            if lay.off_line >= 0:
+                d["line"] = r[lay.off_line:lay.off_line + lay.line_len].copy()
+            out.append(d)
+        return out
+
     def stats(self):
         st = Stats()
         _check(lib().fdtd_get_stats(self.h, C.byref(st)))
@@ -394,6 +429,18 @@ class Batch:
         k, g = C.c_longlong(), C.c_longlong()
         _check(lib().fdtd_batch_get_stats(self.h, C.byref(k), C.byref(g)))
         return k.value, g.value
+
+    def tuning(self):
+        """The launch shapes the batch's autotuner chose (fdtd_batch_get_tuning)."""
+        t = BatchTuning()
+        _check(lib().fdtd_batch_get_tuning(self.h, C.byref(t)))
+        nb = t.nbuckets
+        return {"tuned": bool(t.tuned), "tile": [t.tile_x, t.tile_y],
+                "buckets": [{"edges": [t.edge_lo[q], t.edge_hi[q] if t.edge_hi[q] < 2 ** 31 - 1 else None],
+                             "members": t.members[q], "kchunk": t.kchunk[q],
+                             "ms": round(float(t.bucket_ms[q]), 4)} for q in range(nb)],
+                "minb": {"h": list(t.minb[0]), "e": list(t.minb[1])},
+                "stages": {"h": list(t.stages[0]), "e": list(t.stages[1])}}
 
     def close(self):
         if getattr(self, "h", None):

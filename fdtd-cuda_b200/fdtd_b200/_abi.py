@@ -107,3 +107,18 @@ class Stats(C.Structure):
                 ("h_pdl", C.c_int), ("e_pdl", C.c_int),
                 ("tfsf_entries_h", C.c_longlong), ("tfsf_entries_e", C.c_longlong),
                 ("dft_rows", C.c_longlong)]
+
+
+class SnapshotLayout(C.Structure):
+    """fdtd_snapshot_layout (include/fdtd_b200.h)."""
+    _fields_ = [("mode", C.c_int), ("t_skip", C.c_int), ("plane_rows", C.c_int), ("plane_cols", C.c_int),
+                ("aux_len", C.c_int), ("line_len", C.c_int), ("off_plane", C.c_int), ("off_plane2", C.c_int),
+                ("off_aux", C.c_int), ("off_line", C.c_int), ("record", C.c_int), ("capacity", C.c_int)]
+
+
+class BatchTuning(C.Structure):
+    """fdtd_batch_tuning (include/fdtd_b200.h)."""
+    _fields_ = [("tuned", C.c_int), ("nbuckets", C.c_int), ("edge_lo", C.c_int * 16), ("edge_hi", C.c_int * 16),
+                ("members", C.c_int * 16), ("kchunk", C.c_int * 16), ("bucket_ms", C.c_float * 16),
+                ("tile_x", C.c_int), ("tile_y", C.c_int), ("minb", (C.c_int * 2) * 2),
+                ("stages", (C.c_int * 2) * 2)]

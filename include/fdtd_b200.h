@@ -302,6 +302,35 @@ fdtd_status fdtd_snapshot_plane(fdtd_sim* s, int comp, int axis, int index,
 fdtd_status fdtd_snapshot_plane_static(fdtd_sim* s, int comp, int axis,
                                        int index, double* dst, size_t count,
                                        void* stream);
+/* Snapshots as the reference writes them (SNAPSHOT_1D / SNAPSHOT_2D /
+ * SNAPSHOT_2D_N, snapshot.cu:23-176), taken on the device by the stepper
+ * after every step t with t % t_skip == 0 (main.cu:2948-2991) into a ring of
+ * `capacity` records.  mode is the reference's Snap_in:
+ *   1  aux lines: ey at (2, 2, k) for k = 0, z_skip, ... (aux_len values)
+ *      and the incident line's E with the same step (line_len values)
+ *   2  the YZ plane at x = nx/2 of |P_d| (the Drude current) and of the
+ *      mean density (NDx + NDy + NDz) / 3 as the reference holds it after
+ *      its step (the density from before the step), rows over y with step
+ *      y_skip, columns over z with step z_skip, row major
+ *   3  the aux lines, then the YZ plane of |E|
+ * A record is `record` doubles: the step index t at offset 0, then the
+ * parts at the offsets in the layout (-1 = absent).  0 turns snapshots
+ * off.  Enabling synchronises the device.  fdtd_step fails with
+ * FDTD_ERR_STATE instead of overwriting records that were not drained. */
+typedef struct fdtd_snapshot_layout {
+  int mode, t_skip;
+  int plane_rows, plane_cols;
+  int aux_len, line_len;
+  int off_plane, off_plane2, off_aux, off_line;
+  int record, capacity;
+} fdtd_snapshot_layout;
+fdtd_status fdtd_snapshots_enable(fdtd_sim* s, int mode, int capacity,
+                                  fdtd_snapshot_layout* out);
+/* Copies the records taken since the last drain (at most max_records, in
+ * step order) to host memory, asynchronously on `stream` (pinned memory
+ * for an overlapped copy); *n gets the number of records. */
+fdtd_status fdtd_snapshots_drain(fdtd_sim* s, double* host, int max_records,
+                                 int* n, void* stream);
 /* Probe record: ex, ey, ez at the probe cell after every completed step,
  * [t][3]. n = number of steps recorded so far. */
 fdtd_status fdtd_get_probe(fdtd_sim* s, double* out, size_t count, int* n);
@@ -415,6 +444,26 @@ fdtd_status fdtd_batch_spectra(fdtd_batch* b, int idx, double* out19);
 /* Kernel launches and graph replays issued by the batch so far. */
 fdtd_status fdtd_batch_get_stats(const fdtd_batch* b, long long* kernels,
                                  long long* graph_launches);
+/* The pass launch shapes fdtd_batch_create chose (its autotuner): members
+ * are bucketed by their largest edge, 16 cells a bucket ([edge_lo, edge_hi]
+ * inclusive); each bucket has its own z-chunk (planes per work item),
+ * timed with the bucket's members alone (bucket_ms: both passes, one step).
+ * Work items are tile_x x tile_y columns; minb / stages are the register
+ * cap (minimum CTAs per SM) and ring depth of each persistent launch,
+ * [0 = H pass, 1 = E pass][0 = CPML edge items, 1 = interior items], timed
+ * over the whole batch.  tuned = 0 when the batch kept the defaults
+ * (FDTD_TUNE=0 or under 2^20 cells). */
+#define FDTD_BATCH_MAX_BUCKETS 16
+typedef struct fdtd_batch_tuning {
+  int tuned;
+  int nbuckets;
+  int edge_lo[FDTD_BATCH_MAX_BUCKETS], edge_hi[FDTD_BATCH_MAX_BUCKETS];
+  int members[FDTD_BATCH_MAX_BUCKETS], kchunk[FDTD_BATCH_MAX_BUCKETS];
+  float bucket_ms[FDTD_BATCH_MAX_BUCKETS];
+  int tile_x, tile_y;
+  int minb[2][2], stages[2][2];
+} fdtd_batch_tuning;
+fdtd_status fdtd_batch_get_tuning(const fdtd_batch* b, fdtd_batch_tuning* out);
 fdtd_status fdtd_batch_destroy(fdtd_batch* b);
 
 #ifdef __cplusplus

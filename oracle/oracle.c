@@ -1356,6 +1356,14 @@ int orc_get_incident(const orc_sim* s, double* re, double* im, size_t n) {
   for (size_t m = 0; m < n; m++) { re[m] = creal(s->Einc[m]); im[m] = cimag(s->Einc[m]); }
   return 0;
 }
+int orc_get_state(const orc_sim* s, int which, int comp, double* out, size_t n) {
+  if (n != s->n || comp < 0 || comp > 2) return -1;
+  if (which < 0 || which > 2) return -1;
+  const double* src = which == 0 ? s->Pd_n[comp] : which == 1 ? s->ND[comp] : s->NDp[comp];
+  if (src) memcpy(out, src, n * sizeof(double));
+  else memset(out, 0, n * sizeof(double)); /* no density without the hydrodynamic model */
+  return 0;
+}
 int orc_get_line(const orc_sim* s, double* e, double* h, size_t n) {
   if (n != (size_t)s->L) return -1;
   memcpy(e, s->e_inc, n * sizeof(double));

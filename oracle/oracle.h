@@ -65,6 +65,12 @@ int orc_spectra(orc_sim* s, double* out19);
 int orc_get_freqs(const orc_sim* s, double* f, size_t n);
 int orc_get_incident(const orc_sim* s, double* re, double* im, size_t n);
 int orc_get_line(const orc_sim* s, double* e_inc, double* h_inc, size_t n);
+/* Dispersive state of component comp, reference layout (n = NX*NY*NZ):
+ * which 0 = the Drude polarisation (local model) or current (hydrodynamic)
+ * of the last step, P*_d after main.cu:1207 / 2034; 1 = ND* as the
+ * reference holds it after its step (the density from before the step,
+ * main.cu:1267-1269); 2 = ND*_prev (the density after the step). */
+int orc_get_state(const orc_sim* s, int which, int comp, double* out, size_t n);
 int orc_get_probe(const orc_sim* s, double* out, size_t n);
 
 /* Coefficient tables for unit tests.  which: 0=kedx 1=kedy 2=kedz

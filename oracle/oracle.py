@@ -54,6 +54,7 @@ def lib():
         L.orc_get_freqs.argtypes = [C.c_void_p, dp, C.c_size_t]
         L.orc_get_incident.argtypes = [C.c_void_p, dp, dp, C.c_size_t]
         L.orc_get_line.argtypes = [C.c_void_p, dp, dp, C.c_size_t]
+        L.orc_get_state.argtypes = [C.c_void_p, C.c_int, C.c_int, dp, C.c_size_t]
         L.orc_get_probe.argtypes = [C.c_void_p, dp, C.c_size_t]
         L.orc_get_cpml.argtypes = [C.c_void_p, C.c_int, dp, C.c_size_t]
         L.orc_get_ade.argtypes = [C.c_void_p, dp, C.c_size_t]
@@ -177,6 +178,12 @@ class OracleSim:
         h = np.empty(self.dims.inc_length)
         lib().orc_get_line(self.h, _dp(e), _dp(h), e.size)
         return e, h
+
+    def state(self, which, comp):
+        """Dispersive state in the reference layout (see orc_get_state)."""
+        out = np.empty(self.shape, np.float64)
+        assert lib().orc_get_state(self.h, which, comp, _dp(out), out.size) == 0
+        return out
 
     def probe(self):
         out = np.empty((self.t, 3))

@@ -48,6 +48,15 @@ CASES = {
 }
 
 
+# Snapshot decks (Snap_in 3: aux lines and the |E| plane; Snap_in 2: the
+# |P_d| and mean-density planes of the hydrodynamic model), with y/z skips
+SNAP_CASES = {
+    "snap_field": dict(BASE, Tend=400, Snap_in=3, t_skip=100, y_skip=2, z_skip=3),
+    "snap_hydro": dict(BASE, NONLOCAL=3, Tend=400, nano_sphere_radius=12e-9, Snap_in=2, t_skip=100,
+                       y_skip=1, z_skip=2),
+}
+
+
 def deck(case):
     """Input.txt text for a case dict."""
     lines = ["Input"]
@@ -61,7 +70,8 @@ if __name__ == "__main__":
     import os
     import sys
     out = sys.argv[1]
-    for name, case in CASES.items():
+    which = sys.argv[2] if len(sys.argv) > 2 else "spectra"
+    for name, case in (SNAP_CASES if which == "snap" else CASES).items():
         d = os.path.join(out, name)
         os.makedirs(d, exist_ok=True)
         with open(os.path.join(d, "Input.txt"), "w") as f:

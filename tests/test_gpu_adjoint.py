@@ -307,3 +307,26 @@ def test_backward_spectra_rejects_field_free_columns(fp64_grad):
     with pytest.raises(F.FdtdError) as e:  # forward_spectra has no objective of its own
         s.backward()
     assert e.value.status == 5
+
+
+@pytest.mark.parametrize("prec", [F.FDTD_FP32, F.FDTD_FP64])
+def test_staged_gathers_match_fused_blocks(prec, monkeypatch):
+    """The staged z-march gathers (32 x 8 x 16 tiles away from the CPML and
+    the material box) do the fused gathers' arithmetic in the same order:
+    the gradient with them and without them agrees to rounding (the
+    objective's source adds to shared face-corner cells with atomics)."""
+    box = [40, 48, 40, 48, 44, 48]
+    out = []
+    for mode in ("1", "0"):
+        monkeypatch.setenv("FDTD_ADJ_STAGED", mode)
+        s = F.Sim(make(F, "sphere_big", precision=prec, nano_sphere=0, Tend=420, design_box=box, **GOLD))
+        rng = np.random.default_rng(3)
+        s.set_design(rng.uniform(0, 1, (box[5] - box[4], box[3] - box[2], box[1] - box[0])).astype(np.float32))
+        L = s.forward(SEL, 40)
+        g, gp = s.backward()
+        out.append((L, g, gp))
+        s.close()
+    assert out[0][0] == out[1][0]
+    tol = 1e-12 if prec == F.FDTD_FP64 else 1e-5
+    assert np.abs(out[0][1] - out[1][1]).max() <= tol * np.abs(out[1][1]).max()
+    np.testing.assert_allclose(out[0][2], out[1][2], rtol=tol)

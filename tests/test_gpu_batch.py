@@ -100,3 +100,26 @@ def test_batch_rejects_mixed_members():
         F.Batch([make(F, "sphere_au", precision=F.FDTD_FP32),
                  make(F, "sphere_au", precision=F.FDTD_FP32, Tend=500)])
     assert e.value.status == 1 and "Tend" in str(e.value)
+
+
+def test_tuned_batch_is_bit_identical_and_reports_its_shapes():
+    """Members of three size buckets, 2^21 cells in all: the autotuner
+    picks a z-chunk per bucket and a variant per launch; the result stays
+    bit-identical to the members run alone."""
+    sizes = [(84, 76, 80), (60, 60, 60), (44, 44, 44)]
+    params = [make(F, "sphere_big", precision=F.FDTD_FP32, NCELLX=x, NCELLY=y, NCELLZ=z) for x, y, z in sizes]
+    b = F.Batch(params)
+    tu = b.tuning()
+    print(tu)
+    assert tu["tuned"] and tu["tile"] == [32, 4]
+    assert sum(q["members"] for q in tu["buckets"]) == len(params) and len(tu["buckets"]) == 3
+    assert all(q["kchunk"] in (8, 16, 32) and q["ms"] > 0 for q in tu["buckets"])
+    steps = 140
+    b.step(steps)
+    for i, p in enumerate(params):
+        alone = F.Sim(p)
+        alone.step(steps)
+        for c in range(6):
+            np.testing.assert_array_equal(b.sim(i).field(c), alone.field(c), err_msg=f"member {i} component {c}")
+        alone.close()
+    b.close()
