@@ -1088,7 +1088,7 @@ __global__ void __launch_bounds__(32 * kAdjTY) adj_gather_h_staged(const __grid_
   const size_t plane = s.plane;
   const int k0 = tl.z * kAdjKC, k1 = min(NZ, k0 + kAdjKC);
   CopyTasks<T, TY> tasks;
-  tasks.init(sbase, a.lE[0], a.lE[1], a.lE[2], a.lH[0], a.lH[1], a.lH[2], NY, PX, plane, k0, i0, j0, 0, 0);
+  tasks.init(sbase, a.lE[0], a.lE[1], a.lE[2], a.lH[0], a.lH[1], a.lH[2], s.NX, NY, PX, plane, k0, i0, j0, 0, 0, false);
   int pnext = k0;
 #pragma unroll
   for (int q = 0; q < S - 1; q++) {
@@ -1156,7 +1156,7 @@ __global__ void __launch_bounds__(32 * kAdjTY) adj_gather_e_staged(const __grid_
   const size_t plane = s.plane;
   const int k0 = tl.z * kAdjKC, k1 = min(NZ, k0 + kAdjKC);
   CopyTasks<T, TY> tasks;
-  tasks.init(sbase, a.lH[0], a.lH[1], a.lH[2], a.lE[0], a.lE[1], a.lE[2], NY, PX, plane, k0 - 1, i0, j0, -1, -L::CH);
+  tasks.init(sbase, a.lH[0], a.lH[1], a.lH[2], a.lE[0], a.lE[1], a.lE[2], s.NX, NY, PX, plane, k0 - 1, i0, j0, -1, -L::CH, false);
   int pnext = k0 - 1;
 #pragma unroll
   for (int q = 0; q < S - 1; q++) {

@@ -516,6 +516,8 @@ static fdtd_status batch_create_impl(const fdtd_params* ps, int n, int device, f
   auto b = std::make_unique<fdtd_batch>();
   b->device = device;
   CUDA_TRY(cudaSetDevice(device));
+  for (int i = 0; i < n; i++)
+    if (ps[i].periodic_xy) return fail(FDTD_ERR_UNSUPPORTED, "periodic_xy simulations do not batch (member " + std::to_string(i) + ")");
   for (int i = 0; i < n; i++) {
     fdtd_sim* s = nullptr;
     const fdtd_status st = create_impl(&ps[i], device, &s, /*tune*/ false);

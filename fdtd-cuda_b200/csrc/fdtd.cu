@@ -356,7 +356,7 @@ static fdtd_status build_views(fdtd_sim* s) {
   for (int c = 0; c < 3; c++)
     for (int slot = 0; slot < 2; slot++) {
       const int ax = (c + 1 + slot) % 3;
-      const int Nc = su.Nc[ax];
+      const int Nc = std::max(su.Nc[ax], 0);  // -1 along a periodic axis: no slab
       size_t cells_e, cells_h;
       if (ax == 2) { cells_e = (size_t)(Nc + 1) * s->plane; cells_h = (size_t)Nc * s->plane; }
       else if (ax == 1) { cells_e = (size_t)s->NZ * (Nc + 1) * s->PX; cells_h = (size_t)s->NZ * Nc * s->PX; }
@@ -378,6 +378,8 @@ static fdtd_status build_views(fdtd_sim* s) {
   tf.sth = su.sth; tf.cth = su.cth; tf.sph = su.sph; tf.cph = su.cph;
   for (int c = 0; c < 3; c++) { tf.fe[c] = su.fe[c]; tf.fh[c] = su.fh[c]; }
   tf.dscale = su.p.dx / su.d1D;
+  tf.closed = su.p.periodic_xy ? 0 : 1;  // periodic: the lower z face only (main.cu:698)
+  v.periodic = su.p.periodic_xy ? 1 : 0;
   v.h_inc = s->h_inc;
   v.nonfinite = &s->clk->nonfinite;
   // dispersive cells
@@ -558,6 +560,7 @@ static fdtd_status create_impl(const fdtd_params* p, int device, fdtd_sim** out,
               const int N3[3] = {s->NX, s->NY, s->NZ};
               bool active = true;
               for (int a = 0; a < 3; a++) {
+                if (su.p.periodic_xy && a < 2) continue;  // x and y wrap around
                 if (q[a] >= N3[a] - 1) active = false;
                 if (a != c && q[a] < 1) active = false;
               }
@@ -597,7 +600,7 @@ static fdtd_status create_impl(const fdtd_params* p, int device, fdtd_sim** out,
         for (const int4& e : cells[c]) {
           const int q[3] = {e.x, e.y, e.z};
           for (int a = 0; a < 3; a++)
-            if (q[a] <= su.Nc[a] + 1 || q[a] >= su.F[a] - 1) s->pml_metal = true;
+            if (su.Nc[a] >= 0 && (q[a] <= su.Nc[a] + 1 || q[a] >= su.F[a] - 1)) s->pml_metal = true;
         }
     }
     CUDA_TRY(s->alloc(&s->mat, s->ncell));
@@ -655,9 +658,22 @@ static fdtd_status create_impl(const fdtd_params* p, int device, fdtd_sim** out,
     static const int fcomp[3][4] = {{1, 2, 4, 5}, {0, 2, 3, 5}, {0, 1, 3, 4}};
     DftView& d = s->dft;
     std::memset(&d, 0, sizeof(d));
-    d.nfaces = 12;
+    d.nfaces = su.p.periodic_xy ? 2 : 12;
     long long row = 0;
-    for (int b = 0; b < 2; b++) {
+    // periodic x and y: the reflection and the transmission plane, whole
+    // xy planes (Spectral.cu:11-16, 32-120)
+    for (int f = 0; su.p.periodic_xy && f < 2; f++) {
+      DftFace& F = d.face[f];
+      F.ax = 2;
+      F.pos = f == 0 ? su.k_refl : su.k_trans;
+      F.s1 = 0; F.s2 = 0;
+      F.na = s->NX; F.nb = s->NY;
+      for (int c = 0; c < 4; c++) F.comp[c] = fcomp[2][c];
+      F.row0 = row;
+      F.npad = ((long long)F.na * F.nb + kDftRows - 1) / kDftRows * kDftRows;
+      row += 4LL * F.npad;
+    }
+    for (int b = 0; b < 2 && !su.p.periodic_xy; b++) {
       const int* S = b == 0 ? su.absS : su.scaS;
       const int* En = b == 0 ? su.absE : su.scaE;
       for (int f = 0; f < 6; f++) {
@@ -691,10 +707,18 @@ static fdtd_status create_impl(const fdtd_params* p, int device, fdtd_sim** out,
   // CPML slab cells and TFSF shells
   {
     int lo[3], hi[3];
-    for (int a = 0; a < 3; a++) { lo[a] = su.Nt[a] - 1; hi[a] = (a == 0 ? s->NX : a == 1 ? s->NY : s->NZ) - su.Nt[a]; }
-    s->shell_h.init(lo, hi);
-    for (int a = 0; a < 3; a++) lo[a] = su.Nt[a];
-    s->shell_e.init(lo, hi);
+    if (su.p.periodic_xy) {
+      // the lower z face only: planes Nt_z - 1 (H) and Nt_z (E), every cell
+      // of both once (a box two planes thick is all shell)
+      const int l[3] = {0, 0, su.Nt[2] - 1}, h[3] = {s->NX - 1, s->NY - 1, su.Nt[2]};
+      s->shell_h.init(l, h);
+      s->shell_e.init(l, h);
+    } else {
+      for (int a = 0; a < 3; a++) { lo[a] = su.Nt[a] - 1; hi[a] = (a == 0 ? s->NX : a == 1 ? s->NY : s->NZ) - su.Nt[a]; }
+      s->shell_h.init(lo, hi);
+      for (int a = 0; a < 3; a++) lo[a] = su.Nt[a];
+      s->shell_e.init(lo, hi);
+    }
   }
   fdtd_status st = s->fp64 ? build_views<double>(s.get()) : build_views<float>(s.get());
   if (st != FDTD_OK) return st;
@@ -1179,8 +1203,8 @@ static void launch_metal(fdtd_sim* s, cudaStream_t st) {
 template <typename T>
 static void launch_sample(fdtd_sim* s, cudaStream_t st) {
   int maxn = 0;
-  for (int f = 0; f < 12; f++) maxn = std::max(maxn, s->dft.face[f].na * s->dft.face[f].nb);
-  dim3 g((maxn + 255) / 256, 12);
+  for (int f = 0; f < s->dft.nfaces; f++) maxn = std::max(maxn, s->dft.face[f].na * s->dft.face[f].nb);
+  dim3 g((maxn + 255) / 256, s->dft.nfaces);
   dft_sample<T><<<g, 256, 0, st>>>(view<T>(s), s->dft, (T*)s->ring, s->clk);
   s->kernels++;
 }
@@ -1392,6 +1416,8 @@ extern "C" fdtd_status fdtd_spectral_finalize(fdtd_sim* s, double* out) {
   if (!s || !out) return fail(FDTD_ERR_INVALID, "null argument");
   CUDA_TRY(cudaSetDevice(s->device));
   CUDA_TRY(cudaDeviceSynchronize());
+  if (s->su.p.periodic_xy)
+    return fail(FDTD_ERR_STATE, "a periodic_xy simulation has no DFT box: fdtd_reflectance gives its spectra");
   fdtd_status st = flush_dft(s);
   if (st != FDTD_OK) return st;
   const int nf = s->dft.nf;
@@ -1437,12 +1463,47 @@ extern "C" fdtd_status fdtd_write_scatabs(fdtd_sim* s, const char* path) {
   return FDTD_OK;
 }
 
+// R and T of a periodic simulation (Reflectance_XZ, main.cu:3195-3320):
+// per frequency P = sum Re(Ey conj(Hx) - Ex conj(Hy)) dA over the
+// reflection plane (scattered field: the reflected wave, P > 0) and the
+// transmission plane (total field: the transmitted wave, P < 0), over the
+// plane's area and |E_inc / dft_every|^2 (the planes are sampled every
+// dft_every steps, E_inc sums every step).  flux_reduce sums Re(Ex conj(Hy)
+// - Ey conj(Hx)) = -P / dA per plane.
+extern "C" fdtd_status fdtd_reflectance(fdtd_sim* s, double* out) {
+  if (!s || !out) return fail(FDTD_ERR_INVALID, "null argument");
+  if (!s->su.p.periodic_xy) return fail(FDTD_ERR_STATE, "fdtd_reflectance needs a periodic_xy simulation");
+  CUDA_TRY(cudaSetDevice(s->device));
+  CUDA_TRY(cudaDeviceSynchronize());
+  fdtd_status st = flush_dft(s);
+  if (st != FDTD_OK) return st;
+  const int nf = s->dft.nf;
+  flux_reduce<<<dim3(2, nf), 256>>>(s->dft, s->flux);
+  CUDA_TRY(cudaGetLastError());
+  std::vector<double> Q((size_t)2 * nf);
+  CUDA_TRY(cudaMemcpy(Q.data(), s->flux, Q.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  const Setup& su = s->su;
+  const double cells = (double)s->NX * s->NY;  // area / (dx dy)
+  for (int m = 0; m < nf; m++) {
+    const double amp = std::abs(su.Einc[m]), as = amp / su.p.dft_every;
+    const double inc = cells * as * as;
+    const double R = -Q[m] / inc, T = Q[(size_t)nf + m] / inc;
+    double* row = out + 7 * (size_t)m;
+    row[0] = su.c0 / su.freq[m];
+    row[1] = R; row[2] = T; row[3] = 1.0 - R - T;
+    row[4] = amp; row[5] = su.Einc[m].real(); row[6] = su.Einc[m].imag();
+  }
+  return FDTD_OK;
+}
+
 extern "C" fdtd_status fdtd_get_dft(fdtd_sim* s, int box, int face, int comp, double* re, double* im,
                                     size_t count) {
   if (!s || !re || !im || box < 0 || box > 1 || face < 0 || face > 5 || comp < 0 || comp > 3)
     return fail(FDTD_ERR_INVALID, "bad argument");
   CUDA_TRY(cudaSetDevice(s->device));
   CUDA_TRY(cudaDeviceSynchronize());
+  if (s->su.p.periodic_xy && (box != 0 || face > 1))
+    return fail(FDTD_ERR_INVALID, "periodic_xy: box 0, face 0 (reflection plane) or 1 (transmission plane)");
   fdtd_status st = flush_dft(s);
   if (st != FDTD_OK) return st;
   const DftFace& F = s->dft.face[box * 6 + face];

@@ -53,6 +53,7 @@ struct TfsfView {
   float sth, cth, sph, cph;  // sinf/cosf of the angles (host-computed)
   float fe[3], fh[3];        // E and H direction factors
   double dscale;             // dx / d_1D
+  int closed;                // 1: all six faces; 0: the lower z face only (periodic x and y)
 };
 
 template <typename T>
@@ -74,6 +75,7 @@ struct SimView {
                         // line's E is double-buffered and passed per launch
   int* nonfinite;
   const SimView* self;  // a copy of this view in device memory (cold paths)
+  int periodic;         // 1: x and y wrap around (every x and y index is updated)
 };
 
 // Dispersive (Drude + 2 critical points, optionally hydrodynamic) cells.

@@ -94,7 +94,7 @@ __device__ __forceinline__ void tfsf_h_walk(const SimView<T>& s, int c, int i, i
   const int Tx = tf.Tx, Ty = tf.Ty, Tz = tf.Tz;
   const int di = 2 * (i - tf.i0), dj = 2 * (j - tf.j0), dk = 2 * (k - tf.k0);
   if (c == 0) {  // hx: CORRECT_Y then CORRECT_Z
-    if (i >= Tx && i <= NX - Tx && k >= Tz && k < NZ - Tz) {
+    if (tf.closed && i >= Tx && i <= NX - Tx && k >= Tz && k < NZ - Tz) {
       if (j == Ty - 1) {  // source at j+1
         fn(+1, 1, 2, tf_proj(tf, di, dj + 2, dk + 1));
       } else if (j == NY - Ty) {
@@ -104,12 +104,12 @@ __device__ __forceinline__ void tfsf_h_walk(const SimView<T>& s, int c, int i, i
     if (i >= Tx && i <= NX - Tx && j >= Ty && j < NY - Ty) {
       if (k == Tz - 1) {
         fn(-1, 2, 1, tf_proj(tf, di, dj + 1, dk + 2));
-      } else if (k == NZ - Tz) {
+      } else if (k == NZ - Tz && tf.closed) {
         fn(+1, 2, 1, tf_proj(tf, di, dj + 1, dk));
       }
     }
   } else if (c == 1) {  // hy: CORRECT_X then CORRECT_Z
-    if (j >= Ty && j <= NY - Ty && k >= Tz && k < NZ - Tz) {
+    if (tf.closed && j >= Ty && j <= NY - Ty && k >= Tz && k < NZ - Tz) {
       if (i == Tx - 1) {
         fn(-1, 0, 2, tf_proj(tf, di + 2, dj, dk + 1));
       } else if (i == NX - Tx) {
@@ -119,19 +119,19 @@ __device__ __forceinline__ void tfsf_h_walk(const SimView<T>& s, int c, int i, i
     if (i >= Tx && i < NX - Tx && j >= Ty && j <= NY - Ty) {
       if (k == Tz - 1) {
         fn(+1, 2, 0, tf_proj(tf, di + 1, dj, dk + 2));
-      } else if (k == NZ - Tz) {
+      } else if (k == NZ - Tz && tf.closed) {
         fn(-1, 2, 0, tf_proj(tf, di + 1, dj, dk));
       }
     }
   } else {  // hz: CORRECT_X then CORRECT_Y
-    if (j >= Ty && j < NY - Ty && k >= Tz && k <= NZ - Tz) {
+    if (tf.closed && j >= Ty && j < NY - Ty && k >= Tz && k <= NZ - Tz) {
       if (i == Tx - 1) {
         fn(+1, 0, 1, tf_proj(tf, di + 2, dj + 1, dk));
       } else if (i == NX - Tx) {
         fn(-1, 0, 1, tf_proj(tf, di, dj + 1, dk));
       }
     }
-    if (i >= Tx && i < NX - Tx && k >= Tz && k <= NZ - Tz) {
+    if (tf.closed && i >= Tx && i < NX - Tx && k >= Tz && k <= NZ - Tz) {
       if (j == Ty - 1) {
         fn(-1, 1, 0, tf_proj(tf, di + 1, dj + 2, dk));
       } else if (j == NY - Ty) {
@@ -151,7 +151,7 @@ __device__ __forceinline__ void tfsf_e_walk(const SimView<T>& s, int c, int i, i
   const int Tx = tf.Tx, Ty = tf.Ty, Tz = tf.Tz;
   const int di = 2 * (i - tf.i0), dj = 2 * (j - tf.j0), dk = 2 * (k - tf.k0);
   if (c == 0) {  // ex: CORRECT_Y then CORRECT_Z
-    if (i >= Tx && i < NX - Tx && k >= Tz && k <= NZ - Tz) {
+    if (tf.closed && i >= Tx && i < NX - Tx && k >= Tz && k <= NZ - Tz) {
       if (j == Ty) {
         fn(-1, 1, 2, tf_proj(tf, di + 1, dj - 1, dk));
       } else if (j == NY - Ty) {
@@ -161,12 +161,12 @@ __device__ __forceinline__ void tfsf_e_walk(const SimView<T>& s, int c, int i, i
     if (i >= Tx && i < NX - Tx && j >= Ty && j <= NY - Ty) {
       if (k == Tz) {
         fn(+1, 2, 1, tf_proj(tf, di + 1, dj, dk - 1));
-      } else if (k == NZ - Tz) {
+      } else if (k == NZ - Tz && tf.closed) {
         fn(-1, 2, 1, tf_proj(tf, di + 1, dj, dk + 1));
       }
     }
   } else if (c == 1) {  // ey: CORRECT_X then CORRECT_Z
-    if (j >= Ty && j < NY - Ty && k >= Tz && k <= NZ - Tz) {
+    if (tf.closed && j >= Ty && j < NY - Ty && k >= Tz && k <= NZ - Tz) {
       if (i == Tx) {
         fn(+1, 0, 2, tf_proj(tf, di - 1, dj + 1, dk));
       } else if (i == NX - Tx) {
@@ -176,19 +176,19 @@ __device__ __forceinline__ void tfsf_e_walk(const SimView<T>& s, int c, int i, i
     if (i >= Tx && i <= NX - Tx && j >= Ty && j < NY - Ty) {
       if (k == Tz) {
         fn(-1, 2, 0, tf_proj(tf, di, dj + 1, dk - 1));
-      } else if (k == NZ - Tz) {
+      } else if (k == NZ - Tz && tf.closed) {
         fn(+1, 2, 0, tf_proj(tf, di, dj + 1, dk + 1));
       }
     }
   } else {  // ez: CORRECT_X then CORRECT_Y
-    if (j >= Ty && j <= NY - Ty && k >= Tz && k < NZ - Tz) {
+    if (tf.closed && j >= Ty && j <= NY - Ty && k >= Tz && k < NZ - Tz) {
       if (i == Tx) {
         fn(-1, 0, 1, tf_proj(tf, di - 1, dj, dk + 1));
       } else if (i == NX - Tx) {
         fn(+1, 0, 1, tf_proj(tf, di + 1, dj, dk + 1));
       }
     }
-    if (i >= Tx && i <= NX - Tx && k >= Tz && k < NZ - Tz) {
+    if (tf.closed && i >= Tx && i <= NX - Tx && k >= Tz && k < NZ - Tz) {
       if (j == Ty) {
         fn(+1, 1, 0, tf_proj(tf, di, dj - 1, dk + 1));
       } else if (j == NY - Ty) {
@@ -343,17 +343,20 @@ __device__ __forceinline__ T curl_h_at(const SimView<T>& s, int c, int i, int j,
   const T* hx = s.H[0];
   const T* hy = s.H[1];
   const T* hz = s.H[2];
+  // offsets of the -x and -y neighbours (periodic x and y wrap around)
+  const long long mx = (s.periodic && i == 0) ? -(long long)(s.NX - 1) : 1;
+  const long long my = (s.periodic && j == 0) ? -(long long)(s.NY - 1) * s.PX : (long long)s.PX;
   if (c == 0) {
-    T dhz = hz[id] - hz[id - s.PX], dhy = hy[id] - hy[id - s.plane];
+    T dhz = hz[id] - hz[id - my], dhy = hy[id] - hy[id - s.plane];
     *dh_a = dhz; *dh_b = dhy;  // y-slab diff, z-slab diff
     return dhz * s.cp[1].inv_ked[j] - dhy * s.cp[2].inv_ked[k];
   }
   if (c == 1) {
-    T dhx = hx[id] - hx[id - s.plane], dhz = hz[id] - hz[id - 1];
+    T dhx = hx[id] - hx[id - s.plane], dhz = hz[id] - hz[id - mx];
     *dh_a = dhx; *dh_b = dhz;  // z-slab diff, x-slab diff
     return dhx * s.cp[2].inv_ked[k] - dhz * s.cp[0].inv_ked[i];
   }
-  T dhy = hy[id] - hy[id - 1], dhx = hx[id] - hx[id - s.PX];
+  T dhy = hy[id] - hy[id - mx], dhx = hx[id] - hx[id - my];
   *dh_a = dhy; *dh_b = dhx;  // x-slab diff, y-slab diff
   return dhy * s.cp[0].inv_ked[i] - dhx * s.cp[1].inv_ked[j];
 }

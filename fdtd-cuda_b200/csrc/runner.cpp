@@ -7,6 +7,14 @@
 //   ScatAbs.<t>.txt      the spectra (CalculateAbsScatt, Spectral.cu) after
 //                        every step t with t % (Tend/10) == 0
 //                        (main.cu:3042-3172; at Tend only when Tend < 10)
+//   Reflectivity{TE,TM}.<trial>.<t>.txt
+//                        periodic_xy runs instead of ScatAbs: after every
+//                        step t > 0 with t % (Tend/10) == 0 (main.cu:2994-
+//                        3037), per frequency but the first: lambda (or
+//                        the frequency), R, the reference's transmitted
+//                        flux ratio (negative for a wave leaving through
+//                        +z), |E_inc|^2, and the two fluxes over the area
+//                        unnormalised (fdtd_reflectance)
 //   aux_sim.<n>.txt, aux_sim.<n>_2.txt, videofiles/YZ_sim.<n>.txt,
 //   videofiles/YZ_sim.<n>_N.txt
 //                        the snapshots of Snap_in 1, 2, 3 every t_skip
@@ -16,6 +24,11 @@
 //                        reference's snapshot_count does
 //
 //   fdtd_runner [Input.txt] [--out DIR] [--fp32 | --fp64] [--device N]
+//               [--periodic-xy]
+//
+// --periodic-xy switches on the reference's Periodic_XY path, which its
+// Input.txt cannot select (main.cu:2398 forces it off); the deck must then
+// set NcpmlX = NcpmlY = 0.
 //
 // Exit status: 0 on success, 1 on a library error (its text on stderr), 2
 // on bad arguments, 3 when the watchdog saw a non-finite field ("NAN
@@ -34,10 +47,11 @@ namespace {
 
 void usage() {
   std::fprintf(stderr,
-               "usage: fdtd_runner [Input.txt] [--out DIR] [--fp32 | --fp64] [--device N]\n"
+               "usage: fdtd_runner [Input.txt] [--out DIR] [--fp32 | --fp64] [--device N] [--periodic-xy]\n"
                "  runs the reference's time loop on the GPU and writes OUT.txt, ScatAbs.<t>.txt\n"
                "  every Tend/10 steps and the Snap_in snapshots into DIR (default: the current\n"
-               "  directory)\n");
+               "  directory); --periodic-xy: periodic x and y, Reflectivity{TE,TM}.<trial>.<t>.txt\n"
+               "  instead of ScatAbs\n");
 }
 
 int fail(const char* what) {
@@ -86,11 +100,30 @@ bool write_snapshot(const std::string& out, const fdtd_snapshot_layout& L, const
   return aux() && plane(L.off_plane, "");
 }
 
+// The periodic run's reflectivity file (main.cu:3026-3035): the columns
+// the reference prints from its E_reflected / E_transmitted (P / A) and the
+// incident amplitude |E_inc|^2.
+bool write_reflectivity(fdtd_sim* sim, const fdtd_params& p, const std::string& path) {
+  const int nf = p.NUM_freq;
+  std::vector<double> rt((size_t)7 * nf), freq(nf);
+  if (fdtd_reflectance(sim, rt.data()) != FDTD_OK || fdtd_get_freqs(sim, freq.data(), nf) != FDTD_OK) return false;
+  FILE* f = std::fopen(path.c_str(), "w");
+  if (!f) return false;
+  for (int m = 1; m < nf; m++) {
+    const double* r = &rt[(size_t)7 * m];
+    const double amp = r[4] * r[4];
+    const double refl = r[1] * amp, trans = -r[2] * amp;  // P_refl / A, P_trans / A
+    std::fprintf(f, "%e\t%e\t%e\t%e\t%e\t%e\n", p.WL_or_freq == 1 ? r[0] : freq[m], r[1], -r[2], amp, refl, trans);
+  }
+  std::fclose(f);
+  return true;
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
   std::string input = "Input.txt", out = ".";
-  int precision = -1, device = 0;
+  int precision = -1, device = 0, periodic = 0;
   for (int a = 1; a < argc; a++) {
     const char* s = argv[a];
     if (!std::strcmp(s, "--help") || !std::strcmp(s, "-h")) {
@@ -100,6 +133,8 @@ int main(int argc, char** argv) {
       out = argv[++a];
     } else if (!std::strcmp(s, "--device") && a + 1 < argc) {
       device = std::atoi(argv[++a]);
+    } else if (!std::strcmp(s, "--periodic-xy")) {
+      periodic = 1;
     } else if (!std::strcmp(s, "--fp32")) {
       precision = FDTD_FP32;
     } else if (!std::strcmp(s, "--fp64")) {
@@ -115,6 +150,7 @@ int main(int argc, char** argv) {
   fdtd_params_default(&p);
   if (fdtd_load_input_txt(input.c_str(), &p) != FDTD_OK) return fail("reading the input");
   if (precision >= 0) p.precision = precision;
+  if (periodic) p.periodic_xy = 1;
   fdtd_sim* sim = nullptr;
   if (fdtd_create(&p, device, &sim) != FDTD_OK) return fail("setting up");
   // snapshots: taken on the device, drained after every chunk of steps
@@ -137,8 +173,13 @@ int main(int argc, char** argv) {
   const int total = p.Tend + 1;
   const int period = p.Tend / 10;
   std::vector<int> dumps;
-  for (int t = 0; t <= p.Tend; t++)
-    if (period > 0 ? t % period == 0 : t == p.Tend) dumps.push_back(t);
+  for (int t = 0; t <= p.Tend; t++) {
+    if (p.periodic_xy) {
+      if (t > 0 && period > 0 && t % period == 0) dumps.push_back(t);
+    } else if (period > 0 ? t % period == 0 : t == p.Tend) {
+      dumps.push_back(t);
+    }
+  }
   std::vector<std::string> written;
   int done = 0;
   size_t next_dump = 0;
@@ -165,8 +206,17 @@ int main(int argc, char** argv) {
         }
     }
     if (next_dump < dumps.size() && done == dumps[next_dump] + 1) {
-      const std::string sca = out + "/ScatAbs." + std::to_string(dumps[next_dump]) + ".txt";
-      if (fdtd_write_scatabs(sim, sca.c_str()) != FDTD_OK) {
+      const std::string t = std::to_string(dumps[next_dump]);
+      std::string sca;
+      bool ok;
+      if (p.periodic_xy) {
+        sca = out + "/Reflectivity" + (p.TE_TM == 1 ? "TM." : "TE.") + std::to_string(p.min_trials) + "." + t + ".txt";
+        ok = write_reflectivity(sim, p, sca);
+      } else {
+        sca = out + "/ScatAbs." + t + ".txt";
+        ok = fdtd_write_scatabs(sim, sca.c_str()) == FDTD_OK;
+      }
+      if (!ok) {
         fdtd_destroy(sim);
         return fail("writing the spectra");
       }

@@ -212,7 +212,8 @@ static void rasterise(Setup& s) {
         }
     if (p.nano_sphere == 1 || p.nano_sphere == 3) {
       const int r = (int)(p.nano_sphere_radius / p.dx);
-      const double cx = NX / 2, cy = NY / 2, cz = NZ / 2;
+      // periodic x and y: the particle rests on the slab (setup.cu:223, 268)
+      const double cx = NX / 2, cy = NY / 2, cz = p.periodic_xy ? (double)(slab - r) : (double)(NZ / 2);
       const double off[3][3] = {{0.5, 0, 0}, {0, 0.5, 0}, {0, 0, 0.5}};
       for (int i = 0; i < NX; i++)
         for (int j = 0; j < NY; j++)
@@ -294,13 +295,24 @@ const char* setup_build(const fdtd_params& pin, Setup& s) {
   if (p.geometry == FDTD_GEOM_DISK_ARRAY && p.slab_thickness > 0 && !(p.slab_eps >= 1.0))
     return "slab_eps must be >= 1";
   if (p.precision != FDTD_FP32 && p.precision != FDTD_FP64) return "precision must be FDTD_FP32 or FDTD_FP64";
+  const bool per = p.periodic_xy != 0;
+  if (per) {
+    if (p.NcpmlX != 0 || p.NcpmlY != 0) return "periodic_xy needs NcpmlX = NcpmlY = 0 (CPML in z only)";
+    if (p.NCELLX % 8 != 0 || p.NCELLX < 8 || p.NCELLY < 2) return "periodic_xy needs NCELLX a multiple of 8 and NCELLY >= 2";
+    if (p.NONLOCAL == 3) return "periodic_xy does not support the hydrodynamic model";
+    const int* b = p.design_box;
+    if (b[1] > b[0] || b[3] > b[2] || b[5] > b[4]) return "periodic_xy does not support a design region";
+    if (std::fabs(p.inc_theta_deg) > 1e-12) return "periodic_xy needs normal incidence (inc_theta_deg = 0)";
+  }
   // SETUP_CONST (setup.cu:347-510)
   s.z0 = kZ0; s.ep0 = kEP0; s.mu0 = kMU0; s.c0 = kC0; s.pi = kPI; s.e0 = kE0; s.me = kME;
   s.L = p.NCELLZ * 6;
   if (p.NCELLX == 1 || p.NCELLY == 1 || p.NCELLZ == 1) s.dt = 0.9 * p.dy / (kC0 * std::pow(2, 0.5));
   else s.dt = 0.5 * p.dy / kC0 / (double)p.TimeFactor;
-  s.NX = p.NCELLX + 2 * p.NcpmlX + 1;
-  s.NY = p.NCELLY + 2 * p.NcpmlY + 1;
+  // periodic x and y: the reference drops the grid's extra cell
+  // (setup.cu:401-404) and has no lateral TFSF faces (setup.cu:429)
+  s.NX = per ? p.NCELLX : p.NCELLX + 2 * p.NcpmlX + 1;
+  s.NY = per ? p.NCELLY : p.NCELLY + 2 * p.NcpmlY + 1;
   s.NZ = p.NCELLZ + 2 * p.NcpmlZ + 1;
   const int N3[3] = {s.NX, s.NY, s.NZ};
   const int ncp[3] = {p.NcpmlX, p.NcpmlY, p.NcpmlZ};
@@ -309,12 +321,29 @@ const char* setup_build(const fdtd_params& pin, Setup& s) {
     s.Nc[a] = ncp[a];
     s.F[a] = N3[a] - 1 - ncp[a];
     s.Nt[a] = p.tfsf_inset + ncp[a];
+    if (per && a < 2) {
+      // no slab along a periodic axis: every slab test (index <= Nc or
+      // >= F) fails
+      s.Nc[a] = -1;
+      s.F[a] = N3[a] + 1;
+      s.Nt[a] = 0;
+      s.absS[a] = s.scaS[a] = 0;
+      s.absE[a] = s.scaE[a] = N3[a];
+      continue;
+    }
     s.absS[a] = s.Nt[a] + p.box_offset;
     s.absE[a] = N3[a] - s.Nt[a] - p.box_offset;
     s.scaS[a] = s.Nt[a] - p.box_offset;
     s.scaE[a] = N3[a] - s.Nt[a] + p.box_offset;
     if (s.scaS[a] < 1 || s.scaE[a] > N3[a] - 1 || s.absE[a] - s.absS[a] < 2)
       return "TFSF/DFT boxes do not fit the grid";
+  }
+  if (per) {
+    // reflection and transmission planes (Spectral.cu:11-16)
+    s.k_refl = s.Nt[2] - 5;
+    s.k_trans = s.NZ - s.Nt[2] - 5;
+    if (s.k_refl < s.Nc[2] + 1 || s.k_trans <= s.Nt[2] || s.k_trans >= s.F[2])
+      return "periodic_xy: the reflection and transmission planes do not fit between the z CPML slabs";
   }
   s.hydro = p.NONLOCAL == 3;
   s.f0 = kC0 / p.lam_0;

@@ -22,6 +22,7 @@ struct Setup {
   int NX = 0, NY = 0, NZ = 0;
   int Nc[3] = {0, 0, 0}, F[3] = {0, 0, 0}, Nt[3] = {0, 0, 0};
   int absS[3], absE[3], scaS[3], scaE[3];
+  int k_refl = 0, k_trans = 0;  // periodic_xy: reflection and transmission planes
   int L = 0, m0 = 0, i0 = 0, j0 = 0, k0 = 0;
   double d1D = 0, dt = 0, delay = 0, width = 0, f0 = 0;
   double z0, ep0, mu0, c0, pi, e0, me;

@@ -121,8 +121,8 @@ struct CopyTasks {
   bool has[L::MAXT];
 
   __device__ __forceinline__ void init(unsigned sbase, const T* h0, const T* h1, const T* h2, const T* o0,
-                                       const T* o1, const T* o2, int NY, int PX, size_t plane, int p0, int i0,
-                                       int j0, int halo_row0, int halo_col0) {
+                                       const T* o1, const T* o2, int NX, int NY, int PX, size_t plane, int p0,
+                                       int i0, int j0, int halo_row0, int halo_col0, bool per) {
     const int tid = threadIdx.y * 32 + threadIdx.x;
 #pragma unroll
     for (int t = 0; t < L::MAXT; t++) {
@@ -143,6 +143,14 @@ struct CopyTasks {
         gi = i0 + halo_col0 + ch * L::CH;
         d = (a * (TY + 1) + r) * L::HW + ch * L::CH;
         base = a == 0 ? h0 : a == 1 ? h1 : h2;
+        if (per) {
+          // periodic x and y: the halo row -1 is row NY-1, row NY is row 0,
+          // and the halo chunks left of column 0 or at column NX come from
+          // the other side (NX is a multiple of the chunk width, so no chunk
+          // straddles the seam)
+          if (gj == -1) gj = NY - 1; else if (gj == NY) gj = 0;
+          if (gi < 0) gi += NX; else if (gi >= NX && gi < NX + L::CH) gi -= NX;
+        }
       } else {
         const int q2 = q - L::TASKS_HALO;
         a = q2 / (TY * L::NCH_OWN);
@@ -201,7 +209,8 @@ __device__ __forceinline__ void h_pass_tile(const SimView<T>& s, int kchunk, int
   const int k1 = min(NZ, k0 + kchunk);
   const T* any = s.E[0];
   CopyTasks<T, TY> tasks;
-  tasks.init(sbase, s.E[0], s.E[1], s.E[2], s.H[0], s.H[1], s.H[2], NY, PX, plane, k0, i0, j0, 0, 0);
+  tasks.init(sbase, s.E[0], s.E[1], s.E[2], s.H[0], s.H[1], s.H[2], NX, NY, PX, plane, k0, i0, j0, 0, 0,
+             s.periodic != 0);
   int pnext = k0;
 #pragma unroll
   for (int q = 0; q < S - 1; q++) {  // prologue: planes k0 .. k0+S-2 into stages 0 .. S-2
@@ -209,7 +218,9 @@ __device__ __forceinline__ void h_pass_tile(const SimView<T>& s, int kchunk, int
     cp_async_commit();
   }
   const bool live = i < NX && j < NY;
-  const bool hasx = i + 1 < NX, hasy = j + 1 < NY;
+  // periodic x and y: every column has its +x and +y neighbour
+  const bool per = s.periodic != 0;
+  const bool hasx = per || i + 1 < NX, hasy = per || j + 1 < NY;
   const T ikx = live ? ldg(s.cp[0].inv_khd + i) : T(0);
   const T iky = live ? ldg(s.cp[1].inv_khd + j) : T(0);
   const T* __restrict__ ikzp = s.cp[2].inv_khd + k0;
@@ -221,7 +232,7 @@ __device__ __forceinline__ void h_pass_tile(const SimView<T>& s, int kchunk, int
   const int o = ty * L::HW + tx, oo = ty * 32 + tx;
   constexpr int FH = (TY + 1) * L::HW;  // one halo component
   // CPML of this column: x and y slabs are fixed, z slabs follow the plane
-  const bool pml_xy = PML && live && hasx && hasy;  // i < NX-1 and j < NY-1
+  const bool pml_xy = PML && live && hasx && hasy;  // i < NX-1 and j < NY-1 (any column when periodic)
   SlabAt<T> sx, sy;
   sx.side = sy.side = 0; sx.q = sy.q = 0; sx.b = sx.c = sy.b = sy.c = T(0);
   if (pml_xy) { sx = slab_h(s.cp[0], i); sy = slab_h(s.cp[1], j); }
@@ -265,12 +276,19 @@ __device__ __forceinline__ void h_pass_tile(const SimView<T>& s, int kchunk, int
     if (sy.side) { ny0 = by0[oyk]; ny1 = by1[oyk]; }
   };
   fetch(k0, ox, oy);
+  // Ex, Ey of plane k+1 read in one plane are plane k's in the next (kept
+  // in registers), and 1/(kappa dz) of the next plane is loaded ahead
+  T cex = T(0), cey = T(0);
+  bool carry = false;
+  T ikz_next = ldg(ikzp);
   for (int k = k0; k < k1;) {
 #pragma unroll
     for (int u = 0; u < S; u++) {
       if (k < k1) {
         const T cz0 = nz0, cz1 = nz1, cx0 = nx0, cx1 = nx1, cy0 = ny0, cy1 = ny1;
         if (k + 1 < k1) fetch(k + 1, ox + xstep, oy + ystep);
+        const T ikz = ikz_next;
+        if (k + 1 < k1) ikz_next = ldg(ikzp + 1);
         cp_async_wait<S - 3>();  // planes up to k+1 have landed
         __syncthreads();
         // stage (u+S-1)%S held plane k-1, last read in the previous iteration
@@ -280,11 +298,13 @@ __device__ __forceinline__ void h_pass_tile(const SimView<T>& s, int kchunk, int
           const T* eh = sm + u * L::STAGE;
           const T* en = sm + ((u + 1) % S) * L::STAGE;
           const T* hown = eh + L::HALO;
-          const T exk = eh[o], eyk = eh[FH + o], ezk = eh[2 * FH + o];
+          const T exk = carry ? cex : eh[o], eyk = carry ? cey : eh[FH + o], ezk = eh[2 * FH + o];
           const T ex_j = eh[o + L::HW], ez_j = eh[2 * FH + o + L::HW];
           const T ey_i = eh[FH + o + 1], ez_i = eh[2 * FH + o + 1];
           const T exk1 = en[o], eyk1 = en[FH + o];
-          const T ikz = ldg(ikzp);
+          cex = exk1;
+          cey = eyk1;
+          carry = true;
           const bool hask = k + 1 < NZ;
           T vx = rfma(che, rcurl(rsub(eyk1, eyk), ikz, rsub(ez_j, ezk), iky), rmul(chh, hown[oo]));
           T vy = rfma(che, rcurl(rsub(ez_i, ezk), ikx, rsub(exk1, exk), ikz), rmul(chh, hown[TY * 32 + oo]));
@@ -387,7 +407,8 @@ __device__ __forceinline__ void e_pass_tile(const SimView<T>& s, int kchunk, int
   const int k1 = min(NZ, k0 + kchunk);
   const T* any = s.H[0];
   CopyTasks<T, TY> tasks;
-  tasks.init(sbase, s.H[0], s.H[1], s.H[2], s.E[0], s.E[1], s.E[2], NY, PX, plane, k0 - 1, i0, j0, -1, -L::CH);
+  tasks.init(sbase, s.H[0], s.H[1], s.H[2], s.E[0], s.E[1], s.E[2], NX, NY, PX, plane, k0 - 1, i0, j0, -1,
+             -L::CH, s.periodic != 0);
   int pnext = k0 - 1;
 #pragma unroll
   for (int q = 0; q < S - 1; q++) {  // prologue: planes k0-1 .. k0+S-3 into stages 0 .. S-2
@@ -396,10 +417,12 @@ __device__ __forceinline__ void e_pass_tile(const SimView<T>& s, int kchunk, int
   }
   const bool live = i < NX && j < NY;
   // active-range masks of ex, ey, ez in this column (main.cu:1172, 1476, 1767)
+  // (periodic x and y: every column, main.cu:1072, 1364, 1668)
+  const bool per = s.periodic != 0;
   const bool okx = i < NX - 1, oky = j < NY - 1;
-  const bool colx = live && okx && j > 0 && oky;
-  const bool coly = live && i > 0 && okx && oky;
-  const bool colz = live && i > 0 && okx && j > 0 && oky;
+  const bool colx = live && (per || (okx && j > 0 && oky));
+  const bool coly = live && (per || (i > 0 && okx && oky));
+  const bool colz = live && (per || (i > 0 && okx && j > 0 && oky));
   const T ikx = live ? ldg(s.cp[0].inv_ked + i) : T(0);
   const T iky = live ? ldg(s.cp[1].inv_ked + j) : T(0);
   const T* __restrict__ ikzp = s.cp[2].inv_ked + k0;
@@ -413,7 +436,7 @@ __device__ __forceinline__ void e_pass_tile(const SimView<T>& s, int kchunk, int
   const int o = (ty + 1) * L::HW + tx + L::CH, oo = ty * 32 + tx;
   constexpr int FH = (TY + 1) * L::HW;
   // CPML of this column: x and y slabs are fixed, z slabs follow the plane
-  const bool pml_xy = PML && live && okx && oky;  // i < NX-1 and j < NY-1
+  const bool pml_xy = PML && live && (per || (okx && oky));  // i < NX-1 and j < NY-1 (any column when periodic)
   SlabAt<T> sx, sy;
   sx.side = sy.side = 0; sx.q = sy.q = 0; sx.b = sx.c = sy.b = sy.c = T(0);
   T cx_ey = T(0);
@@ -462,12 +485,19 @@ __device__ __forceinline__ void e_pass_tile(const SimView<T>& s, int kchunk, int
   };
   fetch(k0, ox, oy);
   T check = T(0);
+  // Hx, Hy of plane k are plane k-1's in the next plane (kept in
+  // registers), and 1/(kappa dz) of the next plane is loaded ahead
+  T chx = T(0), chy = T(0);
+  bool carry = false;
+  T ikz_next = ldg(ikzp);
   for (int k = k0; k < k1;) {
 #pragma unroll
     for (int u = 0; u < S; u++) {
       if (k < k1) {
         const T cz0 = nz0, cz1 = nz1, cx0 = nx0, cx1 = nx1, cy0 = ny0, cy1 = ny1;
         if (k + 1 < k1) fetch(k + 1, ox + xstep, oy + ystep);
+        const T ikz = ikz_next;
+        if (k + 1 < k1) ikz_next = ldg(ikzp + 1);
         cp_async_wait<S - 3>();  // planes up to k have landed
         __syncthreads();
         // stage (u+S-1)%S held plane k-2, last read in the previous iteration
@@ -479,9 +509,11 @@ __device__ __forceinline__ void e_pass_tile(const SimView<T>& s, int kchunk, int
           const T hxk = cur[o], hyk = cur[FH + o], hzk = cur[2 * FH + o];
           const T hx_j = cur[o - L::HW], hz_j = cur[2 * FH + o - L::HW];
           const T hy_i = cur[FH + o - 1], hz_i = cur[2 * FH + o - 1];
-          const T hxm = prv[o], hym = prv[FH + o];
+          const T hxm = carry ? chx : prv[o], hym = carry ? chy : prv[FH + o];
+          chx = hxk;
+          chy = hyk;
+          carry = true;
           const T* eown = cur + L::HALO;
-          const T ikz = ldg(ikzp);
           const bool okz = k < NZ - 1, hasz = k > 0;
           unsigned m = 0;
           T cee = cee0, ceh = ceh0;

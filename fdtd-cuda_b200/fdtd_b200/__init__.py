@@ -36,6 +36,7 @@ EXPORTS = [
     "fdtd_plan", "fdtd_rasterise", "fdtd_coefficients", "fdtd_get_probe_range",
     "fdtd_set_source", "fdtd_get_stats", "fdtd_time_kernel", "fdtd_forward_spectra",
     "fdtd_backward_spectra", "fdtd_snapshots_enable", "fdtd_snapshots_drain", "fdtd_batch_get_tuning",
+    "fdtd_reflectance",
 ]
 
 
@@ -75,6 +76,7 @@ def lib():
         "fdtd_get_time": (C.c_int, [vp, P(C.c_int)]),
         "fdtd_check": (C.c_int, [vp]),
         "fdtd_spectral_finalize": (C.c_int, [vp, dp]),
+        "fdtd_reflectance": (C.c_int, [vp, dp]),
         "fdtd_write_scatabs": (C.c_int, [vp, C.c_char_p]),
         "fdtd_get_dft": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, dp, dp, sz]),
         "fdtd_get_freqs": (C.c_int, [vp, dp, sz]),
@@ -361,6 +363,8 @@ class Sim:
 
     def dft_shape(self, box, face):
         d = self.dims
+        if self.params.periodic_xy:  # the reflection (0) and transmission (1) planes
+            return (d.num_freq, d.nx + 1, d.ny + 1)
         S = d.abs_start if box == 0 else d.sca_start
         E = d.abs_end if box == 0 else d.sca_end
         ax = face // 2
@@ -378,6 +382,13 @@ class Sim:
     def spectra(self):
         out = np.empty((self.dims.num_freq, 19))
         _check(lib().fdtd_spectral_finalize(self.h, _dp(out)))
+        return out
+
+    def reflectance(self):
+        """Periodic simulations: (NUM_freq, 7) of lambda, R, T, 1 - R - T,
+        |E_inc|, Re E_inc, Im E_inc (fdtd_reflectance)."""
+        out = np.empty((self.dims.num_freq, 7))
+        _check(lib().fdtd_reflectance(self.h, _dp(out)))
         return out
 
     def write_scatabs(self, path):

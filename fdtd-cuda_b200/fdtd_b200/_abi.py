@@ -44,6 +44,8 @@ _PARAM_FIELDS = [
     ("probe_i", C.c_int), ("probe_j", C.c_int), ("probe_k", C.c_int),
     # adjoint design region
     ("design_box", C.c_int * 6),
+    # periodic x and y
+    ("periodic_xy", C.c_int),
 ]
 
 

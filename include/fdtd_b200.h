@@ -167,6 +167,19 @@ typedef struct fdtd_params {
    * fdtd_set_design blends each cell's ADE coefficients between vacuum and
    * the metal.  It must lie inside the absorption box, off the CPML. */
   int design_box[6];
+
+  /* ---- periodic x and y (the reference's Periodic_XY path) ---- */
+  /* 1 = the lateral boundaries are periodic, as in the reference's
+   * Periodic_XY branches (main.cu:781-1912, real fields: no Bloch phase),
+   * which its main() switches off (main.cu:2398).  The grid is NX = NCELLX,
+   * NY = NCELLY (setup.cu:401-404), NZ = NCELLZ + 2 NcpmlZ + 1; NcpmlX and
+   * NcpmlY must be 0 (CPML in z only), NX a multiple of 8.  The plane wave
+   * enters through the lower z face of the TFSF box only (main.cu:698); the
+   * spectra are the reflectance and transmittance of two xy planes
+   * (Fourier_Transform, Spectral.cu:8-120, and Reflectance_XZ,
+   * main.cu:3195-3320): fdtd_reflectance.  No design region, hydrodynamic
+   * model or batch membership. */
+  int periodic_xy;
 } fdtd_params;
 
 typedef struct fdtd_sim fdtd_sim;   /* opaque */
@@ -262,11 +275,27 @@ fdtd_status fdtd_check(fdtd_sim* s);
 fdtd_status fdtd_spectral_finalize(fdtd_sim* s, double* out19);
 /* Same, written as ScatAbs.<t>.txt in the reference's format. */
 fdtd_status fdtd_write_scatabs(fdtd_sim* s, const char* path);
+/* Periodic simulations (periodic_xy): reflectance and transmittance from
+ * the DFT of Ex, Ey, Hx, Hy on two whole xy planes, the reflection plane
+ * at k = Nt_z - 5 below the TFSF face (scattered field) and the
+ * transmission plane at k = NZ - Nt_z - 5 (total field) (Spectral.cu:11-16).
+ * Per frequency and plane P = sum Re(Ey conj(Hx) - Ex conj(Hy)) dA, as
+ * Reflectance_XZ sums it (main.cu:3295-3300); R = P_refl / (A |E_s|^2)
+ * and T = -P_trans / (A |E_s|^2), A the plane's area and E_s = E_inc /
+ * dft_every the incident spectrum as the planes sample it (H is stored as
+ * Z0 H, so a plane wave carries |E|^2 per unit area; the transmitted wave
+ * runs along +z, where P < 0).
+ * out7 (NUM_freq x 7): lambda, R, T, 1 - R - T, |E_inc|, Re E_inc,
+ * Im E_inc.  FDTD_ERR_STATE for a simulation that is not periodic (and
+ * fdtd_spectral_finalize fails for one that is). */
+fdtd_status fdtd_reflectance(fdtd_sim* s, double* out7);
 /* Raw DFT phasors of one face/component in the reference's layout
  * [F][a][b] (main.cu:86 ThreeDMapD(f,II,JJ,...)), FP64 re/im.
  * box: 0 = Abs, 1 = Sca.  face: 0..5 = -X +X -Y +Y -Z +Z.
  * comp: 0..3 = the face's (E_a, E_b, H_a, H_b) in the reference's order
- * (Z faces: Ex Ey Hx Hy; Y faces: Ex Ez Hx Hz; X faces: Ey Ez Hy Hz). */
+ * (Z faces: Ex Ey Hx Hy; Y faces: Ex Ez Hx Hz; X faces: Ey Ez Hy Hz).
+ * periodic_xy: box 0, face 0 = the reflection plane, 1 = the transmission
+ * plane (Ex Ey Hx Hy over the whole xy plane). */
 fdtd_status fdtd_get_dft(fdtd_sim* s, int box, int face, int comp,
                          double* re, double* im, size_t count);
 fdtd_status fdtd_get_freqs(const fdtd_sim* s, double* freq, size_t count);

@@ -39,6 +39,8 @@ struct orc_sim {
   int Nc[3], F[3];            /* Ncpml, cpml_F_* */
   int Nt[3];                  /* Ntfsf* */
   int absS[3], absE[3], scaS[3], scaE[3];
+  int per;                    /* periodic x and y (the Periodic_XY branches) */
+  int k_refl, k_trans;        /* periodic: reflection and transmission planes */
   int L, m0, i0, j0, k0;
   double d1D;
   double dt, z0, ep0, mu0, c0, pi, e0, me;
@@ -167,8 +169,9 @@ static void setup_cpml_axis(orc_sim* s, int ax, double d) {
   for (int i = 0; i < Ntot; i++) s->ked[ax][i] = s->khd[ax][i] = d;
   c->be_N = zalloc(Nc + 1); c->ce_N = zalloc(Nc + 1);
   c->be_F = zalloc(Nc + 1); c->ce_F = zalloc(Nc + 1);
-  c->bh_N = zalloc(Nc); c->ch_N = zalloc(Nc);
-  c->bh_F = zalloc(Nc); c->ch_F = zalloc(Nc);
+  int nh = Nc > 0 ? Nc : 0; /* Nc = -1: a periodic axis, no slab */
+  c->bh_N = zalloc(nh); c->ch_N = zalloc(nh);
+  c->bh_F = zalloc(nh); c->ch_F = zalloc(nh);
   if (Nc <= 0) return;
   double dt = s->dt;
 #define GRADE(xs, xa, bout, cout, kscale)                                   \
@@ -220,7 +223,8 @@ static void rasterise(orc_sim* s) {
       }
   if (p->geometry == FDTD_GEOM_REFERENCE && (p->nano_sphere == 1 || p->nano_sphere == 3)) {
     int r = (int)(p->nano_sphere_radius / p->dx);
-    double cz = NZ / 2, cx = NX / 2, cy = NY / 2;
+    /* periodic x and y: the particle sits on the slab (setup.cu:223, 268) */
+    double cz = s->per ? (double)(slab - r) : (double)(NZ / 2), cx = NX / 2, cy = NY / 2;
     for (int i = 0; i < NX; i++)
       for (int j = 0; j < NY; j++)
         for (int k = 0; k < NZ; k++) {
@@ -432,8 +436,18 @@ orc_sim* orc_create(const fdtd_params* pin, char* err) {
     s->dt = 0.5 * p->dy / K_C0 / (double)p->TimeFactor;
   s->z0 = K_Z0; s->ep0 = K_EP0; s->mu0 = K_MU0; s->c0 = K_C0; s->pi = K_PI;
   s->me = K_ME; s->e0 = K_E0;
-  s->NX = p->NCELLX + 2 * p->NcpmlX + 1;
-  s->NY = p->NCELLY + 2 * p->NcpmlY + 1;
+  s->per = p->periodic_xy != 0;
+  if (s->per) {
+    /* Periodic_XY (setup.cu:401-404, 429): no x or y CPML, no lateral
+     * TFSF faces; the plane wave enters at normal incidence */
+    if (p->NcpmlX != 0 || p->NcpmlY != 0) FAIL("periodic_xy needs NcpmlX = NcpmlY = 0");
+    if (p->NCELLX % 8 != 0 || p->NCELLX < 8 || p->NCELLY < 2) FAIL("periodic_xy grid");
+    if (p->NONLOCAL == 3) FAIL("periodic_xy does not support the hydrodynamic model");
+    if (fabs(p->inc_theta_deg) > 1e-12) FAIL("periodic_xy needs normal incidence");
+  }
+  /* periodic: the reference drops the grid's extra cell (setup.cu:401-404) */
+  s->NX = p->NCELLX + 2 * p->NcpmlX + (s->per ? 0 : 1);
+  s->NY = p->NCELLY + 2 * p->NcpmlY + (s->per ? 0 : 1);
   s->NZ = p->NCELLZ + 2 * p->NcpmlZ + 1;
   s->Nc[0] = p->NcpmlX; s->Nc[1] = p->NcpmlY; s->Nc[2] = p->NcpmlZ;
   s->F[0] = s->NX - 1 - p->NcpmlX;
@@ -441,6 +455,16 @@ orc_sim* orc_create(const fdtd_params* pin, char* err) {
   s->F[2] = s->NZ - 1 - p->NcpmlZ;
   int N3[3] = {s->NX, s->NY, s->NZ};
   for (int a = 0; a < 3; a++) {
+    if (s->per && a < 2) {
+      /* every index of a periodic axis is updated and no slab test holds
+       * (index <= Nc or >= F); the DFT planes span it */
+      s->Nc[a] = -1;
+      s->F[a] = N3[a] + 1;
+      s->Nt[a] = 0;
+      s->absS[a] = s->scaS[a] = 0;
+      s->absE[a] = s->scaE[a] = N3[a];
+      continue;
+    }
     s->Nt[a] = p->tfsf_inset + s->Nc[a];
     s->absS[a] = s->Nt[a] + p->box_offset;
     s->absE[a] = N3[a] - s->Nt[a] - p->box_offset;
@@ -448,6 +472,13 @@ orc_sim* orc_create(const fdtd_params* pin, char* err) {
     s->scaE[a] = N3[a] - s->Nt[a] + p->box_offset;
     if (s->scaS[a] < 1 || s->scaE[a] > N3[a] - 1 || s->absE[a] - s->absS[a] < 2)
       FAIL("TFSF/DFT boxes do not fit the grid");
+  }
+  if (s->per) {
+    /* Fourier_Transform (Spectral.cu:11-16) */
+    s->k_refl = s->Nt[2] - 5;
+    s->k_trans = s->NZ - s->Nt[2] - 5;
+    if (s->k_refl < s->Nc[2] + 1 || s->k_trans <= s->Nt[2] || s->k_trans >= s->F[2])
+      FAIL("periodic_xy: the reflection and transmission planes do not fit");
   }
   s->n = (size_t)s->NX * s->NY * s->NZ;
   s->hydro = p->NONLOCAL == 3;
@@ -544,8 +575,9 @@ orc_sim* orc_create(const fdtd_params* pin, char* err) {
   for (int c = 0; c < 3; c++)
     for (int q = 0; q < 2; q++) {
       int ax = (c + 1 + q) % 3; /* ex: y,z  ey: z,x  ez: x,y */
+      int w = s->Nc[ax] > 0 ? s->Nc[ax] : 0;
       size_t ne = s->n / N3[ax] * (s->Nc[ax] + 1);
-      size_t nh = s->n / N3[ax] * (s->Nc[ax]);
+      size_t nh = s->n / N3[ax] * w;
       s->psiE_N[c][q] = zalloc(ne); s->psiE_F[c][q] = zalloc(ne);
       s->psiH_N[c][q] = zalloc(nh); s->psiH_F[c][q] = zalloc(nh);
     }
@@ -558,8 +590,14 @@ orc_sim* orc_create(const fdtd_params* pin, char* err) {
       s->Einc[m] += pulse * (cos(th_) + I * sin(th_));
     }
   }
-  /* DFT boxes (ScattAbs main.cu:35-366): face extents */
-  for (int b = 0; b < 2; b++) {
+  /* DFT boxes (ScattAbs main.cu:35-366): face extents; periodic: box 0
+   * faces 0 and 1 are the reflection and transmission planes */
+  for (int b = 0; b < 2 && s->per; b++)
+    for (int f = 0; f < 6; f++) {
+      s->dft_a[b][f] = b == 0 && f < 2 ? s->NX + 1 : 0;
+      s->dft_b[b][f] = b == 0 && f < 2 ? s->NY + 1 : 0;
+    }
+  for (int b = 0; b < 2 && !s->per; b++) {
     const int* S = b == 0 ? s->absS : s->scaS;
     const int* E = b == 0 ? s->absE : s->scaE;
     for (int f = 0; f < 6; f++) {
@@ -762,6 +800,57 @@ static void update_h(orc_sim* s) {
       }
 }
 
+/* UPDATE_hx/hy/hz, Periodic_XY branches (main.cu:781-820, 877-920,
+ * 962-1000): every x and y index is updated, the +x and +y neighbours of
+ * the last column and row are the first (real fields: no Bloch phase).
+ * hx and hy are updated for k < NZ-1 and hz for every k, as in the
+ * non-periodic branch (the reference's periodic hx and hy run to k = NZ-1
+ * and read E at k = NZ there, outside the array); the z CPML applies over
+ * the whole plane. */
+static void update_h_periodic(orc_sim* s) {
+  int NX = s->NX, NY = s->NY, NZ = s->NZ;
+  double **E = s->E, **H = s->H;
+  const cpml_axis* z = &s->cp[2];
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < NX; i++)
+    for (int j = 0; j < NY; j++) {
+      int ip = i + 1 == NX ? 0 : i + 1, jp = j + 1 == NY ? 0 : j + 1;
+      for (int k = 0; k < NZ; k++) {
+        size_t id = IDX(s, i, j, k);
+        if (k < NZ - 1) {
+          double dey = E[1][IDX(s, i, j, k + 1)] - E[1][id];
+          double dez = E[2][IDX(s, i, jp, k)] - E[2][id];
+          H[0][id] = s->Chh * H[0][id] + s->Che * (dey / s->khd[2][k] - dez / s->khd[1][j]);
+          double dez_x = E[2][IDX(s, ip, j, k)] - E[2][id];
+          double dex = E[0][IDX(s, i, j, k + 1)] - E[0][id];
+          H[1][id] = s->Chh * H[1][id] + s->Che * (dez_x / s->khd[0][i] - dex / s->khd[2][k]);
+          double* p0 = NULL;
+          double* p1 = NULL;
+          double b = 0, c = 0;
+          if (k < s->Nc[2]) {
+            p0 = &s->psiH_N[0][1][pidx(s, 2, s->Nc[2], i, j, k)];
+            p1 = &s->psiH_N[1][0][pidx(s, 2, s->Nc[2], i, j, k)];
+            b = z->bh_N[k]; c = z->ch_N[k];
+          } else if (k >= s->F[2]) {
+            int k2 = k - s->F[2];
+            p0 = &s->psiH_F[0][1][pidx(s, 2, s->Nc[2], i, j, k2)];
+            p1 = &s->psiH_F[1][0][pidx(s, 2, s->Nc[2], i, j, k2)];
+            b = z->bh_F[k2]; c = z->ch_F[k2];
+          }
+          if (p0) {
+            *p0 = b * *p0 + c * dey / s->p.dz;
+            H[0][id] += s->Che * *p0;
+            *p1 = b * *p1 + c * dex / s->p.dz;
+            H[1][id] -= s->Che * *p1;
+          }
+        }
+        double dex_y = E[0][IDX(s, i, jp, k)] - E[0][id];
+        double dey_x = E[1][IDX(s, ip, j, k)] - E[1][id];
+        H[2][id] = s->Chh * H[2][id] + s->Che * (dex_y / s->khd[1][j] - dey_x / s->khd[0][i]);
+      }
+    }
+}
+
 /* Projection of a staggered point onto the incidence direction, in cells,
  * with the reference's mixed precision: a term whose offset is a whole
  * number of cells is int * float * float (single precision), a half-cell
@@ -818,6 +907,26 @@ static void tfsf(orc_sim* s) {
   double Che = s->Che, Ceh = s->Ceh;
   double dx = s->p.dx, dy = s->p.dy, dz = s->p.dz;
   const float* fe = s->fe; const float* fh = s->fh;
+  if (s->per) {
+    /* Periodic_XY: the lower z face of CORRECT_Z only (main.cu:698), over
+     * the whole plane.  The reference also launches CORRECT_X and _Y, whose
+     * faces then sit at i = 0 and j = 0 and write H at index -1, outside
+     * its arrays; with x and y periodic the lateral faces of a box that
+     * spans the period add nothing, and they are left out. */
+    int k = Tz;
+    for (int i = 0; i < NX; i++)
+      for (int j = 0; j < NY; j++) {
+        double eyi = einc_at(s, proj(s, 2 * (i - i0), 2 * (j - j0) + 1, 2 * (k - k0))) * fe[1];
+        H[0][IDX(s, i, j, k - 1)] -= Che * eyi / dz;
+        double exi = einc_at(s, proj(s, 2 * (i - i0) + 1, 2 * (j - j0), 2 * (k - k0))) * fe[0];
+        H[1][IDX(s, i, j, k - 1)] += Che * exi / dz;
+        double hxi = hinc_at(s, proj(s, 2 * (i - i0), 2 * (j - j0) + 1, 2 * (k - k0) - 1)) * fh[0];
+        E[1][IDX(s, i, j, k)] -= Ceh * hxi / dz;
+        double hyi = hinc_at(s, proj(s, 2 * (i - i0) + 1, 2 * (j - j0), 2 * (k - k0) - 1)) * fh[1];
+        E[0][IDX(s, i, j, k)] += Ceh * hyi / dz;
+      }
+    return;
+  }
   /* CORRECT_X */
   for (int j = Ty; j <= NY - Ty; j++)
     for (int k = Tz; k <= NZ - Tz; k++)
@@ -960,14 +1069,17 @@ static void hydro_p(orc_sim* s) {
 static inline double curl_h(const orc_sim* s, int c, int i, int j, int k) {
   double *const *H = s->H;
   size_t id = IDX(s, i, j, k);
+  /* the -x and -y neighbours; periodic x and y wrap (main.cu:1074-1081) */
+  int im = s->per && i == 0 ? s->NX - 1 : i - 1;
+  int jm = s->per && j == 0 ? s->NY - 1 : j - 1;
   if (c == 0)
-    return (H[2][id] - H[2][IDX(s, i, j - 1, k)]) / s->ked[1][j] -
+    return (H[2][id] - H[2][IDX(s, i, jm, k)]) / s->ked[1][j] -
            (H[1][id] - H[1][IDX(s, i, j, k - 1)]) / s->ked[2][k];
   if (c == 1)
     return (H[0][id] - H[0][IDX(s, i, j, k - 1)]) / s->ked[2][k] -
-           (H[2][id] - H[2][IDX(s, i - 1, j, k)]) / s->ked[0][i];
-  return (H[1][id] - H[1][IDX(s, i - 1, j, k)]) / s->ked[0][i] -
-         (H[0][id] - H[0][IDX(s, i, j - 1, k)]) / s->ked[1][j];
+           (H[2][id] - H[2][IDX(s, im, j, k)]) / s->ked[0][i];
+  return (H[1][id] - H[1][IDX(s, im, j, k)]) / s->ked[0][i] -
+         (H[0][id] - H[0][IDX(s, i, jm, k)]) / s->ked[1][j];
 }
 
 /* Hydrodynamic continuity for the density perturbation of component c
@@ -1017,22 +1129,26 @@ static double hydro_nd(const orc_sim* s, int c, int i, int j, int k) {
                    ((V1[0] - V2[0]) + (V1[1] - V2[1]) + 0.5 * (V1[2] - V2[2])) * NEQ);
 }
 
-/* UPDATE_ex / UPDATE_ey / UPDATE_ez (main.cu:1048-1912), non-periodic,
- * run one component after the other as the reference launches them.
+/* UPDATE_ex / UPDATE_ey / UPDATE_ez (main.cu:1048-1912), run one component
+ * after the other as the reference launches them.  Periodic x and y
+ * (main.cu:1067-1090, 1359-1380, 1663-1690): every x and y index, the -1
+ * neighbours wrap (curl_h), the z CPML only.
  * Within one component the hydrodynamic neighbour reads see the state from
  * before that component's launch (the reference races there; this is the
  * outcome when reads precede the neighbours' rotations). */
 static void update_e_comp(orc_sim* s, int c) {
   int NX = s->NX, NY = s->NY, NZ = s->NZ;
   int lo[3] = {c == 0 ? 0 : 1, c == 1 ? 0 : 1, c == 2 ? 0 : 1};
+  int hi[2] = {NX - 1, NY - 1};
+  if (s->per) { lo[0] = lo[1] = 0; hi[0] = NX; hi[1] = NY; }
   double* E = s->E[c];
   int ax1 = (c + 1) % 3, ax2 = (c + 2) % 3; /* ex: y z; ey: z x; ez: x y */
   double dsp[3] = {s->p.dx, s->p.dy, s->p.dz};
   double* dnd = NULL;
   if (s->hydro) dnd = zalloc(s->n);
 #pragma omp parallel for schedule(static)
-  for (int i = lo[0]; i < NX - 1; i++)
-    for (int j = lo[1]; j < NY - 1; j++)
+  for (int i = lo[0]; i < hi[0]; i++)
+    for (int j = lo[1]; j < hi[1]; j++)
       for (int k = lo[2]; k < NZ - 1; k++) {
         size_t id = IDX(s, i, j, k);
         double curl = curl_h(s, c, i, j, k);
@@ -1111,6 +1227,7 @@ static void update_e_comp(orc_sim* s, int c) {
         else { order[0] = 1; order[1] = 0; }
         for (int q = 0; q < 2; q++) {
           int ax = order[q];
+          if (s->per && ax < 2) continue;  /* no x or y CPML */
           int slot = ax == ax1 ? 0 : 1;
           int idx_ax = ax == 0 ? i : ax == 1 ? j : k;
           int Nc = s->Nc[ax];
@@ -1176,7 +1293,25 @@ static void dft_accumulate(orc_sim* s) {
     double ph_e = (double)(float)2.0 * s->pi * (t + 1.0) * s->dt * s->freq[m];
     double ph_h = (double)(float)2.0 * s->pi * (t + 0.5) * s->dt * s->freq[m];
     double cre = cos(ph_e), cim = sin(ph_e), hre = cos(ph_h), him = sin(ph_h);
-    for (int b = 0; b < 2; b++) {
+    /* periodic x and y: Ex, Ey, Hx, Hy on the reflection and transmission
+     * planes (Fourier_Transform, Spectral.cu:32-120, which is not called
+     * in the reference; sampled here with the phases of the box DFT) */
+    for (int f = 0; f < 2 && s->per; f++) {
+      int k = f == 0 ? s->k_refl : s->k_trans;
+      int A = s->dft_a[0][f], B = s->dft_b[0][f];
+      for (int i = 0; i < s->NX; i++)
+        for (int j = 0; j < s->NY; j++) {
+          size_t id = IDX(s, i, j, k);
+          size_t o = ((size_t)m * A + i) * B + j;
+          for (int c = 0; c < 4; c++) {
+            int comp = fcomp[2][c];
+            double x = comp < 3 ? s->E[comp][id] : s->H[comp - 3][id];
+            s->dft[0][f][c][0][o] += x * (comp < 3 ? cre : hre);
+            s->dft[0][f][c][1][o] += x * (comp < 3 ? cim : him);
+          }
+        }
+    }
+    for (int b = 0; b < 2 && !s->per; b++) {
       const int* S = b == 0 ? s->absS : s->scaS;
       const int* En = b == 0 ? s->absE : s->scaE;
       for (int f = 0; f < 6; f++) {
@@ -1213,7 +1348,7 @@ static void dft_accumulate(orc_sim* s) {
 
 void orc_step(orc_sim* s) {
   if (g_threads > 0) omp_set_num_threads(g_threads);
-  update_h(s);
+  if (s->per) update_h_periodic(s); else update_h(s);
   line_h(s);
   tfsf(s);
   line_e(s);
@@ -1237,6 +1372,7 @@ void orc_run(orc_sim* s, int nsteps) {
 int orc_spectra(orc_sim* s, double* out) {
   static const int fcomp[3][4] = {{1, 2, 4, 5}, {0, 2, 3, 5}, {0, 1, 3, 4}};
   (void)fcomp;
+  if (s->per) return -1;  /* no DFT box: orc_reflectance */
   for (int b = 0; b < 2; b++)
     for (int f = 0; f < 6; f++)
       if (!s->dft[b][f][0][0]) return -1;
@@ -1295,6 +1431,42 @@ int orc_spectra(orc_sim* s, double* out) {
 
 /* ------------------------------------------------------------------ */
 /* accessors                                                           */
+
+/* Reflectance_XZ (main.cu:3195-3320) on the two planes: per frequency
+ * P = sum Re(Ey conj(Hx) - Ex conj(Hy)) dA; R = P_refl / (A |E_s|^2),
+ * T = -P_trans / (A |E_s|^2) with A the plane's area and E_s = E_inc /
+ * dft_every, the incident spectrum as the planes see it (they are sampled
+ * every dft_every steps, E_inc sums every step).  P is reset for every
+ * frequency (the reference's P_t is not).  out: lambda, R, T, 1 - R - T,
+ * |E_inc|, Re E_inc, Im E_inc. */
+int orc_reflectance(orc_sim* s, double* out) {
+  if (!s->per || !s->dft[0][0][0][0]) return -1;
+  double dA = s->p.dx * s->p.dy, area = 0.0;
+  for (int i = 0; i < s->NX; i++)
+    for (int j = 0; j < s->NY; j++) area += dA;
+  for (int m = 0; m < s->NF; m++) {
+    double P[2] = {0.0, 0.0};
+    for (int f = 0; f < 2; f++) {
+      int A = s->dft_a[0][f], B = s->dft_b[0][f];
+      for (int i = 0; i < s->NX; i++)
+        for (int j = 0; j < s->NY; j++) {
+          size_t o = ((size_t)m * A + i) * B + j;
+          double complex cEx = s->dft[0][f][0][0][o] + I * s->dft[0][f][0][1][o];
+          double complex cEy = s->dft[0][f][1][0][o] + I * s->dft[0][f][1][1][o];
+          double complex ccHx = s->dft[0][f][2][0][o] - I * s->dft[0][f][2][1][o];
+          double complex ccHy = s->dft[0][f][3][0][o] - I * s->dft[0][f][3][1][o];
+          P[f] += creal(cEy * ccHx - cEx * ccHy) * dA;
+        }
+    }
+    double amp = cabs(s->Einc[m]), as = amp / s->p.dft_every;
+    double R = P[0] / area / (as * as), T = -P[1] / area / (as * as);
+    double* row = out + 7 * (size_t)m;
+    row[0] = s->c0 / s->freq[m];
+    row[1] = R; row[2] = T; row[3] = 1.0 - R - T;
+    row[4] = amp; row[5] = creal(s->Einc[m]); row[6] = cimag(s->Einc[m]);
+  }
+  return 0;
+}
 
 void orc_dims(const orc_sim* s, fdtd_dims* d) {
   memset(d, 0, sizeof(*d));
@@ -1391,6 +1563,7 @@ int orc_get_cpml(const orc_sim* s, int which, double* out, size_t n) {
   const cpml_axis* c = &s->cp[ax];
   const double* tabs[8] = {c->be_N, c->ce_N, c->be_F, c->ce_F, c->bh_N, c->ch_N, c->bh_F, c->ch_F};
   int len = slot < 4 ? s->Nc[ax] + 1 : s->Nc[ax];
+  if (len < 0) len = 0;
   if (n < (size_t)len) return -1;
   memcpy(out, tabs[slot], len * sizeof(double));
   return len;

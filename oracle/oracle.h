@@ -62,6 +62,9 @@ int orc_get_material(const orc_sim* s, unsigned char* bits, int* matX,
 int orc_get_dft(const orc_sim* s, int box, int face, int comp, double* re,
                 double* im, size_t n);
 int orc_spectra(orc_sim* s, double* out19);
+/* periodic_xy: lambda, R, T, 1 - R - T, |E_inc|, Re E_inc, Im E_inc per
+ * frequency (NUM_freq x 7); -1 for a simulation that is not periodic. */
+int orc_reflectance(orc_sim* s, double* out7);
 int orc_get_freqs(const orc_sim* s, double* f, size_t n);
 int orc_get_incident(const orc_sim* s, double* re, double* im, size_t n);
 int orc_get_line(const orc_sim* s, double* e_inc, double* h_inc, size_t n);

@@ -51,6 +51,7 @@ def lib():
                                        P(C.c_int), C.c_size_t]
         L.orc_get_dft.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, dp, dp, C.c_size_t]
         L.orc_spectra.argtypes = [C.c_void_p, dp]
+        L.orc_reflectance.argtypes = [C.c_void_p, dp]
         L.orc_get_freqs.argtypes = [C.c_void_p, dp, C.c_size_t]
         L.orc_get_incident.argtypes = [C.c_void_p, dp, dp, C.c_size_t]
         L.orc_get_line.argtypes = [C.c_void_p, dp, dp, C.c_size_t]
@@ -135,6 +136,8 @@ class OracleSim:
 
     def dft_shape(self, box, face):
         d = self.dims
+        if self.params.periodic_xy:  # the reflection (0) and transmission (1) planes
+            return (d.num_freq, d.nx + 1, d.ny + 1)
         S = d.abs_start if box == 0 else d.sca_start
         E = d.abs_end if box == 0 else d.sca_end
         ax = face // 2
@@ -160,6 +163,14 @@ class OracleSim:
         out = np.empty((self.dims.num_freq, 19), np.float64)
         if lib().orc_spectra(self.h, _dp(out)) != 0:
             raise RuntimeError("no DFT data")
+        return out
+
+    def reflectance(self):
+        """periodic_xy: (NUM_freq, 7) of lambda, R, T, 1 - R - T, |E_inc|,
+        Re E_inc, Im E_inc."""
+        out = np.empty((self.dims.num_freq, 7), np.float64)
+        if lib().orc_reflectance(self.h, _dp(out)) != 0:
+            raise RuntimeError("not a periodic simulation")
         return out
 
     def freqs(self):

@@ -41,3 +41,36 @@ def make(mod, name, **over):
     kw = dict(CASES[name])
     kw.update(over)
     return mod.default_params(**kw)
+
+# Periodic x and y (periodic_xy): an 8 x 8 x 77 column with CPML in z only.
+# "periodic_film" holds a 20 nm gold film (the reference's finite slab,
+# inf_disp_slab = 2, thickness nano_sphere_radius); "periodic_spheres"
+# puts a gold sphere on a 10 nm film in a 16 x 16 cell.
+PERIODIC = dict(SMALL, nano_sphere=0, NCELLX=8, NCELLY=8, NCELLZ=60, NcpmlX=0, NcpmlY=0,
+                NcpmlZ=8, tfsf_inset=8, periodic_xy=1, Tend=3000)
+CASES.update({
+    "periodic_vacuum": dict(PERIODIC),
+    "periodic_film": dict(PERIODIC, inf_disp_slab=2, dispersive_slab=40, nano_sphere_radius=20e-9),
+    "periodic_spheres": dict(PERIODIC, NCELLX=16, NCELLY=16, nano_sphere=1, inf_disp_slab=2,
+                             dispersive_slab=40, nano_sphere_radius=10e-9, inc_phi_deg=30.0),
+})
+
+
+def gold_film_rt(lam, d):
+    """R and T of a free-standing film of thickness d (m) at normal
+    incidence from the Drude + two-critical-point gold permittivity the
+    reference uses (setup.cu:1164-1211), by the Airy sums."""
+    import numpy as np
+    c0 = 2.99792458e8
+    w = 2 * np.pi * c0 / np.asarray(lam)
+    eps = 1.1431 - 1.3202e16 ** 2 / (w ** 2 + 1j * 1.0805e14 * w)
+    for a, ph, om, ga in ((0.26698, -1.2371, 3.8711e15, 4.4642e14),
+                          (3.0834, -1.0968, 4.1684e15, 2.3555e15)):
+        eps = eps + a * om * (np.exp(1j * ph) / (om - w - 1j * ga) + np.exp(-1j * ph) / (om + w + 1j * ga))
+    n = np.sqrt(eps)
+    r12, r23 = (1 - n) / (1 + n), (n - 1) / (n + 1)
+    e = np.exp(1j * n * w / c0 * d)
+    den = 1 + r12 * r23 * e ** 2
+    r = (r12 + r23 * e ** 2) / den
+    t = (2 / (1 + n)) * (2 * n / (n + 1)) * e / den
+    return np.abs(r) ** 2, np.abs(t) ** 2

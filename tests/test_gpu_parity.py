@@ -282,7 +282,7 @@ def test_spectral_error_table():
     scattering, absorption and extinction columns.  Written as a table to
     the path in FDTD_PARITY_REPORT when set."""
     rows = []
-    for name in sorted(CASES):
+    for name in sorted(n for n in CASES if not CASES[n].get("periodic_xy")):  # periodic: no ScatAbs
         errs = {}
         for prec, tag in ((F.FDTD_FP64, "f64"), (F.FDTD_FP32, "f32")):
             s, o = spectra_pair(name, prec)
