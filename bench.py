@@ -342,8 +342,7 @@ def large_params(mod, precision=None):
 def large_bench(mod, torch, stream, sp, dev, blocks=2, adjoint_steps=12000):
     """Forward throughput of the large nonlocal workload over a bounded
     number of 128-step blocks (the full run is 12000 steps), and the device
-    memory the simulation holds.  Its adjoint is not built: the
-    hydrodynamic model is nonlinear."""
+    memory the simulation holds (its adjoint: large_adjoint_bench)."""
     free0, _ = torch.cuda.mem_get_info(dev)
     s = mod.Sim(large_params(mod), device=dev)
     free1, _ = torch.cuda.mem_get_info(dev)
@@ -401,6 +400,7 @@ def large_adjoint_bench(mod, torch, dev, steps=12000, every=400):
     g, gp = s.backward()
     t2 = time.perf_counter()
     s.check()
+    st = s.stats()
     d = s.dims
     cs = d.nx * d.ny * d.nz * steps
     out = {"grid": [d.nx, d.ny, d.nz], "design": [64, 64, 10], "time_steps": steps,
@@ -409,8 +409,14 @@ def large_adjoint_bench(mod, torch, dev, steps=12000, every=400):
            "ratio": round((t2 - t1) / (t1 - t0), 3),
            "forward_gcell_steps_per_s": round(cs / (t1 - t0) / 1e9, 2),
            "backward_gcell_steps_per_s": round(cs / (t2 - t1) / 1e9, 2),
-           "sim_bytes": int(free0 - free1), "checkpoint_bytes": int(free1 - free2),
+           "sim_bytes": int(free0 - free1),
+           "forward_state_bytes": int(free1 - free2),
            "adjoint_state_bytes": int(free2 - free3),
+           "recorded_steps": int(st.adj_record_steps), "record_bytes": int(st.adj_record_bytes),
+           "checkpoints": int(st.adj_checkpoints),
+           "memory_note": "forward_state_bytes: the adjoint state, the trajectory record of the recorded "
+                          "steps and the checkpoints of the others, all allocated by the forward; the "
+                          "backward recomputes only the steps that were not recorded",
            "objective": L, "grad_rho_max": float(np.abs(g).max()),
            "timing": "host wall clock around each blocking C-ABI call, after a warm-up pair"}
     s.close()
@@ -442,6 +448,7 @@ def adjoint_bench(mod, torch, stream, dev, steps=4000, every=200):
         fw.append(t1 - t0)
         bw.append(t2 - t1)
     s.check()
+    st = s.stats()
     s.close()
     f_s, b_s = statistics.median(fw), statistics.median(bw)
     # a finite-difference check of one design cell: central differences
@@ -467,6 +474,8 @@ def adjoint_bench(mod, torch, stream, dev, steps=4000, every=200):
                         "rel": abs(float(g[cell]) - fd) / abs(fd)},
            "forward_gcell_steps_per_s": round(cells / f_s / 1e9, 2),
            "time_steps": steps, "checkpoint_every": every, "grid": 96, "design": [32, 32, 16],
+           "recorded_steps": int(st.adj_record_steps), "record_bytes": int(st.adj_record_bytes),
+           "checkpoints": int(st.adj_checkpoints),
            "timing": "host wall clock around each blocking C-ABI call, median of 3"}
     return out
 

@@ -3,15 +3,18 @@
 // segment recompute.  Included at the end of fdtd.cu (it uses the
 // simulation internals defined there).
 //
-// fdtd_forward runs the whole time loop from zero fields, copying the state
-// (fields, psi, dispersive-cell states, incident line, clock) aside at the
-// start of every checkpoint_every steps.  fdtd_backward walks the segments
-// from the last: it restores a segment's checkpoint, recomputes its steps
-// with DFT sampling off while the dispersive-cell kernel records, per step,
-// the local values the gradient needs, then runs the transposed steps of
-// that segment in reverse.  The transposed Yee and CPML operators need no
-// forward values (the step is linear with fixed coefficients), so only the
-// dispersive cells are recorded.
+// The transposed Yee and CPML operators need no forward values (the step is
+// linear with fixed coefficients), so the reverse sweep needs, per step, only
+// the dispersive cells' local values (their trajectory record).
+// fdtd_forward runs the whole time loop from zero fields in segments of
+// checkpoint_every steps.  The last segments, as many as the record budget
+// holds (all of them when it fits), record their trajectory as they run;
+// every earlier segment starts with a copy of the state (fields, psi,
+// dispersive-cell states, incident line, clock) set aside.  fdtd_backward
+// walks the segments from the last: a recorded segment goes straight into
+// its transposed steps; an earlier one first restores its checkpoint and
+// recomputes its steps with DFT sampling off while the dispersive-cell
+// kernels record, into the rows the later segments no longer need.
 
 struct fdtd_sim::Adjoint {
   std::vector<std::unique_ptr<DevBuf>> bufs;
@@ -20,6 +23,15 @@ struct fdtd_sim::Adjoint {
   size_t ck_bytes = 0;
   std::unique_ptr<DevBuf> ck;  // nseg * ck_bytes
   int every = 0, nseg = 0, tend = 0;
+  // trajectory record: rows = nrec * every, the last nrec segments recorded
+  // by the forward (their first step rec_base), the others recomputed
+  int nrec = 0, rows = 0, rec_base = 0;
+  size_t rec_bytes = 0;
+  // graph of one DFT period of the recording forward (the main step graph
+  // does not record), with the generation of the main graph it matches
+  cudaGraphExec_t g_fwd = nullptr;
+  long long g_fwd_kernels = 0;
+  int g_fwd_len = 0, g_fwd_epoch = -1;
   // objective: weights on the ScatAbs table (fdtd_forward's own, for
   // fdtd_backward), the frequencies with a nonzero weight and the faces the
   // objective reads (bit b*6+f)
@@ -43,16 +55,17 @@ struct fdtd_sim::Adjoint {
   std::vector<char> view_bytes;
   std::vector<std::pair<void*, size_t>> zero;  // buffers zeroed before each sweep
   void* rec = nullptr;
-  double* hrec = nullptr;  // hydrodynamic cells' record (MetalView::hrec)
+  void* hrec = nullptr;  // hydrodynamic cells' record (MetalView::hrec)
   long long rec_slots = 0;
   int rec_off[3] = {0, 0, 0};
   double* grho[3] = {nullptr, nullptr, nullptr};
   double* gpar = nullptr;
   int* step = nullptr;
-  // staged-gather tiles (adj_gather_*_staged) and the blocks the fused
-  // gathers take, per gather (0 = H, 1 = E)
-  std::unique_ptr<DevBuf> gtab[2][2];
-  int ntile[2] = {0, 0}, nleft[2] = {0, 0};
+  // gather tables per gather (0 = H, 1 = E): the staged tiles of the plain
+  // form, the staged tiles of the slab form, and the one-plane blocks of
+  // the tiles over the material box, which the fused gathers take
+  std::unique_ptr<DevBuf> gtab[2][3];
+  int ngt[2][3] = {{0, 0, 0}, {0, 0, 0}};
   bool tabs = false;
   // graphs of one full segment: the recompute (DFT off, recording on) and
   // the reverse sweep; replayed for every full segment
@@ -62,7 +75,8 @@ struct fdtd_sim::Adjoint {
   void drop_graphs() {
     if (g_rec) cudaGraphExecDestroy(g_rec);
     if (g_adj) cudaGraphExecDestroy(g_adj);
-    g_rec = g_adj = nullptr;
+    if (g_fwd) cudaGraphExecDestroy(g_fwd);
+    g_rec = g_adj = g_fwd = nullptr;
   }
   ~Adjoint() {
     drop_graphs();
@@ -112,19 +126,86 @@ static fdtd_status adj_checks(fdtd_sim* s) {
   return FDTD_OK;
 }
 
-// The checkpointed forward: every field, auxiliary state and accumulator
-// zeroed, then the whole time loop t = 0..Tend with a copy of the state
-// (without the DFT accumulators, the sample ring and the probe record) at
-// the start of every segment of checkpoint_every steps.  The DFT
-// accumulators of the run stay in place for the objective.
-static fdtd_status adj_forward_run(fdtd_sim* s, int checkpoint_every) {
-  if (!s->adj) s->adj = std::make_unique<fdtd_sim::Adjoint>();
+template <typename T>
+static fdtd_status adj_prepare(fdtd_sim* s);
+
+static void adj_stats(const fdtd_sim* s, fdtd_stats* out) {
+  out->adj_record_steps = out->adj_record_bytes = out->adj_checkpoints = 0;
+  if (!s->adj || !s->adj->forward_done) return;
+  const fdtd_sim::Adjoint& A = *s->adj;
+  out->adj_record_steps = A.tend + 1 - A.rec_base;
+  out->adj_record_bytes = (long long)A.rec_bytes;
+  out->adj_checkpoints = A.nseg - A.nrec;
+}
+
+// The record rows of the forward: nrec segments, as many as the budget
+// holds (FDTD_ADJ_RECORD_GB, else 60% of the device's memory and all but 4
+// GB of what is free), at least one.  Reallocated only when the depth
+// changes; the graphs hold the record's address.
+template <typename T>
+static fdtd_status adj_record_alloc(fdtd_sim* s) {
+  fdtd_sim::Adjoint& A = *s->adj;
+  const size_t per_row = (size_t)A.rec_slots * (5 + (s->su.hydro ? 6 : 0)) * sizeof(T);
+  const size_t per_seg = per_row * (size_t)A.every;
+  size_t free_b = 0, total_b = 0;
+  CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+  const size_t avail = free_b + A.rec_bytes;  // the current record is given back
+  const size_t reserve = (size_t)4 << 30;
+  double budget = std::min(0.6 * (double)total_b, avail > reserve ? (double)(avail - reserve) : 0.0);
+  if (const char* e = std::getenv("FDTD_ADJ_RECORD_GB")) budget = std::min(budget, std::atof(e) * (double)(1ull << 30));
+  const int nrec = std::max(1, std::min(A.nseg, (int)(budget / (double)std::max<size_t>(per_seg, 1))));
+  if (nrec == A.nrec && A.rec) return FDTD_OK;
+  A.drop_graphs();
+  for (auto it = A.bufs.begin(); it != A.bufs.end();) {
+    if ((*it)->p == A.rec || (A.hrec && (*it)->p == A.hrec)) it = A.bufs.erase(it);
+    else ++it;
+  }
+  A.rec = nullptr;
+  A.hrec = nullptr;
+  A.rec_bytes = 0;
+  A.nrec = nrec;
+  A.rows = nrec * A.every;
+  T* rec;
+  CUDA_TRY(A.alloc(&rec, (size_t)A.rows * 5 * A.rec_slots, false));
+  A.rec = rec;
+  A.rec_bytes = (size_t)A.rows * 5 * A.rec_slots * sizeof(T);
+  if (s->su.hydro) {
+    T* hr;
+    CUDA_TRY(A.alloc(&hr, (size_t)A.rows * 6 * A.rec_slots, false));
+    A.hrec = hr;
+    A.rec_bytes += (size_t)A.rows * 6 * A.rec_slots * sizeof(T);
+  }
+  return FDTD_OK;
+}
+
+// Points the dispersive-cell kernels at the record (or off, rec == nullptr).
+template <typename T>
+static void adj_record_view(fdtd_sim* s, bool on) {
+  fdtd_sim::Adjoint& A = *s->adj;
+  MetalView<T>& m = mview<T>(s);
+  m.rec = on ? static_cast<T*>(A.rec) : nullptr;
+  m.hrec = on ? static_cast<T*>(A.hrec) : nullptr;
+  m.rec_rows = A.rows;
+  m.rec_base = A.rec_base;
+  m.rec_slots = A.rec_slots;
+  for (int c = 0; c < 3; c++) m.rec_off[c] = A.rec_off[c];
+}
+
+// The forward: every field, auxiliary state and accumulator zeroed, then
+// the whole time loop t = 0..Tend in segments of checkpoint_every steps,
+// with a copy of the state (without the DFT accumulators, the sample ring
+// and the probe record) at the start of every segment that is not
+// recorded.  The DFT accumulators of the run stay in place for the
+// objective.
+template <typename T>
+static fdtd_status adj_forward_run_t(fdtd_sim* s, int checkpoint_every) {
   fdtd_sim::Adjoint& A = *s->adj;
   A.forward_done = false;
   A.has_objective = false;
   if (A.every != checkpoint_every) {
     A.drop_graphs();  // they hold the segment length
     A.ready = false;  // the record depth follows the segment
+    A.nrec = 0;
   }
   fdtd_status st = fdtd_reset(s);
   if (st != FDTD_OK) return st;
@@ -141,26 +222,53 @@ static fdtd_status adj_forward_run(fdtd_sim* s, int checkpoint_every) {
   A.tend = s->su.p.Tend;
   const int total = A.tend + 1;
   A.nseg = (total + A.every - 1) / A.every;
-  const size_t need = (size_t)A.nseg * A.ck_bytes;
-  if (!A.ck || A.ck->bytes < need) {
+  if (!A.ready) {
+    st = adj_prepare<T>(s);
+    if (st != FDTD_OK) return st;
+  }
+  st = adj_record_alloc<T>(s);
+  if (st != FDTD_OK) return st;
+  const int nck = A.nseg - A.nrec;  // segments that are recomputed
+  A.rec_base = nck * A.every;
+  const size_t need = (size_t)nck * A.ck_bytes;
+  if (need > 0 && (!A.ck || A.ck->bytes < need)) {
     A.ck.reset();
     auto b = std::make_unique<DevBuf>();
     CUDA_TRY(b->alloc(need));
     A.ck = std::move(b);
   }
-  for (int seg = 0; seg < A.nseg; seg++) {
+  for (int seg = 0; seg < nck; seg++) {
     char* dst = static_cast<char*>(A.ck->p) + (size_t)seg * A.ck_bytes;
     for (const auto& b : A.ck_bufs) {
       CUDA_TRY(cudaMemcpyAsync(dst, b.first, b.second, cudaMemcpyDeviceToDevice, 0));
       dst += (b.second + 255) / 256 * 256;
     }
-    const int n = std::min(A.every, total - seg * A.every);
-    st = fdtd_step(s, n, nullptr);
+    st = fdtd_step(s, A.every, nullptr);
     if (st != FDTD_OK) return st;
   }
+  // the recorded segments, with their own step graph
+  if (A.g_fwd && A.g_fwd_epoch != s->graph_epoch) {
+    cudaGraphExecDestroy(A.g_fwd);
+    A.g_fwd = nullptr;
+  }
+  adj_record_view<T>(s, true);
+  std::swap(s->graph, A.g_fwd);
+  std::swap(s->graph_kernels, A.g_fwd_kernels);
+  std::swap(s->graph_len, A.g_fwd_len);
+  st = fdtd_step(s, total - A.rec_base, nullptr);
+  std::swap(s->graph, A.g_fwd);
+  std::swap(s->graph_kernels, A.g_fwd_kernels);
+  std::swap(s->graph_len, A.g_fwd_len);
+  A.g_fwd_epoch = s->graph_epoch;
+  adj_record_view<T>(s, false);
+  if (st != FDTD_OK) return st;
   CUDA_TRY(cudaDeviceSynchronize());
   A.forward_done = true;
   return FDTD_OK;
+}
+static fdtd_status adj_forward_run(fdtd_sim* s, int checkpoint_every) {
+  if (!s->adj) s->adj = std::make_unique<fdtd_sim::Adjoint>();
+  return s->fp64 ? adj_forward_run_t<double>(s, checkpoint_every) : adj_forward_run_t<float>(s, checkpoint_every);
 }
 
 // The objective L = sum_m sum_c G[m][c] spectra[m][c] over the ScatAbs
@@ -303,6 +411,10 @@ static fdtd_status adj_prepare(fdtd_sim* s) {
   A.drop_graphs();  // they hold the buffers released here
   A.bufs.clear();  // a re-preparation (another checkpoint interval) starts afresh
   A.zero.clear();
+  A.rec = nullptr;  // the record goes with them (adj_record_alloc makes it again)
+  A.hrec = nullptr;
+  A.rec_bytes = 0;
+  A.nrec = 0;
   AdjView<T> a;
   std::memset(&a, 0, sizeof(a));
   const size_t nc = s->ncell;
@@ -353,16 +465,7 @@ static fdtd_status adj_prepare(fdtd_sim* s) {
   CUDA_TRY(A.alloc(&a.step, 1, false));
   CUDA_TRY(A.alloc(&a.flags, s->ncell, false));
   A.step = a.step;
-  A.rec_slots = std::max(1LL, slots);
-  T* rec;
-  CUDA_TRY(A.alloc(&rec, (size_t)A.every * 5 * A.rec_slots, false));
-  A.rec = rec;
-  A.hrec = nullptr;
-  if (su.hydro) {
-    double* hr;
-    CUDA_TRY(A.alloc(&hr, (size_t)A.every * 6 * A.rec_slots, false));
-    A.hrec = hr;
-  }
+  A.rec_slots = std::max(1LL, slots);  // the record itself: adj_record_alloc
   // derivatives of the metal's coupling and dynamics coefficients with
   // respect to omega_D and gamma (ade_coefficients, non-hydrodynamic form)
   const double dt = su.dt, wD = su.wD, gam = su.gam;
@@ -395,11 +498,7 @@ static fdtd_status adj_sweep(fdtd_sim* s) {
   const AdjView<T>& a = *reinterpret_cast<const AdjView<T>*>(A.view_bytes.data());
   for (const auto& z : A.zero) CUDA_TRY(cudaMemset(z.first, 0, z.second));
   MetalView<T>& m = mview<T>(s);
-  m.rec = static_cast<T*>(A.rec);
-  m.hrec = A.hrec;
-  m.rec_rows = A.every;
-  m.rec_slots = A.rec_slots;
-  for (int c = 0; c < 3; c++) m.rec_off[c] = A.rec_off[c];
+  adj_record_view<T>(s, true);
   const int every_dft = s->line.dft_every;
   const bool graphs = s->use_graphs, snaps = s->snap_on;
   s->line.dft_every = 0;  // the recompute needs no DFT samples
@@ -432,18 +531,26 @@ static fdtd_status adj_sweep(fdtd_sim* s) {
   }
   const dim3 gtile((unsigned)((s->NX + 31) / 32), (unsigned)((s->NY + 7) / 8), (unsigned)s->NZ);
   if (fused) adj_build_flags<T><<<gtile, dim3(32, 8)>>>(view<T>(s), a.flags);
-  // staged tiles: 32 x kAdjTY x kAdjKC boxes whose cells and halo (+1 for
-  // the H gather, -1 for the E gather) are simple (adj_block_simple); the
-  // fused gathers take every other 32 x 8 block, one plane each
+  // staged tiles: 32 x kAdjTY x kAdjKC boxes.  A tile whose cells and halo
+  // (+1 for the H gather, -1 for the E gather) lie away from the material
+  // box runs staged: the plain form away from the CPML slabs and the grid's
+  // faces, the slab form otherwise; a tile over the material box goes to
+  // the fused gathers, one plane per block
+  // the z-march tiles keep a CTA on 16 planes: on a small grid too few of
+  // them would run (fewer than 4 a multiprocessor), and the fused gathers,
+  // one plane per block, win; FDTD_ADJ_STAGED=1 / 0 forces either
   const char* senv = std::getenv("FDTD_ADJ_STAGED");
-  const bool staged = fused && !(senv && senv[0] == '0');
+  int nsm = 148;
+  CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, s->device));
+  const long long ntiles =
+      (long long)((s->NX + 31) / 32) * ((s->NY + 7) / 8) * ((s->NZ + kAdjKC - 1) / kAdjKC);
+  const bool staged = fused && (senv ? senv[0] != '0' : ntiles >= 4LL * nsm);
   if (staged && !A.tabs) {
     static_assert(kAdjTY == 8, "the staged tiles and the fused gathers' blocks share the 32 x 8 xy grid");
     const int nbx = (s->NX + 31) / 32, nby = (s->NY + 7) / 8, nbz = (s->NZ + kAdjKC - 1) / kAdjKC;
     for (int g = 0; g < 2; g++) {
       const int lo_off = g == 0 ? 0 : -1, hi_off = g == 0 ? 1 : 0;
-      std::vector<int4> tiles, left;
-      std::vector<char> cover((size_t)nbx * nby * nbz, 0);
+      std::vector<int4> v[3];
       for (int bz = 0; bz < nbz; bz++)
         for (int by = 0; by < nby; by++)
           for (int bx = 0; bx < nbx; bx++) {
@@ -455,33 +562,30 @@ static fdtd_status adj_sweep(fdtd_sim* s) {
               inside = inside && lo[ax] >= s->su.Nc[ax] + 1 && hi[ax] < s->su.F[ax];
               off_mat = off_mat || hi[ax] < s->mat_lo[ax] || lo[ax] >= s->mat_hi[ax];
             }
-            if (inside && off_mat) {
-              tiles.push_back(make_int4(bx, by, bz, 0));
-              cover[((size_t)bz * nby + by) * nbx + bx] = 1;
+            if (!off_mat) {
+              for (int k = bz * kAdjKC; k < std::min(s->NZ, (bz + 1) * kAdjKC); k++) v[2].push_back(make_int4(bx, by, k, 0));
+            } else {
+              v[inside ? 0 : 1].push_back(make_int4(bx, by, bz, 0));
             }
           }
-      for (int k = 0; k < s->NZ; k++)
-        for (int by = 0; by < nby; by++)
-          for (int bx = 0; bx < nbx; bx++)
-            if (!cover[((size_t)(k / kAdjKC) * nby + by) * nbx + bx]) left.push_back(make_int4(bx, by, k, 0));
-      for (int q = 0; q < 2; q++) {
-        const std::vector<int4>& v = q == 0 ? tiles : left;
+      for (int q = 0; q < 3; q++) {
         auto b = std::make_unique<DevBuf>();
-        CUDA_TRY(b->alloc(std::max<size_t>(1, v.size()) * sizeof(int4)));
-        if (!v.empty()) CUDA_TRY(cudaMemcpy(b->p, v.data(), v.size() * sizeof(int4), cudaMemcpyHostToDevice));
+        CUDA_TRY(b->alloc(std::max<size_t>(1, v[q].size()) * sizeof(int4)));
+        if (!v[q].empty()) CUDA_TRY(cudaMemcpy(b->p, v[q].data(), v[q].size() * sizeof(int4), cudaMemcpyHostToDevice));
         A.gtab[g][q] = std::move(b);
+        A.ngt[g][q] = (int)v[q].size();
       }
-      A.ntile[g] = (int)tiles.size();
-      A.nleft[g] = (int)left.size();
     }
     const int smem = (int)(kAdjS * StageLayout<T, kAdjTY>::STAGE * sizeof(T));
-    CUDA_TRY(cudaFuncSetAttribute(adj_gather_h_staged<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    CUDA_TRY(cudaFuncSetAttribute(adj_gather_e_staged<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    CUDA_TRY(cudaFuncSetAttribute(adj_gather_h_staged<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    CUDA_TRY(cudaFuncSetAttribute(adj_gather_e_staged<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    CUDA_TRY(cudaFuncSetAttribute(adj_gather_h_staged<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    CUDA_TRY(cudaFuncSetAttribute(adj_gather_e_staged<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     A.tabs = true;
   }
   const size_t gsmem = kAdjS * StageLayout<T, kAdjTY>::STAGE * sizeof(T);
-  // one gather: the staged tiles and the fused blocks (disjoint outputs,
-  // inputs they do not write); returns the launches
+  // one gather: the staged tiles of both forms and the fused blocks
+  // (disjoint outputs, inputs they do not write); returns the launches
   auto gather = [&](int g, cudaStream_t stream) -> int {
     if (!staged) {
       if (g == 0) adj_gather_h_fused<T><<<gtile, dim3(32, 8), 0, stream>>>(view<T>(s), a, nullptr);
@@ -489,16 +593,23 @@ static fdtd_status adj_sweep(fdtd_sim* s) {
       return 1;
     }
     int k = 0;
-    const int4* tt = static_cast<const int4*>(A.gtab[g][0]->p);
-    const int4* lt = static_cast<const int4*>(A.gtab[g][1]->p);
-    if (A.ntile[g]) {
-      if (g == 0) adj_gather_h_staged<T><<<A.ntile[g], dim3(32, kAdjTY), gsmem, stream>>>(view<T>(s), a, tt);
-      else adj_gather_e_staged<T><<<A.ntile[g], dim3(32, kAdjTY), gsmem, stream>>>(view<T>(s), a, tt);
+    const int4* t[3];
+    for (int q = 0; q < 3; q++) t[q] = static_cast<const int4*>(A.gtab[g][q]->p);
+    const dim3 blk(32, kAdjTY);
+    const int* n = A.ngt[g];
+    if (n[2]) {
+      if (g == 0) adj_gather_h_fused<T><<<n[2], dim3(32, 8), 0, stream>>>(view<T>(s), a, t[2]);
+      else adj_gather_e_fused<T><<<n[2], dim3(32, 8), 0, stream>>>(view<T>(s), a, t[2]);
       k++;
     }
-    if (A.nleft[g]) {
-      if (g == 0) adj_gather_h_fused<T><<<A.nleft[g], dim3(32, 8), 0, stream>>>(view<T>(s), a, lt);
-      else adj_gather_e_fused<T><<<A.nleft[g], dim3(32, 8), 0, stream>>>(view<T>(s), a, lt);
+    if (n[1]) {
+      if (g == 0) adj_gather_h_staged<T, true><<<n[1], blk, gsmem, stream>>>(view<T>(s), a, t[1]);
+      else adj_gather_e_staged<T, true><<<n[1], blk, gsmem, stream>>>(view<T>(s), a, t[1]);
+      k++;
+    }
+    if (n[0]) {
+      if (g == 0) adj_gather_h_staged<T, false><<<n[0], blk, gsmem, stream>>>(view<T>(s), a, t[0]);
+      else adj_gather_e_staged<T, false><<<n[0], blk, gsmem, stream>>>(view<T>(s), a, t[0]);
       k++;
     }
     return k;
@@ -509,7 +620,7 @@ static fdtd_status adj_sweep(fdtd_sim* s) {
   const bool hydro = s->su.hydro;
   auto launch_design = [&](cudaStream_t stream) -> int {
     if (!hydro) {
-      adj_e_design<T><<<(ntot + 127) / 128, 128, 0, stream>>>(view<T>(s), m, a, static_cast<const T*>(A.rec), A.every);
+      adj_e_design<T><<<(ntot + 127) / 128, 128, 0, stream>>>(view<T>(s), m, a, static_cast<const T*>(A.rec), A.rows);
       return 1;
     }
     int k = 0;
@@ -548,15 +659,22 @@ static fdtd_status adj_sweep(fdtd_sim* s) {
   for (int seg = A.nseg - 1; seg >= 0 && st == FDTD_OK; seg--) {
     const int n0 = seg * A.every, n1 = std::min(total, n0 + A.every);
     const bool full = n1 - n0 == A.every;
-    const char* src = static_cast<const char*>(A.ck->p) + (size_t)seg * A.ck_bytes;
-    for (const auto& b : A.ck_bufs) {
-      CUDA_TRY(cudaMemcpyAsync(b.first, src, b.second, cudaMemcpyDeviceToDevice, 0));
-      src += (b.second + 255) / 256 * 256;
+    // a segment the forward recorded goes straight into its reverse sweep;
+    // an earlier one restores its checkpoint and recomputes, recording into
+    // the rows of the segments already swept
+    const bool recorded = seg >= A.nseg - A.nrec;
+    if (!recorded) {
+      const char* src = static_cast<const char*>(A.ck->p) + (size_t)seg * A.ck_bytes;
+      for (const auto& b : A.ck_bufs) {
+        CUDA_TRY(cudaMemcpyAsync(b.first, src, b.second, cudaMemcpyDeviceToDevice, 0));
+        src += (b.second + 255) / 256 * 256;
+      }
+      s->t = n0;
+      s->host_nsamp = 0;
     }
-    s->t = n0;
-    s->host_nsamp = 0;
-    // recompute: records the dispersive cells, row n % every
-    if (full) {
+    if (recorded) {
+      // nothing to recompute
+    } else if (full) {
       if (!A.g_rec) {
         cudaGraph_t g;
         const long long k0 = s->kernels;
@@ -611,12 +729,9 @@ static fdtd_status adj_backward(fdtd_sim* s, float* dL_drho, size_t count, doubl
     if (dL_dparams) dL_dparams[0] = dL_dparams[1] = 0.0;
     return FDTD_OK;
   }
-  fdtd_status st;
-  if (!A.ready) {
-    st = s->fp64 ? adj_prepare<double>(s) : adj_prepare<float>(s);
-    if (st != FDTD_OK) return st;
-  }
-  st = s->fp64 ? adj_sweep<double>(s) : adj_sweep<float>(s);
+  // the forward prepared the adjoint state and made the record
+  if (!A.ready || !A.rec) return fail(FDTD_ERR_STATE, "the adjoint state is missing: run the forward again");
+  fdtd_status st = s->fp64 ? adj_sweep<double>(s) : adj_sweep<float>(s);
   if (st != FDTD_OK) return st;
   if (dL_drho) {
     std::vector<double> g[3];

@@ -59,25 +59,38 @@ struct ShellCells {
 // Applying a term adds sign * coefficient * (interpolated incident value)
 // * (polarisation factor) / d_axis, the arithmetic of the walk forms in
 // kernels.cuh with the projection and the truncation already done.
+// The table is one 16-byte entry per corrected component (cell offset, the
+// two term numbers, component | terms << 2 | dielectric class << 8) and a
+// table of the distinct terms: a plane wave's terms depend on the face cell
+// only through its projection on the incidence direction, so at normal
+// incidence a face holds a few hundred distinct terms for its ~10^5 cells.
+struct TfsfTerm {
+  double dp;  // interpolation weight of the right point
+  int idx;    // line index of the left point
+  int meta;
+};
 struct TfsfTable {
-  int n;                      // groups
-  const unsigned* id;         // cell offset in the device layout
-  const unsigned char* cn;    // component | terms << 2
-  const int* idx[2];          // line index of the left interpolation point
-  const double* dp[2];        // interpolation weight of the right point
-  const unsigned char* meta[2];
+  int n;                  // entries
+  const uint4* ent;       // (cell offset, term 0, term 1, component | terms << 2 | class << 8)
+  const TfsfTerm* term;   // distinct terms
 };
 
 // dense build: slot (q, c) of shell cell q and component c
 template <typename T>
 __global__ void tfsf_tabulate(const SimView<T>* __restrict__ gv, const ShellCells sh, int efield, unsigned* id,
-                              unsigned char* cn, int* idx0, int* idx1, double* dp0, double* dp1,
+                              unsigned* cn, int* idx0, int* idx1, double* dp0, double* dp1,
                               unsigned char* m0, unsigned char* m1) {
   const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= sh.total()) return;
   const SimView<T>& g = *gv;
   int i, j, k;
   sh.cell(q, i, j, k);
+  const size_t cell = fidx(g.PX, g.plane, i, j, k);
+  // the E corrections take the cell's dielectric class coefficient
+  unsigned cls = 0;
+  if (efield && i >= g.mat_lo[0] && i < g.mat_hi[0] && j >= g.mat_lo[1] && j < g.mat_hi[1] && k >= g.mat_lo[2] &&
+      k < g.mat_hi[2])
+    cls = (unsigned)g.mat[cell] >> 3;
   for (int c = 0; c < 3; c++) {
     int nt = 0;
     int ix[2] = {0, 0};
@@ -104,8 +117,8 @@ __global__ void tfsf_tabulate(const SimView<T>* __restrict__ gv, const ShellCell
     if (efield) tfsf_e_walk(g, c, i, j, k, rec);
     else tfsf_h_walk(g, c, i, j, k, rec);
     const size_t o = (size_t)q * 3 + c;
-    id[o] = (unsigned)fidx(g.PX, g.plane, i, j, k);
-    cn[o] = (unsigned char)(c | (min(nt, 3) << 2));  // 3 terms would be a bug: flagged, not applied
+    id[o] = (unsigned)cell;
+    cn[o] = (unsigned)c | ((unsigned)min(nt, 3) << 2) | (cls << 8);  // 3 terms would be a bug: flagged, not applied
     idx0[o] = ix[0]; idx1[o] = ix[1];
     dp0[o] = w[0]; dp1[o] = w[1];
     m0[o] = mm[0]; m1[o] = mm[1];
@@ -113,9 +126,10 @@ __global__ void tfsf_tabulate(const SimView<T>* __restrict__ gv, const ShellCell
 }
 
 template <typename T>
-__device__ __forceinline__ T tfsf_term(const double* line, const float* dir, int idx, double dp, unsigned meta, T v,
-                                       T coef, const T* dd) {
-  const T x = (T)(((1 - dp) * line[idx] + dp * line[idx + 1]) * (double)dir[meta >> 3]);
+__device__ __forceinline__ T tfsf_term(const double* line, const float* dir, const TfsfTerm& t, T v, T coef,
+                                       const T* dd) {
+  const unsigned meta = (unsigned)t.meta;
+  const T x = (T)(((1 - t.dp) * line[t.idx] + t.dp * line[t.idx + 1]) * (double)dir[meta >> 3]);
   const int ax = (meta >> 1) & 3;
   if (meta & 1) v += coef * x / dd[ax];
   else v -= coef * x / dd[ax];
@@ -126,36 +140,26 @@ __device__ __forceinline__ T tfsf_term(const double* line, const float* dir, int
 // step's line update.
 template <typename T>
 __device__ __forceinline__ void tfsf_h_entry(const SimView<T>& s, const TfsfTable& tb, int g, const double* e_line) {
-  const unsigned id = tb.id[g];
-  const unsigned cn = tb.cn[g];
-  const int c = cn & 3, nt = cn >> 2;
+  const uint4 e = tb.ent[g];
+  const int c = e.w & 3, nt = (e.w >> 2) & 3;
   const T dd[3] = {s.dxyz[0], s.dxyz[1], s.dxyz[2]};
-  T v = s.H[c][id];
-  v = tfsf_term(e_line, s.tf.fe, tb.idx[0][g], tb.dp[0][g], tb.meta[0][g], v, s.che, dd);
-  if (nt > 1) v = tfsf_term(e_line, s.tf.fe, tb.idx[1][g], tb.dp[1][g], tb.meta[1][g], v, s.che, dd);
-  s.H[c][id] = v;
+  T v = s.H[c][e.x];
+  v = tfsf_term(e_line, s.tf.fe, tb.term[e.y], v, s.che, dd);
+  if (nt > 1) v = tfsf_term(e_line, s.tf.fe, tb.term[e.z], v, s.che, dd);
+  s.H[c][e.x] = v;
 }
 
 // Entry g of the E table (the line's H after this step's line update).
 template <typename T>
 __device__ __forceinline__ void tfsf_e_entry(const SimView<T>& s, const TfsfTable& tb, int g) {
-  const unsigned id = tb.id[g];
-  const unsigned cn = tb.cn[g];
-  const int c = cn & 3, nt = cn >> 2;
-  const size_t plane = s.plane;
-  const int k = (int)(id / plane);
-  const int r = (int)(id - (size_t)k * plane);
-  const int j = r / s.PX, i = r - j * s.PX;
-  unsigned m = 0;
-  if (i >= s.mat_lo[0] && i < s.mat_hi[0] && j >= s.mat_lo[1] && j < s.mat_hi[1] && k >= s.mat_lo[2] &&
-      k < s.mat_hi[2])
-    m = s.mat[id];
-  const T ceh = s.ceh[m >> 3];
+  const uint4 e = tb.ent[g];
+  const int c = e.w & 3, nt = (e.w >> 2) & 3;
+  const T ceh = s.ceh[e.w >> 8];
   const T dd[3] = {s.dxyz[0], s.dxyz[1], s.dxyz[2]};
-  T v = s.E[c][id];
-  v = tfsf_term(s.h_inc, s.tf.fh, tb.idx[0][g], tb.dp[0][g], tb.meta[0][g], v, ceh, dd);
-  if (nt > 1) v = tfsf_term(s.h_inc, s.tf.fh, tb.idx[1][g], tb.dp[1][g], tb.meta[1][g], v, ceh, dd);
-  s.E[c][id] = v;
+  T v = s.E[c][e.x];
+  v = tfsf_term(s.h_inc, s.tf.fh, tb.term[e.y], v, ceh, dd);
+  if (nt > 1) v = tfsf_term(s.h_inc, s.tf.fh, tb.term[e.z], v, ceh, dd);
+  s.E[c][e.x] = v;
 }
 
 // The halves as separate launches (the split per-half entry points) and

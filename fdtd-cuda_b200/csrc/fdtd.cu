@@ -11,6 +11,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/fdtd_b200.h"
@@ -127,9 +128,10 @@ struct fdtd_sim {
   // kernels enqueued by this handle (graph replays counted per node)
   long long kernels = 0, steps_done = 0, graph_launches = 0;
   long long graph_kernels = 0;
-  // graph replay of a whole DFT period block
+  // graph replay of a whole DFT period block; graph_epoch counts the times
+  // a captured graph was dropped because the step's launches changed
   cudaGraphExec_t graph = nullptr;
-  int graph_len = 0;
+  int graph_len = 0, graph_epoch = 0;
   cudaStream_t graph_stream = nullptr;
   bool use_graphs = true;
 
@@ -451,57 +453,70 @@ static fdtd_status build_tfsf_table(fdtd_sim* s, const ShellCells& sh, int efiel
   if (nq <= 0) return FDTD_OK;
   const size_t n = (size_t)nq * 3;
   DevBuf b;
-  const size_t bytes = n * (4 + 1 + 4 + 4 + 8 + 8 + 1 + 1);
+  const size_t bytes = n * (4 + 4 + 4 + 4 + 8 + 8 + 1 + 1);
   CUDA_TRY(b.alloc(bytes));
   char* p = static_cast<char*>(b.p);
   double* dp0 = reinterpret_cast<double*>(p);
   double* dp1 = dp0 + n;
   unsigned* id = reinterpret_cast<unsigned*>(dp1 + n);
-  int* i0 = reinterpret_cast<int*>(id + n);
+  unsigned* cn = id + n;
+  int* i0 = reinterpret_cast<int*>(cn + n);
   int* i1 = i0 + n;
-  unsigned char* cn = reinterpret_cast<unsigned char*>(i1 + n);
-  unsigned char* m0 = cn + n;
+  unsigned char* m0 = reinterpret_cast<unsigned char*>(i1 + n);
   unsigned char* m1 = m0 + n;
   tfsf_tabulate<T><<<(unsigned)((nq + 127) / 128), 128>>>(static_cast<const SimView<T>*>(s->dview), sh, efield, id,
                                                           cn, i0, i1, dp0, dp1, m0, m1);
   CUDA_TRY(cudaGetLastError());
   std::vector<char> h(bytes);
   CUDA_TRY(cudaMemcpy(h.data(), b.p, bytes, cudaMemcpyDeviceToHost));
-  const double* hdp0 = reinterpret_cast<const double*>(h.data());
-  const double* hdp1 = hdp0 + n;
-  const unsigned* hid = reinterpret_cast<const unsigned*>(hdp1 + n);
-  const int* hi0 = reinterpret_cast<const int*>(hid + n);
-  const int* hi1 = hi0 + n;
-  const unsigned char* hcn = reinterpret_cast<const unsigned char*>(hi1 + n);
-  const unsigned char* hm0 = hcn + n;
-  const unsigned char* hm1 = hm0 + n;
-  std::vector<unsigned> cid;
-  std::vector<unsigned char> ccn, cm0, cm1;
-  std::vector<int> ci0, ci1;
-  std::vector<double> cd0, cd1;
+  const double* hdp[2] = {reinterpret_cast<const double*>(h.data()), reinterpret_cast<const double*>(h.data()) + n};
+  const unsigned* hid = reinterpret_cast<const unsigned*>(hdp[1] + n);
+  const unsigned* hcn = hid + n;
+  const int* hix[2] = {reinterpret_cast<const int*>(hcn + n), reinterpret_cast<const int*>(hcn + n) + n};
+  const unsigned char* hm[2] = {reinterpret_cast<const unsigned char*>(hix[1] + n),
+                                reinterpret_cast<const unsigned char*>(hix[1] + n) + n};
+  // entries, with every term numbered in a table of the distinct terms
+  struct Key {
+    long long idx_meta;
+    unsigned long long dp_bits;
+    bool operator==(const Key& o) const { return idx_meta == o.idx_meta && dp_bits == o.dp_bits; }
+  };
+  struct KeyHash {
+    size_t operator()(const Key& k) const {
+      return std::hash<unsigned long long>()(k.dp_bits * 0x9E3779B97F4A7C15ull ^ (unsigned long long)k.idx_meta);
+    }
+  };
+  std::unordered_map<Key, unsigned, KeyHash> seen;
+  std::vector<TfsfTerm> terms;
+  std::vector<uint4> ent;
+  auto term_of = [&](size_t q, int t) -> unsigned {
+    Key key{(long long)hix[t][q] << 8 | hm[t][q], 0};
+    std::memcpy(&key.dp_bits, &hdp[t][q], sizeof(double));
+    auto it = seen.find(key);
+    if (it != seen.end()) return it->second;
+    const unsigned k = (unsigned)terms.size();
+    terms.push_back(TfsfTerm{hdp[t][q], hix[t][q], (int)hm[t][q]});
+    seen.emplace(key, k);
+    return k;
+  };
   for (size_t q = 0; q < n; q++) {
-    const int nt = hcn[q] >> 2;
+    const unsigned nt = (hcn[q] >> 2) & 3;
     if (nt == 0) continue;
     if (nt > 2) return fail(FDTD_ERR_INVALID, "a TFSF face cell has more than two corrections");
-    cid.push_back(hid[q]); ccn.push_back(hcn[q]); cm0.push_back(hm0[q]); cm1.push_back(hm1[q]);
-    ci0.push_back(hi0[q]); ci1.push_back(hi1[q]); cd0.push_back(hdp0[q]); cd1.push_back(hdp1[q]);
+    const unsigned t0 = term_of(q, 0), t1 = nt > 1 ? term_of(q, 1) : t0;
+    ent.push_back(make_uint4(hid[q], t0, t1, hcn[q]));
   }
-  const size_t m = cid.size();
+  const size_t m = ent.size();
   out.n = (int)m;
   if (m == 0) return FDTD_OK;
-  unsigned* did; unsigned char *dcn, *dm0, *dm1; int *di0, *di1; double *dd0, *dd1;
-  CUDA_TRY(s->alloc(&did, m)); CUDA_TRY(s->alloc(&dcn, m)); CUDA_TRY(s->alloc(&dm0, m)); CUDA_TRY(s->alloc(&dm1, m));
-  CUDA_TRY(s->alloc(&di0, m)); CUDA_TRY(s->alloc(&di1, m)); CUDA_TRY(s->alloc(&dd0, m)); CUDA_TRY(s->alloc(&dd1, m));
-  CUDA_TRY(cudaMemcpy(did, cid.data(), m * 4, cudaMemcpyHostToDevice));
-  CUDA_TRY(cudaMemcpy(dcn, ccn.data(), m, cudaMemcpyHostToDevice));
-  CUDA_TRY(cudaMemcpy(dm0, cm0.data(), m, cudaMemcpyHostToDevice));
-  CUDA_TRY(cudaMemcpy(dm1, cm1.data(), m, cudaMemcpyHostToDevice));
-  CUDA_TRY(cudaMemcpy(di0, ci0.data(), m * 4, cudaMemcpyHostToDevice));
-  CUDA_TRY(cudaMemcpy(di1, ci1.data(), m * 4, cudaMemcpyHostToDevice));
-  CUDA_TRY(cudaMemcpy(dd0, cd0.data(), m * 8, cudaMemcpyHostToDevice));
-  CUDA_TRY(cudaMemcpy(dd1, cd1.data(), m * 8, cudaMemcpyHostToDevice));
-  out.id = did; out.cn = dcn; out.meta[0] = dm0; out.meta[1] = dm1;
-  out.idx[0] = di0; out.idx[1] = di1; out.dp[0] = dd0; out.dp[1] = dd1;
+  uint4* dent;
+  TfsfTerm* dterm;
+  CUDA_TRY(s->alloc(&dent, m));
+  CUDA_TRY(s->alloc(&dterm, terms.size()));
+  CUDA_TRY(cudaMemcpy(dent, ent.data(), m * sizeof(uint4), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(dterm, terms.data(), terms.size() * sizeof(TfsfTerm), cudaMemcpyHostToDevice));
+  out.ent = dent;
+  out.term = dterm;
   return FDTD_OK;
 }
 
@@ -1729,6 +1744,9 @@ extern "C" fdtd_status fdtd_set_source(fdtd_sim* s, int t0, int n, const double*
   return FDTD_OK;
 }
 
+// the adjoint's part of the statistics (adjoint_host.cuh)
+static void adj_stats(const fdtd_sim* s, fdtd_stats* out);
+
 extern "C" fdtd_status fdtd_get_stats(const fdtd_sim* s, fdtd_stats* out) {
   if (!s || !out) return fail(FDTD_ERR_INVALID, "null argument");
   out->kernels = s->kernels;
@@ -1747,6 +1765,7 @@ extern "C" fdtd_status fdtd_get_stats(const fdtd_sim* s, fdtd_stats* out) {
   long long rows = 0;
   for (int f = 0; f < s->dft.nfaces; f++) rows += 4LL * s->dft.face[f].na * s->dft.face[f].nb;
   out->dft_rows = rows;
+  adj_stats(s, out);
   return FDTD_OK;
 }
 
@@ -1778,6 +1797,7 @@ extern "C" fdtd_status fdtd_snapshots_enable(fdtd_sim* s, int mode, int capacity
     cudaGraphExecDestroy(s->graph);
     s->graph = nullptr;
   }
+  s->graph_epoch++;
   s->snap_on = false;
   if (mode == 0) {
     if (out) std::memset(out, 0, sizeof(*out));

@@ -94,16 +94,18 @@ struct MetalView {
   double* nd[3][2];     // hydro density ring
   const float* rho[3];  // design blend per slot (null: plain metal coefficients)
   double vac;           // vacuum C_E = C_E_1 = ep0, the rho = 0 end of the blend
-  // forward record for the adjoint (null = off): per step row (t % rec_rows)
-  // five values per slot, [row][value][rec_off[c] + slot], value = E^n,
-  // E^{n-1}, J^n, J^{n-1}, E^{n+1}
+  // forward record for the adjoint (null = off): per step t the row
+  // (t - rec_base) mod rec_rows (rec_row), five values per slot,
+  // [row][value][rec_off[c] + slot], value = E^n, E^{n-1}, J^n, J^{n-1},
+  // E^{n+1}
   T* rec;
-  int rec_rows;
+  int rec_rows, rec_base;
   int rec_off[3];
   long long rec_slots;
-  // hydrodynamic cells: six FP64 values per slot and row, [row][value]
-  // [rec_off[c] + slot], value = J^{n-1}, J^n, J^{n+1}, N^{n-1}, N^n, N^{n+1}
-  double* hrec;
+  // hydrodynamic cells: six values per slot and row (FP64 state recorded in
+  // the field type), [row][value][rec_off[c] + slot], value = J^{n-1}, J^n,
+  // J^{n+1}, N^{n-1}, N^n, N^{n+1}
+  T* hrec;
   // hydrodynamic neighbour slots, 12 per cell (see hydro_neighbours)
   const int* nbr[3];
   // ADE coefficients, FP64 in both builds: the CP pole recursions sit close

@@ -377,6 +377,12 @@ __device__ __forceinline__ T cpml_e_all(const SimView<T>& s, int c, int i, int j
   return v;
 }
 
+// Row of step t in the adjoint's trajectory record (MetalView::rec).
+__device__ __forceinline__ size_t rec_row(int t, int base, int rows) {
+  const int d = (t - base) % rows;
+  return (size_t)(d < 0 ? d + rows : d);
+}
+
 // Non-hydrodynamic dispersive update of all three components (they do not
 // couple within a step).  pd ring: n = t%3, n-1 = (t+2)%3, new = (t+1)%3.
 template <typename T>
@@ -429,7 +435,7 @@ __device__ __forceinline__ void metal_e_body(const SimView<T>& s, const MetalVie
   const double npd = m.d1 * pdn + m.d2 * pdn1 + D3 * nvd + D4 * en + D5 * en1 + m.dNL * 0.0;
   T nv = (T)nvd;
   if (m.rec) {
-    T* r = m.rec + (size_t)(t % m.rec_rows) * 5 * m.rec_slots + m.rec_off[c] + sl;
+    T* r = m.rec + rec_row(t, m.rec_base, m.rec_rows) * 5 * m.rec_slots + m.rec_off[c] + sl;
     r[0] = en; r[m.rec_slots] = en1; r[2 * m.rec_slots] = (T)pdn; r[3 * m.rec_slots] = (T)pdn1; r[4 * m.rec_slots] = nv;
   }
   m.en1[c][sl] = en1;
@@ -575,10 +581,10 @@ __device__ __forceinline__ void hydro_e_cell(const SimView<T>& s, const MetalVie
   const double ncp1 = m.C1[1] * cpn1 + m.C2[1] * cpn1_1 + C3[1] * nvd + C4[1] * en + C5[1] * en1;
   T nv = (T)nvd;
   if (m.rec) {
-    T* rr = m.rec + (size_t)(t % m.rec_rows) * 5 * m.rec_slots + m.rec_off[c] + sl;
+    T* rr = m.rec + rec_row(t, m.rec_base, m.rec_rows) * 5 * m.rec_slots + m.rec_off[c] + sl;
     rr[0] = en; rr[m.rec_slots] = en1; rr[4 * m.rec_slots] = nv;
   }
-  if (m.hrec) m.hrec[((size_t)(t % m.rec_rows) * 6 + 5) * m.rec_slots + m.rec_off[c] + sl] = nd;
+  if (m.hrec) m.hrec[(rec_row(t, m.rec_base, m.rec_rows) * 6 + 5) * m.rec_slots + m.rec_off[c] + sl] = (T)nd;
   m.en1[c][sl] = en1;
   m.en[c][sl] = en;
   m.cpn1[c][0][sl] = cpn0;
@@ -602,13 +608,13 @@ __device__ __forceinline__ void hydro_p_cell(const SimView<T>& s, const MetalVie
   if (m.hrec) {
     // J^{n-1}, J^n, J^{n+1}, N^{n-1}, N^n of the slot; N^{n+1} follows in
     // hydro_e_cell
-    double* h = m.hrec + (size_t)(t % m.rec_rows) * 6 * m.rec_slots + m.rec_off[c] + e.w;
+    T* h = m.hrec + rec_row(t, m.rec_base, m.rec_rows) * 6 * m.rec_slots + m.rec_off[c] + e.w;
     const long long S = m.rec_slots;
-    h[0] = m.pd[c][(t + 2) % 3][e.w];
-    h[S] = m.pd[c][t % 3][e.w];
-    h[2 * S] = jd;
-    h[3 * S] = m.nd[c][(t + 1) & 1][e.w];
-    h[4 * S] = m.nd[c][t & 1][e.w];
+    h[0] = (T)m.pd[c][(t + 2) % 3][e.w];
+    h[S] = (T)m.pd[c][t % 3][e.w];
+    h[2 * S] = (T)jd;
+    h[3 * S] = (T)m.nd[c][(t + 1) & 1][e.w];
+    h[4 * S] = (T)m.nd[c][t & 1][e.w];
   }
   m.pd[c][(t + 1) % 3][e.w] = jd;
   if (c == 0) hydro_e_cell<T, 0>(s, m, t, e, P, N, jd);

@@ -108,7 +108,9 @@ class Stats(C.Structure):
                 ("e_eminb", C.c_int), ("e_estages", C.c_int),
                 ("h_pdl", C.c_int), ("e_pdl", C.c_int),
                 ("tfsf_entries_h", C.c_longlong), ("tfsf_entries_e", C.c_longlong),
-                ("dft_rows", C.c_longlong)]
+                ("dft_rows", C.c_longlong),
+                ("adj_record_steps", C.c_longlong), ("adj_record_bytes", C.c_longlong),
+                ("adj_checkpoints", C.c_longlong)]
 
 
 class SnapshotLayout(C.Structure):

@@ -393,6 +393,11 @@ typedef struct fdtd_stats {
    * TFSF table entries of the H and E shells, and DFT rows (one per
    * tangential component and flux-face cell, padding excluded) */
   long long tfsf_entries_h, tfsf_entries_e, dft_rows;
+  /* adjoint (after fdtd_forward / fdtd_forward_spectra): the steps whose
+   * dispersive-cell trajectory the forward recorded (the backward recomputes
+   * the others from checkpoints), the record's device bytes, and the number
+   * of checkpoints kept */
+  long long adj_record_steps, adj_record_bytes, adj_checkpoints;
 } fdtd_stats;
 fdtd_status fdtd_get_stats(const fdtd_sim* s, fdtd_stats* out);
 /* Measurement hook (no counterpart in the reference): runs one Yee pass

@@ -311,13 +311,15 @@ def test_backward_spectra_rejects_field_free_columns(fp64_grad):
 
 @pytest.mark.parametrize("prec", [F.FDTD_FP32, F.FDTD_FP64])
 def test_staged_gathers_match_fused_blocks(prec, monkeypatch):
-    """The staged z-march gathers (32 x 8 x 16 tiles away from the CPML and
-    the material box) do the fused gathers' arithmetic in the same order:
-    the gradient with them and without them agrees to rounding (the
-    objective's source adds to shared face-corner cells with atomics)."""
+    """The staged z-march gathers (32 x 8 x 16 tiles: the plain form away
+    from the CPML, the grid's faces and the material box, the general form,
+    driven by the cells' flags, everywhere else) do the fused gathers'
+    arithmetic in the same order: the gradient with them and without them
+    agrees to rounding (the objective's source adds to shared face-corner
+    cells with atomics)."""
     box = [40, 48, 40, 48, 44, 48]
     out = []
-    for mode in ("1", "0"):
+    for mode in ("1", "0"):  # forced on (the grid is below the automatic threshold), off
         monkeypatch.setenv("FDTD_ADJ_STAGED", mode)
         s = F.Sim(make(F, "sphere_big", precision=prec, nano_sphere=0, Tend=420, design_box=box, **GOLD))
         rng = np.random.default_rng(3)
@@ -330,3 +332,42 @@ def test_staged_gathers_match_fused_blocks(prec, monkeypatch):
     tol = 1e-12 if prec == F.FDTD_FP64 else 1e-5
     assert np.abs(out[0][1] - out[1][1]).max() <= tol * np.abs(out[1][1]).max()
     np.testing.assert_allclose(out[0][2], out[1][2], rtol=tol)
+
+
+@pytest.mark.parametrize("model", ["local", "hydro"])
+def test_recorded_and_recomputed_segments_agree(model, monkeypatch):
+    """The forward records the dispersive cells' trajectory of as many of
+    the last segments as the record budget holds; the backward recomputes
+    the others from checkpoints into the rows already swept.  Every split
+    gives the same rho gradient bit for bit (the recompute repeats the
+    forward's arithmetic); the parameter gradients are sums over all cells
+    by FP64 atomics, equal to rounding."""
+    def run(budget_gb):
+        if budget_gb is None:
+            monkeypatch.delenv("FDTD_ADJ_RECORD_GB", raising=False)
+        else:
+            monkeypatch.setenv("FDTD_ADJ_RECORD_GB", str(budget_gb))
+        if model == "local":
+            s = design_sim(F.FDTD_FP64, **GOLD)
+        else:
+            s = F.Sim(make(F, "hydro", precision=F.FDTD_FP64, Tend=300, design_box=[14, 20, 14, 20, 14, 20],
+                           **GOLD))
+        b = s.params.design_box
+        rng = np.random.default_rng(2)
+        s.set_design(rng.uniform(0, 1, (b[5] - b[4], b[3] - b[2], b[1] - b[0])).astype(np.float32))
+        L = s.forward(SEL, 50)
+        st = s.stats()
+        g, gp = s.backward()
+        s.close()
+        return L, g, gp, (st.adj_record_steps, st.adj_checkpoints, st.adj_record_bytes)
+
+    # 301 steps in segments of 50: six full ones and the last step
+    full = run(None)
+    one = run(0)  # the last segment recorded, six recomputed
+    assert full[3][:2] == (301, 0) and one[3][:2] == (1, 6)
+    part = run(3.5 * full[3][2] / 7 / 2 ** 30)  # the last three segments
+    assert part[3][:2] == (101, 4)
+    for other in (one, part):
+        assert other[0] == full[0]
+        np.testing.assert_array_equal(other[1], full[1])
+        np.testing.assert_allclose(other[2], full[2], rtol=1e-12)
