@@ -819,34 +819,6 @@ __device__ __forceinline__ T adj_h_coef_f(const SimView<T>& s, const AdjView<T>&
   return adj_mul(sg * s.che * ldg(s.cp[ax].inv_khd + n), lam);
 }
 
-// The same coefficients for a cell outside the material box, where the
-// flags follow from the indices alone: active range, and special = active
-// and in a CPML slab across the component.
-template <typename T>
-__device__ __forceinline__ T adj_e_coef_ix(const SimView<T>& s, const AdjView<T>& a, int c, int sl, int i, int j,
-                                           int k, size_t id, T lam) {
-  if (!adj_e_act(s, c, i, j, k)) return T(0);
-  const int ijk[3] = {i, j, k};
-  const int a0 = (c + 1) % 3, a1 = (c + 2) % 3;
-  if (adj_in_slab(s, a0, ijk[a0], true) || adj_in_slab(s, a1, ijk[a1], true)) return a.a[c][sl][id];
-  const int ax = (c + 1 + sl) % 3;
-  const T sg = sl == 0 ? T(1) : T(-1);
-  return adj_mul(sg * s.ceh[0] * ldg(s.cp[ax].inv_ked + ijk[ax]), lam);
-}
-template <typename T>
-__device__ __forceinline__ T adj_h_coef_ix(const SimView<T>& s, const AdjView<T>& a, int h, int sl, int i, int j,
-                                           int k, size_t id, T lam) {
-  if (!adj_h_act(s, h, i, j, k)) return T(0);
-  const int ijk[3] = {i, j, k};
-  const int a0 = (h + 1) % 3, a1 = (h + 2) % 3;
-  if (i < s.NX - 1 && j < s.NY - 1 && k < s.NZ - 1 &&
-      (adj_in_slab(s, a0, ijk[a0], false) || adj_in_slab(s, a1, ijk[a1], false)))
-    return a.a[h][sl][id];
-  const int ax = (h + 1 + sl) % 3;
-  const T sg = sl == 0 ? T(-1) : T(1);
-  return adj_mul(sg * s.che * ldg(s.cp[ax].inv_khd + ijk[ax]), lam);
-}
-
 // E sub-step transposed at the special slab components (the dispersive ones
 // are adj_e_design's): coefficients, psi_E adjoints, lambda_E <- cee lambda_E.
 template <typename T>
@@ -1090,19 +1062,15 @@ __global__ void __launch_bounds__(256) adj_gather_e_fused(const __grid_constant_
 // reads lambda_E at planes k and k + 1 with the +x and +y halo and updates
 // lambda_H, as the H pass reads E and updates H; adj_gather_e reads
 // lambda_H at k - 1 and k with the -x and -y halo and updates lambda_E, as
-// the E pass.  SLAB = false: tiles whose cells and halo lie away from the
+// the E pass.  The tiles are those whose cells and halo lie away from the
 // CPML slabs, the grid's faces and the material box, where every
-// coefficient is sg ceh0 ik lambda_E (or sg che ik lambda_H).  SLAB = true:
-// tiles outside the material box that touch a slab or a face; each
-// coefficient follows the cell's active range and whether it is special
-// (in a slab across the component: the slab kernels have written its
-// coefficient to a.a), both from the indices (adj_e_coef_ix).  Each
+// coefficient is sg ceh0 ik lambda_E (or sg che ik lambda_H).  Each
 // difference term has the product and sum order of the fused gathers, so
-// the results are theirs bit for bit.  The host builds the two tile tables
-// and hands the tiles that overlap the material box to the fused gathers.
+// the results are theirs bit for bit.  The host builds the tile table and
+// hands the remaining blocks to the fused gathers.
 constexpr int kAdjTY = 8, kAdjS = 4, kAdjKC = 16;
 
-template <typename T, bool SLAB>
+template <typename T>
 __global__ void __launch_bounds__(32 * kAdjTY) adj_gather_h_staged(const __grid_constant__ SimView<T> s,
                                                                    const __grid_constant__ AdjView<T> a,
                                                                    const int4* __restrict__ tiles) {
@@ -1128,11 +1096,9 @@ __global__ void __launch_bounds__(32 * kAdjTY) adj_gather_h_staged(const __grid_
     tasks.issue(q * SB, pnext++, NZ, a.lE[0], plane);
     cp_async_commit();
   }
-  const bool live = !SLAB || (i < NX && j < NY);
-  const bool nx = i + 1 < NX, ny = j + 1 < NY;
   const T ceh = s.ceh[0];
-  const T kx = live ? ldg(s.cp[0].inv_ked + i) : T(0), kx1 = SLAB ? T(0) : ldg(s.cp[0].inv_ked + i + 1);
-  const T ky = live ? ldg(s.cp[1].inv_ked + j) : T(0), ky1 = SLAB ? T(0) : ldg(s.cp[1].inv_ked + j + 1);
+  const T kx = ldg(s.cp[0].inv_ked + i), kx1 = ldg(s.cp[0].inv_ked + i + 1);
+  const T ky = ldg(s.cp[1].inv_ked + j), ky1 = ldg(s.cp[1].inv_ked + j + 1);
   const T* __restrict__ kzp = s.cp[2].inv_ked + k0;
   const size_t id0 = fidx(PX, plane, i, j, k0);
   T* __restrict__ phx = a.lH[0] + id0;
@@ -1140,7 +1106,6 @@ __global__ void __launch_bounds__(32 * kAdjTY) adj_gather_h_staged(const __grid_
   T* __restrict__ phz = a.lH[2] + id0;
   const int o = ty * L::HW + tx, oo = ty * 32 + tx;
   constexpr int FH = (TY + 1) * L::HW;
-  size_t id = id0;
   for (int k = k0; k < k1;) {
 #pragma unroll
     for (int u = 0; u < S; u++) {
@@ -1156,34 +1121,17 @@ __global__ void __launch_bounds__(32 * kAdjTY) adj_gather_h_staged(const __grid_
         const T ex_y = eh[o + L::HW], ez_y = eh[2 * FH + o + L::HW];
         const T ey_x = eh[FH + o + 1], ez_x = eh[2 * FH + o + 1];
         const T ex_z = en[o], ey_z = en[FH + o];
-        if (!SLAB) {
-          const T kz = ldg(kzp), kz1 = ldg(kzp + 1);
-          // Hx: Ey slot 0 (axis z, sg +1), Ez slot 1 (axis y, sg -1)
-          *phx = hown[oo] + (adj_mul(T(1) * ceh * kz, ey0) - adj_mul(T(1) * ceh * kz1, ey_z) +
-                             adj_mul(T(-1) * ceh * ky, ez0) - adj_mul(T(-1) * ceh * ky1, ez_y));
-          // Hy: Ex slot 1 (axis z, sg -1), Ez slot 0 (axis x, sg +1)
-          *phy = hown[TY * 32 + oo] + (adj_mul(T(-1) * ceh * kz, ex0) - adj_mul(T(-1) * ceh * kz1, ex_z) +
-                                       adj_mul(T(1) * ceh * kx, ez0) - adj_mul(T(1) * ceh * kx1, ez_x));
-          // Hz: Ex slot 0 (axis y, sg +1), Ey slot 1 (axis x, sg -1)
-          *phz = hown[2 * TY * 32 + oo] + (adj_mul(T(1) * ceh * ky, ex0) - adj_mul(T(1) * ceh * ky1, ex_y) +
-                                           adj_mul(T(-1) * ceh * kx, ey0) - adj_mul(T(-1) * ceh * kx1, ey_x));
-        } else if (live) {
-          const bool nz = k + 1 < NZ;
-          const size_t sx = 1, sy = PX, sz = plane;
-          *phx = hown[oo] + (adj_e_coef_ix(s, a, 1, 0, i, j, k, id, ey0) -
-                             (nz ? adj_e_coef_ix(s, a, 1, 0, i, j, k + 1, id + sz, ey_z) : T(0)) +
-                             adj_e_coef_ix(s, a, 2, 1, i, j, k, id, ez0) -
-                             (ny ? adj_e_coef_ix(s, a, 2, 1, i, j + 1, k, id + sy, ez_y) : T(0)));
-          *phy = hown[TY * 32 + oo] + (adj_e_coef_ix(s, a, 0, 1, i, j, k, id, ex0) -
-                                       (nz ? adj_e_coef_ix(s, a, 0, 1, i, j, k + 1, id + sz, ex_z) : T(0)) +
-                                       adj_e_coef_ix(s, a, 2, 0, i, j, k, id, ez0) -
-                                       (nx ? adj_e_coef_ix(s, a, 2, 0, i + 1, j, k, id + sx, ez_x) : T(0)));
-          *phz = hown[2 * TY * 32 + oo] + (adj_e_coef_ix(s, a, 0, 0, i, j, k, id, ex0) -
-                                           (ny ? adj_e_coef_ix(s, a, 0, 0, i, j + 1, k, id + sy, ex_y) : T(0)) +
-                                           adj_e_coef_ix(s, a, 1, 1, i, j, k, id, ey0) -
-                                           (nx ? adj_e_coef_ix(s, a, 1, 1, i + 1, j, k, id + sx, ey_x) : T(0)));
-        }
-        phx += plane; phy += plane; phz += plane; kzp++; id += plane;
+        const T kz = ldg(kzp), kz1 = ldg(kzp + 1);
+        // Hx: Ey slot 0 (axis z, sg +1), Ez slot 1 (axis y, sg -1)
+        *phx = hown[oo] + (adj_mul(T(1) * ceh * kz, ey0) - adj_mul(T(1) * ceh * kz1, ey_z) +
+                           adj_mul(T(-1) * ceh * ky, ez0) - adj_mul(T(-1) * ceh * ky1, ez_y));
+        // Hy: Ex slot 1 (axis z, sg -1), Ez slot 0 (axis x, sg +1)
+        *phy = hown[TY * 32 + oo] + (adj_mul(T(-1) * ceh * kz, ex0) - adj_mul(T(-1) * ceh * kz1, ex_z) +
+                                     adj_mul(T(1) * ceh * kx, ez0) - adj_mul(T(1) * ceh * kx1, ez_x));
+        // Hz: Ex slot 0 (axis y, sg +1), Ey slot 1 (axis x, sg -1)
+        *phz = hown[2 * TY * 32 + oo] + (adj_mul(T(1) * ceh * ky, ex0) - adj_mul(T(1) * ceh * ky1, ex_y) +
+                                         adj_mul(T(-1) * ceh * kx, ey0) - adj_mul(T(-1) * ceh * kx1, ey_x));
+        phx += plane; phy += plane; phz += plane; kzp++;
         k++;
       }
     }
@@ -1191,7 +1139,7 @@ __global__ void __launch_bounds__(32 * kAdjTY) adj_gather_h_staged(const __grid_
   cp_async_wait<0>();
 }
 
-template <typename T, bool SLAB>
+template <typename T>
 __global__ void __launch_bounds__(32 * kAdjTY) adj_gather_e_staged(const __grid_constant__ SimView<T> s,
                                                                    const __grid_constant__ AdjView<T> a,
                                                                    const int4* __restrict__ tiles) {
@@ -1218,11 +1166,9 @@ __global__ void __launch_bounds__(32 * kAdjTY) adj_gather_e_staged(const __grid_
     tasks.issue(q * SB, pnext++, NZ, a.lH[0], plane);
     cp_async_commit();
   }
-  const bool live = !SLAB || (i < NX && j < NY);
-  const bool px = i > 0, py = j > 0;
   const T che = s.che, cee = s.cee[0];
-  const T kx = live ? ldg(s.cp[0].inv_khd + i) : T(0), kxm = SLAB ? T(0) : ldg(s.cp[0].inv_khd + i - 1);
-  const T ky = live ? ldg(s.cp[1].inv_khd + j) : T(0), kym = SLAB ? T(0) : ldg(s.cp[1].inv_khd + j - 1);
+  const T kx = ldg(s.cp[0].inv_khd + i), kxm = ldg(s.cp[0].inv_khd + i - 1);
+  const T ky = ldg(s.cp[1].inv_khd + j), kym = ldg(s.cp[1].inv_khd + j - 1);
   const T* __restrict__ kzp = s.cp[2].inv_khd + k0;
   const size_t id0 = fidx(PX, plane, i, j, k0);
   T* __restrict__ pex = a.lE[0] + id0;
@@ -1230,7 +1176,6 @@ __global__ void __launch_bounds__(32 * kAdjTY) adj_gather_e_staged(const __grid_
   T* __restrict__ pez = a.lE[2] + id0;
   const int o = (ty + 1) * L::HW + tx + L::CH, oo = ty * 32 + tx;
   constexpr int FH = (TY + 1) * L::HW;
-  size_t id = id0;
   for (int k = k0; k < k1;) {
 #pragma unroll
     for (int u = 0; u < S; u++) {
@@ -1246,50 +1191,21 @@ __global__ void __launch_bounds__(32 * kAdjTY) adj_gather_e_staged(const __grid_
         const T hx_y = cur[o - L::HW], hz_y = cur[2 * FH + o - L::HW];
         const T hy_x = cur[FH + o - 1], hz_x = cur[2 * FH + o - 1];
         const T hx_z = prv[o], hy_z = prv[FH + o];
-        if (!SLAB) {
-          const T kz = ldg(kzp), kzm = ldg(kzp - 1);
-          T l0 = adj_mul(cee, eown[oo]), l1 = adj_mul(cee, eown[TY * 32 + oo]), l2 = adj_mul(cee, eown[2 * TY * 32 + oo]);
-          // Ex: Hy slot 0 (axis z, sg -1), Hz slot 1 (axis y, sg +1)
-          l0 += adj_mul(T(-1) * che * kzm, hy_z) - adj_mul(T(-1) * che * kz, hy0) +
-                adj_mul(T(1) * che * kym, hz_y) - adj_mul(T(1) * che * ky, hz0);
-          // Ey: Hx slot 1 (axis z, sg +1), Hz slot 0 (axis x, sg -1)
-          l1 += adj_mul(T(1) * che * kzm, hx_z) - adj_mul(T(1) * che * kz, hx0) +
-                adj_mul(T(-1) * che * kxm, hz_x) - adj_mul(T(-1) * che * kx, hz0);
-          // Ez: Hx slot 0 (axis y, sg -1), Hy slot 1 (axis x, sg +1)
-          l2 += adj_mul(T(-1) * che * kym, hx_y) - adj_mul(T(-1) * che * ky, hx0) +
-                adj_mul(T(1) * che * kxm, hy_x) - adj_mul(T(1) * che * kx, hy0);
-          *pex = l0;
-          *pey = l1;
-          *pez = l2;
-        } else if (live) {
-          const bool pz = k > 0;
-          const size_t sx = 1, sy = PX, sz = plane;
-          T l[3] = {eown[oo], eown[TY * 32 + oo], eown[2 * TY * 32 + oo]};
-          // lambda_E <- cee lambda_E for the active components that are not
-          // special (the slab kernel has done the special ones)
-          const int ijk[3] = {i, j, k};
-#pragma unroll
-          for (int c = 0; c < 3; c++)
-            if (adj_e_act(s, c, i, j, k) && !adj_in_slab(s, (c + 1) % 3, ijk[(c + 1) % 3], true) &&
-                !adj_in_slab(s, (c + 2) % 3, ijk[(c + 2) % 3], true))
-              l[c] = adj_mul(cee, l[c]);
-          l[0] += (pz ? adj_h_coef_ix(s, a, 1, 0, i, j, k - 1, id - sz, hy_z) : T(0)) -
-                  adj_h_coef_ix(s, a, 1, 0, i, j, k, id, hy0) +
-                  (py ? adj_h_coef_ix(s, a, 2, 1, i, j - 1, k, id - sy, hz_y) : T(0)) -
-                  adj_h_coef_ix(s, a, 2, 1, i, j, k, id, hz0);
-          l[1] += (pz ? adj_h_coef_ix(s, a, 0, 1, i, j, k - 1, id - sz, hx_z) : T(0)) -
-                  adj_h_coef_ix(s, a, 0, 1, i, j, k, id, hx0) +
-                  (px ? adj_h_coef_ix(s, a, 2, 0, i - 1, j, k, id - sx, hz_x) : T(0)) -
-                  adj_h_coef_ix(s, a, 2, 0, i, j, k, id, hz0);
-          l[2] += (py ? adj_h_coef_ix(s, a, 0, 0, i, j - 1, k, id - sy, hx_y) : T(0)) -
-                  adj_h_coef_ix(s, a, 0, 0, i, j, k, id, hx0) +
-                  (px ? adj_h_coef_ix(s, a, 1, 1, i - 1, j, k, id - sx, hy_x) : T(0)) -
-                  adj_h_coef_ix(s, a, 1, 1, i, j, k, id, hy0);
-          *pex = l[0];
-          *pey = l[1];
-          *pez = l[2];
-        }
-        pex += plane; pey += plane; pez += plane; kzp++; id += plane;
+        const T kz = ldg(kzp), kzm = ldg(kzp - 1);
+        T l0 = adj_mul(cee, eown[oo]), l1 = adj_mul(cee, eown[TY * 32 + oo]), l2 = adj_mul(cee, eown[2 * TY * 32 + oo]);
+        // Ex: Hy slot 0 (axis z, sg -1), Hz slot 1 (axis y, sg +1)
+        l0 += adj_mul(T(-1) * che * kzm, hy_z) - adj_mul(T(-1) * che * kz, hy0) +
+              adj_mul(T(1) * che * kym, hz_y) - adj_mul(T(1) * che * ky, hz0);
+        // Ey: Hx slot 1 (axis z, sg +1), Hz slot 0 (axis x, sg -1)
+        l1 += adj_mul(T(1) * che * kzm, hx_z) - adj_mul(T(1) * che * kz, hx0) +
+              adj_mul(T(-1) * che * kxm, hz_x) - adj_mul(T(-1) * che * kx, hz0);
+        // Ez: Hx slot 0 (axis y, sg -1), Hy slot 1 (axis x, sg +1)
+        l2 += adj_mul(T(-1) * che * kym, hx_y) - adj_mul(T(-1) * che * ky, hx0) +
+              adj_mul(T(1) * che * kxm, hy_x) - adj_mul(T(1) * che * kx, hy0);
+        *pex = l0;
+        *pey = l1;
+        *pez = l2;
+        pex += plane; pey += plane; pez += plane; kzp++;
         k++;
       }
     }

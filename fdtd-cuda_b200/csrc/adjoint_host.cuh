@@ -27,10 +27,11 @@ struct fdtd_sim::Adjoint {
   // by the forward (their first step rec_base), the others recomputed
   int nrec = 0, rows = 0, rec_base = 0;
   size_t rec_bytes = 0;
-  // graph of one DFT period of the recording forward (the main step graph
-  // does not record), with the generation of the main graph it matches
-  cudaGraphExec_t g_fwd = nullptr;
-  long long g_fwd_kernels = 0;
+  // graphs of the two launch periods of the recording forward (the main
+  // step graphs do not record), with the generation of the main graphs they
+  // match
+  cudaGraphExec_t g_fwd[2] = {nullptr, nullptr};
+  long long g_fwd_kernels[2] = {0, 0};
   int g_fwd_len = 0, g_fwd_epoch = -1;
   // objective: weights on the ScatAbs table (fdtd_forward's own, for
   // fdtd_backward), the frequencies with a nonzero weight and the faces the
@@ -61,11 +62,10 @@ struct fdtd_sim::Adjoint {
   double* grho[3] = {nullptr, nullptr, nullptr};
   double* gpar = nullptr;
   int* step = nullptr;
-  // gather tables per gather (0 = H, 1 = E): the staged tiles of the plain
-  // form, the staged tiles of the slab form, and the one-plane blocks of
-  // the tiles over the material box, which the fused gathers take
-  std::unique_ptr<DevBuf> gtab[2][3];
-  int ngt[2][3] = {{0, 0, 0}, {0, 0, 0}};
+  // gather tables per gather (0 = H, 1 = E): the staged tiles and the
+  // one-plane blocks of the other tiles, which the fused gathers take
+  std::unique_ptr<DevBuf> gtab[2][2];
+  int ngt[2][2] = {{0, 0}, {0, 0}};
   bool tabs = false;
   // graphs of one full segment: the recompute (DFT off, recording on) and
   // the reverse sweep; replayed for every full segment
@@ -75,8 +75,9 @@ struct fdtd_sim::Adjoint {
   void drop_graphs() {
     if (g_rec) cudaGraphExecDestroy(g_rec);
     if (g_adj) cudaGraphExecDestroy(g_adj);
-    if (g_fwd) cudaGraphExecDestroy(g_fwd);
-    g_rec = g_adj = g_fwd = nullptr;
+    for (auto& g : g_fwd)
+      if (g) cudaGraphExecDestroy(g);
+    g_rec = g_adj = g_fwd[0] = g_fwd[1] = nullptr;
   }
   ~Adjoint() {
     drop_graphs();
@@ -247,18 +248,23 @@ static fdtd_status adj_forward_run_t(fdtd_sim* s, int checkpoint_every) {
     if (st != FDTD_OK) return st;
   }
   // the recorded segments, with their own step graph
-  if (A.g_fwd && A.g_fwd_epoch != s->graph_epoch) {
-    cudaGraphExecDestroy(A.g_fwd);
-    A.g_fwd = nullptr;
-  }
+  if (A.g_fwd_epoch != s->graph_epoch)
+    for (auto& g : A.g_fwd)
+      if (g) {
+        cudaGraphExecDestroy(g);
+        g = nullptr;
+      }
   adj_record_view<T>(s, true);
-  std::swap(s->graph, A.g_fwd);
-  std::swap(s->graph_kernels, A.g_fwd_kernels);
-  std::swap(s->graph_len, A.g_fwd_len);
+  auto swap_graphs = [&]() {
+    for (int q = 0; q < 2; q++) {
+      std::swap(s->graph[q], A.g_fwd[q]);
+      std::swap(s->graph_kernels_p[q], A.g_fwd_kernels[q]);
+    }
+    std::swap(s->graph_len, A.g_fwd_len);
+  };
+  swap_graphs();
   st = fdtd_step(s, total - A.rec_base, nullptr);
-  std::swap(s->graph, A.g_fwd);
-  std::swap(s->graph_kernels, A.g_fwd_kernels);
-  std::swap(s->graph_len, A.g_fwd_len);
+  swap_graphs();
   A.g_fwd_epoch = s->graph_epoch;
   adj_record_view<T>(s, false);
   if (st != FDTD_OK) return st;
@@ -531,14 +537,12 @@ static fdtd_status adj_sweep(fdtd_sim* s) {
   }
   const dim3 gtile((unsigned)((s->NX + 31) / 32), (unsigned)((s->NY + 7) / 8), (unsigned)s->NZ);
   if (fused) adj_build_flags<T><<<gtile, dim3(32, 8)>>>(view<T>(s), a.flags);
-  // staged tiles: 32 x kAdjTY x kAdjKC boxes.  A tile whose cells and halo
-  // (+1 for the H gather, -1 for the E gather) lie away from the material
-  // box runs staged: the plain form away from the CPML slabs and the grid's
-  // faces, the slab form otherwise; a tile over the material box goes to
-  // the fused gathers, one plane per block
-  // the z-march tiles keep a CTA on 16 planes: on a small grid too few of
-  // them would run (fewer than 4 a multiprocessor), and the fused gathers,
-  // one plane per block, win; FDTD_ADJ_STAGED=1 / 0 forces either
+  // staged tiles: 32 x kAdjTY x kAdjKC boxes whose cells and halo (+1 for
+  // the H gather, -1 for the E gather) lie away from the CPML slabs, the
+  // grid's faces and the material box; the other tiles go to the fused
+  // gathers, one plane per block.  A tile keeps a CTA on 16 planes: on a
+  // small grid too few of them would run (fewer than 4 a multiprocessor),
+  // and the fused gathers win there; FDTD_ADJ_STAGED=1 / 0 forces either.
   const char* senv = std::getenv("FDTD_ADJ_STAGED");
   int nsm = 148;
   CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, s->device));
@@ -550,7 +554,7 @@ static fdtd_status adj_sweep(fdtd_sim* s) {
     const int nbx = (s->NX + 31) / 32, nby = (s->NY + 7) / 8, nbz = (s->NZ + kAdjKC - 1) / kAdjKC;
     for (int g = 0; g < 2; g++) {
       const int lo_off = g == 0 ? 0 : -1, hi_off = g == 0 ? 1 : 0;
-      std::vector<int4> v[3];
+      std::vector<int4> v[2];
       for (int bz = 0; bz < nbz; bz++)
         for (int by = 0; by < nby; by++)
           for (int bx = 0; bx < nbx; bx++) {
@@ -562,13 +566,13 @@ static fdtd_status adj_sweep(fdtd_sim* s) {
               inside = inside && lo[ax] >= s->su.Nc[ax] + 1 && hi[ax] < s->su.F[ax];
               off_mat = off_mat || hi[ax] < s->mat_lo[ax] || lo[ax] >= s->mat_hi[ax];
             }
-            if (!off_mat) {
-              for (int k = bz * kAdjKC; k < std::min(s->NZ, (bz + 1) * kAdjKC); k++) v[2].push_back(make_int4(bx, by, k, 0));
+            if (inside && off_mat) {
+              v[0].push_back(make_int4(bx, by, bz, 0));
             } else {
-              v[inside ? 0 : 1].push_back(make_int4(bx, by, bz, 0));
+              for (int k = bz * kAdjKC; k < std::min(s->NZ, (bz + 1) * kAdjKC); k++) v[1].push_back(make_int4(bx, by, k, 0));
             }
           }
-      for (int q = 0; q < 3; q++) {
+      for (int q = 0; q < 2; q++) {
         auto b = std::make_unique<DevBuf>();
         CUDA_TRY(b->alloc(std::max<size_t>(1, v[q].size()) * sizeof(int4)));
         if (!v[q].empty()) CUDA_TRY(cudaMemcpy(b->p, v[q].data(), v[q].size() * sizeof(int4), cudaMemcpyHostToDevice));
@@ -577,15 +581,13 @@ static fdtd_status adj_sweep(fdtd_sim* s) {
       }
     }
     const int smem = (int)(kAdjS * StageLayout<T, kAdjTY>::STAGE * sizeof(T));
-    CUDA_TRY(cudaFuncSetAttribute(adj_gather_h_staged<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    CUDA_TRY(cudaFuncSetAttribute(adj_gather_e_staged<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    CUDA_TRY(cudaFuncSetAttribute(adj_gather_h_staged<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    CUDA_TRY(cudaFuncSetAttribute(adj_gather_e_staged<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    CUDA_TRY(cudaFuncSetAttribute(adj_gather_h_staged<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    CUDA_TRY(cudaFuncSetAttribute(adj_gather_e_staged<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     A.tabs = true;
   }
   const size_t gsmem = kAdjS * StageLayout<T, kAdjTY>::STAGE * sizeof(T);
-  // one gather: the staged tiles of both forms and the fused blocks
-  // (disjoint outputs, inputs they do not write); returns the launches
+  // one gather: the staged tiles and the fused blocks (disjoint outputs,
+  // inputs they do not write); returns the launches
   auto gather = [&](int g, cudaStream_t stream) -> int {
     if (!staged) {
       if (g == 0) adj_gather_h_fused<T><<<gtile, dim3(32, 8), 0, stream>>>(view<T>(s), a, nullptr);
@@ -593,23 +595,17 @@ static fdtd_status adj_sweep(fdtd_sim* s) {
       return 1;
     }
     int k = 0;
-    const int4* t[3];
-    for (int q = 0; q < 3; q++) t[q] = static_cast<const int4*>(A.gtab[g][q]->p);
-    const dim3 blk(32, kAdjTY);
+    const int4* tt = static_cast<const int4*>(A.gtab[g][0]->p);
+    const int4* lt = static_cast<const int4*>(A.gtab[g][1]->p);
     const int* n = A.ngt[g];
-    if (n[2]) {
-      if (g == 0) adj_gather_h_fused<T><<<n[2], dim3(32, 8), 0, stream>>>(view<T>(s), a, t[2]);
-      else adj_gather_e_fused<T><<<n[2], dim3(32, 8), 0, stream>>>(view<T>(s), a, t[2]);
-      k++;
-    }
     if (n[1]) {
-      if (g == 0) adj_gather_h_staged<T, true><<<n[1], blk, gsmem, stream>>>(view<T>(s), a, t[1]);
-      else adj_gather_e_staged<T, true><<<n[1], blk, gsmem, stream>>>(view<T>(s), a, t[1]);
+      if (g == 0) adj_gather_h_fused<T><<<n[1], dim3(32, 8), 0, stream>>>(view<T>(s), a, lt);
+      else adj_gather_e_fused<T><<<n[1], dim3(32, 8), 0, stream>>>(view<T>(s), a, lt);
       k++;
     }
     if (n[0]) {
-      if (g == 0) adj_gather_h_staged<T, false><<<n[0], blk, gsmem, stream>>>(view<T>(s), a, t[0]);
-      else adj_gather_e_staged<T, false><<<n[0], blk, gsmem, stream>>>(view<T>(s), a, t[0]);
+      if (g == 0) adj_gather_h_staged<T><<<n[0], dim3(32, kAdjTY), gsmem, stream>>>(view<T>(s), a, tt);
+      else adj_gather_e_staged<T><<<n[0], dim3(32, kAdjTY), gsmem, stream>>>(view<T>(s), a, tt);
       k++;
     }
     return k;

@@ -58,22 +58,29 @@ __global__ void dft_sample_batch(const BatchSim<T>* __restrict__ b) {
   const BatchSim<T>& x = b[blockIdx.z];
   dft_sample_body(x.v, x.dft, x.ring, x.clk);
 }
+// The members keep filling the first half of their rings: every launch
+// period each member's job is its samples once the half cannot take
+// another period (dft_job_ready_body), contracted, then the half emptied.
+// A flush before the spectra are read goes through the member's own
+// contraction kernels (fdtd_spectral_finalize) and takes the samples no job
+// has taken.
+template <typename T>
+__global__ void dft_job_ready_batch(const BatchSim<T>* __restrict__ b) {
+  dft_job_ready_body(b[blockIdx.y].clk);
+}
 template <typename T>
 __global__ void dft_twiddles_batch(const BatchSim<T>* __restrict__ b) {
   const BatchSim<T>& x = b[blockIdx.y];
-  dft_twiddles_body(x.dft, x.clk, x.tw, 0);
+  dft_twiddles_body(x.dft, x.clk, x.tw);
 }
 template <typename T>
 __global__ void __launch_bounds__(128) dft_contract_batch(const BatchSim<T>* __restrict__ b) {
   const BatchSim<T>& x = b[blockIdx.y];
-  dft_contract_body(x.dft, x.ring, x.clk, x.tw, 0);
+  dft_contract_body(x.dft, x.ring, x.clk, x.tw);
 }
-// a flush before the spectra are read goes through the member's own
-// contraction kernels (fdtd_spectral_finalize)
 template <typename T>
-__global__ void dft_reset_batch(const BatchSim<T>* __restrict__ b) {
-  DevClock* clk = b[blockIdx.y].clk;
-  if (dft_ring_ready(clk, 0)) clk->nsamp = 0;
+__global__ void dft_job_done_batch(const BatchSim<T>* __restrict__ b) {
+  dft_job_done_body(b[blockIdx.y].clk);
 }
 
 }  // namespace fdtd
@@ -369,10 +376,11 @@ static void batch_enqueue_step(fdtd_batch* b, cudaStream_t st) {
     k++;
     if (++b->host_nsamp == kSampleBlock) {
       // the members' rings fill together: these contract once they are full
+      dft_job_ready_batch<T><<<dim3(1, n), 1, 0, st>>>(d);
       dft_twiddles_batch<T><<<dim3(b->g_tw, n), 256, 0, st>>>(d);
       dft_contract_batch<T><<<dim3(b->g_c, n), 128, dft_smem_bytes<T>(), st>>>(d);
-      dft_reset_batch<T><<<dim3(1, n), 1, 0, st>>>(d);
-      k += 3;
+      dft_job_done_batch<T><<<dim3(1, n), 1, 0, st>>>(d);
+      k += 4;
       b->host_nsamp = 0;
     }
   }

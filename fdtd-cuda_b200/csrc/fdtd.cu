@@ -116,7 +116,7 @@ struct fdtd_sim {
   double* flux = nullptr;  // [12][nf]
   double2* twiddles = nullptr;  // [2][kRingSlots][nf]
   bool dft_on = true;
-  int host_nsamp = 0;  // samples since the last contraction launch (launch period position)
+  int host_nsamp = 0;  // DFT samples into the contraction period (0 .. kRingSlots - 1)
   // views (one of them is used, by precision)
   SimView<float> vf;
   SimView<double> vd;
@@ -127,11 +127,18 @@ struct fdtd_sim {
   int t = 0;
   // kernels enqueued by this handle (graph replays counted per node)
   long long kernels = 0, steps_done = 0, graph_launches = 0;
-  long long graph_kernels = 0;
-  // graph replay of a whole DFT period block; graph_epoch counts the times
-  // a captured graph was dropped because the step's launches changed
-  cudaGraphExec_t graph = nullptr;
+  // graph replays of the two launch periods of a DFT contraction period
+  // (the first forks the contraction of the last period's samples);
+  // graph_epoch counts the times captured graphs were dropped because the
+  // step's launches changed
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  long long graph_kernels_p[2] = {0, 0};
   int graph_len = 0, graph_epoch = 0;
+  // the DFT contraction beside the steps: its stream and fork/join events,
+  // and whether a forked contraction still has to be joined
+  cudaStream_t side_dft = nullptr;
+  cudaEvent_t dft_fork_ev = nullptr, dft_join_ev = nullptr;
+  bool dft_pending = false;
   cudaStream_t graph_stream = nullptr;
   bool use_graphs = true;
 
@@ -162,7 +169,11 @@ struct fdtd_sim {
   cudaEvent_t fork3_ev = nullptr, join3_ev = nullptr;  // the line step beside the H pass
 
   void destroy_streams() {
-    if (graph) cudaGraphExecDestroy(graph);
+    for (auto& g : graph)
+      if (g) cudaGraphExecDestroy(g);
+    if (side_dft) cudaStreamDestroy(side_dft);
+    if (dft_fork_ev) cudaEventDestroy(dft_fork_ev);
+    if (dft_join_ev) cudaEventDestroy(dft_join_ev);
     if (graph_stream) cudaStreamDestroy(graph_stream);
     if (side) cudaStreamDestroy(side);
     if (fork_ev) cudaEventDestroy(fork_ev);
@@ -430,10 +441,10 @@ static fdtd_status build_views(fdtd_sim* s) {
     s->dview = dv;
     CUDA_TRY(cudaMemcpy(dv, &v, sizeof(v), cudaMemcpyHostToDevice));
   }
-  // DFT sample ring
+  // DFT sample ring: two halves of kRingSlots samples
   if (s->dft.rows > 0) {
     T* r;
-    cudaError_t e = s->alloc(&r, (size_t)kRingSlots * s->dft.rows, true);
+    cudaError_t e = s->alloc(&r, (size_t)2 * kRingSlots * s->dft.rows, true);
     if (e != cudaSuccess) return fail(FDTD_ERR_ALLOC, cudaGetErrorString(e));
     s->ring = r;
   }
@@ -759,6 +770,9 @@ static fdtd_status create_impl(const fdtd_params* p, int device, fdtd_sim** out,
   L.dft_every = s->dft_on ? su.p.dft_every : 0;
   CUDA_TRY(cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking));
   CUDA_TRY(cudaStreamCreateWithFlags(&s->side2, cudaStreamNonBlocking));
+  CUDA_TRY(cudaStreamCreateWithFlags(&s->side_dft, cudaStreamNonBlocking));
+  CUDA_TRY(cudaEventCreateWithFlags(&s->dft_fork_ev, cudaEventDisableTiming));
+  CUDA_TRY(cudaEventCreateWithFlags(&s->dft_join_ev, cudaEventDisableTiming));
   CUDA_TRY(cudaEventCreateWithFlags(&s->fork2_ev, cudaEventDisableTiming));
   CUDA_TRY(cudaEventCreateWithFlags(&s->join2_ev, cudaEventDisableTiming));
   CUDA_TRY(cudaEventCreateWithFlags(&s->fork3_ev, cudaEventDisableTiming));
@@ -803,6 +817,7 @@ extern "C" fdtd_status fdtd_reset(fdtd_sim* s) {
   for (const auto& b : s->state) CUDA_TRY(cudaMemset(b.first, 0, b.second));
   s->t = 0;
   s->host_nsamp = 0;
+  s->dft_pending = false;
   s->snap_first = s->snap_drained = 0;
   return FDTD_OK;
 }
@@ -1223,25 +1238,45 @@ static void launch_sample(fdtd_sim* s, cudaStream_t st) {
   dft_sample<T><<<g, 256, 0, st>>>(view<T>(s), s->dft, (T*)s->ring, s->clk);
   s->kernels++;
 }
+// The contraction of the clock's job (dft_job_*): phasors, then the FP64
+// product into the accumulators.
 template <typename T>
-static void launch_contract(fdtd_sim* s, cudaStream_t st, bool force) {
+static void launch_contract(fdtd_sim* s, cudaStream_t st) {
   const int ntw = 2 * kRingSlots * s->dft.nf;
-  dft_twiddles<<<(ntw + 255) / 256, 256, 0, st>>>(s->dft, s->clk, s->twiddles, (int)force);
+  dft_twiddles<<<(ntw + 255) / 256, 256, 0, st>>>(s->dft, s->clk, s->twiddles);
   dft_contract<T><<<(unsigned)(s->dft.rows / kDftRows), 128, dft_smem_bytes<T>(), st>>>(
-      s->dft, (const T*)s->ring, s->clk, s->twiddles, (int)force);
-  dft_reset_count<<<1, 1, 0, st>>>(s->clk, (int)force);
-  s->kernels += 3;
+      s->dft, (const T*)s->ring, s->clk, s->twiddles);
+  s->kernels += 2;
 }
 
-// One DFT sample of the step; every kSampleBlock samples the contraction
-// kernels are launched, and they contract once the ring is full.
+// A contraction period is kRingSlots samples, two launch periods.  Its first
+// sample step, before its line step reserves a ring slot, switches the
+// ring's halves and forks the contraction of the half the last period
+// filled onto the DFT stream, where it runs beside the steps (it touches
+// only that half, the phasors and the accumulators).
+template <typename T>
+static void dft_period_begin(fdtd_sim* s, cudaStream_t st) {
+  if (s->line.dft_every <= 0 || s->t % s->line.dft_every != 0 || s->host_nsamp != 0) return;
+  dft_job_period<<<1, 1, 0, st>>>(s->clk);
+  cudaEventRecord(s->dft_fork_ev, st);
+  cudaStreamWaitEvent(s->side_dft, s->dft_fork_ev, 0);
+  launch_contract<T>(s, s->side_dft);
+  cudaEventRecord(s->dft_join_ev, s->side_dft);
+  s->dft_pending = true;
+  s->kernels++;
+}
+
+// One DFT sample of the step; the end of the first launch period of a
+// contraction period joins the forked contraction, so each captured launch
+// period is self-contained.
 template <typename T>
 static void sample_and_contract(fdtd_sim* s, cudaStream_t st) {
   launch_sample<T>(s, st);
-  if (++s->host_nsamp == kSampleBlock) {
-    launch_contract<T>(s, st, false);
-    s->host_nsamp = 0;
+  if (++s->host_nsamp == kSampleBlock && s->dft_pending) {
+    cudaStreamWaitEvent(st, s->dft_join_ev, 0);
+    s->dft_pending = false;
   }
+  if (s->host_nsamp == kRingSlots) s->host_nsamp = 0;
 }
 
 // One full step.  The 1-D line step runs on the second side stream beside
@@ -1254,6 +1289,7 @@ static void sample_and_contract(fdtd_sim* s, cudaStream_t st) {
 // t from the device.
 template <typename T>
 static void enqueue_step(fdtd_sim* s, cudaStream_t st) {
+  dft_period_begin<T>(s, st);
   cudaEventRecord(s->fork3_ev, st);
   cudaStreamWaitEvent(s->side2, s->fork3_ev, 0);
   launch_line<T>(s, s->side2);
@@ -1285,9 +1321,12 @@ static fdtd_status step_impl(fdtd_sim* s, int nsteps, cudaStream_t st) {
   const int G = every * kSampleBlock;  // launch pattern period
   int done = 0;
   while (done < nsteps) {
-    const bool aligned = s->t % G == 0 && s->host_nsamp == 0 && nsteps - done >= G;
+    // the two launch periods of a contraction period have their own graphs
+    const int ph = s->line.dft_every > 0 ? s->host_nsamp / kSampleBlock : 0;
+    const bool aligned =
+        s->t % G == 0 && s->host_nsamp % kSampleBlock == 0 && !s->dft_pending && nsteps - done >= G;
     if (s->use_graphs && aligned) {
-      if (!s->graph) {
+      if (!s->graph[ph]) {
         // capture one period on a private stream, then replay it
         if (!s->graph_stream) CUDA_TRY(cudaStreamCreateWithFlags(&s->graph_stream, cudaStreamNonBlocking));
         cudaGraph_t g;
@@ -1296,19 +1335,20 @@ static fdtd_status step_impl(fdtd_sim* s, int nsteps, cudaStream_t st) {
         CUDA_TRY(cudaStreamBeginCapture(s->graph_stream, cudaStreamCaptureModeThreadLocal));
         for (int q = 0; q < G; q++) enqueue_step<T>(s, s->graph_stream);
         CUDA_TRY(cudaStreamEndCapture(s->graph_stream, &g));
-        s->graph_kernels = s->kernels - k_save;
+        s->graph_kernels_p[ph] = s->kernels - k_save;
         s->kernels = k_save;
         s->t = t_save;
         s->host_nsamp = n_save;
-        cudaError_t e = cudaGraphInstantiate(&s->graph, g, 0);
+        cudaError_t e = cudaGraphInstantiate(&s->graph[ph], g, 0);
         cudaGraphDestroy(g);
         CUDA_TRY(e);
         s->graph_len = G;
       }
-      CUDA_TRY(cudaGraphLaunch(s->graph, st));
-      s->kernels += s->graph_kernels;
+      CUDA_TRY(cudaGraphLaunch(s->graph[ph], st));
+      s->kernels += s->graph_kernels_p[ph];
       s->graph_launches++;
       s->t += G;
+      if (s->line.dft_every > 0) s->host_nsamp = (s->host_nsamp + kSampleBlock) % kRingSlots;
       done += G;
     } else {
       enqueue_step<T>(s, st);
@@ -1345,7 +1385,13 @@ extern "C" fdtd_status fdtd_update_h(fdtd_sim* s, void* stream) {
 extern "C" fdtd_status fdtd_update_line(fdtd_sim* s, void* stream) {
   if (!s) return fail(FDTD_ERR_INVALID, "null argument");
   CUDA_TRY(cudaSetDevice(s->device));
-  if (s->fp64) launch_line<double>(s, as_stream(stream)); else launch_line<float>(s, as_stream(stream));
+  if (s->fp64) {
+    dft_period_begin<double>(s, as_stream(stream));
+    launch_line<double>(s, as_stream(stream));
+  } else {
+    dft_period_begin<float>(s, as_stream(stream));
+    launch_line<float>(s, as_stream(stream));
+  }
   CUDA_TRY(cudaGetLastError());
   return FDTD_OK;
 }
@@ -1418,11 +1464,14 @@ extern "C" fdtd_status fdtd_check(fdtd_sim* s) {
 // spectra
 
 // Contracts what the device ring holds (nothing when it is empty).
+// (the callers have synchronised the device, so no contraction is in flight)
+// The samples of the half being filled that no contraction has taken; the
+// stepper's contraction period goes on where it was.
 static fdtd_status flush_dft(fdtd_sim* s) {
   if (s->dft.rows > 0 && s->line.dft_every > 0) {
-    if (s->fp64) launch_contract<double>(s, 0, true); else launch_contract<float>(s, 0, true);
+    dft_job_flush<<<1, 1>>>(s->clk);
+    if (s->fp64) launch_contract<double>(s, 0); else launch_contract<float>(s, 0);
   }
-  s->host_nsamp = 0;
   CUDA_TRY(cudaGetLastError());
   return FDTD_OK;
 }
@@ -1793,10 +1842,11 @@ extern "C" fdtd_status fdtd_snapshots_enable(fdtd_sim* s, int mode, int capacity
   CUDA_TRY(cudaSetDevice(s->device));
   CUDA_TRY(cudaDeviceSynchronize());
   // a captured step graph holds the step's launches: capture it again
-  if (s->graph) {
-    cudaGraphExecDestroy(s->graph);
-    s->graph = nullptr;
-  }
+  for (auto& g : s->graph)
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
   s->graph_epoch++;
   s->snap_on = false;
   if (mode == 0) {

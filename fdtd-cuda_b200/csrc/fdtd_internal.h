@@ -19,18 +19,25 @@
 namespace fdtd {
 
 constexpr int kMaxClasses = 32;   // dielectric classes (bits 3..7)
-constexpr int kSampleBlock = 32;  // DFT samples per launch period of the stepper
-constexpr int kRingSlots = 64;    // DFT samples per FP64 contraction (ring depth)
-static_assert(kRingSlots % kSampleBlock == 0, "the ring holds whole launch periods");
+constexpr int kSampleBlock = 32;  // DFT samples per launch period of the stepper (a graph block)
+constexpr int kRingSlots = 64;    // DFT samples per FP64 contraction (one half of the ring)
+static_assert(kRingSlots == 2 * kSampleBlock, "a contraction period is two launch periods");
 
 // Step clock kept in device memory so captured graphs can be replayed.
+// The DFT sample ring has two halves of kRingSlots slots: samples go into
+// the half at `base`; a contraction (its "job": ring slots job_off ..
+// job_off + job_n) takes one half's samples, so that it can run beside
+// the steps that fill the other half.
 struct DevClock {
   int t;          // steps completed by the 1D-line kernel (current step + 1)
-  int nsamp;      // DFT samples waiting in the ring
+  int nsamp;      // DFT samples in the half being filled
   int nonfinite;  // watchdog flag
   int samp_slot;  // ring slot of the current step's DFT sample
   double e1, e2;  // Mur history of the incident line ends (main.cu:2835-2838)
-  int samp_t[kRingSlots];
+  int base;       // first slot of the half being filled (0 or kRingSlots)
+  int cstart;     // samples of that half a flush has already contracted
+  int job_off, job_n, job_reset;
+  int samp_t[2 * kRingSlots];
 };
 
 // Per-axis CPML tables.  The E tables have Nc+1 entries, the H tables Nc.

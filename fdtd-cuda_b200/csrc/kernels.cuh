@@ -10,8 +10,9 @@
 //               compact lists
 //   dft_sample  every dft_every steps: gather the flux-plane tangential
 //               components into a sample ring
-//   dft_contract once the ring holds kRingSlots samples: FP64 contraction
-//               of the ring with the phasors into the accumulators
+//   dft_contract once a half of the ring holds kRingSlots samples: FP64
+//               contraction of that half with the phasors into the
+//               accumulators, beside the steps that fill the other half
 // This file holds the bodies of everything but the Yee passes and the TFSF
 // tables.
 #pragma once
@@ -308,13 +309,14 @@ __device__ __forceinline__ void line_step_body(const LineArgs& a, const SimView<
     // reserve this step's slot in the DFT sample ring (ScattAbs runs when
     // t % 4 == 0, main.cu:2920)
     if (a.dft_every > 0 && t % a.dft_every == 0) {
-      const int slot = a.clk->nsamp;
-      if (slot < kRingSlots) {
+      const int n = a.clk->nsamp;
+      if (n < kRingSlots) {
+        const int slot = a.clk->base + n;
         a.clk->samp_slot = slot;
         a.clk->samp_t[slot] = t;
-        a.clk->nsamp = slot + 1;
+        a.clk->nsamp = n + 1;
       } else {
-        a.clk->samp_slot = -1;  // ring full: the caller skipped a contraction
+        a.clk->samp_slot = -1;  // half full: the caller skipped a contraction
       }
     }
     a.clk->t = t + 1;
@@ -678,7 +680,7 @@ struct DftView {
 template <typename T>
 __device__ __forceinline__ void dft_sample_body(const SimView<T>& s, const DftView& d, T* ring, const DevClock* clk) {
   const int slot = clk->samp_slot;
-  if (slot < 0 || slot >= kRingSlots) return;
+  if (slot < 0 || slot >= 2 * kRingSlots) return;
   const int f = blockIdx.y;
   const DftFace F = d.face[f];
   const int n = F.na * F.nb;
@@ -703,33 +705,64 @@ __global__ void dft_sample(const __grid_constant__ SimView<T> s, const __grid_co
   dft_sample_body(s, d, ring, clk);
 }
 
-// Phasors of the samples waiting in the ring: tw[h][s][f] = exp(i 2 pi
-// (t_s + delta_h) dt freq[f]) with delta = 1 for E (sampled after the E
-// update) and 1/2 for H (main.cu:62-76).  [2][kRingSlots][nf] of double2.
-// The stepper launches the contraction kernels every kSampleBlock samples.
-// Unless `force` is set (a flush before the spectra are read) they return
-// at once while the ring can take another kSampleBlock samples, so the
-// ring never overflows whatever the ring held when the launches began.
-__device__ __forceinline__ bool dft_ring_ready(const DevClock* clk, int force) {
-  return force || clk->nsamp > kRingSlots - kSampleBlock;
+// The contraction's job, set on the device before its kernels run:
+//   dft_job_period  (a simulation's stepper, at the start of every
+//                    contraction period) the samples of the half just
+//                    filled; the other half becomes the one being filled
+//   dft_job_flush   (before the spectra are read) the samples of the half
+//                    being filled that no job has taken yet
+//   dft_job_ready / dft_job_done  (the batch, whose members never switch
+//                    halves) the half's samples once the half can no
+//                    longer take another launch period, then empty it
+__device__ __forceinline__ void dft_take(DevClock* clk, int upto) {
+  clk->job_off = clk->base + clk->cstart;
+  clk->job_n = upto - clk->cstart;
 }
-__device__ __forceinline__ void dft_twiddles_body(const DftView& d, const DevClock* clk, double2* tw, int force) {
-  if (!dft_ring_ready(clk, force)) return;
+__global__ void dft_job_period(DevClock* clk) {
+  dft_take(clk, clk->nsamp);
+  clk->base ^= kRingSlots;
+  clk->nsamp = 0;
+  clk->cstart = 0;
+}
+__global__ void dft_job_flush(DevClock* clk) {
+  dft_take(clk, clk->nsamp);
+  clk->cstart = clk->nsamp;
+}
+__device__ __forceinline__ void dft_job_ready_body(DevClock* clk) {
+  const bool ready = clk->nsamp > kRingSlots - kSampleBlock;
+  dft_take(clk, ready ? min(kRingSlots, clk->nsamp) : clk->cstart);
+  clk->job_reset = ready;
+}
+__device__ __forceinline__ void dft_job_done_body(DevClock* clk) {
+  if (clk->job_reset) {
+    clk->nsamp = 0;
+    clk->cstart = 0;
+    clk->job_reset = 0;
+  }
+}
+
+// Phasors of the job's samples: tw[h][s][f] = exp(i 2 pi (t_s + delta_h)
+// dt freq[f]) with delta = 1 for E (sampled after the E update) and 1/2 for
+// H (main.cu:62-76).  [2][kRingSlots][nf] of double2; slots past the job
+// hold zeros.
+__device__ __forceinline__ void dft_twiddles_body(const DftView& d, const DevClock* clk, double2* tw) {
+  const int n = clk->job_n;
+  if (n <= 0) return;
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= 2 * kRingSlots * d.nf) return;
   const int h = q / (kRingSlots * d.nf);
   const int r = q - h * kRingSlots * d.nf;
   const int sidx = r / d.nf, f = r - sidx * d.nf;
   double c = 0, sv = 0;
-  if (sidx < min(kRingSlots, clk->nsamp)) {
-    const int ts = clk->samp_t[sidx];
+  if (sidx < n) {
+    const int ts = clk->samp_t[clk->job_off + sidx];
     const double ph = (double)(float)2.0 * 3.1415926535897932384626433832795 * (ts + (h ? 0.5 : 1.0)) * d.dt * d.freq[f];
     sincos(ph, &sv, &c);
   }
   tw[q] = make_double2(c, sv);
 }
-__global__ void dft_twiddles(const __grid_constant__ DftView d, const DevClock* clk, double2* tw, int force) {
-  dft_twiddles_body(d, clk, tw, force);
+__global__ void dft_twiddles(const __grid_constant__ DftView d, const DevClock* clk, double2* tw) {
+  dft_twiddles_body(d, clk, tw);
 }
 
 // acc[f][r] += sum_s x[s][r] tw[h(r)][s][f] in FP64, as a real matrix
@@ -770,15 +803,15 @@ __device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, dou
 
 template <typename T>
 __device__ __forceinline__ void dft_contract_body(const DftView& d, const T* ring, const DevClock* clk,
-                                                  const double2* tw, int force) {
+                                                  const double2* tw) {
   extern __shared__ __align__(16) unsigned char dft_smem[];
   constexpr size_t kXs = sizeof(T) * kRingSlots * kDftXsPitch;
   T(*xs)[kDftXsPitch] = reinterpret_cast<T(*)[kDftXsPitch]>(dft_smem);
   double(*ar)[kDftAccPitch] = reinterpret_cast<double(*)[kDftAccPitch]>(dft_smem + kXs);
   double(*ai)[kDftAccPitch] = ar + kDftFreqs;
-  if (!dft_ring_ready(clk, force)) return;
-  const int nsamp = min(kRingSlots, clk->nsamp);
-  if (nsamp == 0) return;  // an empty ring adds nothing
+  const int nsamp = clk->job_n;
+  if (nsamp <= 0) return;  // an empty job adds nothing
+  ring += (size_t)clk->job_off * d.rows;
   const int nk = (nsamp + 3) & ~3;  // K padded to whole m8n8k4 steps with zero samples
   const long long r0 = (long long)blockIdx.x * kDftRows;
   if (r0 >= d.rows) return;  // batched launches size the grid for the largest simulation
@@ -862,14 +895,8 @@ __device__ __forceinline__ void dft_contract_body(const DftView& d, const T* rin
 }
 template <typename T>
 __global__ void __launch_bounds__(128) dft_contract(const __grid_constant__ DftView d, const T* ring,
-                                                     const DevClock* clk, const double2* tw, int force) {
-  dft_contract_body(d, ring, clk, tw, force);
-}
-
-// empties the ring after a contraction (the same condition as the
-// contraction kernels, which ran before it on the stream)
-__global__ void dft_reset_count(DevClock* clk, int force) {
-  if (dft_ring_ready(clk, force)) clk->nsamp = 0;
+                                                     const DevClock* clk, const double2* tw) {
+  dft_contract_body(d, ring, clk, tw);
 }
 
 // Per (box-face, frequency): sum over the face of Re(cEx conj(HY) -

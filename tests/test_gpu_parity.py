@@ -148,9 +148,11 @@ def test_graph_replay_equals_direct_launches():
 
 
 def test_spectra_read_mid_run():
-    """Reading the spectra contracts whatever the DFT sample ring holds (the
-    ring takes 64 samples, the stepper launches its contraction every 32);
-    the run then continues.  Only the grouping of the FP64 sums changes."""
+    """Reading the spectra contracts the samples that no contraction has
+    taken yet (the ring's halves take 64 samples each; the stepper contracts
+    a half beside the steps that fill the other); the run then continues in
+    the same contraction period, so its 128-step graph replays resume.
+    Only the grouping of the FP64 sums changes."""
     n = 420
     a = run_sim("sphere_au", n, F.FDTD_FP64)
     b = F.Sim(make(F, "sphere_au", precision=F.FDTD_FP64))
@@ -160,6 +162,7 @@ def test_spectra_read_mid_run():
         b.step(k)
         b.spectra()
     assert b.t == n
+    assert b.stats().graph_launches == 2  # steps 0-127, then 256-383 after the reads
     sa, sb = a.spectra(), b.spectra()
     for col in (1, 2, 3):
         assert rel(sb[:, col], sa[:, col]) < 1e-13, col
