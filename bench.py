@@ -346,7 +346,7 @@ def large_bench(mod, torch, stream, sp, dev, blocks=2, adjoint_steps=12000):
     free0, _ = torch.cuda.mem_get_info(dev)
     s = mod.Sim(large_params(mod), device=dev)
     free1, _ = torch.cuda.mem_get_info(dev)
-    s.step(BLOCK, sp)
+    s.step(2 * BLOCK, sp)  # warm-up: the two graphs of a DFT contraction period
     torch.cuda.synchronize()
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
     ev[0].record(stream)
@@ -572,8 +572,10 @@ def run_reference(args, rank, world):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
-    ap.add_argument("--warmup", type=int, default=3)
+    # a DFT contraction period is two bench steps (blocks): the defaults time
+    # whole periods
+    ap.add_argument("--steps", type=int, default=6)
+    ap.add_argument("--warmup", type=int, default=4)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -737,7 +739,7 @@ def main():
     if not args.no_fp64:
         sim64 = F.Sim(workload_params(F, F.FDTD_FP64, grid=args.grid, NUM_freq=args.num_freq),
                       device=dev)
-        for _ in range(max(1, args.warmup)):
+        for _ in range(max(2, args.warmup)):  # both graphs of a DFT contraction period
             sim64.step(BLOCK, sp)
         torch.cuda.synchronize()
         ms64, _ = timed_blocks(sim64, args.steps)
@@ -764,7 +766,7 @@ def main():
         for prec, name in ((F.FDTD_FP64, "f64"), (F.FDTD_FP32, "f32")):
             pr.precision = prec
             sm = F.Sim(pr, device=dev)
-            for _ in range(max(1, args.warmup)):
+            for _ in range(max(2, args.warmup)):  # both graphs of a DFT contraction period
                 sm.step(BLOCK, sp)
             torch.cuda.synchronize()
             msr, _ = timed_blocks(sm, args.steps)
@@ -800,6 +802,9 @@ def main():
                        "time_steps_per_step": BLOCK, "num_freq": d.num_freq,
                        "dispersive_cells": list(d.n_metal_cells),
                        "l2": "no flush: working set (403 MB of fields + 7 GB DFT) > 126 MB L2",
+                       "dft_period": "one FP64 contraction of 64 samples per 2 steps (blocks), beside the "
+                                     "steps; the timed steps " + ("cover whole periods" if args.steps % 2 == 0
+                                                                  else "end half a period off (odd --steps)"),
                        "tuning": {k: getattr(tune, k) for k in ("h_stages", "h_minb", "h_ty", "h_kchunk", "h_eminb", "h_estages", "e_stages", "e_minb", "e_ty", "e_kchunk", "e_eminb", "e_estages", "h_pdl", "e_pdl", "h_ms", "e_ms")},
                        "parallelism": f"replicas x{world}"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,

@@ -99,3 +99,32 @@ def test_runner_writes_reflectivity_files(tmp_path):
     want = np.c_[ref[1:, 0], ref[1:, 1], -ref[1:, 2], amp, ref[1:, 1] * amp, -ref[1:, 2] * amp]
     np.testing.assert_allclose(got, want, rtol=1e-6, atol=1e-12)
     s.close()
+
+
+def test_reflectance_error_table():
+    """The error of R and T against the FP64 oracle, FP64 and FP32 builds,
+    max over wavelengths; written as a table to the path in
+    FDTD_PARITY_REPORT_PERIODIC when set."""
+    rows = []
+    for name in NAMES:
+        ro = None
+        errs = []
+        for prec in (F.FDTD_FP64, F.FDTD_FP32):
+            p = make(F, name, precision=prec)
+            s = F.Sim(p)
+            s.run()
+            r = s.reflectance()
+            s.close()
+            if ro is None:
+                o = O.OracleSim(make(O, name))
+                o.step(p.Tend + 1)
+                ro = o.reflectance()
+            errs += [float(np.abs(r[:, 1] - ro[:, 1]).max()), float(np.abs(r[:, 2] - ro[:, 2]).max())]
+        assert max(errs[:2]) < 1e-9 and max(errs[2:]) < 1e-4, (name, errs)
+        rows.append((name, errs, float(ro[:, 1].max()), float(ro[:, 2].min())))
+    path = os.environ.get("FDTD_PARITY_REPORT_PERIODIC")
+    if path:
+        with open(path, "w") as f:
+            f.write("| case | max R | min T | FP64 R | FP64 T | FP32 R | FP32 T |\n|---|---|---|---|---|---|---|\n")
+            for name, e, rmax, tmin in rows:
+                f.write(f"| {name} | {rmax:.3f} | {tmin:.3f} | " + " | ".join("%.1e" % x for x in e) + " |\n")
