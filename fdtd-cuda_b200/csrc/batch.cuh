@@ -14,7 +14,9 @@
 //   e_pass_batch      two persistent grids as for H
 //   metal_e           one launch
 //   dft_sample        one launch every dft_every steps, blockIdx.z = member
-//   twiddles + contraction + reset, one launch each, every 32 samples
+//   the DFT contraction (job, phasors, product, reset), one launch each,
+//                     every 32 samples; it contracts each member's first
+//                     ring half once that holds 64 samples
 // so the launch count per step does not grow with the member count, and
 // small members that could not fill the GPU alone share it.  Runs of
 // 32 * dft_every steps are captured into one CUDA graph and replayed.
