@@ -424,15 +424,18 @@ fdtd_status fdtd_get_material(fdtd_sim* s, uint8_t* out, size_t count);
  * per-cell ADE update with linearly blended coefficients. */
 fdtd_status fdtd_set_design(fdtd_sim* s, const int box[6], const float* rho,
                             size_t count);
-/* Forward with checkpoints: zeroes the state, runs t = 0..Tend and keeps a
- * copy of the state every checkpoint_every steps for the reverse sweep.
- * out19 (NUM_freq x 19, may be NULL) gets the ScatAbs table of
- * fdtd_spectral_finalize. */
+/* Forward for the reverse sweep: zeroes the state and runs t = 0..Tend in
+ * segments of checkpoint_every steps.  The last segments, as many as the
+ * device memory holds (env FDTD_ADJ_RECORD_GB caps it; at least one),
+ * record the dispersive cells' trajectory as they run; every earlier
+ * segment starts with a copy of the state, from which the backward
+ * recomputes it.  fdtd_get_stats reports the split.  out19 (NUM_freq x 19,
+ * may be NULL) gets the ScatAbs table of fdtd_spectral_finalize. */
 fdtd_status fdtd_forward_spectra(fdtd_sim* s, int checkpoint_every,
                                  double* out19);
-/* Reverse-time adjoint of the last forward, with segment recompute, for
- * the objective whose gradient with respect to the ScatAbs table is
- * dL_dspectra (NUM_freq x 19, row major): any weighted sum of the
+/* Reverse-time adjoint of the last forward (recomputing the segments that
+ * were not recorded), for the objective whose gradient with respect to the
+ * ScatAbs table is dL_dspectra (NUM_freq x 19, row major): any weighted sum of the
  * scattering, absorption and extinction columns and of the 12 face
  * fluxes (columns 1-15; columns 0 and 16-18 do not depend on the fields
  * and must be zero).  dL_drho (may be NULL) has the design box's cell
