@@ -1463,10 +1463,10 @@ extern "C" fdtd_status fdtd_check(fdtd_sim* s) {
 // ---------------------------------------------------------------------
 // spectra
 
-// Contracts what the device ring holds (nothing when it is empty).
-// (the callers have synchronised the device, so no contraction is in flight)
-// The samples of the half being filled that no contraction has taken; the
-// stepper's contraction period goes on where it was.
+// Contracts the samples of the ring half being filled that no contraction
+// has taken (nothing when there are none); the stepper's contraction period
+// goes on where it was.  The callers have synchronised the device, so no
+// forked contraction is in flight.
 static fdtd_status flush_dft(fdtd_sim* s) {
   if (s->dft.rows > 0 && s->line.dft_every > 0) {
     dft_job_flush<<<1, 1>>>(s->clk);
