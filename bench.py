@@ -805,7 +805,7 @@ def main():
                        "dft_period": "one FP64 contraction of 64 samples per 2 steps (blocks), beside the "
                                      "steps; the timed steps " + ("cover whole periods" if args.steps % 2 == 0
                                                                   else "end half a period off (odd --steps)"),
-                       "tuning": {k: getattr(tune, k) for k in ("h_stages", "h_minb", "h_ty", "h_kchunk", "h_eminb", "h_estages", "e_stages", "e_minb", "e_ty", "e_kchunk", "e_eminb", "e_estages", "h_pdl", "e_pdl", "h_ms", "e_ms")},
+                       "tuning": {k: getattr(tune, k) for k in ("h_stages", "h_minb", "h_ty", "h_kchunk", "h_eminb", "h_estages", "e_stages", "e_minb", "e_ty", "e_kchunk", "e_eminb", "e_estages", "h_pdl", "e_pdl", "h_tma", "h_etma", "e_tma", "e_etma", "h_ms", "e_ms")},
                        "parallelism": f"replicas x{world}"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "clocks": clk.summary(), "gpu_launches": launches, "fp64": fp64,

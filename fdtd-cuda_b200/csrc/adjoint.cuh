@@ -1105,7 +1105,7 @@ __global__ void __launch_bounds__(32 * kAdjTY) adj_gather_h_staged(const __grid_
   T* __restrict__ phy = a.lH[1] + id0;
   T* __restrict__ phz = a.lH[2] + id0;
   const int o = ty * L::HW + tx, oo = ty * 32 + tx;
-  constexpr int FH = (TY + 1) * L::HW;
+  constexpr int FH = L::FH;
   for (int k = k0; k < k1;) {
 #pragma unroll
     for (int u = 0; u < S; u++) {
@@ -1175,7 +1175,7 @@ __global__ void __launch_bounds__(32 * kAdjTY) adj_gather_e_staged(const __grid_
   T* __restrict__ pey = a.lE[1] + id0;
   T* __restrict__ pez = a.lE[2] + id0;
   const int o = (ty + 1) * L::HW + tx + L::CH, oo = ty * 32 + tx;
-  constexpr int FH = (TY + 1) * L::HW;
+  constexpr int FH = L::FH;
   for (int k = k0; k < k1;) {
 #pragma unroll
     for (int u = 0; u < S; u++) {

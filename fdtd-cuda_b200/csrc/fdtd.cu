@@ -77,7 +77,7 @@ struct fdtd_sim {
   // (interior tiles: minb/stages, CPML edge tiles: eminb/estages)
   // pdl = 1: the edge and interior launches of a pass go on one stream
   // with a programmatic dependency instead of on two streams
-  struct PassCfg { int minb = 1, ty = 4, kchunk = 16, staged = 1, stages = 4, eminb = 1, estages = 4, pdl = 0; float ms = 0; };
+  struct PassCfg { int minb = 1, ty = 4, kchunk = 16, staged = 1, stages = 4, eminb = 1, estages = 4, pdl = 0, tma = 0, etma = 0; float ms = 0; };
   // pass tiles for one (tile height, z-chunk): the interior box of tiles
   // that touch no CPML slab and the table of the others
   struct TileSet {
@@ -87,6 +87,14 @@ struct fdtd_sim {
     unsigned nedge = 0;
   };
   std::vector<TileSet> tilesets;
+  // tensor maps of the field arrays for the tensor-copy staging of the
+  // passes, one set per tile height (0 = the encoder is not available)
+  struct TmaSet {
+    int ty = 0;
+    TmaMaps h, e;  // H pass: halo E, own H; E pass: halo H, own E
+  };
+  std::vector<TmaSet> tmasets;
+  int tma_avail = -1;  // -1 not yet known
   ShellCells shell_h, shell_e;
   TfsfTable tf_h{}, tf_e{};  // tabulated TFSF corrections of the two shells
   const void* dview = nullptr;  // device copy of the view
@@ -840,7 +848,66 @@ MetalView<double>& mview<double>(fdtd_sim* s) { return s->md; }
 
 template <typename T, int TY, int S>
 static size_t staged_smem() {
-  return (size_t)S * StageLayout<T, TY>::STAGE * sizeof(T);
+  return (size_t)S * StageLayout<T, TY>::STAGE * sizeof(T) + (size_t)S * 8;  // ring + its mbarriers
+}
+
+// The tensor maps of one tile height: each field component as a {PX, NY,
+// NZ} array (row and plane pitches in bytes), the halo family's tile
+// (32 + CH) x (TY + 1) and the own family's 32 x TY, zero fill outside.
+// Null when the driver's encoder is not available or refuses a map (the
+// passes then stage with cp.async).
+using EncodeTiledFn = decltype(&cuTensorMapEncodeTiled);
+static EncodeTiledFn tensor_map_encoder() {
+  static EncodeTiledFn fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+template <typename T>
+static const fdtd_sim::TmaSet* tma_maps(fdtd_sim* s, int ty) {
+  if (s->tma_avail == 0) return nullptr;
+  for (const auto& m : s->tmasets)
+    if (m.ty == ty) return &m;
+  EncodeTiledFn enc = tensor_map_encoder();
+  if (!enc || s->su.p.periodic_xy) {
+    s->tma_avail = 0;
+    return nullptr;
+  }
+  constexpr int CH = 16 / (int)sizeof(T);
+  const CUtensorMapDataType dt = sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  const cuuint64_t dims[3] = {(cuuint64_t)s->PX, (cuuint64_t)s->NY, (cuuint64_t)s->NZ};
+  const cuuint64_t strides[2] = {(cuuint64_t)s->PX * sizeof(T), (cuuint64_t)s->plane * sizeof(T)};
+  const cuuint32_t halo_box[3] = {(cuuint32_t)(32 + CH), (cuuint32_t)(ty + 1), 1};
+  const cuuint32_t own_box[3] = {32, (cuuint32_t)ty, 1};
+  const cuuint32_t unit[3] = {1, 1, 1};
+  fdtd_sim::TmaSet m;
+  m.ty = ty;
+  bool ok = true;
+  auto encode = [&](CUtensorMap* map, const void* base, const cuuint32_t* box) {
+    ok = ok && enc(map, dt, 3, const_cast<void*>(base), dims, strides, box, unit, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                   CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+  };
+  for (int a = 0; a < 3; a++) {
+    encode(&m.h.halo[a], s->E[a], halo_box);
+    encode(&m.h.own[a], s->H[a], own_box);
+    encode(&m.e.halo[a], s->H[a], halo_box);
+    encode(&m.e.own[a], s->E[a], own_box);
+  }
+  if (!ok) {
+    s->tma_avail = 0;
+    return nullptr;
+  }
+  s->tma_avail = 1;
+  s->tmasets.push_back(m);
+  return &s->tmasets.back();
 }
 
 // Staged-pass variants: tile height TY and a register cap given as the
@@ -861,6 +928,14 @@ static void staged_attributes() {
   cudaFuncSetAttribute(e_pass_s<T, TY, S, MB, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,   \
                        (int)staged_smem<T, TY, S>());                                                \
   cudaFuncSetAttribute(e_pass_s<T, TY, S, MB, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,    \
+                       (int)staged_smem<T, TY, S>());                                                \
+  cudaFuncSetAttribute(h_pass_t<T, TY, S, MB, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,   \
+                       (int)staged_smem<T, TY, S>());                                                \
+  cudaFuncSetAttribute(h_pass_t<T, TY, S, MB, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,    \
+                       (int)staged_smem<T, TY, S>());                                                \
+  cudaFuncSetAttribute(e_pass_t<T, TY, S, MB, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,   \
+                       (int)staged_smem<T, TY, S>());                                                \
+  cudaFuncSetAttribute(e_pass_t<T, TY, S, MB, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,    \
                        (int)staged_smem<T, TY, S>());
   FDTD_STAGED_VARIANTS(FDTD_ATTR)
 #undef FDTD_ATTR
@@ -915,47 +990,39 @@ static const fdtd_sim::TileSet& tiles(const fdtd_sim* s, const fdtd_sim::PassCfg
 // One launch of a pass variant over a tile map (box grid or table); pdl =
 // true gives it a programmatic dependency on the launch before it on the
 // stream.
-template <typename T, bool PML>
-static void launch_h_variant(fdtd_sim* s, int ty, int mb, int sg, dim3 g, const TileMap& tm, int kchunk,
-                             cudaStream_t st, bool pdl = false) {
-#define FDTD_LAUNCH(TY, MB, S)                                                                   \
-  if (ty == TY && mb == MB && sg == S) {                                                         \
-    if (pdl) {                                                                                   \
-      cudaLaunchConfig_t cfg = {};                                                               \
-      cfg.gridDim = g; cfg.blockDim = dim3(32, TY); cfg.dynamicSmemBytes = staged_smem<T, TY, S>(); cfg.stream = st; \
-      cudaLaunchAttribute at[1];                                                                 \
-      at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;                             \
-      at[0].val.programmaticStreamSerializationAllowed = 1;                                      \
-      cfg.attrs = at; cfg.numAttrs = 1;                                                          \
-      cudaLaunchKernelEx(&cfg, h_pass_s<T, TY, S, MB, PML>, view<T>(s), kchunk, tm);             \
-    } else {                                                                                     \
-      h_pass_s<T, TY, S, MB, PML><<<g, dim3(32, TY), staged_smem<T, TY, S>(), st>>>(view<T>(s), kchunk, tm); \
-    }                                                                                            \
-    return;                                                                                      \
+// One launch of a pass variant: the cp.async or (tma) the tensor-copy
+// staging, optionally with a programmatic dependency on the previous
+// launch of the stream.
+template <typename T, bool PML, bool EPASS>
+static void launch_variant(fdtd_sim* s, int ty, int mb, int sg, bool tma, dim3 g, const TileMap& tm, int kchunk,
+                           cudaStream_t st, bool pdl = false) {
+  const fdtd_sim::TmaSet* maps = tma ? tma_maps<T>(s, ty) : nullptr;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+#define FDTD_LAUNCH(TY, MB, S)                                                                             \
+  if (ty == TY && mb == MB && sg == S) {                                                                   \
+    cudaLaunchConfig_t cfg = {};                                                                           \
+    cfg.gridDim = g; cfg.blockDim = dim3(32, TY); cfg.dynamicSmemBytes = staged_smem<T, TY, S>(); cfg.stream = st; \
+    cfg.attrs = at; cfg.numAttrs = pdl ? 1 : 0;                                                            \
+    if (maps && EPASS) cudaLaunchKernelEx(&cfg, e_pass_t<T, TY, S, MB, PML>, view<T>(s), kchunk, tm, maps->e); \
+    else if (maps) cudaLaunchKernelEx(&cfg, h_pass_t<T, TY, S, MB, PML>, view<T>(s), kchunk, tm, maps->h);  \
+    else if (EPASS) cudaLaunchKernelEx(&cfg, e_pass_s<T, TY, S, MB, PML>, view<T>(s), kchunk, tm);           \
+    else cudaLaunchKernelEx(&cfg, h_pass_s<T, TY, S, MB, PML>, view<T>(s), kchunk, tm);                      \
+    return;                                                                                                \
   }
   FDTD_STAGED_VARIANTS(FDTD_LAUNCH)
 #undef FDTD_LAUNCH
 }
 template <typename T, bool PML>
-static void launch_e_variant(fdtd_sim* s, int ty, int mb, int sg, dim3 g, const TileMap& tm, int kchunk,
+static void launch_h_variant(fdtd_sim* s, int ty, int mb, int sg, bool tma, dim3 g, const TileMap& tm, int kchunk,
                              cudaStream_t st, bool pdl = false) {
-#define FDTD_LAUNCH(TY, MB, S)                                                                   \
-  if (ty == TY && mb == MB && sg == S) {                                                         \
-    if (pdl) {                                                                                   \
-      cudaLaunchConfig_t cfg = {};                                                               \
-      cfg.gridDim = g; cfg.blockDim = dim3(32, TY); cfg.dynamicSmemBytes = staged_smem<T, TY, S>(); cfg.stream = st; \
-      cudaLaunchAttribute at[1];                                                                 \
-      at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;                             \
-      at[0].val.programmaticStreamSerializationAllowed = 1;                                      \
-      cfg.attrs = at; cfg.numAttrs = 1;                                                          \
-      cudaLaunchKernelEx(&cfg, e_pass_s<T, TY, S, MB, PML>, view<T>(s), kchunk, tm);             \
-    } else {                                                                                     \
-      e_pass_s<T, TY, S, MB, PML><<<g, dim3(32, TY), staged_smem<T, TY, S>(), st>>>(view<T>(s), kchunk, tm); \
-    }                                                                                            \
-    return;                                                                                      \
-  }
-  FDTD_STAGED_VARIANTS(FDTD_LAUNCH)
-#undef FDTD_LAUNCH
+  launch_variant<T, PML, false>(s, ty, mb, sg, tma, g, tm, kchunk, st, pdl);
+}
+template <typename T, bool PML>
+static void launch_e_variant(fdtd_sim* s, int ty, int mb, int sg, bool tma, dim3 g, const TileMap& tm, int kchunk,
+                             cudaStream_t st, bool pdl = false) {
+  launch_variant<T, PML, true>(s, ty, mb, sg, tma, g, tm, kchunk, st, pdl);
 }
 
 // Launches one pass as its interior box (PML-free) and its edge table so
@@ -967,11 +1034,11 @@ static int launch_pass_cfg(fdtd_sim* s, const fdtd_sim::PassCfg& c, cudaStream_t
   const fdtd_sim::TileSet& ts = tiles(s, c);
   if (c.pdl && ts.inner.x && ts.nedge) {
     if (EPASS) {
-      launch_e_variant<T, true>(s, c.ty, c.eminb, c.estages, dim3(ts.nedge), ts.edge_map, c.kchunk, st);
-      launch_e_variant<T, false>(s, c.ty, c.minb, c.stages, ts.inner, ts.inner_map, c.kchunk, st, true);
+      launch_e_variant<T, true>(s, c.ty, c.eminb, c.estages, c.etma, dim3(ts.nedge), ts.edge_map, c.kchunk, st);
+      launch_e_variant<T, false>(s, c.ty, c.minb, c.stages, c.tma, ts.inner, ts.inner_map, c.kchunk, st, true);
     } else {
-      launch_h_variant<T, true>(s, c.ty, c.eminb, c.estages, dim3(ts.nedge), ts.edge_map, c.kchunk, st);
-      launch_h_variant<T, false>(s, c.ty, c.minb, c.stages, ts.inner, ts.inner_map, c.kchunk, st, true);
+      launch_h_variant<T, true>(s, c.ty, c.eminb, c.estages, c.etma, dim3(ts.nedge), ts.edge_map, c.kchunk, st);
+      launch_h_variant<T, false>(s, c.ty, c.minb, c.stages, c.tma, ts.inner, ts.inner_map, c.kchunk, st, true);
     }
     return 2;
   }
@@ -983,12 +1050,12 @@ static int launch_pass_cfg(fdtd_sim* s, const fdtd_sim::PassCfg& c, cudaStream_t
     est = s->side;
   }
   if (ts.nedge) {
-    if (EPASS) launch_e_variant<T, true>(s, c.ty, c.eminb, c.estages, dim3(ts.nedge), ts.edge_map, c.kchunk, est);
-    else launch_h_variant<T, true>(s, c.ty, c.eminb, c.estages, dim3(ts.nedge), ts.edge_map, c.kchunk, est);
+    if (EPASS) launch_e_variant<T, true>(s, c.ty, c.eminb, c.estages, c.etma, dim3(ts.nedge), ts.edge_map, c.kchunk, est);
+    else launch_h_variant<T, true>(s, c.ty, c.eminb, c.estages, c.etma, dim3(ts.nedge), ts.edge_map, c.kchunk, est);
   }
   if (ts.inner.x) {
-    if (EPASS) launch_e_variant<T, false>(s, c.ty, c.minb, c.stages, ts.inner, ts.inner_map, c.kchunk, st);
-    else launch_h_variant<T, false>(s, c.ty, c.minb, c.stages, ts.inner, ts.inner_map, c.kchunk, st);
+    if (EPASS) launch_e_variant<T, false>(s, c.ty, c.minb, c.stages, c.tma, ts.inner, ts.inner_map, c.kchunk, st);
+    else launch_h_variant<T, false>(s, c.ty, c.minb, c.stages, c.tma, ts.inner, ts.inner_map, c.kchunk, st);
   }
   if (fork) {
     cudaEventRecord(s->join_ev, s->side);
@@ -1034,6 +1101,11 @@ static fdtd_status tune_passes(fdtd_sim* s, bool time_variants) {
   }
   def.eminb = def.minb;
   def.estages = def.stages;
+  // FDTD_TMA=0 / 1 fixes the staging of both launches (cp.async / tensor
+  // copies) instead of timing both
+  const char* tma_env = std::getenv("FDTD_TMA");
+  const int tma_force = tma_env && (tma_env[0] == '0' || tma_env[0] == '1') ? tma_env[0] - '0' : -1;
+  if (tma_force == 1 && tma_maps<T>(s, def.ty)) def.tma = def.etma = 1;
   // FDTD_PDL=0 / 1 fixes how the two launches of a pass overlap (two
   // streams / one stream with a programmatic dependency) instead of timing
   // both
@@ -1070,9 +1142,11 @@ static fdtd_status tune_passes(fdtd_sim* s, bool time_variants) {
         probe.ty = ty; probe.kchunk = kc;
         const fdtd_sim::TileSet& ts = tiles(s, probe);
         float bin = ts.inner.x ? 1e30f : 0.f, bed = ts.nedge ? 1e30f : 0.f;
-        int in_mb = 1, in_sg = 4, ed_mb = 1, ed_sg = 4;
+        int in_mb = 1, in_sg = 4, ed_mb = 1, ed_sg = 4, in_tma = 0, ed_tma = 0;
         bool any = false;
-        for (const auto& v : variants) {
+        const bool tma_ok = tma_force != 0 && tma_maps<T>(s, ty) != nullptr;
+        for (const auto& v : variants)
+        for (int tm = tma_force == 1 && tma_ok ? 1 : 0; tm < (tma_ok ? 2 : 1); tm++) {
           if (v[0] != ty) continue;
           const size_t sm = sizeof(T) * (size_t)v[2] * (ty == 4 ? StageLayout<T, 4>::STAGE : StageLayout<T, 8>::STAGE);
           if (sm * std::max(1, v[1]) > 220 * 1024) continue;
@@ -1081,11 +1155,11 @@ static fdtd_status tune_passes(fdtd_sim* s, bool time_variants) {
             if (part == 0 ? !ts.inner.x : !ts.nedge) continue;
             auto go = [&]() {
               if (part == 0) {
-                if (pass == 0) launch_h_variant<T, false>(s, ty, v[1], v[2], ts.inner, ts.inner_map, kc, 0);
-                else launch_e_variant<T, false>(s, ty, v[1], v[2], ts.inner, ts.inner_map, kc, 0);
+                if (pass == 0) launch_h_variant<T, false>(s, ty, v[1], v[2], tm, ts.inner, ts.inner_map, kc, 0);
+                else launch_e_variant<T, false>(s, ty, v[1], v[2], tm, ts.inner, ts.inner_map, kc, 0);
               } else {
-                if (pass == 0) launch_h_variant<T, true>(s, ty, v[1], v[2], dim3(ts.nedge), ts.edge_map, kc, 0);
-                else launch_e_variant<T, true>(s, ty, v[1], v[2], dim3(ts.nedge), ts.edge_map, kc, 0);
+                if (pass == 0) launch_h_variant<T, true>(s, ty, v[1], v[2], tm, dim3(ts.nedge), ts.edge_map, kc, 0);
+                else launch_e_variant<T, true>(s, ty, v[1], v[2], tm, dim3(ts.nedge), ts.edge_map, kc, 0);
               }
             };
             go();
@@ -1097,10 +1171,11 @@ static fdtd_status tune_passes(fdtd_sim* s, bool time_variants) {
             CUDA_TRY(cudaEventElapsedTime(&ms, a, b));
             ms /= 3;
             if (verbose)
-              std::fprintf(stderr, "[fdtd tune] %s %s minb=%d ty=%d kchunk=%d stages=%d %.4f ms\n",
-                           pass == 0 ? "H" : "E", part == 0 ? "interior" : "edge", v[1], ty, kc, v[2], ms);
-            if (part == 0 && ms < bin) { bin = ms; in_mb = v[1]; in_sg = v[2]; }
-            if (part == 1 && ms < bed) { bed = ms; ed_mb = v[1]; ed_sg = v[2]; }
+              std::fprintf(stderr, "[fdtd tune] %s %s minb=%d ty=%d kchunk=%d stages=%d %s %.4f ms\n",
+                           pass == 0 ? "H" : "E", part == 0 ? "interior" : "edge", v[1], ty, kc, v[2],
+                           tm ? "tensor-copy" : "cp.async", ms);
+            if (part == 0 && ms < bin) { bin = ms; in_mb = v[1]; in_sg = v[2]; in_tma = tm; }
+            if (part == 1 && ms < bed) { bed = ms; ed_mb = v[1]; ed_sg = v[2]; ed_tma = tm; }
           }
         }
         if (!any) continue;
@@ -1109,6 +1184,7 @@ static fdtd_status tune_passes(fdtd_sim* s, bool time_variants) {
           best = fdtd_sim::PassCfg();
           best.staged = 1; best.ty = ty; best.kchunk = kc;
           best.minb = in_mb; best.stages = in_sg; best.eminb = ed_mb; best.estages = ed_sg;
+          best.tma = in_tma; best.etma = ed_tma;
           best.ms = tot;
         }
       }
@@ -1456,6 +1532,7 @@ extern "C" fdtd_status fdtd_check(fdtd_sim* s) {
   CUDA_TRY(cudaSetDevice(s->device));
   DevClock c;
   CUDA_TRY(cudaMemcpy(&c, s->clk, sizeof(c), cudaMemcpyDeviceToHost));
+  if (c.nonfinite & 2) return fail(FDTD_ERR_TIMEOUT, "a Yee pass gave up waiting for its plane copies");
   if (c.nonfinite) return fail(FDTD_ERR_NONFINITE, "non-finite field value detected");
   return FDTD_OK;
 }
@@ -1809,6 +1886,8 @@ extern "C" fdtd_status fdtd_get_stats(const fdtd_sim* s, fdtd_stats* out) {
   out->h_eminb = s->hcfg.eminb; out->h_estages = s->hcfg.estages;
   out->e_eminb = s->ecfg.eminb; out->e_estages = s->ecfg.estages;
   out->h_pdl = s->hcfg.pdl; out->e_pdl = s->ecfg.pdl;
+  out->h_tma = s->hcfg.tma; out->h_etma = s->hcfg.etma;
+  out->e_tma = s->ecfg.tma; out->e_etma = s->ecfg.etma;
   out->tfsf_entries_h = s->tf_h.n;
   out->tfsf_entries_e = s->tf_e.n;
   long long rows = 0;

@@ -31,7 +31,7 @@ static_assert(kRingSlots == 2 * kSampleBlock, "a contraction period is two launc
 struct DevClock {
   int t;          // steps completed by the 1D-line kernel (current step + 1)
   int nsamp;      // DFT samples in the half being filled
-  int nonfinite;  // watchdog flag
+  int nonfinite;  // watchdog flag: bit 0 NaN/Inf seen, bit 1 a pass gave up waiting for a plane copy
   int samp_slot;  // ring slot of the current step's DFT sample
   double e1, e2;  // Mur history of the incident line ends (main.cu:2835-2838)
   int base;       // first slot of the half being filled (0 or kRingSlots)

@@ -6,9 +6,11 @@
 //
 // Each CTA owns a 32 x TY tile of (x, y) columns and marches along z through
 // its z-chunk.  The planes it needs are streamed into a ring of S shared-
-// memory stages with 16-byte cp.async copies, so two planes of loads are in
-// flight while a third is computed, independent of occupancy.  Per plane a
-// stage holds
+// memory stages, so two planes of loads are in flight while a third is
+// computed, independent of occupancy: either every thread issues a share of
+// the plane's 16-byte cp.async copies, or one thread issues the plane's six
+// tensor copies (cp.async.bulk.tensor, completing on the stage's mbarrier);
+// the autotuner picks per launch.  Per plane a stage holds
 //   the "halo" family  (3 components, TY+1 rows, 32+CH columns): the field
 //                      read at the +-1 neighbours (E in the H pass, H in the
 //                      E pass), CH = 16 bytes / sizeof(T) columns of x halo
@@ -24,6 +26,8 @@
 // overlaps one plane of work; every psi element belongs to one cell and is
 // read and written only by that cell's thread.
 #pragma once
+#include <cuda.h>
+
 #include "kernels.cuh"
 
 namespace fdtd {
@@ -74,6 +78,64 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
 
+// Tensor-copy staging (the alternative to the per-thread cp.async tasks):
+// one thread of the CTA moves each plane's six component tiles with
+// cp.async.bulk.tensor into the stage and the copies complete on that
+// stage's mbarrier; every thread waits on the barrier's phase.  The tensor
+// maps describe each component array as a {PX, NY, NZ} box; the halo
+// family's tile is (32 + CH) x (TY + 1), the own family's 32 x TY, and
+// rows or columns outside the arrays read as zero.  No multicast.
+struct TmaMaps {
+  CUtensorMap halo[3];
+  CUtensorMap own[3];
+};
+
+__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
+}
+// makes the initialised barriers visible to the tensor-copy unit
+__device__ __forceinline__ void mbar_fence_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(unsigned bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
+  return t;
+}
+// Waits for the phase of the given parity to complete, for one second at
+// most; false when it gave up.
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  for (;;) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if (global_ns() - t0 > 1000000000ull) return false;
+  }
+}
+__device__ __forceinline__ void tma_load_3d(unsigned dst, const CUtensorMap* map, int x, int y, int z, unsigned bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];\n" ::"r"(
+          dst),
+      "l"(map), "r"(x), "r"(y), "r"(z), "r"(bar)
+      : "memory");
+}
+
 // Which tile a CTA of a pass owns: a box launch (grid = box of tiles,
 // origin added) or a table launch (one (bx, by, bz) entry per CTA).  The
 // passes are launched twice per half step: the interior box, whose tiles
@@ -92,13 +154,19 @@ __device__ __forceinline__ void tile_of(const TileMap& tm, int& bx, int& by, int
   }
 }
 
+// One stage of the ring: the three halo-family components ((TY + 1) rows of
+// HW, each component block starting on a 128-byte boundary, which a tensor
+// copy's destination needs), then the three own-family components (TY rows
+// of 32).
 template <typename T, int TY>
 struct StageLayout {
   static constexpr int CH = 16 / (int)sizeof(T);   // elements per 16-byte chunk
   static constexpr int HW = 32 + CH;               // halo row width
   static constexpr int NCH_HALO = HW / CH;         // chunks per halo row
   static constexpr int NCH_OWN = 32 / CH;          // chunks per own row
-  static constexpr int HALO = 3 * (TY + 1) * HW;   // elements per stage
+  static constexpr int AL = 128 / (int)sizeof(T);  // elements per 128 bytes
+  static constexpr int FH = ((TY + 1) * HW + AL - 1) / AL * AL;  // halo component stride
+  static constexpr int HALO = 3 * FH;              // elements per stage
   static constexpr int OWN = 3 * TY * 32;
   static constexpr int STAGE = HALO + OWN;
   static constexpr int TASKS_HALO = 3 * (TY + 1) * NCH_HALO;
@@ -141,7 +209,7 @@ struct CopyTasks {
         ch = rem - r * L::NCH_HALO;
         gj = j0 + halo_row0 + r;
         gi = i0 + halo_col0 + ch * L::CH;
-        d = (a * (TY + 1) + r) * L::HW + ch * L::CH;
+        d = a * L::FH + r * L::HW + ch * L::CH;
         base = a == 0 ? h0 : a == 1 ? h1 : h2;
         if (per) {
           // periodic x and y: the halo row -1 is row NY-1, row NY is row 0,
@@ -184,6 +252,82 @@ struct CopyTasks {
   }
 };
 
+// The stage ring filled by tensor copies.  The S mbarriers (one per stage,
+// arrival count 1) sit after the ring; a stage's barrier completes one
+// phase per plane copied into it, so the parity a wait needs is the lowest
+// bit of the stage's use count.  Only thread (0, 0) issues.  Planes beyond
+// the last one the chunk reads are not copied, so every copy issued is
+// waited for inside the plane loop; a plane outside [0, NZ) is not copied
+// either (no value computed from it is stored) and its phase completes by
+// a plain arrival.  A wait gives up after a second: the thread sets bit 2
+// of the watchdog word and skips its later waits, the issuing thread stops
+// issuing and, before the CTA ends, waits (again for a second at most) for
+// the copies it has in flight.
+template <typename T, int TY, int S>
+struct TmaRing {
+  using L = StageLayout<T, TY>;
+  static constexpr unsigned SB = L::STAGE * sizeof(T);
+  static constexpr unsigned HB = (TY + 1) * L::HW * sizeof(T);  // bytes of one halo tile
+  static constexpr unsigned OB = TY * 32 * sizeof(T);           // bytes of one own tile
+  unsigned sbase, bar0;
+  int hx, hy, i0, j0;  // tile origins of the halo and own families
+  int pfirst, plast;   // first and last plane of the chunk's ring
+  int pdone;           // one past the last plane issued
+  bool lead, bad;
+
+  __device__ __forceinline__ void init(unsigned sbase_, int hx_, int hy_, int i0_, int j0_, int pfirst_,
+                                       int plast_, int* flag) {
+    sbase = sbase_;
+    bar0 = sbase + S * SB;
+    hx = hx_; hy = hy_; i0 = i0_; j0 = j0_;
+    pfirst = pdone = pfirst_;
+    plast = plast_;
+    lead = threadIdx.x == 0 && threadIdx.y == 0;
+    bad = false;
+    if (lead) {
+#pragma unroll
+      for (int q = 0; q < S; q++) mbar_init(bar0 + 8 * q, 1);
+      mbar_fence_init();
+      // the tile destinations need 128-byte alignment
+      if (sbase & 127) {
+        bad = true;
+        atomicOr(flag, 2);
+      }
+    }
+    __syncthreads();
+  }
+  __device__ __forceinline__ void issue(const TmaMaps& m, int st, int p, int NZ) {
+    if (!lead || bad || p > plast) return;
+    const unsigned bar = bar0 + 8 * st, stage = sbase + st * SB;
+    pdone = p + 1;
+    if ((unsigned)p >= (unsigned)NZ) {
+      mbar_arrive(bar);
+      return;
+    }
+    mbar_expect_tx(bar, 3 * (HB + OB));
+#pragma unroll
+    for (int a = 0; a < 3; a++) tma_load_3d(stage + a * L::FH * sizeof(T), &m.halo[a], hx, hy, p, bar);
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+      tma_load_3d(stage + (L::HALO + a * TY * 32) * sizeof(T), &m.own[a], i0, j0, p, bar);
+  }
+  __device__ __forceinline__ void wait(int st, int use, int* flag) {
+    if (bad) return;
+    if (!mbar_wait(bar0 + 8 * st, (unsigned)use & 1u)) {
+      bad = true;
+      atomicOr(flag, 2);
+    }
+  }
+  __device__ __forceinline__ void drain() {
+    if (!lead || !bad) return;
+#pragma unroll
+    for (int st = 0; st < S; st++) {
+      const int n = pdone > pfirst + st ? (pdone - pfirst - st + S - 1) / S : 0;  // planes issued into st
+      if (n > 0) mbar_wait(bar0 + 8 * st, (unsigned)(n - 1) & 1u);
+    }
+  }
+};
+
 // ---------------------------------------------------------------------
 // H pass (UPDATE_hx/hy/hz, main.cu:762-1044).
 // Needs E at k and k+1 (halo family) and H at k (own family).  hx is
@@ -193,8 +337,9 @@ struct CopyTasks {
 // hy: z then x; hz: x then y).  The stage ring is counted from the chunk's
 // first plane and the plane loop is unrolled by S, so every stage offset is
 // a compile-time constant.
-template <typename T, int TY, int S, bool PML>
-__device__ __forceinline__ void h_pass_tile(const SimView<T>& s, int kchunk, int bx, int by, int bz) {
+template <typename T, int TY, int S, bool PML, bool TMA = false>
+__device__ __forceinline__ void h_pass_tile(const SimView<T>& s, int kchunk, int bx, int by, int bz,
+                                            const TmaMaps* maps = nullptr) {
   using L = StageLayout<T, TY>;
   constexpr unsigned SB = L::STAGE * sizeof(T);  // stage bytes
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -209,13 +354,20 @@ __device__ __forceinline__ void h_pass_tile(const SimView<T>& s, int kchunk, int
   const int k1 = min(NZ, k0 + kchunk);
   const T* any = s.E[0];
   CopyTasks<T, TY> tasks;
-  tasks.init(sbase, s.E[0], s.E[1], s.E[2], s.H[0], s.H[1], s.H[2], NX, NY, PX, plane, k0, i0, j0, 0, 0,
-             s.periodic != 0);
+  TmaRing<T, TY, S> ring;
   int pnext = k0;
+  if constexpr (TMA) {
+    ring.init(sbase, i0, j0, i0, j0, k0, k1, s.nonfinite);  // planes k0 .. k1
 #pragma unroll
-  for (int q = 0; q < S - 1; q++) {  // prologue: planes k0 .. k0+S-2 into stages 0 .. S-2
-    tasks.issue(q * SB, pnext++, NZ, any, plane);
-    cp_async_commit();
+    for (int q = 0; q < S - 1; q++) ring.issue(*maps, q, pnext++, NZ);
+  } else {
+    tasks.init(sbase, s.E[0], s.E[1], s.E[2], s.H[0], s.H[1], s.H[2], NX, NY, PX, plane, k0, i0, j0, 0, 0,
+               s.periodic != 0);
+#pragma unroll
+    for (int q = 0; q < S - 1; q++) {  // prologue: planes k0 .. k0+S-2 into stages 0 .. S-2
+      tasks.issue(q * SB, pnext++, NZ, any, plane);
+      cp_async_commit();
+    }
   }
   const bool live = i < NX && j < NY;
   // periodic x and y: every column has its +x and +y neighbour
@@ -230,7 +382,7 @@ __device__ __forceinline__ void h_pass_tile(const SimView<T>& s, int kchunk, int
   T* __restrict__ phy = s.H[1] + id0;
   T* __restrict__ phz = s.H[2] + id0;
   const int o = ty * L::HW + tx, oo = ty * 32 + tx;
-  constexpr int FH = (TY + 1) * L::HW;  // one halo component
+  constexpr int FH = L::FH;  // one halo component
   // CPML of this column: x and y slabs are fixed, z slabs follow the plane
   const bool pml_xy = PML && live && hasx && hasy;  // i < NX-1 and j < NY-1 (any column when periodic)
   SlabAt<T> sx, sy;
@@ -281,7 +433,8 @@ __device__ __forceinline__ void h_pass_tile(const SimView<T>& s, int kchunk, int
   T cex = T(0), cey = T(0);
   bool carry = false;
   T ikz_next = ldg(ikzp);
-  for (int k = k0; k < k1;) {
+  int use = 0;  // ring passes completed (the use count of stage u)
+  for (int k = k0; k < k1; use++) {
 #pragma unroll
     for (int u = 0; u < S; u++) {
       if (k < k1) {
@@ -289,11 +442,20 @@ __device__ __forceinline__ void h_pass_tile(const SimView<T>& s, int kchunk, int
         if (k + 1 < k1) fetch(k + 1, ox + xstep, oy + ystep);
         const T ikz = ikz_next;
         if (k + 1 < k1) ikz_next = ldg(ikzp + 1);
-        cp_async_wait<S - 3>();  // planes up to k+1 have landed
-        __syncthreads();
-        // stage (u+S-1)%S held plane k-1, last read in the previous iteration
-        tasks.issue(((u + S - 1) % S) * SB, pnext++, NZ, any, plane);
-        cp_async_commit();
+        // planes k and k+1 (stages u and u+1) have landed; then stage
+        // (u+S-1)%S, which held plane k-1 (last read in the previous
+        // iteration), takes plane k+S-1
+        if constexpr (TMA) {
+          ring.wait(u, use, s.nonfinite);
+          ring.wait((u + 1) % S, u + 1 < S ? use : use + 1, s.nonfinite);
+          __syncthreads();
+          ring.issue(*maps, (u + S - 1) % S, pnext++, NZ);
+        } else {
+          cp_async_wait<S - 3>();
+          __syncthreads();
+          tasks.issue(((u + S - 1) % S) * SB, pnext++, NZ, any, plane);
+          cp_async_commit();
+        }
         if (live) {
           const T* eh = sm + u * L::STAGE;
           const T* en = sm + ((u + 1) % S) * L::STAGE;
@@ -338,7 +500,8 @@ __device__ __forceinline__ void h_pass_tile(const SimView<T>& s, int kchunk, int
       }
     }
   }
-  cp_async_wait<0>();
+  if constexpr (TMA) ring.drain();
+  else cp_async_wait<0>();
 }
 // Programmatic dependent launch of the two launches of a pass on one
 // stream (the CPML edge tiles, then the interior box): the first lets the
@@ -357,6 +520,17 @@ __global__ void __launch_bounds__(32 * TY, MINB) h_pass_s(const __grid_constant_
   int bx, by, bz;
   tile_of(tm, bx, by, bz);
   h_pass_tile<T, TY, S, PML>(s, kchunk, bx, by, bz);
+  pdl_wait();
+}
+// The same with tensor-copy staging.
+template <typename T, int TY, int S, int MINB, bool PML>
+__global__ void __launch_bounds__(32 * TY, MINB) h_pass_t(const __grid_constant__ SimView<T> s, int kchunk,
+                                                      const __grid_constant__ TileMap tm,
+                                                      const __grid_constant__ TmaMaps maps) {
+  pdl_launch_dependents();
+  int bx, by, bz;
+  tile_of(tm, bx, by, bz);
+  h_pass_tile<T, TY, S, PML, true>(s, kchunk, bx, by, bz, &maps);
   pdl_wait();
 }
 
@@ -391,8 +565,9 @@ __global__ void __launch_bounds__(32 * TY, MINB) h_pass_batch(const SimView<T>* 
 // kernels update them, CPML included); dielectric classes select their
 // coefficients.  CPML per axis in the order z, y, x (ex: z then y; ey: z
 // then x; ez: y then x).  The stage ring is counted from plane k0-1.
-template <typename T, int TY, int S, bool PML>
-__device__ __forceinline__ void e_pass_tile(const SimView<T>& s, int kchunk, int bx, int by, int bz) {
+template <typename T, int TY, int S, bool PML, bool TMA = false>
+__device__ __forceinline__ void e_pass_tile(const SimView<T>& s, int kchunk, int bx, int by, int bz,
+                                            const TmaMaps* maps = nullptr) {
   using L = StageLayout<T, TY>;
   constexpr unsigned SB = L::STAGE * sizeof(T);
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -407,13 +582,20 @@ __device__ __forceinline__ void e_pass_tile(const SimView<T>& s, int kchunk, int
   const int k1 = min(NZ, k0 + kchunk);
   const T* any = s.H[0];
   CopyTasks<T, TY> tasks;
-  tasks.init(sbase, s.H[0], s.H[1], s.H[2], s.E[0], s.E[1], s.E[2], NX, NY, PX, plane, k0 - 1, i0, j0, -1,
-             -L::CH, s.periodic != 0);
+  TmaRing<T, TY, S> ring;
   int pnext = k0 - 1;
+  if constexpr (TMA) {
+    ring.init(sbase, i0 - L::CH, j0 - 1, i0, j0, k0 - 1, k1 - 1, s.nonfinite);  // planes k0-1 .. k1-1
 #pragma unroll
-  for (int q = 0; q < S - 1; q++) {  // prologue: planes k0-1 .. k0+S-3 into stages 0 .. S-2
-    tasks.issue(q * SB, pnext++, NZ, any, plane);
-    cp_async_commit();
+    for (int q = 0; q < S - 1; q++) ring.issue(*maps, q, pnext++, NZ);
+  } else {
+    tasks.init(sbase, s.H[0], s.H[1], s.H[2], s.E[0], s.E[1], s.E[2], NX, NY, PX, plane, k0 - 1, i0, j0, -1,
+               -L::CH, s.periodic != 0);
+#pragma unroll
+    for (int q = 0; q < S - 1; q++) {  // prologue: planes k0-1 .. k0+S-3 into stages 0 .. S-2
+      tasks.issue(q * SB, pnext++, NZ, any, plane);
+      cp_async_commit();
+    }
   }
   const bool live = i < NX && j < NY;
   // active-range masks of ex, ey, ez in this column (main.cu:1172, 1476, 1767)
@@ -434,7 +616,7 @@ __device__ __forceinline__ void e_pass_tile(const SimView<T>& s, int kchunk, int
   T* __restrict__ pey = s.E[1] + id0;
   T* __restrict__ pez = s.E[2] + id0;
   const int o = (ty + 1) * L::HW + tx + L::CH, oo = ty * 32 + tx;
-  constexpr int FH = (TY + 1) * L::HW;
+  constexpr int FH = L::FH;
   // CPML of this column: x and y slabs are fixed, z slabs follow the plane
   const bool pml_xy = PML && live && (per || (okx && oky));  // i < NX-1 and j < NY-1 (any column when periodic)
   SlabAt<T> sx, sy;
@@ -490,7 +672,8 @@ __device__ __forceinline__ void e_pass_tile(const SimView<T>& s, int kchunk, int
   T chx = T(0), chy = T(0);
   bool carry = false;
   T ikz_next = ldg(ikzp);
-  for (int k = k0; k < k1;) {
+  int use = 0;  // ring passes completed (the use count of stage u)
+  for (int k = k0; k < k1; use++) {
 #pragma unroll
     for (int u = 0; u < S; u++) {
       if (k < k1) {
@@ -498,11 +681,20 @@ __device__ __forceinline__ void e_pass_tile(const SimView<T>& s, int kchunk, int
         if (k + 1 < k1) fetch(k + 1, ox + xstep, oy + ystep);
         const T ikz = ikz_next;
         if (k + 1 < k1) ikz_next = ldg(ikzp + 1);
-        cp_async_wait<S - 3>();  // planes up to k have landed
-        __syncthreads();
-        // stage (u+S-1)%S held plane k-2, last read in the previous iteration
-        tasks.issue(((u + S - 1) % S) * SB, pnext++, NZ, any, plane);
-        cp_async_commit();
+        // planes k-1 and k (stages u and u+1) have landed; then stage
+        // (u+S-1)%S, which held plane k-2 (last read in the previous
+        // iteration), takes plane k+S-2
+        if constexpr (TMA) {
+          ring.wait(u, use, s.nonfinite);
+          ring.wait((u + 1) % S, u + 1 < S ? use : use + 1, s.nonfinite);
+          __syncthreads();
+          ring.issue(*maps, (u + S - 1) % S, pnext++, NZ);
+        } else {
+          cp_async_wait<S - 3>();
+          __syncthreads();
+          tasks.issue(((u + S - 1) % S) * SB, pnext++, NZ, any, plane);
+          cp_async_commit();
+        }
         if (live) {
           const T* cur = sm + ((u + 1) % S) * L::STAGE;
           const T* prv = sm + u * L::STAGE;
@@ -558,7 +750,8 @@ __device__ __forceinline__ void e_pass_tile(const SimView<T>& s, int kchunk, int
       }
     }
   }
-  cp_async_wait<0>();
+  if constexpr (TMA) ring.drain();
+  else cp_async_wait<0>();
   // NaN/Inf watchdog: a non-finite value makes the running sum non-finite
   if (!isfinite(check)) atomicOr(s.nonfinite, 1);
 }
@@ -569,6 +762,16 @@ __global__ void __launch_bounds__(32 * TY, MINB) e_pass_s(const __grid_constant_
   int bx, by, bz;
   tile_of(tm, bx, by, bz);
   e_pass_tile<T, TY, S, PML>(s, kchunk, bx, by, bz);
+  pdl_wait();
+}
+template <typename T, int TY, int S, int MINB, bool PML>
+__global__ void __launch_bounds__(32 * TY, MINB) e_pass_t(const __grid_constant__ SimView<T> s, int kchunk,
+                                                      const __grid_constant__ TileMap tm,
+                                                      const __grid_constant__ TmaMaps maps) {
+  pdl_launch_dependents();
+  int bx, by, bz;
+  tile_of(tm, bx, by, bz);
+  e_pass_tile<T, TY, S, PML, true>(s, kchunk, bx, by, bz, &maps);
   pdl_wait();
 }
 

@@ -110,7 +110,8 @@ class Stats(C.Structure):
                 ("tfsf_entries_h", C.c_longlong), ("tfsf_entries_e", C.c_longlong),
                 ("dft_rows", C.c_longlong),
                 ("adj_record_steps", C.c_longlong), ("adj_record_bytes", C.c_longlong),
-                ("adj_checkpoints", C.c_longlong)]
+                ("adj_checkpoints", C.c_longlong),
+                ("h_tma", C.c_int), ("h_etma", C.c_int), ("e_tma", C.c_int), ("e_etma", C.c_int)]
 
 
 class SnapshotLayout(C.Structure):

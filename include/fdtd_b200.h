@@ -262,7 +262,9 @@ fdtd_status fdtd_step(fdtd_sim* s, int nsteps, void* stream);
 fdtd_status fdtd_run(fdtd_sim* s, void* stream);
 fdtd_status fdtd_get_time(const fdtd_sim* s, int* t);
 
-/* Polls the device NaN/Inf watchdog; FDTD_ERR_NONFINITE if it fired. */
+/* Polls the device NaN/Inf watchdog; FDTD_ERR_NONFINITE if it fired,
+ * FDTD_ERR_TIMEOUT if a Yee pass gave up waiting (one second) for the
+ * tensor copies of a plane (the fields are then not valid). */
 fdtd_status fdtd_check(fdtd_sim* s);
 
 /* ---------------------------------------------------------------------- */
@@ -398,6 +400,10 @@ typedef struct fdtd_stats {
    * the others from checkpoints), the record's device bytes, and the number
    * of checkpoints kept */
   long long adj_record_steps, adj_record_bytes, adj_checkpoints;
+  /* how the launches of the passes stage their planes: 1 = tensor copies
+   * (one thread per CTA, completion on an mbarrier), 0 = per-thread
+   * cp.async; interior and edge launch of the H and E passes */
+  int h_tma, h_etma, e_tma, e_etma;
 } fdtd_stats;
 fdtd_status fdtd_get_stats(const fdtd_sim* s, fdtd_stats* out);
 /* Measurement hook (no counterpart in the reference): runs one Yee pass

@@ -272,6 +272,27 @@ def test_pass_overlap_modes_agree(prec, monkeypatch):
         np.testing.assert_array_equal(out[0][c], out[1][c])
 
 
+@pytest.mark.parametrize("prec", [F.FDTD_FP32, F.FDTD_FP64])
+def test_tensor_copy_staging_agrees(prec, monkeypatch):
+    """The two ways a pass fills its shared-memory ring (per-thread cp.async
+    copies, or tensor copies completing on an mbarrier) move the same
+    values, zero fill outside the grid included: fields are bit-identical,
+    for every tile height and ring depth."""
+    for spec in ("staged:4:6:16:4", "staged:8:3:8:4", "staged:4:6:32:6"):
+        monkeypatch.setenv("FDTD_PASS", spec)
+        out = []
+        for mode in ("0", "1"):
+            monkeypatch.setenv("FDTD_TMA", mode)
+            s = run_sim("sphere_big", 120, prec)
+            st = s.stats()
+            assert st.h_tma == st.h_etma == st.e_tma == st.e_etma == int(mode)
+            s.check()
+            out.append([s.field(c) for c in range(6)])
+            s.close()
+        for c in range(6):
+            np.testing.assert_array_equal(out[0][c], out[1][c])
+
+
 def test_unbuilt_pass_variant_is_rejected(monkeypatch):
     monkeypatch.setenv("FDTD_PASS", "staged:8:5:16:4")
     with pytest.raises(F.FdtdError) as e:
