@@ -910,9 +910,9 @@ static const fdtd_sim::TmaSet* tma_maps(fdtd_sim* s, int ty) {
   return &s->tmasets.back();
 }
 
-// Staged-pass variants: tile height TY and a register cap given as the
-// minimum number of resident CTAs per SM (MINB; 1 = no cap).
-// and the ring depth S (S-2 planes of lookahead beyond the ones in use).
+// Staged-pass variants: tile height TY, a register cap given as the
+// minimum number of resident CTAs per SM (MINB; 1 = no cap) and the ring
+// depth S (S-2 planes of lookahead beyond the ones in use).
 #define FDTD_STAGED_VARIANTS(X) X(4, 1, 4) X(4, 6, 4) X(4, 8, 4) X(8, 3, 4) X(4, 6, 6)
 
 // Opt the staged kernels into more than 48 KB of dynamic shared memory once.
@@ -987,12 +987,9 @@ static const fdtd_sim::TileSet& tiles(const fdtd_sim* s, const fdtd_sim::PassCfg
   return s->tilesets.front();  // unreachable: every configuration is built at create
 }
 
-// One launch of a pass variant over a tile map (box grid or table); pdl =
-// true gives it a programmatic dependency on the launch before it on the
-// stream.
-// One launch of a pass variant: the cp.async or (tma) the tensor-copy
-// staging, optionally with a programmatic dependency on the previous
-// launch of the stream.
+// One launch of a pass variant over a tile map (box grid or table): the
+// cp.async or (tma) the tensor-copy staging, optionally (pdl) with a
+// programmatic dependency on the launch before it on the stream.
 template <typename T, bool PML, bool EPASS>
 static void launch_variant(fdtd_sim* s, int ty, int mb, int sg, bool tma, dim3 g, const TileMap& tm, int kchunk,
                            cudaStream_t st, bool pdl = false) {
