@@ -292,24 +292,6 @@ static fdtd_status batch_upload_items(fdtd_batch* b, const std::vector<int>* onl
   return FDTD_OK;
 }
 
-// A launch with a programmatic dependency on the launch before it on the
-// stream (both persistent pass launches of a half step: the second fills
-// the tail of the first).
-template <typename... P, typename... A>
-static void launch_dependent(void (*kern)(P...), dim3 g, dim3 blk, size_t smem, cudaStream_t st, A&&... args) {
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = g;
-  cfg.blockDim = blk;
-  cfg.dynamicSmemBytes = smem;
-  cfg.stream = st;
-  cudaLaunchAttribute at[1];
-  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  at[0].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = at;
-  cfg.numAttrs = 1;
-  cudaLaunchKernelEx(&cfg, kern, std::forward<A>(args)...);
-}
-
 // One persistent pass launch of variant `var` over items [off, off + n),
 // counting its work from queue; pdl = a programmatic dependency on the
 // launch before it on the stream.
@@ -323,11 +305,11 @@ static void batch_pass_launch(fdtd_batch* b, int var, int grid, int off, int n, 
   if (mb == MB && sg == S) {                                                                                   \
     const size_t smem = staged_smem<T, kBatchTY, S>();                                                        \
     if (EPASS) {                                                                                              \
-      if (pdl) launch_dependent(e_pass_batch<T, kBatchTY, S, MB, PML>, dim3(grid), dim3(32, kBatchTY), smem,  \
+      if (pdl) launch_ex(true, e_pass_batch<T, kBatchTY, S, MB, PML>, dim3(grid), dim3(32, kBatchTY), smem,  \
                                 st, v, items, n, queue);                                                      \
       else e_pass_batch<T, kBatchTY, S, MB, PML><<<grid, dim3(32, kBatchTY), smem, st>>>(v, items, n, queue); \
     } else {                                                                                                  \
-      if (pdl) launch_dependent(h_pass_batch<T, kBatchTY, S, MB, PML>, dim3(grid), dim3(32, kBatchTY), smem,  \
+      if (pdl) launch_ex(true, h_pass_batch<T, kBatchTY, S, MB, PML>, dim3(grid), dim3(32, kBatchTY), smem,  \
                                 st, v, items, n, queue);                                                      \
       else h_pass_batch<T, kBatchTY, S, MB, PML><<<grid, dim3(32, kBatchTY), smem, st>>>(v, items, n, queue); \
     }                                                                                                         \

@@ -1026,18 +1026,24 @@ static void launch_e_variant(fdtd_sim* s, int ty, int mb, int sg, bool tma, dim3
 // that the two overlap: the edge launch on the side stream, or (c.pdl) the
 // edge launch then the interior launch with a programmatic dependency on
 // one stream; returns the number of launches.
+// chained (one-stream configurations only): the launch before this pass on
+// `st` triggers early and touches none of the pass's cells, so the pass's
+// first launch carries a programmatic dependency on it too.
 template <typename T, bool EPASS>
-static int launch_pass_cfg(fdtd_sim* s, const fdtd_sim::PassCfg& c, cudaStream_t st) {
+static int launch_pass_cfg(fdtd_sim* s, const fdtd_sim::PassCfg& c, cudaStream_t st, bool chained = false) {
   const fdtd_sim::TileSet& ts = tiles(s, c);
-  if (c.pdl && ts.inner.x && ts.nedge) {
-    if (EPASS) {
-      launch_e_variant<T, true>(s, c.ty, c.eminb, c.estages, c.etma, dim3(ts.nedge), ts.edge_map, c.kchunk, st);
-      launch_e_variant<T, false>(s, c.ty, c.minb, c.stages, c.tma, ts.inner, ts.inner_map, c.kchunk, st, true);
-    } else {
-      launch_h_variant<T, true>(s, c.ty, c.eminb, c.estages, c.etma, dim3(ts.nedge), ts.edge_map, c.kchunk, st);
-      launch_h_variant<T, false>(s, c.ty, c.minb, c.stages, c.tma, ts.inner, ts.inner_map, c.kchunk, st, true);
+  if (c.pdl && ((ts.inner.x && ts.nedge) || chained)) {
+    bool dep = chained;
+    if (ts.nedge) {
+      if (EPASS) launch_e_variant<T, true>(s, c.ty, c.eminb, c.estages, c.etma, dim3(ts.nedge), ts.edge_map, c.kchunk, st, dep);
+      else launch_h_variant<T, true>(s, c.ty, c.eminb, c.estages, c.etma, dim3(ts.nedge), ts.edge_map, c.kchunk, st, dep);
+      dep = true;
     }
-    return 2;
+    if (ts.inner.x) {
+      if (EPASS) launch_e_variant<T, false>(s, c.ty, c.minb, c.stages, c.tma, ts.inner, ts.inner_map, c.kchunk, st, dep);
+      else launch_h_variant<T, false>(s, c.ty, c.minb, c.stages, c.tma, ts.inner, ts.inner_map, c.kchunk, st, dep);
+    }
+    return (ts.inner.x ? 1 : 0) + (ts.nedge ? 1 : 0);
   }
   const bool fork = ts.inner.x && ts.nedge;
   cudaStream_t est = st;
@@ -1061,12 +1067,12 @@ static int launch_pass_cfg(fdtd_sim* s, const fdtd_sim::PassCfg& c, cudaStream_t
   return (ts.inner.x ? 1 : 0) + (ts.nedge ? 1 : 0);
 }
 template <typename T>
-static int launch_h_cfg(fdtd_sim* s, const fdtd_sim::PassCfg& c, cudaStream_t st) {
-  return launch_pass_cfg<T, false>(s, c, st);
+static int launch_h_cfg(fdtd_sim* s, const fdtd_sim::PassCfg& c, cudaStream_t st, bool chained = false) {
+  return launch_pass_cfg<T, false>(s, c, st, chained);
 }
 template <typename T>
-static int launch_e_cfg(fdtd_sim* s, const fdtd_sim::PassCfg& c, cudaStream_t st) {
-  return launch_pass_cfg<T, true>(s, c, st);
+static int launch_e_cfg(fdtd_sim* s, const fdtd_sim::PassCfg& c, cudaStream_t st, bool chained = false) {
+  return launch_pass_cfg<T, true>(s, c, st, chained);
 }
 
 // Autotuner: times every launch shape of the E and H passes on the zero
@@ -1221,6 +1227,24 @@ static fdtd_status tune_passes(fdtd_sim* s, bool time_variants) {
   return FDTD_OK;
 }
 
+// A launch on `st` that, when pdl is set, carries a programmatic dependency
+// on the launch before it on the stream: it may start once every CTA of
+// that launch has started, and orders itself with griddepcontrol.wait.
+template <typename... P, typename... A>
+static void launch_ex(bool pdl, void (*kern)(P...), dim3 g, dim3 blk, size_t smem, cudaStream_t st, A&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = g;
+  cfg.blockDim = blk;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = pdl ? 1 : 0;
+  cudaLaunchKernelEx(&cfg, kern, std::forward<A>(args)...);
+}
+
 // The split per-half entry points (fdtd_update_h / _line / _e) launch the
 // H pass + the H half of CORRECT_*, the line, then the E half + the E pass.
 template <typename T>
@@ -1238,7 +1262,7 @@ static void launch_line(fdtd_sim* s, cudaStream_t st) {
   s->kernels++;
 }
 template <typename T>
-static void launch_metal(fdtd_sim* s, cudaStream_t st);
+static void launch_metal(fdtd_sim* s, cudaStream_t st, bool chained = false);
 template <typename T>
 static void launch_e_pass(fdtd_sim* s, cudaStream_t st);
 
@@ -1270,6 +1294,15 @@ static void launch_e_pass(fdtd_sim* s, cudaStream_t st) {
   // dispersive E component and writes none, and the dispersive kernels read
   // E^n of their own cells and the final H only.
   const bool metal = s->nmetal[0] + s->nmetal[1] + s->nmetal[2] > 0;
+  if (metal && s->ecfg.pdl) {
+    // one stream, without a fork: the dispersive kernels, then the pass,
+    // each launch with a programmatic dependency on the one before (a
+    // dispersive phase waits for the previous phase at its start, the pass
+    // for the dispersive kernels at its end)
+    launch_metal<T>(s, st, true);
+    s->kernels += launch_e_cfg<T>(s, s->ecfg, st, true);
+    return;
+  }
   if (metal) {
     cudaEventRecord(s->fork2_ev, st);
     cudaStreamWaitEvent(s->side2, s->fork2_ev, 0);
@@ -1282,8 +1315,11 @@ static void launch_e_pass(fdtd_sim* s, cudaStream_t st) {
   }
 }
 
+// The dispersive cells' kernels; chained: the hydrodynamic phases after the
+// first carry a programmatic dependency on the phase before (they wait for
+// it at their start).
 template <typename T>
-static void launch_metal(fdtd_sim* s, cudaStream_t st) {
+static void launch_metal(fdtd_sim* s, cudaStream_t st, bool chained) {
   const int ntot = s->nmetal[0] + s->nmetal[1] + s->nmetal[2];
   if (ntot == 0) return;
   if (!s->su.hydro) {
@@ -1294,11 +1330,13 @@ static void launch_metal(fdtd_sim* s, cudaStream_t st) {
     hydro_p_ex<T><<<(ntot + 127) / 128, 128, 0, st>>>(view<T>(s), mview<T>(s), s->clk);
     s->kernels++;
     if (s->nmetal[1] > 0) {
-      hydro_e<T, 1><<<(s->nmetal[1] + 127) / 128, 128, 0, st>>>(view<T>(s), mview<T>(s), s->clk);
+      launch_ex(chained, hydro_e<T, 1>, dim3((s->nmetal[1] + 127) / 128), dim3(128), 0, st, view<T>(s), mview<T>(s),
+                (const DevClock*)s->clk);
       s->kernels++;
     }
     if (s->nmetal[2] > 0) {
-      hydro_e<T, 2><<<(s->nmetal[2] + 127) / 128, 128, 0, st>>>(view<T>(s), mview<T>(s), s->clk);
+      launch_ex(chained, hydro_e<T, 2>, dim3((s->nmetal[2] + 127) / 128), dim3(128), 0, st, view<T>(s), mview<T>(s),
+                (const DevClock*)s->clk);
       s->kernels++;
     }
   }
@@ -1352,23 +1390,33 @@ static void sample_and_contract(fdtd_sim* s, cudaStream_t st) {
   if (s->host_nsamp == kRingSlots) s->host_nsamp = 0;
 }
 
-// One full step.  The 1-D line step runs on the second side stream beside
-// the H pass: it reads the line, E at the probe cell and the clock, none of
-// which the H pass touches, and writes the line's other E buffer, so the H
-// half of CORRECT_* still sees the line's E from before the update, as in
-// the reference's order (UPDATE_h*, CORRECT_* H, UPDATE_h_inc/e_inc,
-// CORRECT_* E, UPDATE_e*).  Both TFSF halves then run as one launch.  Host
+// One full step.  The 1-D line step runs beside the H pass (on the second
+// side stream, or before it on the same stream with the pass launched as a
+// programmatic dependent when the pass's launches run on one stream): it
+// reads the line, E at the probe cell and the clock, none of which the H
+// pass touches, and writes the line's other E buffer, so the H half of
+// CORRECT_* still sees the line's E from before the update, as in the
+// reference's order (UPDATE_h*, CORRECT_* H, UPDATE_h_inc/e_inc, CORRECT_* E,
+// UPDATE_e*).  Both TFSF halves then run as one launch.  Host
 // mirrors of the clock decide which optional kernels run; the kernels read
 // t from the device.
 template <typename T>
 static void enqueue_step(fdtd_sim* s, cudaStream_t st) {
   dft_period_begin<T>(s, st);
-  cudaEventRecord(s->fork3_ev, st);
-  cudaStreamWaitEvent(s->side2, s->fork3_ev, 0);
-  launch_line<T>(s, s->side2);
-  s->kernels += launch_h_cfg<T>(s, s->hcfg, st);
-  cudaEventRecord(s->join3_ev, s->side2);
-  cudaStreamWaitEvent(st, s->join3_ev, 0);
+  if (s->hcfg.pdl) {
+    // one stream, without a fork: the line, then the H pass with a
+    // programmatic dependency on it (the pass starts at once and waits for
+    // the line at its end)
+    launch_line<T>(s, st);
+    s->kernels += launch_h_cfg<T>(s, s->hcfg, st, true);
+  } else {
+    cudaEventRecord(s->fork3_ev, st);
+    cudaStreamWaitEvent(s->side2, s->fork3_ev, 0);
+    launch_line<T>(s, s->side2);
+    s->kernels += launch_h_cfg<T>(s, s->hcfg, st);
+    cudaEventRecord(s->join3_ev, s->side2);
+    cudaStreamWaitEvent(st, s->join3_ev, 0);
+  }
   launch_tfsf<T>(s, st);
   launch_e_pass<T>(s, st);
   if (s->line.dft_every > 0 && s->t % s->line.dft_every == 0) sample_and_contract<T>(s, st);

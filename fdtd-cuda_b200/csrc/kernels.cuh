@@ -322,9 +322,21 @@ __device__ __forceinline__ void line_step_body(const LineArgs& a, const SimView<
     a.clk->t = t + 1;
   }
 }
+// Programmatic dependent launch.  A kernel that triggers lets the launch
+// after it on its stream, when that launch carries a programmatic
+// dependency, start its CTAs as soon as all of this one's have started;
+// griddepcontrol.wait in the later kernel then waits for the earlier one to
+// finish (and its writes to be visible).  Both are no-ops in a launch
+// without a programmatic dependency.
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+
+// The line step triggers at once: the H pass launched after it reads
+// nothing it writes (and waits for it at its own end).
 template <typename T>
 __global__ void __launch_bounds__(1024) line_step(const __grid_constant__ LineArgs a, const __grid_constant__ SimView<T> s,
                                                   size_t probe_id) {
+  pdl_launch_dependents();
   line_step_body(a, s, probe_id);
 }
 
@@ -453,6 +465,7 @@ __device__ __forceinline__ void metal_e_body(const SimView<T>& s, const MetalVie
 }
 template <typename T>
 __global__ void metal_e(const __grid_constant__ SimView<T> s, const __grid_constant__ MetalView<T> m, const DevClock* clk) {
+  pdl_launch_dependents();  // the E pass after it touches none of its cells
   metal_e_body(s, m, clk);
 }
 
@@ -628,6 +641,7 @@ __device__ __forceinline__ void hydro_p_cell(const SimView<T>& s, const MetalVie
 template <typename T>
 __global__ void hydro_p_ex(const __grid_constant__ SimView<T> s, const __grid_constant__ MetalView<T> m,
                            const DevClock* clk) {
+  pdl_launch_dependents();  // the next phase waits for this one itself; the E pass touches none of its cells
   const int t = clk->t - 1;
   int q = blockIdx.x * blockDim.x + threadIdx.x;
   int c = 0;
@@ -642,6 +656,8 @@ __global__ void hydro_p_ex(const __grid_constant__ SimView<T> s, const __grid_co
 template <typename T, int c>
 __global__ void hydro_e(const __grid_constant__ SimView<T> s, const __grid_constant__ MetalView<T> m,
                         const DevClock* clk) {
+  pdl_launch_dependents();
+  pdl_wait();  // the previous phase has finished
   const int t = clk->t - 1;
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= m.n[c]) return;

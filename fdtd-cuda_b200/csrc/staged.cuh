@@ -508,10 +508,10 @@ __device__ __forceinline__ void h_pass_tile(const SimView<T>& s, int kchunk, int
 // second start its CTAs as soon as all of its own are running, so the
 // second fills the first's tail, and the second waits, after its own work,
 // for the first to finish, so that its completion implies both.  The two
-// launches touch disjoint cells and read only the other field.  Both are
-// no-ops in a launch without a programmatic dependency.
-__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
-__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+// launches touch disjoint cells and read only the other field.  The first
+// may itself carry a programmatic dependency on the kernels before it on
+// the stream (the 1D line before the H pass, the dispersive kernels before
+// the E pass), which touch none of the pass's cells.
 
 template <typename T, int TY, int S, int MINB, bool PML>
 __global__ void __launch_bounds__(32 * TY, MINB) h_pass_s(const __grid_constant__ SimView<T> s, int kchunk,
