@@ -255,21 +255,33 @@ def test_pass_variants_agree(prec, monkeypatch):
 
 
 @pytest.mark.parametrize("prec", [F.FDTD_FP32, F.FDTD_FP64])
-def test_pass_overlap_modes_agree(prec, monkeypatch):
-    """The interior and CPML-edge launches of a pass write disjoint cells, so
-    running them on two streams or on one stream with a programmatic
-    dependency gives identical fields."""
+@pytest.mark.parametrize("nonlocal_", [0, 3])
+def test_pass_overlap_modes_agree(prec, nonlocal_, monkeypatch):
+    """The interior and CPML-edge launches of a pass write disjoint cells, and
+    the 1D line and the dispersive kernels touch none of the passes' cells,
+    so the two arrangements of a step give identical fields: the CPML tables
+    and the line and dispersive kernels on side streams (FDTD_PDL=0), or all
+    on one stream, each launch with a programmatic dependency on the one
+    before (FDTD_PDL=1), with the local Drude + 2CP model and with the
+    hydrodynamic model (three dependent phases).  The FP64 hydrodynamic run
+    is also checked against the oracle."""
     monkeypatch.setenv("FDTD_PASS", "staged:4:6:16:4")
+    steps = 300
     out = []
     for mode in ("0", "1"):
         monkeypatch.setenv("FDTD_PDL", mode)
-        s = run_sim("sphere_big", 150, prec)
+        s = run_sim("sphere_big", steps, prec, NONLOCAL=nonlocal_)
         st = s.stats()
         assert st.h_pdl == st.e_pdl == int(mode)
+        s.check()
         out.append([s.field(c) for c in range(6)])
         s.close()
     for c in range(6):
         np.testing.assert_array_equal(out[0][c], out[1][c])
+    if nonlocal_ and prec == F.FDTD_FP64:
+        o = oracle_run("sphere_big", steps, NONLOCAL=nonlocal_)
+        errs = field_errors(out[1], [o.field(c) for c in range(6)])
+        assert max(errs) < FP64_TOL, errs
 
 
 @pytest.mark.parametrize("prec", [F.FDTD_FP32, F.FDTD_FP64])
