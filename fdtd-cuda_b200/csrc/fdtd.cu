@@ -170,8 +170,9 @@ struct fdtd_sim {
   // interior launch (fork/join by events, also inside graph capture)
   cudaStream_t side = nullptr;
   cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
-  // second side stream: the dispersive-cell kernels run beside the E pass
-  // (they touch only dispersive components, which the pass skips)
+  // second side stream: the dispersive-cell kernels beside the E pass and
+  // the 1D line beside the H pass, when a pass's launches use two streams
+  // (they touch nothing the pass touches)
   cudaStream_t side2 = nullptr;
   cudaEvent_t fork2_ev = nullptr, join2_ev = nullptr;
   cudaEvent_t fork3_ev = nullptr, join3_ev = nullptr;  // the line step beside the H pass
@@ -1289,10 +1290,10 @@ static void launch_tfsf(fdtd_sim* s, cudaStream_t st) {
 
 template <typename T>
 static void launch_e_pass(fdtd_sim* s, cudaStream_t st) {
-  // The dispersive components (Drude + 2CP, hydrodynamic current) run on a
-  // second stream beside the E pass: the pass skips them, reads no
-  // dispersive E component and writes none, and the dispersive kernels read
-  // E^n of their own cells and the final H only.
+  // The dispersive components (Drude + 2CP, hydrodynamic current) run beside
+  // the E pass: the pass skips them, reads no dispersive E component and
+  // writes none, and the dispersive kernels read E^n of their own cells and
+  // the final H only.
   const bool metal = s->nmetal[0] + s->nmetal[1] + s->nmetal[2] > 0;
   if (metal && s->ecfg.pdl) {
     // one stream, without a fork: the dispersive kernels, then the pass,
