@@ -821,6 +821,9 @@ __device__ __forceinline__ T adj_h_coef_f(const SimView<T>& s, const AdjView<T>&
 
 // E sub-step transposed at the special slab components (the dispersive ones
 // are adj_e_design's): coefficients, psi_E adjoints, lambda_E <- cee lambda_E.
+// A cell's loads (its components' adjoints, psi adjoints and slab tables)
+// do not depend on one another and are all issued before the arithmetic and
+// the stores, which no load of the cell reads back.
 template <typename T>
 __global__ void adj_e_slab(const __grid_constant__ SimView<T> s, const __grid_constant__ AdjView<T> a,
                            const SlabShell sh) {
@@ -832,39 +835,57 @@ __global__ void adj_e_slab(const __grid_constant__ SimView<T> s, const __grid_co
   const unsigned m = adj_mat(s, i, j, k, id);
   const T cee = s.cee[m >> 3], ceh = s.ceh[m >> 3];
   const int ijk[3] = {i, j, k};
+  bool sp[3];
+  T lam[3], ik[3][2], old[3][2], bt[3][2], ct[3][2];
+  T* lp[3][2];
 #pragma unroll
   for (int c = 0; c < 3; c++) {
-    if ((m & (1u << c)) || !adj_e_special(s, c, i, j, k, m)) continue;
-    const T lam = a.lE[c][id];
+    sp[c] = !(m & (1u << c)) && adj_e_special(s, c, i, j, k, m);
+    lam[c] = sp[c] ? a.lE[c][id] : T(0);
+#pragma unroll
+    for (int sl = 0; sl < 2; sl++) {
+      const int ax = (c + 1 + sl) % 3;
+      const CpmlAxis<T>& cp = s.cp[ax];
+      lp[c][sl] = nullptr;
+      ik[c][sl] = old[c][sl] = bt[c][sl] = ct[c][sl] = T(0);
+      if (!sp[c]) continue;
+      ik[c][sl] = ldg(cp.inv_ked + ijk[ax]);
+      int qs;
+      lp[c][sl] = adj_psi(s, &a.lpE_N[c][sl], &a.lpE_F[c][sl], ax, true, i, j, k, &qs);
+      if (lp[c][sl]) {
+        if (qs >= 0) {
+          bt[c][sl] = ldg(cp.be_N + qs);
+          ct[c][sl] = ldg(((c == 1 && ax == 0) ? cp.ce_N_ey : cp.ce_N) + qs);
+        } else {
+          bt[c][sl] = ldg(cp.be_F + (-1 - qs));
+          ct[c][sl] = ldg(cp.ce_F + (-1 - qs));
+        }
+        old[c][sl] = *lp[c][sl];
+      }
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    if (!sp[c]) continue;
 #pragma unroll
     for (int sl = 0; sl < 2; sl++) {
       const int ax = (c + 1 + sl) % 3;
       const T sg = sl == 0 ? T(1) : T(-1);
-      const CpmlAxis<T>& cp = s.cp[ax];
-      T coef = sg * ceh * ldg(cp.inv_ked + ijk[ax]) * lam;
-      int qs;
-      T* lp = adj_psi(s, &a.lpE_N[c][sl], &a.lpE_F[c][sl], ax, true, i, j, k, &qs);
-      if (lp) {
-        T b, cc;
-        if (qs >= 0) {
-          b = ldg(cp.be_N + qs);
-          cc = ldg(((c == 1 && ax == 0) ? cp.ce_N_ey : cp.ce_N) + qs);
-        } else {
-          b = ldg(cp.be_F + (-1 - qs));
-          cc = ldg(cp.ce_F + (-1 - qs));
-        }
-        const T tot = *lp + sg * ceh * lam;
-        *lp = b * tot;
-        coef += cc * cp.inv_d * tot;
+      T coef = sg * ceh * ik[c][sl] * lam[c];
+      if (lp[c][sl]) {
+        const T tot = old[c][sl] + sg * ceh * lam[c];
+        *lp[c][sl] = bt[c][sl] * tot;
+        coef += ct[c][sl] * s.cp[ax].inv_d * tot;
       }
       a.a[c][sl][id] = coef;
     }
-    a.lE[c][id] = cee * lam;
+    a.lE[c][id] = cee * lam[c];
   }
 }
 
 // H sub-step transposed at the special slab components: coefficients and
-// psi_H adjoints (lambda_H <- chh lambda_H is the identity).
+// psi_H adjoints (lambda_H <- chh lambda_H is the identity).  Loads first,
+// as in adj_e_slab.
 template <typename T>
 __global__ void adj_h_slab(const __grid_constant__ SimView<T> s, const __grid_constant__ AdjView<T> a,
                            const SlabShell sh) {
@@ -875,25 +896,42 @@ __global__ void adj_h_slab(const __grid_constant__ SimView<T> s, const __grid_co
   const size_t id = fidx(s.PX, s.plane, i, j, k);
   const int ijk[3] = {i, j, k};
   const T che = s.che;
+  bool sp[3];
+  T lam[3], ik[3][2], old[3][2], bt[3][2], ct[3][2];
+  T* lp[3][2];
 #pragma unroll
   for (int h = 0; h < 3; h++) {
-    if (!adj_h_special(s, h, i, j, k)) continue;
-    const T lam = a.lH[h][id];
+    sp[h] = adj_h_special(s, h, i, j, k);
+    lam[h] = sp[h] ? a.lH[h][id] : T(0);
+#pragma unroll
+    for (int sl = 0; sl < 2; sl++) {
+      const int ax = (h + 1 + sl) % 3;
+      const CpmlAxis<T>& cp = s.cp[ax];
+      lp[h][sl] = nullptr;
+      ik[h][sl] = old[h][sl] = bt[h][sl] = ct[h][sl] = T(0);
+      if (!sp[h]) continue;
+      ik[h][sl] = ldg(cp.inv_khd + ijk[ax]);
+      int qs;
+      lp[h][sl] = adj_psi(s, &a.lpH_N[h][sl], &a.lpH_F[h][sl], ax, false, i, j, k, &qs);
+      if (lp[h][sl]) {
+        if (qs >= 0) { bt[h][sl] = ldg(cp.bh_N + qs); ct[h][sl] = ldg(cp.ch_N + qs); }
+        else { bt[h][sl] = ldg(cp.bh_F + (-1 - qs)); ct[h][sl] = ldg(cp.ch_F + (-1 - qs)); }
+        old[h][sl] = *lp[h][sl];
+      }
+    }
+  }
+#pragma unroll
+  for (int h = 0; h < 3; h++) {
+    if (!sp[h]) continue;
 #pragma unroll
     for (int sl = 0; sl < 2; sl++) {
       const int ax = (h + 1 + sl) % 3;
       const T sg = sl == 0 ? T(-1) : T(1);
-      const CpmlAxis<T>& cp = s.cp[ax];
-      T coef = sg * che * ldg(cp.inv_khd + ijk[ax]) * lam;
-      int qs;
-      T* lp = adj_psi(s, &a.lpH_N[h][sl], &a.lpH_F[h][sl], ax, false, i, j, k, &qs);
-      if (lp) {
-        T b, cc;
-        if (qs >= 0) { b = ldg(cp.bh_N + qs); cc = ldg(cp.ch_N + qs); }
-        else { b = ldg(cp.bh_F + (-1 - qs)); cc = ldg(cp.ch_F + (-1 - qs)); }
-        const T tot = *lp + sg * che * lam;
-        *lp = b * tot;
-        coef += cc * cp.inv_d * tot;
+      T coef = sg * che * ik[h][sl] * lam[h];
+      if (lp[h][sl]) {
+        const T tot = old[h][sl] + sg * che * lam[h];
+        *lp[h][sl] = bt[h][sl] * tot;
+        coef += ct[h][sl] * s.cp[ax].inv_d * tot;
       }
       a.a[h][sl][id] = coef;
     }
