@@ -795,24 +795,23 @@ __device__ __forceinline__ float adj_mul(float x, float y) { return __fmul_rn(x,
 __device__ __forceinline__ double adj_mul(double x, double y) { return __dmul_rn(x, y); }
 
 // Difference coefficient of E component c, slot sl (axis (c+1+sl)%3), at a
-// cell: from the arrays for a special component, else sg ceh ikd lambda_E
-// (H: sg che ikh lambda_H), from the cell's flags (adj_flags_e /
-// adj_flags_h); n = the cell's coordinate along the slot's axis.
-// lam is the component's adjoint at the cell, loaded by the caller ahead of
-// the flags so that the two loads overlap.
+// cell: the coefficient-array value `pre` for a special component, else sg
+// ceh ikd lambda_E (H: sg che ikh lambda_H), from the cell's flags
+// (adj_flags_e / adj_flags_h); n = the cell's coordinate along the slot's
+// axis.  lam (the component's adjoint at the cell) and pre are loaded by the
+// caller beside the flags (every coefficient array spans the grid), so that
+// no load waits for the flags.
 template <typename T>
-__device__ __forceinline__ T adj_e_coef_f(const SimView<T>& s, const AdjView<T>& a, int c, int sl, int n, size_t id,
-                                          unsigned f, T lam) {
-  if (f & (8u << c)) return a.a[c][sl][id];
+__device__ __forceinline__ T adj_e_coef_v(const SimView<T>& s, int c, int sl, int n, unsigned f, T lam, T pre) {
+  if (f & (8u << c)) return pre;
   if (!(f & (1u << c))) return T(0);
   const int ax = (c + 1 + sl) % 3;
   const T sg = sl == 0 ? T(1) : T(-1);
   return adj_mul(sg * s.ceh[(f >> 8) >> 3] * ldg(s.cp[ax].inv_ked + n), lam);
 }
 template <typename T>
-__device__ __forceinline__ T adj_h_coef_f(const SimView<T>& s, const AdjView<T>& a, int h, int sl, int n, size_t id,
-                                          unsigned f, T lam) {
-  if (f & (8u << h)) return a.a[h][sl][id];
+__device__ __forceinline__ T adj_h_coef_v(const SimView<T>& s, int h, int sl, int n, unsigned f, T lam, T pre) {
+  if (f & (8u << h)) return pre;
   if (!(f & (1u << h))) return T(0);
   const int ax = (h + 1 + sl) % 3;
   const T sg = sl == 0 ? T(-1) : T(1);
@@ -1009,21 +1008,26 @@ __global__ void __launch_bounds__(256) adj_gather_h_fused(const __grid_constant_
   const T h0 = a.lH[0][id], h1 = a.lH[1][id], h2 = a.lH[2][id];
   const unsigned f0 = a.flags[id] & 0xffffu;
   const unsigned fx = a.flags[id + ox] & 0xffffu, fy = a.flags[id + oy] & 0xffffu, fz = a.flags[id + oz] & 0xffffu;
+  // the coefficient-array values of every term, loaded beside the flags
+  // (used where the flags mark the component special)
+  const T p10 = a.a[1][0][id], p10z = a.a[1][0][id + oz], p21 = a.a[2][1][id], p21y = a.a[2][1][id + oy];
+  const T p01 = a.a[0][1][id], p01z = a.a[0][1][id + oz], p20 = a.a[2][0][id], p20x = a.a[2][0][id + ox];
+  const T p00 = a.a[0][0][id], p00y = a.a[0][0][id + oy], p11 = a.a[1][1][id], p11x = a.a[1][1][id + ox];
   // Hx: Ey slot 0 (z), Ez slot 1 (y)
-  a.lH[0][id] = h0 + (adj_e_coef_f(s, a, 1, 0, k, id, f0, ey0) -
-                      (nz ? adj_e_coef_f(s, a, 1, 0, k + 1, id + sz, fz, eyz) : T(0)) +
-                      adj_e_coef_f(s, a, 2, 1, j, id, f0, ez0) -
-                      (ny ? adj_e_coef_f(s, a, 2, 1, j + 1, id + sy, fy, ezy) : T(0)));
+  a.lH[0][id] = h0 + (adj_e_coef_v(s, 1, 0, k, f0, ey0, p10) -
+                      (nz ? adj_e_coef_v(s, 1, 0, k + 1, fz, eyz, p10z) : T(0)) +
+                      adj_e_coef_v(s, 2, 1, j, f0, ez0, p21) -
+                      (ny ? adj_e_coef_v(s, 2, 1, j + 1, fy, ezy, p21y) : T(0)));
   // Hy: Ex slot 1 (z), Ez slot 0 (x)
-  a.lH[1][id] = h1 + (adj_e_coef_f(s, a, 0, 1, k, id, f0, ex0) -
-                      (nz ? adj_e_coef_f(s, a, 0, 1, k + 1, id + sz, fz, exz) : T(0)) +
-                      adj_e_coef_f(s, a, 2, 0, i, id, f0, ez0) -
-                      (nx ? adj_e_coef_f(s, a, 2, 0, i + 1, id + sx, fx, ezx) : T(0)));
+  a.lH[1][id] = h1 + (adj_e_coef_v(s, 0, 1, k, f0, ex0, p01) -
+                      (nz ? adj_e_coef_v(s, 0, 1, k + 1, fz, exz, p01z) : T(0)) +
+                      adj_e_coef_v(s, 2, 0, i, f0, ez0, p20) -
+                      (nx ? adj_e_coef_v(s, 2, 0, i + 1, fx, ezx, p20x) : T(0)));
   // Hz: Ex slot 0 (y), Ey slot 1 (x)
-  a.lH[2][id] = h2 + (adj_e_coef_f(s, a, 0, 0, j, id, f0, ex0) -
-                      (ny ? adj_e_coef_f(s, a, 0, 0, j + 1, id + sy, fy, exy) : T(0)) +
-                      adj_e_coef_f(s, a, 1, 1, i, id, f0, ey0) -
-                      (nx ? adj_e_coef_f(s, a, 1, 1, i + 1, id + sx, fx, eyx) : T(0)));
+  a.lH[2][id] = h2 + (adj_e_coef_v(s, 0, 0, j, f0, ex0, p00) -
+                      (ny ? adj_e_coef_v(s, 0, 0, j + 1, fy, exy, p00y) : T(0)) +
+                      adj_e_coef_v(s, 1, 1, i, f0, ey0, p11) -
+                      (nx ? adj_e_coef_v(s, 1, 1, i + 1, fx, eyx, p11x) : T(0)));
 }
 
 // lambda_E <- (non-special: cee) lambda_E + gather of the H-sub-step
@@ -1080,15 +1084,20 @@ __global__ void __launch_bounds__(256) adj_gather_e_fused(const __grid_constant_
     if ((fe & (1u << c)) && !(fe & (8u << c))) l[c] = adj_mul(cee, l[c]);
   const unsigned f0 = fw >> 16;
   const unsigned fx = a.flags[id - ox] >> 16, fy = a.flags[id - oy] >> 16, fz = a.flags[id - oz] >> 16;
+  // the coefficient-array values of every term, loaded beside the flags
+  // (used where the flags mark the component special)
+  const T p10 = a.a[1][0][id], p10z = a.a[1][0][id - oz], p21 = a.a[2][1][id], p21y = a.a[2][1][id - oy];
+  const T p01 = a.a[0][1][id], p01z = a.a[0][1][id - oz], p20 = a.a[2][0][id], p20x = a.a[2][0][id - ox];
+  const T p00 = a.a[0][0][id], p00y = a.a[0][0][id - oy], p11 = a.a[1][1][id], p11x = a.a[1][1][id - ox];
   // Ex: Hy slot 0 (z), Hz slot 1 (y)
-  l[0] += (pz ? adj_h_coef_f(s, a, 1, 0, k - 1, id - sz, fz, hyz) : T(0)) - adj_h_coef_f(s, a, 1, 0, k, id, f0, hy0) +
-          (py ? adj_h_coef_f(s, a, 2, 1, j - 1, id - sy, fy, hzy) : T(0)) - adj_h_coef_f(s, a, 2, 1, j, id, f0, hz0);
+  l[0] += (pz ? adj_h_coef_v(s, 1, 0, k - 1, fz, hyz, p10z) : T(0)) - adj_h_coef_v(s, 1, 0, k, f0, hy0, p10) +
+          (py ? adj_h_coef_v(s, 2, 1, j - 1, fy, hzy, p21y) : T(0)) - adj_h_coef_v(s, 2, 1, j, f0, hz0, p21);
   // Ey: Hx slot 1 (z), Hz slot 0 (x)
-  l[1] += (pz ? adj_h_coef_f(s, a, 0, 1, k - 1, id - sz, fz, hxz) : T(0)) - adj_h_coef_f(s, a, 0, 1, k, id, f0, hx0) +
-          (px ? adj_h_coef_f(s, a, 2, 0, i - 1, id - sx, fx, hzx) : T(0)) - adj_h_coef_f(s, a, 2, 0, i, id, f0, hz0);
+  l[1] += (pz ? adj_h_coef_v(s, 0, 1, k - 1, fz, hxz, p01z) : T(0)) - adj_h_coef_v(s, 0, 1, k, f0, hx0, p01) +
+          (px ? adj_h_coef_v(s, 2, 0, i - 1, fx, hzx, p20x) : T(0)) - adj_h_coef_v(s, 2, 0, i, f0, hz0, p20);
   // Ez: Hx slot 0 (y), Hy slot 1 (x)
-  l[2] += (py ? adj_h_coef_f(s, a, 0, 0, j - 1, id - sy, fy, hxy) : T(0)) - adj_h_coef_f(s, a, 0, 0, j, id, f0, hx0) +
-          (px ? adj_h_coef_f(s, a, 1, 1, i - 1, id - sx, fx, hyx) : T(0)) - adj_h_coef_f(s, a, 1, 1, i, id, f0, hy0);
+  l[2] += (py ? adj_h_coef_v(s, 0, 0, j - 1, fy, hxy, p00y) : T(0)) - adj_h_coef_v(s, 0, 0, j, f0, hx0, p00) +
+          (px ? adj_h_coef_v(s, 1, 1, i - 1, fx, hyx, p11x) : T(0)) - adj_h_coef_v(s, 1, 1, i, f0, hy0, p11);
 #pragma unroll
   for (int c = 0; c < 3; c++) a.lE[c][id] = l[c];
 }
