@@ -890,6 +890,7 @@ static const fdtd_sim::TmaSet* tma_maps(fdtd_sim* s, int ty) {
   const cuuint32_t unit[3] = {1, 1, 1};
   fdtd_sim::TmaSet m;
   m.ty = ty;
+  m.h.stall = m.e.stall = 0;
   bool ok = true;
   auto encode = [&](CUtensorMap* map, const void* base, const cuuint32_t* box) {
     ok = ok && enc(map, dt, 3, const_cast<void*>(base), dims, strides, box, unit, CU_TENSOR_MAP_INTERLEAVE_NONE,
@@ -995,6 +996,15 @@ template <typename T, bool PML, bool EPASS>
 static void launch_variant(fdtd_sim* s, int ty, int mb, int sg, bool tma, dim3 g, const TileMap& tm, int kchunk,
                            cudaStream_t st, bool pdl = false) {
   const fdtd_sim::TmaSet* maps = tma ? tma_maps<T>(s, ty) : nullptr;
+  // FDTD_TMA_STALL_TEST=1: the launch's copies are never issued (its waits
+  // time out; fdtd_check then reports FDTD_ERR_TIMEOUT)
+  fdtd_sim::TmaSet stalled;
+  const char* stall_env = std::getenv("FDTD_TMA_STALL_TEST");
+  if (maps && stall_env && stall_env[0] == '1') {
+    stalled = *maps;
+    stalled.h.stall = stalled.e.stall = 1;
+    maps = &stalled;
+  }
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   at[0].val.programmaticStreamSerializationAllowed = 1;

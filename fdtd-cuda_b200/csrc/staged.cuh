@@ -88,6 +88,9 @@ __device__ __forceinline__ void cp_async_wait() {
 struct TmaMaps {
   CUtensorMap halo[3];
   CUtensorMap own[3];
+  // test switch (FDTD_TMA_STALL_TEST=1): the issuing thread issues nothing,
+  // so that every wait runs out and the timeout path is exercised
+  int stall;
 };
 
 __device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
@@ -297,7 +300,7 @@ struct TmaRing {
     __syncthreads();
   }
   __device__ __forceinline__ void issue(const TmaMaps& m, int st, int p, int NZ) {
-    if (!lead || bad || p > plast) return;
+    if (!lead || bad || p > plast || m.stall) return;
     const unsigned bar = bar0 + 8 * st, stage = sbase + st * SB;
     pdone = p + 1;
     if ((unsigned)p >= (unsigned)NZ) {

@@ -305,6 +305,26 @@ def test_tensor_copy_staging_agrees(prec, monkeypatch):
             np.testing.assert_array_equal(out[0][c], out[1][c])
 
 
+def test_tensor_copy_wait_timeout_is_reported(monkeypatch):
+    """A tensor-copy wait gives up after one second.  With the copies never
+    issued (the test switch FDTD_TMA_STALL_TEST=1) every wait of the passes
+    runs out, the kernels end, and fdtd_check reports FDTD_ERR_TIMEOUT; the
+    GPU context stays usable for the next simulation."""
+    monkeypatch.setenv("FDTD_TMA", "1")
+    monkeypatch.setenv("FDTD_TMA_STALL_TEST", "1")
+    s = F.Sim(make(F, "vacuum", precision=F.FDTD_FP32))
+    assert s.stats().h_tma == 1 and s.stats().e_etma == 1
+    s.step(1)
+    with pytest.raises(F.FdtdError) as e:
+        s.check()
+    assert e.value.status == 7 and "gave up" in str(e.value)
+    s.close()
+    monkeypatch.delenv("FDTD_TMA_STALL_TEST")
+    t = run_sim("vacuum", 20, F.FDTD_FP32)
+    t.check()
+    assert t.stats().h_tma == 1
+
+
 def test_unbuilt_pass_variant_is_rejected(monkeypatch):
     monkeypatch.setenv("FDTD_PASS", "staged:8:5:16:4")
     with pytest.raises(F.FdtdError) as e:
