@@ -1880,11 +1880,10 @@ extern "C" fdtd_status fdtd_snapshot_plane(fdtd_sim* s, int comp, int axis, int 
 // in the process, so calls that overlap in time on the same device (from
 // several host threads, or on streams that run concurrently) race on it and
 // must be serialised by the caller.  Every call synchronises its stream
-// (also for a device destination), so it cannot run inside a stream
-// capture.  The first call on each device resolves the scratch address
-// with cudaGetSymbolAddress and keeps it for the life of the process; a
-// cudaDeviceReset would leave the kept address stale, so the library must
-// not be used across one.
+// (also for a device destination).  The first call on each device resolves
+// the scratch address with cudaGetSymbolAddress and keeps it for the life
+// of the process; a cudaDeviceReset would leave the kept address stale, so
+// the library must not be used across one.
 constexpr size_t kPlaneScratchCells = (size_t)1 << 20;  // 8 MiB of doubles
 static __device__ __align__(256) double g_plane_scratch[kPlaneScratchCells];
 

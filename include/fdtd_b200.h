@@ -323,8 +323,7 @@ fdtd_status fdtd_snapshot_plane(fdtd_sim* s, int comp, int axis, int index,
  * kind: the plane is gathered into a fixed scratch array in the library's
  * static device memory and copied to dst (host or device) on `stream`.
  * No counterpart in the reference.  Every call synchronises `stream` before
- * it returns, whatever dst is, so it cannot be used while a stream is being
- * captured into a CUDA graph.  Limit: count <= 1048576 cells
+ * it returns, whatever dst is.  Limit: count <= 1048576 cells
  * (FDTD_ERR_INVALID beyond).  The scratch is one per device and shared by
  * all simulations: calls that overlap in time on one device race and must
  * be serialised by the caller.  The scratch's device address is looked up
